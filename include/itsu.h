@@ -1,0 +1,208 @@
+/*
+ * itsu.h - C ABI of the B200 ITS cellular-automaton track finder.
+ *
+ * This is the drop-in boundary for the hot path of the reference tracker: clustering into the
+ * phi-z index table, tracklets, cells, neighbours / CA levels, roads and their Monte Carlo
+ * labels. Plain pointers and sizes only. Every entry point returns an itsu_status; on failure
+ * itsu_last_error() holds a one-line reason. The C++ facade in
+ * tracking-itsu_b200/host/ maps statuses to std::runtime_error the way the reference does
+ * (src/CA/gpu/cuda/Tracker.cu:326-335).
+ *
+ * Record layouts are the reference's, byte for byte:
+ *   itsu_cluster  = Cluster   (include/ITSReconstruction/CA/Cluster.h:36-44)   36 bytes
+ *   itsu_tracklet = Tracklet  (include/ITSReconstruction/CA/Tracklet.h:33-36)  16 bytes
+ *   itsu_cell     = Cell      (include/ITSReconstruction/CA/Cell.h:47-54)      40 bytes
+ *   itsu_road     = Road      (include/ITSReconstruction/CA/Road.h:47-50)      32 bytes
+ * Indices inside records are local to their layer, as in the reference: a tracklet's cluster
+ * indices index the SORTED clusters of layers L and L+1, a cell's tracklet indices index the
+ * tracklets of layers L and L+1, a road's cell_ids[L] indexes the cells of layer L.
+ */
+#ifndef ITSU_H
+#define ITSU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ITSU_LAYERS 7            /* Constants::ITS::LayersNumber (Constants.h:38) */
+#define ITSU_TRACKLET_LAYERS 6   /* Constants::ITS::TrackletsPerRoad (Constants.h:39) */
+#define ITSU_CELL_LAYERS 5       /* Constants::ITS::CellsPerRoad (Constants.h:40) */
+#define ITSU_NEIGHBOUR_LAYERS 4  /* CellsPerRoad - 1 */
+#define ITSU_Z_BINS 20           /* Constants::IndexTable::ZBins (Constants.h:77) */
+#define ITSU_PHI_BINS 20         /* Constants::IndexTable::PhiBins (Constants.h:78) */
+#define ITSU_INDEX_TABLE_SIZE 401 /* ZBins * PhiBins + 1 */
+#define ITSU_UNUSED_INDEX (-1)   /* Constants::ITS::UnusedIndex (Constants.h:41) */
+
+typedef struct itsu_cluster {
+  float x, y, z;   /* global coordinates, cm */
+  float phi;       /* azimuth about the primary vertex, [0, 2pi] (filled by clustering) */
+  float r;         /* transverse distance to the primary vertex (filled by clustering) */
+  int32_t cluster_id;
+  float alpha;     /* sensor angle, carried through */
+  int32_t mc_id;   /* Monte Carlo particle id, -1 for noise */
+  int32_t bin;     /* phi-z index table bin (filled by clustering) */
+} itsu_cluster;
+
+typedef struct itsu_tracklet {
+  int32_t first_cluster;  /* sorted index in layer L */
+  int32_t second_cluster; /* sorted index in layer L+1 */
+  float tan_lambda;
+  float phi;
+} itsu_tracklet;
+
+typedef struct itsu_cell {
+  int32_t first_cluster, second_cluster, third_cluster; /* layers L, L+1, L+2 */
+  int32_t first_tracklet, second_tracklet;              /* tracklet layers L, L+1 */
+  float nx, ny, nz;                                     /* unit normal of the circle plane */
+  float curvature;
+  int32_t level;                                        /* CA level, 1 + longest chain below */
+} itsu_cell;
+
+typedef struct itsu_road {
+  int32_t cell_ids[ITSU_CELL_LAYERS]; /* cell index per cell layer, -1 if unused */
+  int32_t size;
+  int32_t label;   /* Moore-vote Monte Carlo label */
+  uint8_t is_fake; /* C++ bool in the reference layout */
+  uint8_t pad_[3];
+} itsu_road;
+
+typedef enum itsu_status {
+  ITSU_OK = 0,
+  ITSU_ERR_INVALID = 1,  /* malformed input or argument (rejected before any kernel runs) */
+  ITSU_ERR_CAPACITY = 2, /* a result did not fit and the arena could not grow */
+  ITSU_ERR_TIMEOUT = 3,  /* a bounded device wait gave up */
+  ITSU_ERR_CUDA = 4,     /* a CUDA runtime call failed */
+  ITSU_ERR_NOMEM = 5,    /* device or host allocation failed */
+  ITSU_ERR_STATE = 6     /* call out of order (e.g. stage before initialize) */
+} itsu_status;
+
+/* Flags of itsu_config.flags */
+#define ITSU_FLAG_NO_GROW 1u /* report ITSU_ERR_CAPACITY instead of growing and re-running */
+
+typedef struct itsu_config {
+  int32_t device;          /* CUDA device ordinal */
+  uint32_t flags;
+  int64_t max_clusters;    /* initial arena capacities; 0 = defaults. The arena grows on demand */
+  int64_t max_tracklets;   /* unless ITSU_FLAG_NO_GROW is set. */
+  int64_t max_cells;
+  int64_t max_neighbours;
+  int64_t max_roads;
+  int32_t max_events;
+  int32_t reserved_;
+} itsu_config;
+
+/* Per-vertex result sizes. */
+typedef struct itsu_counts {
+  int32_t clusters[ITSU_LAYERS];
+  int32_t tracklets[ITSU_TRACKLET_LAYERS];
+  int32_t cells[ITSU_CELL_LAYERS];
+  int32_t neighbours[ITSU_NEIGHBOUR_LAYERS]; /* links between cell layers L and L+1 */
+  int32_t roads;
+} itsu_counts;
+
+/* Host destinations for itsu_copy_results; any pointer may be NULL to skip that output.
+ * Sizes follow itsu_counts:
+ *   clusters[L]          N_L sorted clusters
+ *   index_tables[L-1]    401 ints for layers L = 1..6 (PrimaryVertexContext::getIndexTables)
+ *   tracklets[L]         T_L
+ *   tracklets_lookup[L]  N_{L+1} ints for L = 0..4 (getTrackletsLookupTable): first tracklet of
+ *                        layer L+1 whose first cluster is that cluster of layer L+1, else -1
+ *   cells[L]             C_L (level filled in by neighbour finding)
+ *   cells_lookup[L]      T_{L+1} ints for L = 0..3 (getCellsLookupTable): first cell of layer
+ *                        L+1 built on that tracklet of layer L+1, else -1
+ *   neighbour_offsets[L] C_{L+1} + 1 ints: CSR row starts over the cells of layer L+1
+ *   neighbours[L]        counts.neighbours[L] ints: cells of layer L, ascending in each row
+ *                        (getCellsNeighbours()[L][c] as a CSR)
+ *   roads                counts.roads roads in the reference's emission order */
+typedef struct itsu_results {
+  itsu_cluster *clusters[ITSU_LAYERS];
+  int32_t *index_tables[ITSU_TRACKLET_LAYERS];
+  itsu_tracklet *tracklets[ITSU_TRACKLET_LAYERS];
+  int32_t *tracklets_lookup[ITSU_CELL_LAYERS];
+  itsu_cell *cells[ITSU_CELL_LAYERS];
+  int32_t *cells_lookup[ITSU_NEIGHBOUR_LAYERS];
+  int32_t *neighbour_offsets[ITSU_NEIGHBOUR_LAYERS];
+  int32_t *neighbours[ITSU_NEIGHBOUR_LAYERS];
+  itsu_road *roads;
+} itsu_results;
+
+/* Device-resident batch of events (one primary vertex each). */
+typedef struct itsu_batch {
+  const itsu_cluster *clusters;  /* device: raw clusters, event-major then layer-major */
+  const int32_t *layer_offsets;  /* device: n_events*7 + 1 offsets into clusters */
+  const float *vertices;         /* device: n_events*3 (x, y, z) */
+  int32_t n_events;
+  int32_t reserved_;
+  int64_t n_clusters;            /* == layer_offsets[n_events*7] */
+} itsu_batch;
+
+typedef struct itsu_context itsu_context;
+
+/* ---- library and context ---- */
+const char *itsu_version(void);
+const char *itsu_status_string(itsu_status status);
+/* Last error message of the context (or of the thread when ctx is NULL). */
+const char *itsu_last_error(const itsu_context *ctx);
+void itsu_config_default(itsu_config *cfg);
+itsu_status itsu_context_create(const itsu_config *cfg, itsu_context **out);
+void itsu_context_destroy(itsu_context *ctx);
+/* All work of the context is ordered on this stream (a cudaStream_t; NULL = a private stream). */
+itsu_status itsu_context_set_stream(itsu_context *ctx, void *cuda_stream);
+void *itsu_context_stream(const itsu_context *ctx);
+
+/* ---- one primary vertex, stage by stage: the reference's per-vertex seam ----
+ * Replaces PrimaryVertexContext::initialize(const Event&, int)
+ *   (include/ITSReconstruction/CA/PrimaryVertexContext.h:51, src/CA/PrimaryVertexContext.cxx:31-142):
+ * per-vertex cluster transform, stable sort by bin and the 6 index tables, on the device.
+ * layers[L] points to counts[L] raw clusters in host memory. */
+itsu_status itsu_pvc_initialize(itsu_context *ctx, const itsu_cluster *const layers[ITSU_LAYERS],
+                                const int32_t counts[ITSU_LAYERS], const float vertex[3]);
+/* Replaces TrackerTraits<IsGPU>::computeLayerTracklets(PrimaryVertexContext&)
+ *   (include/ITSReconstruction/CA/Tracker.h:43,81; src/CA/Tracker.cxx:45-117;
+ *    GPU form src/CA/gpu/cuda/Tracker.cu:285-367). */
+itsu_status itsu_compute_layer_tracklets(itsu_context *ctx);
+/* Replaces TrackerTraits<IsGPU>::computeLayerCells(PrimaryVertexContext&)
+ *   (Tracker.h:44,82; Tracker.cxx:120-235; GPU form Tracker.cu:369-473). */
+itsu_status itsu_compute_layer_cells(itsu_context *ctx);
+/* Replaces Tracker<IsGPU>::findCellsNeighbours() (Tracker.h:69, Tracker.cxx:417-474). */
+itsu_status itsu_find_cells_neighbours(itsu_context *ctx);
+/* Replaces Tracker<IsGPU>::findTracks() + traverseCellsTree() (Tracker.h:70-71, Tracker.cxx:477-571). */
+itsu_status itsu_find_tracks(itsu_context *ctx);
+/* Replaces Tracker<IsGPU>::computeMontecarloLabels() (Tracker.h:72, Tracker.cxx:574-652). */
+itsu_status itsu_compute_montecarlo_labels(itsu_context *ctx);
+
+/* Sizes and host copies of the last run (event index e of a batch; 0 for the per-vertex API).
+ * Replaces the PrimaryVertexContext getters (PrimaryVertexContext.h:52-77). */
+itsu_status itsu_get_counts(itsu_context *ctx, int32_t event, itsu_counts *out);
+itsu_status itsu_copy_results(itsu_context *ctx, int32_t event, const itsu_results *out);
+
+/* Whole path for one vertex (Tracker<IsGPU>::clustersToTracks body for one vertex,
+ * Tracker.cxx:251-262): host clusters in, roads out. roads may be NULL to query the count. */
+itsu_status itsu_clusters_to_tracks(itsu_context *ctx, const itsu_cluster *const layers[ITSU_LAYERS],
+                                    const int32_t counts[ITSU_LAYERS], const float vertex[3],
+                                    itsu_road *roads, int32_t roads_capacity, int32_t *roads_count);
+
+/* ---- batches: many events of uneven multiplicity in one pass of every stage ---- */
+/* Runs every stage for every event of the batch and waits; grows the arena and re-runs
+ * when a result overflowed (unless ITSU_FLAG_NO_GROW). */
+itsu_status itsu_batch_run(itsu_context *ctx, const itsu_batch *batch);
+/* Host in / host out: copies the batch to the device, runs it, and copies back the roads
+ * (event-major) and road_offsets[n_events+1]. roads may be NULL to query the total. */
+itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
+                                const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
+                                int32_t *road_offsets);
+/* Launches every stage of the batch on the context stream without waiting (CUDA-graph
+ * replay after the first call with the same shape); itsu_batch_status waits and reports. */
+itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch);
+itsu_status itsu_batch_status(itsu_context *ctx);
+/* Device pointer to the roads of the last batch (event-major) and to road_offsets[n_events+1]. */
+itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, const int32_t **road_offsets);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ITSU_H */

@@ -1,0 +1,215 @@
+// ref_harness.cpp - drives the reference CPU Tracker and dumps every intermediate result.
+//
+// TEST INFRASTRUCTURE ONLY. Compiled by oracle/build_ref.sh together with the reference's own
+// (patched) sources into oracle/_ref/. Events are read with the reference's own text loader
+// (IOUtils::loadEventData, IOUtils.cxx:38-78).
+//
+//   ref_cr dump <events.txt> <out.bin>   run every vertex stage by stage, write all results
+//   ref_cr time <events.txt> <repeats>   time Tracker::clustersToTracks per event (steady_clock,
+//                                        one warm-up event first, as main.cpp:74-75) -> JSON line
+//
+// The dump needs the tracker's private per-vertex context and its protected stages, so the
+// reference headers are included with private/protected opened up (standard headers first, so
+// only the tracker's classes are affected).
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <memory>
+#include <ostream>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <unordered_set>
+#include <utility>
+#include <vector>
+
+#define private public
+#define protected public
+#include "ITSReconstruction/CA/IOUtils.h"
+#include "ITSReconstruction/CA/Tracker.h"
+#undef private
+#undef protected
+
+#if defined(ITSU_REF_CR)
+extern "C" float itsu_ref_cr_atan2f(float y, float x);
+#endif
+
+using namespace o2::ITS::CA;
+
+namespace
+{
+
+void put_i32(std::FILE *f, int32_t v) { std::fwrite(&v, 4, 1, f); }
+void put_f32(std::FILE *f, float v) { std::fwrite(&v, 4, 1, f); }
+
+void dump_vertex(std::FILE *f, int event, int vertex, PrimaryVertexContext &pvc)
+{
+  put_i32(f, event);
+  put_i32(f, vertex);
+  put_f32(f, pvc.getPrimaryVertex().x);
+  put_f32(f, pvc.getPrimaryVertex().y);
+  put_f32(f, pvc.getPrimaryVertex().z);
+  for (int l = 0; l < Constants::ITS::LayersNumber; ++l) {
+    const auto &cl = pvc.getClusters()[l];
+    put_i32(f, static_cast<int32_t>(cl.size()));
+    for (const Cluster &c : cl) {
+      put_f32(f, c.xCoordinate);
+      put_f32(f, c.yCoordinate);
+      put_f32(f, c.zCoordinate);
+      put_f32(f, c.phiCoordinate);
+      put_f32(f, c.rCoordinate);
+      put_i32(f, c.clusterId);
+      put_f32(f, c.alphaAngle);
+      put_i32(f, c.monteCarloId);
+      put_i32(f, c.indexTableBinIndex);
+    }
+  }
+  for (int l = 0; l < Constants::ITS::TrackletsPerRoad; ++l) {
+    for (int b = 0; b <= Constants::IndexTable::ZBins * Constants::IndexTable::PhiBins; ++b) {
+      put_i32(f, pvc.getIndexTables()[l][b]);
+    }
+  }
+  for (int l = 0; l < Constants::ITS::TrackletsPerRoad; ++l) {
+    const auto &tr = pvc.getTracklets()[l];
+    put_i32(f, static_cast<int32_t>(tr.size()));
+    for (const Tracklet &t : tr) {
+      put_i32(f, t.firstClusterIndex);
+      put_i32(f, t.secondClusterIndex);
+      put_f32(f, t.tanLambda);
+      put_f32(f, t.phiCoordinate);
+    }
+  }
+  for (int l = 0; l < Constants::ITS::CellsPerRoad; ++l) {
+    const auto &lt = pvc.getTrackletsLookupTable()[l];
+    put_i32(f, static_cast<int32_t>(lt.size()));
+    for (int v : lt) put_i32(f, v);
+  }
+  for (int l = 0; l < Constants::ITS::CellsPerRoad; ++l) {
+    const auto &cells = pvc.getCells()[l];
+    put_i32(f, static_cast<int32_t>(cells.size()));
+    for (const Cell &c : cells) {
+      put_i32(f, c.getFirstClusterIndex());
+      put_i32(f, c.getSecondClusterIndex());
+      put_i32(f, c.getThirdClusterIndex());
+      put_i32(f, c.getFirstTrackletIndex());
+      put_i32(f, c.getSecondTrackletIndex());
+      put_f32(f, c.getNormalVectorCoordinates().x);
+      put_f32(f, c.getNormalVectorCoordinates().y);
+      put_f32(f, c.getNormalVectorCoordinates().z);
+      put_f32(f, c.getCurvature());
+      put_i32(f, c.getLevel());
+    }
+  }
+  for (int l = 0; l < Constants::ITS::CellsPerRoad - 1; ++l) {
+    const auto &lt = pvc.getCellsLookupTable()[l];
+    put_i32(f, static_cast<int32_t>(lt.size()));
+    for (int v : lt) put_i32(f, v);
+  }
+  for (int l = 0; l < Constants::ITS::CellsPerRoad - 1; ++l) {
+    const auto &nb = pvc.getCellsNeighbours()[l];
+    put_i32(f, static_cast<int32_t>(nb.size()));
+    for (const auto &list : nb) {
+      put_i32(f, static_cast<int32_t>(list.size()));
+      for (int v : list) put_i32(f, v);
+    }
+  }
+  auto &roads = pvc.getRoads();
+  put_i32(f, static_cast<int32_t>(roads.size()));
+  for (Road &r : roads) {
+    for (int k = 0; k < Constants::ITS::CellsPerRoad; ++k) put_i32(f, r[k]);
+    put_i32(f, r.getRoadSize());
+    put_i32(f, r.getLabel());
+    put_i32(f, r.isFakeRoad() ? 1 : 0);
+  }
+}
+
+int run_dump(const std::string &events_file, const std::string &out_file)
+{
+  std::vector<Event> events = IOUtils::loadEventData(events_file);
+  std::FILE *f = std::fopen(out_file.c_str(), "wb");
+  if (!f) {
+    std::perror("fopen");
+    return 1;
+  }
+  int32_t records = 0;
+  for (const Event &e : events) records += e.getPrimaryVerticesNum();
+  std::fwrite("ITSUREF1", 1, 8, f);
+  put_i32(f, records);
+  Tracker<false> tracker{};
+  for (size_t ie = 0; ie < events.size(); ++ie) {
+    const Event &event = events[ie];
+    for (int iv = 0; iv < event.getPrimaryVerticesNum(); ++iv) {
+      // The body of Tracker::clustersToTracks for one vertex (Tracker.cxx:253-259).
+      tracker.mPrimaryVertexContext.initialize(event, iv);
+      tracker.computeTracklets();
+      tracker.computeCells();
+      tracker.findCellsNeighbours();
+      tracker.findTracks();
+      tracker.computeMontecarloLabels();
+      dump_vertex(f, static_cast<int>(ie), iv, tracker.mPrimaryVertexContext);
+    }
+  }
+  std::fclose(f);
+  return 0;
+}
+
+int run_time(const std::string &events_file, int repeats)
+{
+  std::vector<Event> events = IOUtils::loadEventData(events_file);
+  if (events.empty()) {
+    std::printf("{\"events\": 0}\n");
+    return 0;
+  }
+  Tracker<false> tracker{};
+  tracker.clustersToTracks(events[0]); // warm-up, as main.cpp:74-75
+  long long roads = 0, vertices = 0, clusters = 0;
+  auto t0 = std::chrono::steady_clock::now();
+  for (int rep = 0; rep < repeats; ++rep) {
+    for (const Event &event : events) {
+      std::vector<std::vector<Road>> r = tracker.clustersToTracks(event);
+      for (const auto &v : r) roads += static_cast<long long>(v.size());
+      vertices += event.getPrimaryVerticesNum();
+      clusters += event.getTotalClusters();
+    }
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  const double seconds = std::chrono::duration<double>(t1 - t0).count();
+  std::printf("{\"events\": %lld, \"vertices\": %lld, \"clusters\": %lld, \"roads\": %lld, \"seconds\": %.9f}\n",
+              static_cast<long long>(events.size()) * repeats, vertices, clusters, roads, seconds);
+  return 0;
+}
+
+} // namespace
+
+int main(int argc, char **argv)
+{
+#if defined(ITSU_REF_CR)
+  // The override must be in effect for the reference's calls (same symbol resolution). These
+  // arguments are ones where the C library's atan2f is not correctly rounded.
+  volatile float ya = -4.0587134f, xa = 3.7113914f, yb = 1.96216f, xb = 4.643577f;
+  if (atan2f(ya, xa) != itsu_ref_cr_atan2f(ya, xa) || atan2f(yb, xb) != itsu_ref_cr_atan2f(yb, xb)) {
+    std::fprintf(stderr, "ref_harness: atan2f override is not active\n");
+    return 4;
+  }
+#endif
+  if (argc < 4) {
+    std::fprintf(stderr, "usage: %s dump <events.txt> <out.bin> | time <events.txt> <repeats>\n", argv[0]);
+    return 2;
+  }
+  const std::string mode = argv[1];
+  if (mode == "dump") return run_dump(argv[2], argv[3]);
+  if (mode == "time") return run_time(argv[2], std::atoi(argv[3]));
+  std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
+  return 2;
+}
