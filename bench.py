@@ -1,0 +1,498 @@
+#!/usr/bin/env python
+"""Benchmark of the ITS CA track finder on B200: Pb-Pb-like events/s.
+
+Workload (one "step"): a batch of central Pb-Pb-like events (6000 tracks, pT mean 0.6 GeV/c,
+|eta| < 1, 5% noise; seeded synthetic, each event its own vertex) through the plain path:
+clustering, tracklets, cells, neighbours/levels, roads and labels, every event in one batched
+pass of every kernel, replayed as one CUDA graph. The batch's inputs and intermediates (about
+200 MB of raw clusters, 1.3 GB of tracklets) are larger than the 126 MB L2, so there is no L2
+flush between steps.
+
+  value  events/s with the inputs already resident in HBM (device-side batch API)
+  e2e    events/s through the host-facing C ABI call (itsu_batch_run_host): pinned host clusters
+         in, roads out, every copy inside the timed region
+  roofline  the dominant kernel's algorithmic bytes / its CUDA-event duration, against the
+         measured HBM copy bandwidth
+  cpu_baseline  the reference CPU Tracker (oracle/_ref, compiled from the reference's sources)
+         on a bounded sample of the same events, one process per host core
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun, one rank per GPU): every rank runs its own batch of events (weak
+scaling, no collective on the data path); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "tracking-itsu_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+from itsu import gen  # noqa: E402
+
+METRIC = "Pb-Pb-like events/s on 1 B200: plain vs batched vs learned-prefilter @≥99.5% roads"
+UNIT = "events/s"
+TRACKS = 6000
+WORKLOAD = "pbpb_central_6000trk_5pct_noise"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--events", type=int, default=128, help="events per step per GPU")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------
+# distributed plumbing (one process per GPU, weak scaling)
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+        return dist
+    return None
+
+
+def max_over_ranks(dist, value, device=None):
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, value, device=None):
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------
+# workload
+
+
+def make_events(n, seed):
+    return [gen.pbpb_event(seed * 100000 + i, TRACKS) for i in range(n)]
+
+
+def algorithmic_bytes(counts) -> dict:
+    """Compulsory bytes per stage from one event's output sizes (one touch of every object in
+    the reference layouts: 36 B clusters, 16 B tracklets, 40 B cells, 32 B roads, 4 B indices)."""
+    N, T, C, E, R = counts["N"], counts["T"], counts["C"], counts["E"], counts["R"]
+    b = {}
+    b["cluster_sort"] = sum(72 * n for n in N) + 6 * 401 * 4
+    b["tracklets"] = sum(36 * (N[l] + N[l + 1]) + 16 * T[l] for l in range(6)) + sum(4 * N[l] for l in range(1, 6))
+    b["cells"] = sum(16 * (T[l] + T[l + 1]) + 36 * (N[l] + N[l + 1] + N[l + 2]) + 40 * C[l] for l in range(5)) + sum(
+        4 * T[l] for l in range(1, 5))
+    b["neighbours"] = sum(40 * (C[l] + C[l + 1]) + 4 * E[l] + 4 * C[l + 1] for l in range(4))
+    b["roads"] = 40 * C[4] + 4 * sum(E) + 32 * R
+    b["event"] = sum(b.values())
+    return b
+
+
+# kernel -> stage whose compulsory bytes it moves
+KERNEL_STAGE = {
+    "cluster_sort": "cluster_sort",
+    "tracklets_count": "tracklets",
+    "tracklets_write": "tracklets",
+    "cells_count": "cells",
+    "cells_write": "cells",
+    "neighbours_count": "neighbours",
+    "neighbours_write": "neighbours",
+    "roads_write": "roads",
+}
+
+
+# ------------------------------------------------------------------------------------------
+# clocks during the timed region
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device_index), "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU baseline: the reference tracker (or the oracle port) on all host cores
+
+
+def cpu_workers():
+    return max(1, min(os.cpu_count() or 1, 64))
+
+
+def _reference_binary():
+    from oracle import oracle
+
+    return oracle.ref_binary("cr") if oracle.ref_available("cr") else None
+
+
+def run_reference_sample(events, workers, per_worker, repeats=1):
+    """Runs the reference harness in `workers` parallel processes, each timing `per_worker`
+    events of the file (after its own warm-up event). Returns (events, seconds = max worker)."""
+    binary = _reference_binary()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "events.bin")
+        gen.write_binary_events(events, path)
+        n = len(events)
+        procs = []
+        for w in range(workers):
+            first = (w * per_worker) % max(n - per_worker + 1, 1)
+            procs.append(subprocess.Popen([binary, "timebin", path, str(repeats), str(first), str(per_worker)],
+                                          stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+        results = []
+        for p in procs:
+            out, err = p.communicate(timeout=900)
+            if p.returncode != 0:
+                raise RuntimeError("reference harness failed: %s" % err.strip())
+            results.append(json.loads(out.strip().splitlines()[-1]))
+    total = sum(r["events"] for r in results)
+    return total, max(r["seconds"] for r in results)
+
+
+def _port_worker(args):
+    clusters, offsets, vertices, n = args
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    oracle.lib().oracle_run_batch(clusters.ctypes.data, offsets.ctypes.data, vertices.ctypes.data, n)
+    return time.perf_counter() - t0
+
+
+def run_port_sample(events, workers, per_worker):
+    import multiprocessing as mp
+
+    jobs = []
+    for w in range(workers):
+        sub = [events[(w * per_worker + k) % len(events)] for k in range(per_worker)]
+        c, o, v = gen.pack_batch(sub)
+        jobs.append((c, o, v, len(sub)))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        secs = pool.map(_port_worker, jobs)
+    return workers * per_worker, max(secs)
+
+
+def cpu_baseline(events, budget_s):
+    """Bounded sample of the workload on every host core (one single-threaded process each)."""
+    workers = cpu_workers()
+    ref = _reference_binary() is not None
+    # calibrate: one event on one core, then size the per-worker share to the budget
+    if ref:
+        n1, s1 = run_reference_sample(events[:1], 1, 1)
+    else:
+        n1, s1 = run_port_sample(events[:1], 1, 1)
+    per_event = s1 / max(n1, 1)
+    per_worker = max(1, min(len(events), int(budget_s / max(per_event, 1e-6))))
+    if ref:
+        n, s = run_reference_sample(events, workers, per_worker)
+    else:
+        n, s = run_port_sample(events, workers, per_worker)
+    return {"value": n / s, "unit": UNIT, "cores": workers, "kind": "reference" if ref else "port",
+            "sample": "%d Pb-Pb-like events (%d per process, %d single-threaded processes, one per core) of the "
+                      "benchmark workload; %s" % (n, per_worker, workers,
+                                                  "reference CPU Tracker built from its sources (oracle/_ref/ref_cr)"
+                                                  if ref else "oracle C port")}
+
+
+# ------------------------------------------------------------------------------------------
+# our implementation
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_env()
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    from itsu import capi
+
+    events = make_events(args.events, args.seed + 7919 * rank)
+    clusters, offsets, vertices = gen.pack_batch(events)
+    n_events, n_clusters = len(events), len(clusters)
+
+    # device-resident inputs (torch owns the memory; the library only reads it)
+    d_clusters = torch.from_numpy(clusters.view(np.uint8)).to(device)
+    d_offsets = torch.from_numpy(offsets).to(device)
+    d_vertices = torch.from_numpy(vertices).to(device)
+    stream = torch.cuda.Stream(device=device)
+    ctx = capi.Context(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    batch = ctx.batch_device(d_clusters.data_ptr(), d_offsets.data_ptr(), d_vertices.data_ptr(), n_events, n_clusters)
+    ctx.batch_run(batch)  # sizes the arena, validates the inputs, captures the graph
+    counts = []
+    for e in range(n_events):
+        c = ctx.counts(e)
+        counts.append(dict(N=list(c.clusters), T=list(c.tracklets), C=list(c.cells), E=list(c.neighbours), R=c.roads))
+    total_roads = sum(c["R"] for c in counts)
+
+    for _ in range(args.warmup):
+        ctx.batch_launch(batch)
+    stream.synchronize()
+    kernels = ctx.lib.itsu_kernels_per_run()
+
+    # ---- value: device-resident batch, K graph replays ----
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            ctx.batch_launch(batch)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ctx.batch_status()
+    if dist:
+        dist.barrier()
+    ms_local = start.elapsed_time(end)
+    ms = max_over_ranks(dist, ms_local, device)
+    clock_summary = clocks.summary()
+
+    # ---- e2e: host in / host out through the C ABI ----
+    h_clusters = torch.empty(clusters.nbytes, dtype=torch.uint8, pin_memory=True)
+    h_clusters.numpy()[:] = clusters.view(np.uint8)
+    h_offsets = torch.empty(len(offsets), dtype=torch.int32, pin_memory=True)
+    h_offsets.numpy()[:] = offsets
+    h_vertices = torch.empty(len(vertices), dtype=torch.float32, pin_memory=True)
+    h_vertices.numpy()[:] = vertices
+    roads_cap = int(total_roads * 1.1) + 1024
+    h_roads = torch.empty(roads_cap * 32, dtype=torch.uint8, pin_memory=True)
+    h_road_off = torch.empty(n_events + 1, dtype=torch.int32, pin_memory=True)
+    import ctypes
+
+    def host_run():
+        st = ctx.lib.itsu_batch_run_host(ctx.h, ctypes.c_void_p(h_clusters.data_ptr()), ctypes.c_void_p(h_offsets.data_ptr()),
+                                         ctypes.c_void_p(h_vertices.data_ptr()), n_events, ctypes.c_void_p(h_roads.data_ptr()),
+                                         roads_cap, ctypes.c_void_p(h_road_off.data_ptr()))
+        ctx._check(st)
+
+    for _ in range(max(1, args.warmup)):
+        host_run()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(args.steps):
+        host_run()
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(dist, e_start.elapsed_time(e_end), device)
+    assert int(h_road_off[-1]) == total_roads, "host path road count differs from the device path"
+
+    # ---- live per-kernel timing for the roofline ----
+    prof = ctx.profile(repeats=3)
+    step_bytes = {}
+    for c in counts:
+        for k, v in algorithmic_bytes(c).items():
+            step_bytes[k] = step_bytes.get(k, 0) + v
+    top_name, top_ms = max(prof, key=lambda x: x[1])
+    stage = KERNEL_STAGE.get(top_name)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    achieved = (step_bytes[stage] / (top_ms * 1e-3) / 1e9) if stage else None
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        per_event = tr.get("kernels", {}).get(top_name, {}).get("dram_bytes_per_event")
+        if per_event is not None:
+            traffic = per_event * n_events
+    except (OSError, ValueError):
+        pass
+
+    total_events = sum_over_ranks(dist, n_events * args.steps, device)
+    value = total_events / (ms * 1e-3)
+    e2e_value = total_events / (e2e_ms * 1e-3)
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            cpu = cpu_baseline(events, args.cpu_seconds)
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded helix generator, reference geometry; no public dataset)",
+            "config": {
+                "workload": WORKLOAD,
+                "events_per_step_per_gpu": n_events,
+                "tracks_per_event": TRACKS,
+                "clusters_per_step_per_gpu": n_clusters,
+                "tracklets_per_step_per_gpu": int(sum(sum(c["T"]) for c in counts)),
+                "cells_per_step_per_gpu": int(sum(sum(c["C"]) for c in counts)),
+                "roads_per_step_per_gpu": int(total_roads),
+                "mode": "batched plain path, one CUDA graph per step",
+                "parallelism": "event shards, one rank per GPU" if world > 1 else "single GPU",
+                "l2": "inputs larger than L2 (%.0f MB raw clusters, %.0f MB tracklets per step), no flush" % (
+                    clusters.nbytes / 1e6, 16 * sum(sum(c["T"]) for c in counts) / 1e6),
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(clusters.nbytes + offsets.nbytes + vertices.nbytes),
+                    "d2h_bytes_per_step": int(32 * total_roads + 4 * (n_events + 1)),
+                    "api": "itsu_batch_run_host (pinned host buffers)"},
+            "gpu_launches": kernels * args.steps,
+            "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": step_bytes.get(stage), "launch_ms": top_ms,
+                         "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_src if peak_src == "measured" else "fallback 6.65 TB/s"},
+            "kernel_ms": {name: round(t, 4) for name, t in prof},
+            "algorithmic_bytes_per_step": step_bytes.get("event"),
+            "achieved_gbs_whole_step": step_bytes.get("event") / (ms / args.steps * 1e-3) / 1e9,
+            "clocks": clock_summary,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+# ------------------------------------------------------------------------------------------
+# the reference's own CPU implementation of the path
+
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return None
+    if _reference_binary() is None:
+        impl = "oracle C port (the reference build oracle/_ref is not present)"
+    else:
+        impl = "reference CPU Tracker built from its own sources (oracle/_ref/ref_cr, patched P1-P5)"
+    workers = cpu_workers()
+    events = make_events(max(workers, 8), args.seed)
+    per_worker = 1
+    total_events = 0
+    total_s = 0.0
+    for step in range(args.warmup + args.steps):
+        if _reference_binary() is not None:
+            n, s = run_reference_sample(events, workers, per_worker)
+        else:
+            n, s = run_port_sample(events, workers, per_worker)
+        if step >= args.warmup:
+            total_events += n
+            total_s += s
+    value = total_events / total_s
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_s / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded helix generator, reference geometry; no public dataset)",
+        "config": {"workload": WORKLOAD, "events_per_step": workers * per_worker, "tracks_per_event": TRACKS,
+                   "mode": "reference CPU Tracker::clustersToTracks, one single-threaded process per host core"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers,
+                         "kind": "reference" if _reference_binary() else "port",
+                         "sample": "%d events per step (%d processes x %d), %s" % (workers * per_worker, workers, per_worker, impl)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return line
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

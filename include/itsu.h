@@ -201,6 +201,22 @@ itsu_status itsu_batch_status(itsu_context *ctx);
 /* Device pointer to the roads of the last batch (event-major) and to road_offsets[n_events+1]. */
 itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, const int32_t **road_offsets);
 
+/* ---- instrumentation (no counterpart in the reference beyond its clock() stage timers,
+ *      src/CA/Tracker.cxx:655-684) ---- */
+typedef struct itsu_kernel_time {
+  char name[40];
+  float ms;      /* mean duration over the repeats, CUDA events on the context stream */
+  int32_t launches;
+} itsu_kernel_time;
+
+/* Number of kernels one whole-path or batch run launches. */
+int32_t itsu_kernels_per_run(void);
+/* Re-runs the last batch `repeats` times with every kernel launched on its own and bracketed by
+ * CUDA events on the context stream; fills up to `capacity` entries in launch order. Call after
+ * itsu_batch_run (or itsu_batch_run_host) has sized the arena for that batch. */
+itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_time *times, int32_t capacity,
+                               int32_t *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,10 +35,8 @@
 
 #if defined(__CUDACC__)
 #define ITSU_CR_FN static __host__ __device__ __forceinline__
-#define ITSU_CR_TABLE static __device__ const
 #else
 #define ITSU_CR_FN static inline
-#define ITSU_CR_TABLE static const
 #endif
 
 #if defined(__CUDA_ARCH__)
@@ -58,55 +56,73 @@
 #endif
 
 /* atan(k/32), k = 0..32, as (hi, lo) pairs. */
-ITSU_CR_TABLE double itsu_cr_atan_k32[33][2] = {
-    {0x0.0p+0, 0x0.0p+0},
-    {0x1.ffd55bba97625p-6, -0x1.5ec431444912cp-60},
-    {0x1.ff55bb72cfdeap-5, -0x1.c934d86d23f1dp-60},
-    {0x1.7ee182602f10fp-4, -0x1.cfb654c0c3d98p-58},
-    {0x1.fd5ba9aac2f6ep-4, -0x1.cd37686760c17p-59},
-    {0x1.3d6eee8c6626cp-3, 0x1.61a3b0ce9281bp-57},
-    {0x1.7b97b4bce5b02p-3, 0x1.347b0b4f881cap-58},
-    {0x1.b90d7529260a2p-3, 0x1.17b10d2e0e5abp-61},
-    {0x1.f5b75f92c80ddp-3, 0x1.8ab6e3cf7afbdp-57},
-    {0x1.18bf5a30bf178p-2, 0x1.30ca4748b1bf9p-57},
-    {0x1.362773707ebccp-2, -0x1.963a544b672d8p-57},
-    {0x1.530ad9951cd4ap-2, -0x1.2566480884082p-57},
-    {0x1.6f61941e4def1p-2, -0x1.c63aae6f6e918p-56},
-    {0x1.8b24d394a1b25p-2, 0x1.b6d0ba3748fa8p-56},
-    {0x1.a64eec3cc23fdp-2, -0x1.24dec1b50b7ffp-56},
-    {0x1.c0db4c94ec9f0p-2, -0x1.cc1ce70934c34p-56},
-    {0x1.dac670561bb4fp-2, 0x1.a2b7f222f65e2p-56},
-    {0x1.f40dd0b541418p-2, -0x1.a3992dc382a23p-57},
-    {0x1.0657e94db30d0p-1, -0x1.d5b495f6349e6p-56},
-    {0x1.1255d9bfbd2a9p-1, -0x1.2bdaee1c0ee35p-58},
-    {0x1.1e00babdefeb4p-1, -0x1.928df287a668fp-58},
-    {0x1.2958e59308e31p-1, -0x1.09e73b0c6c087p-56},
-    {0x1.345f01cce37bbp-1, 0x1.1021137c71102p-55},
-    {0x1.3f13fb89e96f4p-1, 0x1.ecf8b492644f0p-56},
-    {0x1.4978fa3269ee1p-1, 0x1.2419a87f2a458p-56},
-    {0x1.538f57b89061fp-1, -0x1.1bb74abda520cp-55},
-    {0x1.5d58987169b18p-1, 0x1.0028e4bc5e7cap-57},
-    {0x1.66d663923e087p-1, -0x1.6ea6febe8bbbap-56},
-    {0x1.700a7c5784634p-1, -0x1.8c34d25aadef6p-56},
-    {0x1.78f6bbd5d315ep-1, 0x1.406a089803740p-55},
-    {0x1.819d0b7158a4dp-1, -0x1.bf76229d3b917p-56},
-    {0x1.89ff5ff57f1f8p-1, -0x1.55b9a5e177a1bp-55},
-    {0x1.921fb54442d18p-1, 0x1.1a62633145c07p-55},
-};
+#define ITSU_CR_ATAN_K32_VALUES \
+  { \
+    {0x0.0p+0, 0x0.0p+0}, \
+    {0x1.ffd55bba97625p-6, -0x1.5ec431444912cp-60}, \
+    {0x1.ff55bb72cfdeap-5, -0x1.c934d86d23f1dp-60}, \
+    {0x1.7ee182602f10fp-4, -0x1.cfb654c0c3d98p-58}, \
+    {0x1.fd5ba9aac2f6ep-4, -0x1.cd37686760c17p-59}, \
+    {0x1.3d6eee8c6626cp-3, 0x1.61a3b0ce9281bp-57}, \
+    {0x1.7b97b4bce5b02p-3, 0x1.347b0b4f881cap-58}, \
+    {0x1.b90d7529260a2p-3, 0x1.17b10d2e0e5abp-61}, \
+    {0x1.f5b75f92c80ddp-3, 0x1.8ab6e3cf7afbdp-57}, \
+    {0x1.18bf5a30bf178p-2, 0x1.30ca4748b1bf9p-57}, \
+    {0x1.362773707ebccp-2, -0x1.963a544b672d8p-57}, \
+    {0x1.530ad9951cd4ap-2, -0x1.2566480884082p-57}, \
+    {0x1.6f61941e4def1p-2, -0x1.c63aae6f6e918p-56}, \
+    {0x1.8b24d394a1b25p-2, 0x1.b6d0ba3748fa8p-56}, \
+    {0x1.a64eec3cc23fdp-2, -0x1.24dec1b50b7ffp-56}, \
+    {0x1.c0db4c94ec9f0p-2, -0x1.cc1ce70934c34p-56}, \
+    {0x1.dac670561bb4fp-2, 0x1.a2b7f222f65e2p-56}, \
+    {0x1.f40dd0b541418p-2, -0x1.a3992dc382a23p-57}, \
+    {0x1.0657e94db30d0p-1, -0x1.d5b495f6349e6p-56}, \
+    {0x1.1255d9bfbd2a9p-1, -0x1.2bdaee1c0ee35p-58}, \
+    {0x1.1e00babdefeb4p-1, -0x1.928df287a668fp-58}, \
+    {0x1.2958e59308e31p-1, -0x1.09e73b0c6c087p-56}, \
+    {0x1.345f01cce37bbp-1, 0x1.1021137c71102p-55}, \
+    {0x1.3f13fb89e96f4p-1, 0x1.ecf8b492644f0p-56}, \
+    {0x1.4978fa3269ee1p-1, 0x1.2419a87f2a458p-56}, \
+    {0x1.538f57b89061fp-1, -0x1.1bb74abda520cp-55}, \
+    {0x1.5d58987169b18p-1, 0x1.0028e4bc5e7cap-57}, \
+    {0x1.66d663923e087p-1, -0x1.6ea6febe8bbbap-56}, \
+    {0x1.700a7c5784634p-1, -0x1.8c34d25aadef6p-56}, \
+    {0x1.78f6bbd5d315ep-1, 0x1.406a089803740p-55}, \
+    {0x1.819d0b7158a4dp-1, -0x1.bf76229d3b917p-56}, \
+    {0x1.89ff5ff57f1f8p-1, -0x1.55b9a5e177a1bp-55}, \
+    {0x1.921fb54442d18p-1, 0x1.1a62633145c07p-55}, \
+  }
 
 /* 1/(2m+1), m = 0..9, as (hi, lo) pairs: coefficients of atan(u) = u sum (-1)^m u^2m/(2m+1). */
-ITSU_CR_TABLE double itsu_cr_inv_odd[10][2] = {
-    {0x1.0p+0, 0x0.0p+0},
-    {0x1.5555555555555p-2, 0x1.5555555555555p-56},
-    {0x1.999999999999ap-3, -0x1.999999999999ap-57},
-    {0x1.2492492492492p-3, 0x1.2492492492492p-57},
-    {0x1.c71c71c71c71cp-4, 0x1.c71c71c71c71cp-58},
-    {0x1.745d1745d1746p-4, -0x1.745d1745d1746p-59},
-    {0x1.3b13b13b13b14p-4, -0x1.3b13b13b13b14p-58},
-    {0x1.1111111111111p-4, 0x1.1111111111111p-60},
-    {0x1.e1e1e1e1e1e1ep-5, 0x1.e1e1e1e1e1e1ep-61},
-    {0x1.af286bca1af28p-5, 0x1.af286bca1af28p-59},
-};
+#define ITSU_CR_INV_ODD_VALUES \
+  { \
+    {0x1.0p+0, 0x0.0p+0}, \
+    {0x1.5555555555555p-2, 0x1.5555555555555p-56}, \
+    {0x1.999999999999ap-3, -0x1.999999999999ap-57}, \
+    {0x1.2492492492492p-3, 0x1.2492492492492p-57}, \
+    {0x1.c71c71c71c71cp-4, 0x1.c71c71c71c71cp-58}, \
+    {0x1.745d1745d1746p-4, -0x1.745d1745d1746p-59}, \
+    {0x1.3b13b13b13b14p-4, -0x1.3b13b13b13b14p-58}, \
+    {0x1.1111111111111p-4, 0x1.1111111111111p-60}, \
+    {0x1.e1e1e1e1e1e1ep-5, 0x1.e1e1e1e1e1e1ep-61}, \
+    {0x1.af286bca1af28p-5, 0x1.af286bca1af28p-59}, \
+  }
+
+/* One copy of each table per side: device code reads the __device__ copy, host code its own. */
+#if defined(__CUDACC__)
+static __device__ const double itsu_cr_atan_k32_dev[33][2] = ITSU_CR_ATAN_K32_VALUES;
+static __device__ const double itsu_cr_inv_odd_dev[10][2] = ITSU_CR_INV_ODD_VALUES;
+#endif
+static const double itsu_cr_atan_k32_host[33][2] = ITSU_CR_ATAN_K32_VALUES;
+static const double itsu_cr_inv_odd_host[10][2] = ITSU_CR_INV_ODD_VALUES;
+#if defined(__CUDA_ARCH__)
+#define itsu_cr_atan_k32 itsu_cr_atan_k32_dev
+#define itsu_cr_inv_odd itsu_cr_inv_odd_dev
+#else
+#define itsu_cr_atan_k32 itsu_cr_atan_k32_host
+#define itsu_cr_inv_odd itsu_cr_inv_odd_host
+#endif
+
 
 #define ITSU_CR_PI_HI 0x1.921fb54442d18p+1
 #define ITSU_CR_PI_LO 0x1.1a62633145c07p-53

@@ -7,6 +7,7 @@
 //   ref_cr dump <events.txt> <out.bin>   run every vertex stage by stage, write all results
 //   ref_cr time <events.txt> <repeats>   time Tracker::clustersToTracks per event (steady_clock,
 //                                        one warm-up event first, as main.cpp:74-75) -> JSON line
+//   ref_cr timebin <events.bin> <repeats> [first count]   the same on binary events
 //
 // The dump needs the tracker's private per-vertex context and its protected stages, so the
 // reference headers are included with private/protected opened up (standard headers first, so
@@ -164,9 +165,61 @@ int run_dump(const std::string &events_file, const std::string &out_file)
   return 0;
 }
 
+// Binary events (test infrastructure format "ITSUEVT1"): int32 n_events, then per event
+// int32 n_vertices, float xyz per vertex, int32 counts[7], and per cluster float x, y, z, alpha
+// and int32 mc, layer by layer. Events are built through the reference's public Event API with
+// the running cluster ids IOUtils::loadEventData assigns (IOUtils.cxx:63,71).
+std::vector<Event> load_binary_events(const std::string &file, int first, int count)
+{
+  std::vector<Event> events;
+  std::FILE *f = std::fopen(file.c_str(), "rb");
+  if (!f) {
+    std::perror("fopen");
+    return events;
+  }
+  char magic[8];
+  int32_t n = 0;
+  if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, "ITSUEVT1", 8) != 0 || std::fread(&n, 4, 1, f) != 1) {
+    std::fclose(f);
+    std::fprintf(stderr, "not an ITSUEVT1 file\n");
+    return events;
+  }
+  const int last = count < 0 ? n : std::min(n, first + count);
+  for (int e = 0; e < last; ++e) {
+    int32_t nv = 0, counts[7];
+    if (std::fread(&nv, 4, 1, f) != 1) break;
+    std::vector<float> v(3 * static_cast<size_t>(nv));
+    std::fread(v.data(), 4, v.size(), f);
+    std::fread(counts, 4, 7, f);
+    const bool keep = e >= first;
+    if (keep) events.emplace_back(static_cast<int>(events.size()));
+    int cluster_id = 0;
+    for (int iv = 0; iv < nv && keep; ++iv) events.back().addPrimaryVertex(v[3 * iv], v[3 * iv + 1], v[3 * iv + 2]);
+    for (int l = 0; l < 7; ++l) {
+      for (int32_t k = 0; k < counts[l]; ++k) {
+        float xyza[4];
+        int32_t mc;
+        std::fread(xyza, 4, 4, f);
+        std::fread(&mc, 4, 1, f);
+        if (keep) events.back().pushClusterToLayer(l, cluster_id, xyza[0], xyza[1], xyza[2], xyza[3], mc);
+        ++cluster_id;
+      }
+    }
+  }
+  std::fclose(f);
+  return events;
+}
+
+int run_time_events(std::vector<Event> &events, int repeats);
+
 int run_time(const std::string &events_file, int repeats)
 {
   std::vector<Event> events = IOUtils::loadEventData(events_file);
+  return run_time_events(events, repeats);
+}
+
+int run_time_events(std::vector<Event> &events, int repeats)
+{
   if (events.empty()) {
     std::printf("{\"events\": 0}\n");
     return 0;
@@ -204,12 +257,21 @@ int main(int argc, char **argv)
   }
 #endif
   if (argc < 4) {
-    std::fprintf(stderr, "usage: %s dump <events.txt> <out.bin> | time <events.txt> <repeats>\n", argv[0]);
+    std::fprintf(stderr,
+                 "usage: %s dump <events.txt> <out.bin> | time <events.txt> <repeats> |"
+                 " timebin <events.bin> <repeats> [first count]\n",
+                 argv[0]);
     return 2;
   }
   const std::string mode = argv[1];
   if (mode == "dump") return run_dump(argv[2], argv[3]);
   if (mode == "time") return run_time(argv[2], std::atoi(argv[3]));
+  if (mode == "timebin") {
+    const int first = argc > 5 ? std::atoi(argv[4]) : 0;
+    const int count = argc > 5 ? std::atoi(argv[5]) : -1;
+    std::vector<Event> events = load_binary_events(argv[2], first, count);
+    return run_time_events(events, std::atoi(argv[3]));
+  }
   std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
   return 2;
 }

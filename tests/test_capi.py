@@ -1,0 +1,56 @@
+"""Host-side checks of the C ABI library: it loads, exports every entry point include/itsu.h
+declares, and its records keep the reference layouts. No kernel runs here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from itsu import capi, gen
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "itsu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(itsu_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_entry_point():
+    lib = capi.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), name
+    assert sorted(n for n, _, _ in capi.SIGNATURES) == names
+
+
+def test_record_layouts_match_the_reference():
+    assert gen.CLUSTER_DTYPE.itemsize == 36
+    assert capi.TRACKLET_DTYPE.itemsize == 16
+    assert capi.CELL_DTYPE.itemsize == 40
+    assert capi.ROAD_DTYPE.itemsize == 32
+    assert ctypes.sizeof(capi.Config) == 56
+    assert ctypes.sizeof(capi.Batch) == 40
+    assert ctypes.sizeof(capi.Counts) == 4 * (7 + 6 + 5 + 4 + 1)
+
+
+def test_status_strings_and_version():
+    lib = capi.load()
+    assert b"sm_100a" in lib.itsu_version()
+    assert lib.itsu_status_string(capi.OK) == b"ok"
+    assert lib.itsu_status_string(capi.ERR_CAPACITY) == b"capacity exceeded"
+
+
+def test_context_creation_fails_loudly_without_a_b200():
+    import torch
+
+    if torch.cuda.is_available():
+        return  # covered by the GPU tests
+    try:
+        capi.Context()
+    except capi.ItsuError as e:
+        assert e.status == capi.ERR_CUDA
+    else:
+        raise AssertionError("a context was created without a GPU")

@@ -1,0 +1,134 @@
+"""Parity of the sm_100a path (through the C ABI) with the reference and the oracle.
+
+Bit-exact equality is required for every output: sorted clusters, index tables, tracklets and
+their lookup tables, cells (including CA levels) and their lookup tables, neighbour rows, and
+roads with their labels.
+"""
+import numpy as np
+import pytest
+
+from helpers import CASES, load_case, vertex_runs
+from itsu import capi, gen
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = capi.Context(device=0)
+    yield c
+    c.close()
+
+
+def _assert_same(got, want, what):
+    mismatches = oracle.diff(got, want)
+    assert mismatches == [], "%s: %s" % (what, mismatches[:6])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_stage_api_matches_reference_fixture(ctx, case):
+    """PrimaryVertexContext::initialize + each Tracker stage, one C ABI call per stage."""
+    events, expected = load_case(case)
+    for k, ((ev, iv), exp) in enumerate(zip(vertex_runs(events), expected)):
+        _assert_same(ctx.run_vertex(ev.layers, ev.vertices[iv]), exp, "%s vertex %d" % (case, k))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_whole_path_roads_match_reference_fixture(ctx, case):
+    events, expected = load_case(case)
+    for (ev, iv), exp in zip(vertex_runs(events), expected):
+        roads = ctx.clusters_to_tracks(ev.layers, ev.vertices[iv])
+        assert np.array_equal(roads.view(np.uint8), exp["roads"].view(np.uint8))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_batch_matches_reference_fixture(ctx, case):
+    """Every vertex of the fixture as one event of a single batch."""
+    events, expected = load_case(case)
+    runs = vertex_runs(events)
+    clusters, offsets, vertices = gen.pack_batch([ev for ev, _ in runs], [iv for _, iv in runs])
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    for e, exp in enumerate(expected):
+        _assert_same(ctx.results(e), exp, "%s batch event %d" % (case, e))
+        assert np.array_equal(roads[road_off[e]:road_off[e + 1]].view(np.uint8), exp["roads"].view(np.uint8))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_pbpb_event_matches_oracle(ctx, seed):
+    ev = gen.pbpb_event(seed)
+    want = oracle.run_vertex(ev.layers, ev.vertices[0])
+    _assert_same(ctx.run_vertex(ev.layers, ev.vertices[0]), want, "Pb-Pb stages")
+    roads = ctx.clusters_to_tracks(ev.layers, ev.vertices[0])
+    assert np.array_equal(roads.view(np.uint8), want["roads"].view(np.uint8))
+    assert len(want["roads"]) > 1000
+
+
+def test_pileup_frame_matches_oracle(ctx):
+    ev = gen.pileup_frame(7)
+    clusters, offsets, vertices = gen.pack_batch([ev] * 5, list(range(5)))
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    for iv in range(5):
+        want = oracle.run_vertex(ev.layers, ev.vertices[iv])
+        _assert_same(ctx.results(iv), want, "pile-up vertex %d" % iv)
+
+
+def test_uneven_batch_matches_per_event_runs(ctx):
+    """A batch of uneven multiplicity (20-8000 tracks, log-uniform) equals event-by-event runs
+    and the oracle, event by event."""
+    events = gen.batch_events(11, n_events=24)
+    clusters, offsets, vertices = gen.pack_batch(events)
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    batch_results = [ctx.results(e) for e in range(len(events))]
+    for e, ev in enumerate(events):
+        want = oracle.run_vertex(ev.layers, ev.vertices[0])
+        _assert_same(batch_results[e], want, "batch event %d" % e)
+        single = ctx.clusters_to_tracks(ev.layers, ev.vertices[0])
+        assert np.array_equal(single.view(np.uint8), roads[road_off[e]:road_off[e + 1]].view(np.uint8))
+
+
+def test_arena_growth_gives_identical_results():
+    """Tiny initial capacities force every growth path; results must not change."""
+    ev = gen.pbpb_event(4, n_tracks=2000)
+    want = oracle.run_vertex(ev.layers, ev.vertices[0])
+    small = capi.Context(device=0, max_clusters=16, max_tracklets=16, max_cells=16, max_neighbours=16, max_roads=16, max_events=1)
+    try:
+        roads = small.clusters_to_tracks(ev.layers, ev.vertices[0])
+        assert np.array_equal(roads.view(np.uint8), want["roads"].view(np.uint8))
+        _assert_same(small.results(0), want, "after growth")
+    finally:
+        small.close()
+    fixed = capi.Context(device=0, flags=capi.FLAG_NO_GROW, max_clusters=16, max_tracklets=16, max_cells=16,
+                         max_neighbours=16, max_roads=16, max_events=1)
+    try:
+        clusters, offsets, vertices = gen.pack_batch([ev])
+        with pytest.raises(capi.ItsuError) as err:
+            fixed.batch_run_host(clusters, offsets, vertices, roads_capacity=100000)
+        assert err.value.status == capi.ERR_CAPACITY
+    finally:
+        fixed.close()
+
+
+def test_malformed_input_is_rejected(ctx):
+    ev = gen.pp_event(5)
+    bad = [l.copy() for l in ev.layers]
+    bad[2]["z"][3] = np.nan
+    with pytest.raises(capi.ItsuError) as err:
+        ctx.run_vertex(bad, ev.vertices[0])
+    assert err.value.status == capi.ERR_INVALID
+    with pytest.raises(capi.ItsuError) as err:
+        ctx.clusters_to_tracks(ev.layers, (np.inf, 0.0, 0.0))
+    assert err.value.status == capi.ERR_INVALID
+    # the context stays usable after a rejected input
+    want = oracle.run_vertex(ev.layers, ev.vertices[0])
+    _assert_same(ctx.run_vertex(ev.layers, ev.vertices[0]), want, "after rejection")
+
+
+def test_stage_order_is_enforced():
+    fresh = capi.Context(device=0)
+    try:
+        with pytest.raises(capi.ItsuError) as err:
+            fresh._check(fresh.lib.itsu_compute_layer_cells(fresh.h))
+        assert err.value.status == capi.ERR_STATE
+    finally:
+        fresh.close()

@@ -1,0 +1,996 @@
+// itsu_capi.cu - C ABI of the track finder: context, device arena, stage orchestration.
+//
+// The per-vertex entry points mirror the reference's seam (PrimaryVertexContext::initialize,
+// TrackerTraits::computeLayerTracklets / computeLayerCells, Tracker::findCellsNeighbours /
+// findTracks / computeMontecarloLabels) and are synchronous like the reference GPU backend
+// (src/CA/gpu/cuda/Tracker.cu synchronises after every stage). Each stage counts, scans, and
+// sizes its outputs exactly before writing them (two-pass sizing). The whole-path and batch
+// entry points enqueue every stage back to back without host round trips (replayed as a CUDA
+// graph), then check the device status once; an output that overflowed the arena is grown to the
+// reported requirement and the run repeated.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "itsu.h"
+#include "itsu_internal.h"
+
+using itsu::Arena;
+using itsu::DevStatus;
+using itsu::Launch;
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+enum Stage { kNone = 0, kInitialized, kTracklets, kCells, kNeighbours, kRoads };
+
+}  // namespace
+
+struct itsu_context {
+  int device = 0;
+  uint32_t flags = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+
+  // capacities
+  int64_t cap_clusters = 0;
+  int32_t cap_events = 0;
+  int64_t cap_tracklets = 0, cap_cells = 0, cap_neighbours = 0, cap_roads = 0, cap_partials = 0;
+  int64_t init_tracklets = 0, init_cells = 0, init_neighbours = 0, init_roads = 0;
+
+  // device buffers: cluster class
+  itsu_cluster *raw = nullptr, *sorted = nullptr, *tmp = nullptr;
+  float4 *xyzr = nullptr;
+  float *phi = nullptr;
+  int32_t *trk_count = nullptr, *trk_off = nullptr, *trk_lookup = nullptr;
+  // event class
+  int32_t *layer_off = nullptr, *index_tables = nullptr, *trk_seg = nullptr, *cell_seg = nullptr, *road_seg = nullptr;
+  float *vtx = nullptr;
+  // tracklet class
+  itsu_tracklet *tracklets = nullptr;
+  int32_t *trk_seg_id = nullptr, *cell_count = nullptr, *cell_off = nullptr, *cell_lookup = nullptr;
+  // cell class
+  itsu_cell *cells = nullptr;
+  int32_t *cell_seg_id = nullptr, *nb_count = nullptr, *nb_off = nullptr, *nb_fill = nullptr, *road_count = nullptr,
+          *road_off = nullptr;
+  int64_t *paths = nullptr;
+  // neighbour and road classes
+  int32_t *nb = nullptr;
+  itsu_road *roads = nullptr;
+  int64_t *scan_partials = nullptr;
+  DevStatus *d_status = nullptr;
+  DevStatus *h_status = nullptr;
+
+  // current run
+  int32_t n_events = 0;
+  int64_t n_clusters = 0;
+  std::vector<int32_t> h_layer_off;
+  const itsu_cluster *in_raw = nullptr;
+  const int32_t *in_layer_off = nullptr;
+  const float *in_vtx = nullptr;
+  int stage = kNone;
+
+  // CUDA graph of the whole batch sequence
+  cudaGraphExec_t graph = nullptr;
+  uint64_t graph_generation = 0;
+  uint64_t generation = 1;  // bumped whenever a buffer is reallocated
+  const void *graph_key[3] = {nullptr, nullptr, nullptr};
+  int32_t graph_events = -1;
+  int64_t graph_clusters = -1;
+
+  std::string error;
+};
+
+namespace {
+
+itsu_status fail(itsu_context *ctx, itsu_status st, const char *fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (ctx) {
+    ctx->error = buf;
+  }
+  g_thread_error = buf;
+  return st;
+}
+
+#define ITSU_CUDA(ctx, call)                                                                                   \
+  do {                                                                                                         \
+    cudaError_t err_ = (call);                                                                                 \
+    if (err_ != cudaSuccess) {                                                                                 \
+      return fail((ctx), err_ == cudaErrorMemoryAllocation ? ITSU_ERR_NOMEM : ITSU_ERR_CUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(err_), __FILE__, __LINE__);                                        \
+    }                                                                                                          \
+  } while (0)
+
+template <typename T>
+void release(T *&p)
+{
+  if (p) {
+    cudaFree((void *)p);
+    p = nullptr;
+  }
+}
+
+template <typename T>
+cudaError_t alloc(T *&p, int64_t count)
+{
+  release(p);
+  return cudaMalloc((void **)&p, (size_t)std::max<int64_t>(count, 1) * sizeof(T));
+}
+
+Launch launch_of(const itsu_context *ctx) { return Launch{ctx->stream, ctx->num_sms}; }
+
+Arena arena_of(const itsu_context *ctx)
+{
+  Arena a{};
+  a.n_events = ctx->n_events;
+  a.n_clusters = ctx->n_clusters;
+  a.raw = ctx->in_raw;
+  a.layer_off = ctx->in_layer_off;
+  a.vtx = ctx->in_vtx;
+  a.sorted = ctx->sorted;
+  a.xyzr = ctx->xyzr;
+  a.phi = ctx->phi;
+  a.tmp = ctx->tmp;
+  a.index_tables = ctx->index_tables;
+  a.trk_count = ctx->trk_count;
+  a.trk_off = ctx->trk_off;
+  a.trk_lookup = ctx->trk_lookup;
+  a.trk_seg = ctx->trk_seg;
+  a.tracklets = ctx->tracklets;
+  a.trk_seg_id = ctx->trk_seg_id;
+  a.cell_count = ctx->cell_count;
+  a.cell_off = ctx->cell_off;
+  a.cell_lookup = ctx->cell_lookup;
+  a.cell_seg = ctx->cell_seg;
+  a.cells = ctx->cells;
+  a.cell_seg_id = ctx->cell_seg_id;
+  a.nb_count = ctx->nb_count;
+  a.nb_off = ctx->nb_off;
+  a.nb_fill = ctx->nb_fill;
+  a.nb = ctx->nb;
+  a.paths = ctx->paths;
+  a.road_count = ctx->road_count;
+  a.road_off = ctx->road_off;
+  a.road_seg = ctx->road_seg;
+  a.roads = ctx->roads;
+  a.scan_partials = ctx->scan_partials;
+  a.status = ctx->d_status;
+  a.cap_tracklets = ctx->cap_tracklets;
+  a.cap_cells = ctx->cap_cells;
+  a.cap_neighbours = ctx->cap_neighbours;
+  a.cap_roads = ctx->cap_roads;
+  return a;
+}
+
+int64_t grow_to(int64_t need) { return need + need / 4 + 1024; }
+
+itsu_status ensure_partials(itsu_context *ctx)
+{
+  const int64_t need = std::max({ctx->cap_clusters, ctx->cap_tracklets, ctx->cap_cells}) / 2048 + 2;
+  if (need > ctx->cap_partials) {
+    ITSU_CUDA(ctx, alloc(ctx->scan_partials, need));
+    ctx->cap_partials = need;
+    ctx->generation++;
+  }
+  return ITSU_OK;
+}
+
+itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_events)
+{
+  if (n_clusters > ctx->cap_clusters) {
+    const int64_t cap = grow_to(n_clusters);
+    ITSU_CUDA(ctx, alloc(ctx->raw, cap));
+    ITSU_CUDA(ctx, alloc(ctx->sorted, cap));
+    ITSU_CUDA(ctx, alloc(ctx->tmp, cap));
+    ITSU_CUDA(ctx, alloc(ctx->xyzr, cap));
+    ITSU_CUDA(ctx, alloc(ctx->phi, cap));
+    ITSU_CUDA(ctx, alloc(ctx->trk_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->trk_off, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->trk_lookup, cap));
+    ctx->cap_clusters = cap;
+    ctx->generation++;
+  }
+  if (n_events > ctx->cap_events) {
+    const int32_t cap = n_events + n_events / 4 + 4;
+    ITSU_CUDA(ctx, alloc(ctx->layer_off, (int64_t)cap * ITSU_LAYERS + 1));
+    ITSU_CUDA(ctx, alloc(ctx->vtx, (int64_t)cap * 3));
+    ITSU_CUDA(ctx, alloc(ctx->index_tables, (int64_t)cap * ITSU_TRACKLET_LAYERS * ITSU_INDEX_TABLE_SIZE));
+    ITSU_CUDA(ctx, alloc(ctx->trk_seg, (int64_t)cap * ITSU_TRACKLET_LAYERS + 1));
+    ITSU_CUDA(ctx, alloc(ctx->cell_seg, (int64_t)cap * ITSU_CELL_LAYERS + 1));
+    ITSU_CUDA(ctx, alloc(ctx->road_seg, (int64_t)cap + 1));
+    ctx->cap_events = cap;
+    ctx->generation++;
+  }
+  return ensure_partials(ctx);
+}
+
+itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
+{
+  if (need > ctx->cap_tracklets) {
+    const int64_t cap = grow_to(need);
+    ITSU_CUDA(ctx, alloc(ctx->tracklets, cap));
+    ITSU_CUDA(ctx, alloc(ctx->trk_seg_id, cap));
+    ITSU_CUDA(ctx, alloc(ctx->cell_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->cell_off, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->cell_lookup, cap));
+    ctx->cap_tracklets = cap;
+    ctx->generation++;
+  }
+  return ensure_partials(ctx);
+}
+
+itsu_status ensure_cells(itsu_context *ctx, int64_t need)
+{
+  if (need > ctx->cap_cells) {
+    const int64_t cap = grow_to(need);
+    ITSU_CUDA(ctx, alloc(ctx->cells, cap));
+    ITSU_CUDA(ctx, alloc(ctx->cell_seg_id, cap));
+    ITSU_CUDA(ctx, alloc(ctx->nb_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->nb_off, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->nb_fill, cap));
+    ITSU_CUDA(ctx, alloc(ctx->paths, cap));
+    ITSU_CUDA(ctx, alloc(ctx->road_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->road_off, cap + 1));
+    ctx->cap_cells = cap;
+    ctx->generation++;
+  }
+  return ensure_partials(ctx);
+}
+
+itsu_status ensure_neighbours(itsu_context *ctx, int64_t need)
+{
+  if (need > ctx->cap_neighbours) {
+    const int64_t cap = grow_to(need);
+    ITSU_CUDA(ctx, alloc(ctx->nb, cap));
+    ctx->cap_neighbours = cap;
+    ctx->generation++;
+  }
+  return ITSU_OK;
+}
+
+itsu_status ensure_roads(itsu_context *ctx, int64_t need)
+{
+  if (need > ctx->cap_roads) {
+    const int64_t cap = grow_to(need);
+    ITSU_CUDA(ctx, alloc(ctx->roads, cap));
+    ctx->cap_roads = cap;
+    ctx->generation++;
+  }
+  return ITSU_OK;
+}
+
+// Initial output capacities for a run of n_clusters clusters (Pb-Pb-like events produce about
+// 8 tracklets, 1 cell and 0.2 roads per cluster; the arena grows past these when needed).
+itsu_status ensure_outputs_for(itsu_context *ctx, int64_t n_clusters)
+{
+  itsu_status st;
+  if ((st = ensure_tracklets(ctx, std::max(ctx->init_tracklets, 10 * n_clusters + 4096))) != ITSU_OK) return st;
+  if ((st = ensure_cells(ctx, std::max(ctx->init_cells, 2 * n_clusters + 4096))) != ITSU_OK) return st;
+  if ((st = ensure_neighbours(ctx, std::max(ctx->init_neighbours, 2 * n_clusters + 4096))) != ITSU_OK) return st;
+  return ensure_roads(ctx, std::max(ctx->init_roads, n_clusters / 2 + 4096));
+}
+
+itsu_status check_launch(itsu_context *ctx)
+{
+  ITSU_CUDA(ctx, cudaGetLastError());
+  return ITSU_OK;
+}
+
+// Copies the device status to the host and waits for the stream.
+itsu_status sync_status(itsu_context *ctx)
+{
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+itsu_status check_invalid(itsu_context *ctx)
+{
+  const DevStatus &s = *ctx->h_status;
+  if (s.flags & itsu::kFlagInvalid) {
+    if (s.invalid_event != INT32_MAX) {
+      return fail(ctx, ITSU_ERR_INVALID, "primary vertex of event %d is not finite or beyond 1e6 cm", s.invalid_event);
+    }
+    return fail(ctx, ITSU_ERR_INVALID,
+                "cluster %d is malformed: a coordinate is not finite or beyond 1e6 cm, or it sits on the beam line "
+                "at the vertex z (r == 0 and z == vertex z)",
+                s.invalid_index);
+  }
+  return ITSU_OK;
+}
+
+itsu_status clear_flags(itsu_context *ctx)
+{
+  ITSU_CUDA(ctx, cudaMemsetAsync(&ctx->d_status->flags, 0, sizeof(int32_t), ctx->stream));
+  return ITSU_OK;
+}
+
+itsu_status count_overflow(itsu_context *ctx)
+{
+  return fail(ctx, ITSU_ERR_CAPACITY, "a result count exceeds the 32-bit index range of the reference layouts");
+}
+
+// Enqueues every stage of the current inputs (no host synchronisation).
+void enqueue_all(itsu_context *ctx)
+{
+  const Arena a = arena_of(ctx);
+  const Launch l = launch_of(ctx);
+  itsu::launch_status_init(a, l);
+  itsu::launch_cluster_sort(a, l);
+  itsu::launch_tracklets_count(a, l);
+  itsu::launch_tracklets_write(a, l);
+  itsu::launch_cells_count(a, l);
+  itsu::launch_cells_write(a, l);
+  itsu::launch_neighbours_count(a, l);
+  itsu::launch_neighbours_write(a, l);
+  itsu::launch_roads_count(a, l);
+  itsu::launch_roads_write(a, l);
+}
+
+void drop_graph(itsu_context *ctx)
+{
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+}
+
+// Launches the whole sequence, through a CUDA graph that is re-captured when the inputs,
+// sizes or arena buffers change.
+itsu_status launch_all(itsu_context *ctx)
+{
+  const bool same = ctx->graph && ctx->graph_generation == ctx->generation && ctx->graph_key[0] == ctx->in_raw &&
+                    ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
+                    ctx->graph_events == ctx->n_events && ctx->graph_clusters == ctx->n_clusters;
+  if (!same) {
+    drop_graph(ctx);
+    cudaGraph_t g = nullptr;
+    ITSU_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_all(ctx);
+    const cudaError_t launch_err = cudaGetLastError();
+    const cudaError_t end_err = cudaStreamEndCapture(ctx->stream, &g);
+    if (launch_err != cudaSuccess || end_err != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(ctx, ITSU_ERR_CUDA, "graph capture failed: %s / %s", cudaGetErrorString(launch_err),
+                  cudaGetErrorString(end_err));
+    }
+    const cudaError_t inst_err = cudaGraphInstantiate(&ctx->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (inst_err != cudaSuccess) {
+      ctx->graph = nullptr;
+      return fail(ctx, ITSU_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(inst_err));
+    }
+    ctx->graph_generation = ctx->generation;
+    ctx->graph_key[0] = ctx->in_raw;
+    ctx->graph_key[1] = ctx->in_layer_off;
+    ctx->graph_key[2] = ctx->in_vtx;
+    ctx->graph_events = ctx->n_events;
+    ctx->graph_clusters = ctx->n_clusters;
+  }
+  ITSU_CUDA(ctx, cudaGraphLaunch(ctx->graph, ctx->stream));
+  return ITSU_OK;
+}
+
+// Runs every stage, growing the arena and repeating after an overflow.
+itsu_status run_all(itsu_context *ctx)
+{
+  itsu_status st;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    if ((st = launch_all(ctx)) != ITSU_OK) return st;
+    if ((st = sync_status(ctx)) != ITSU_OK) return st;
+    if ((st = check_invalid(ctx)) != ITSU_OK) return st;
+    const DevStatus &s = *ctx->h_status;
+    if (!(s.flags & itsu::kCapacityMask)) {
+      ctx->stage = kRoads;
+      return ITSU_OK;
+    }
+    if (s.flags & itsu::kFlagCountOverflow) return count_overflow(ctx);
+    if (ctx->flags & ITSU_FLAG_NO_GROW) {
+      return fail(ctx, ITSU_ERR_CAPACITY, "result exceeds the arena (tracklets %lld/%lld cells %lld/%lld neighbours %lld/%lld roads %lld/%lld)",
+                  (long long)s.total[0], (long long)ctx->cap_tracklets, (long long)s.total[1], (long long)ctx->cap_cells,
+                  (long long)s.total[2], (long long)ctx->cap_neighbours, (long long)s.total[3], (long long)ctx->cap_roads);
+    }
+    if (s.flags & itsu::kFlagCapTracklets) {
+      // cells, neighbours and roads scale with the tracklets: grow them in proportion too
+      const double f = (double)s.total[0] / (double)std::max<int64_t>(ctx->cap_tracklets, 1);
+      if ((st = ensure_tracklets(ctx, s.total[0])) != ITSU_OK) return st;
+      if ((st = ensure_cells(ctx, (int64_t)(ctx->cap_cells * f))) != ITSU_OK) return st;
+      if ((st = ensure_neighbours(ctx, (int64_t)(ctx->cap_neighbours * f))) != ITSU_OK) return st;
+      if ((st = ensure_roads(ctx, (int64_t)(ctx->cap_roads * f))) != ITSU_OK) return st;
+    }
+    if ((s.flags & itsu::kFlagCapCells) && (st = ensure_cells(ctx, s.total[1])) != ITSU_OK) return st;
+    if ((s.flags & itsu::kFlagCapNeighbours) && (st = ensure_neighbours(ctx, s.total[2])) != ITSU_OK) return st;
+    if ((s.flags & itsu::kFlagCapRoads) && (st = ensure_roads(ctx, s.total[3])) != ITSU_OK) return st;
+  }
+  return fail(ctx, ITSU_ERR_CAPACITY, "arena growth did not converge");
+}
+
+itsu_status stage_count_then_write(itsu_context *ctx, void (*count)(const Arena &, const Launch &),
+                                   void (*write)(const Arena &, const Launch &), int total_index,
+                                   itsu_status (*ensure)(itsu_context *, int64_t))
+{
+  itsu_status st;
+  if ((st = clear_flags(ctx)) != ITSU_OK) return st;
+  count(arena_of(ctx), launch_of(ctx));
+  if ((st = check_launch(ctx)) != ITSU_OK) return st;
+  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  const DevStatus &s = *ctx->h_status;
+  if (s.flags & itsu::kFlagCountOverflow) return count_overflow(ctx);
+  if (s.flags & itsu::kCapacityMask) {
+    if (ctx->flags & ITSU_FLAG_NO_GROW) {
+      return fail(ctx, ITSU_ERR_CAPACITY, "stage output of %lld exceeds the arena", (long long)s.total[total_index]);
+    }
+    // exact two-pass sizing: grow the stage's outputs to the counted total. Growth reallocates
+    // only buffers the write pass fills, never the counts and offsets just computed, so the
+    // write proceeds on the existing counts.
+    if ((st = ensure(ctx, s.total[total_index])) != ITSU_OK) return st;
+    if ((st = clear_flags(ctx)) != ITSU_OK) return st;
+  }
+  write(arena_of(ctx), launch_of(ctx));
+  if ((st = check_launch(ctx)) != ITSU_OK) return st;
+  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  if (ctx->h_status->flags & itsu::kCapacityMask) {
+    return fail(ctx, ITSU_ERR_CAPACITY, "stage output exceeds the arena after growth");
+  }
+  return ITSU_OK;
+}
+
+itsu_status require_stage(itsu_context *ctx, int stage, const char *what)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "%s: null context", what);
+  if (ctx->stage < stage) {
+    return fail(ctx, ITSU_ERR_STATE, "%s called before the stage it depends on", what);
+  }
+  return ITSU_OK;
+}
+
+// Host inputs of one vertex -> device arena.
+itsu_status upload_vertex(itsu_context *ctx, const itsu_cluster *const layers[ITSU_LAYERS], const int32_t counts[ITSU_LAYERS],
+                          const float vertex[3])
+{
+  if (!layers || !counts || !vertex) return fail(ctx, ITSU_ERR_INVALID, "null argument");
+  std::vector<int32_t> off(ITSU_LAYERS + 1, 0);
+  for (int l = 0; l < ITSU_LAYERS; ++l) {
+    if (counts[l] < 0) return fail(ctx, ITSU_ERR_INVALID, "negative cluster count on layer %d", l);
+    if (counts[l] > 0 && !layers[l]) return fail(ctx, ITSU_ERR_INVALID, "null cluster array on layer %d", l);
+    if ((int64_t)off[l] + counts[l] > INT32_MAX) return fail(ctx, ITSU_ERR_INVALID, "too many clusters");
+    off[l + 1] = off[l] + counts[l];
+  }
+  itsu_status st;
+  if ((st = ensure_clusters(ctx, off[ITSU_LAYERS], 1)) != ITSU_OK) return st;
+  for (int l = 0; l < ITSU_LAYERS; ++l) {
+    if (counts[l] > 0) {
+      ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw + off[l], layers[l], sizeof(itsu_cluster) * counts[l], cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    }
+  }
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->layer_off, off.data(), sizeof(int32_t) * off.size(), cudaMemcpyHostToDevice, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, vertex, sizeof(float) * 3, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->n_events = 1;
+  ctx->n_clusters = off[ITSU_LAYERS];
+  ctx->h_layer_off = off;
+  ctx->in_raw = ctx->raw;
+  ctx->in_layer_off = ctx->layer_off;
+  ctx->in_vtx = ctx->vtx;
+  ctx->stage = kNone;
+  return ITSU_OK;
+}
+
+template <typename T>
+itsu_status copy_range(itsu_context *ctx, T *dst, const T *src, int64_t count)
+{
+  if (dst && count > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  return ITSU_OK;
+}
+
+struct EventSegments {
+  int32_t lo[ITSU_LAYERS + 1];
+  int32_t ts[ITSU_TRACKLET_LAYERS + 1];
+  int32_t cs[ITSU_CELL_LAYERS + 1];
+  int32_t rs[2];
+  int32_t nbo[ITSU_CELL_LAYERS + 1];  // nb_off at cs[0..5]
+};
+
+itsu_status event_segments(itsu_context *ctx, int32_t e, EventSegments &seg)
+{
+  if (e < 0 || e >= ctx->n_events) return fail(ctx, ITSU_ERR_INVALID, "event %d out of range", e);
+  std::memcpy(seg.lo, ctx->h_layer_off.data() + (int64_t)e * ITSU_LAYERS, sizeof seg.lo);
+  ITSU_CUDA(ctx, cudaMemcpyAsync(seg.ts, ctx->trk_seg + (int64_t)e * ITSU_TRACKLET_LAYERS, sizeof seg.ts, cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(seg.cs, ctx->cell_seg + (int64_t)e * ITSU_CELL_LAYERS, sizeof seg.cs, cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(seg.rs, ctx->road_seg + e, sizeof seg.rs, cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int l = 0; l <= ITSU_CELL_LAYERS; ++l) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(&seg.nbo[l], ctx->nb_off + seg.cs[l], sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+void counts_from(const itsu_context *ctx, const EventSegments &s, itsu_counts *out)
+{
+  for (int l = 0; l < ITSU_LAYERS; ++l) out->clusters[l] = s.lo[l + 1] - s.lo[l];
+  for (int l = 0; l < ITSU_TRACKLET_LAYERS; ++l) out->tracklets[l] = ctx->stage >= kTracklets ? s.ts[l + 1] - s.ts[l] : 0;
+  for (int l = 0; l < ITSU_CELL_LAYERS; ++l) out->cells[l] = ctx->stage >= kCells ? s.cs[l + 1] - s.cs[l] : 0;
+  for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {
+    out->neighbours[l] = ctx->stage >= kNeighbours ? s.nbo[l + 2] - s.nbo[l + 1] : 0;
+  }
+  out->roads = ctx->stage >= kRoads ? s.rs[1] - s.rs[0] : 0;
+}
+
+}  // namespace
+
+// ============================================================================================
+// C ABI
+
+extern "C" {
+
+const char *itsu_version(void) { return "itsu-b200 1.0 (sm_100a)"; }
+
+const char *itsu_status_string(itsu_status status)
+{
+  switch (status) {
+  case ITSU_OK: return "ok";
+  case ITSU_ERR_INVALID: return "invalid input";
+  case ITSU_ERR_CAPACITY: return "capacity exceeded";
+  case ITSU_ERR_TIMEOUT: return "device wait timed out";
+  case ITSU_ERR_CUDA: return "CUDA error";
+  case ITSU_ERR_NOMEM: return "out of memory";
+  case ITSU_ERR_STATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+const char *itsu_last_error(const itsu_context *ctx) { return ctx ? ctx->error.c_str() : g_thread_error.c_str(); }
+
+void itsu_config_default(itsu_config *cfg)
+{
+  if (cfg) {
+    std::memset(cfg, 0, sizeof *cfg);
+  }
+}
+
+itsu_status itsu_context_create(const itsu_config *cfg, itsu_context **out)
+{
+  if (!out) return fail(nullptr, ITSU_ERR_INVALID, "itsu_context_create: null output");
+  *out = nullptr;
+  itsu_config c;
+  itsu_config_default(&c);
+  if (cfg) c = *cfg;
+  int n_dev = 0;
+  cudaError_t err = cudaGetDeviceCount(&n_dev);
+  if (err != cudaSuccess || n_dev == 0) {
+    return fail(nullptr, ITSU_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(err));
+  }
+  if (c.device < 0 || c.device >= n_dev) return fail(nullptr, ITSU_ERR_INVALID, "device %d out of range", c.device);
+  auto *ctx = new itsu_context();
+  ctx->device = c.device;
+  ctx->flags = c.flags;
+  ctx->init_tracklets = c.max_tracklets;
+  ctx->init_cells = c.max_cells;
+  ctx->init_neighbours = c.max_neighbours;
+  ctx->init_roads = c.max_roads;
+  itsu_status st = ITSU_OK;
+  do {
+    if ((err = cudaSetDevice(c.device)) != cudaSuccess) break;
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, c.device);
+    if (major != 10) {
+      st = fail(nullptr, ITSU_ERR_CUDA, "device %d has compute capability %d.x; this build targets sm_100a", c.device, major);
+      break;
+    }
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, c.device);
+    if ((err = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) break;
+    ctx->own_stream = true;
+    if ((err = cudaMalloc((void **)&ctx->d_status, sizeof(DevStatus))) != cudaSuccess) break;
+    if ((err = cudaMallocHost((void **)&ctx->h_status, sizeof(DevStatus))) != cudaSuccess) break;
+    std::memset(ctx->h_status, 0, sizeof(DevStatus));
+    if (c.max_clusters > 0 || c.max_events > 0) {
+      if ((st = ensure_clusters(ctx, c.max_clusters, c.max_events)) != ITSU_OK) break;
+      if ((st = ensure_outputs_for(ctx, c.max_clusters)) != ITSU_OK) break;
+    }
+  } while (false);
+  if (err != cudaSuccess && st == ITSU_OK) {
+    st = fail(nullptr, err == cudaErrorMemoryAllocation ? ITSU_ERR_NOMEM : ITSU_ERR_CUDA, "context setup: %s",
+              cudaGetErrorString(err));
+  }
+  if (st != ITSU_OK) {
+    g_thread_error = ctx->error.empty() ? g_thread_error : ctx->error;
+    itsu_context_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return ITSU_OK;
+}
+
+void itsu_context_destroy(itsu_context *ctx)
+{
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graph(ctx);
+  release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
+  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup);
+  release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
+  release(ctx->road_seg); release(ctx->vtx);
+  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_off); release(ctx->cell_lookup);
+  release(ctx->cells); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
+  release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
+  release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
+  if (ctx->h_status) cudaFreeHost(ctx->h_status);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+itsu_status itsu_context_set_stream(itsu_context *ctx, void *cuda_stream)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->own_stream) {
+    cudaStreamDestroy(ctx->stream);
+    ctx->own_stream = false;
+    ctx->stream = nullptr;
+  }
+  if (cuda_stream) {
+    ctx->stream = (cudaStream_t)cuda_stream;
+  } else {
+    ITSU_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  drop_graph(ctx);
+  return ITSU_OK;
+}
+
+void *itsu_context_stream(const itsu_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+itsu_status itsu_pvc_initialize(itsu_context *ctx, const itsu_cluster *const layers[ITSU_LAYERS], const int32_t counts[ITSU_LAYERS],
+                                const float vertex[3])
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu_status st;
+  if ((st = upload_vertex(ctx, layers, counts, vertex)) != ITSU_OK) return st;
+  const Arena a = arena_of(ctx);
+  itsu::launch_status_init(a, launch_of(ctx));
+  itsu::launch_cluster_sort(a, launch_of(ctx));
+  if ((st = check_launch(ctx)) != ITSU_OK) return st;
+  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  if ((st = check_invalid(ctx)) != ITSU_OK) return st;
+  ctx->stage = kInitialized;
+  return ITSU_OK;
+}
+
+itsu_status itsu_compute_layer_tracklets(itsu_context *ctx)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kInitialized, "itsu_compute_layer_tracklets")) != ITSU_OK) return st;
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((st = ensure_tracklets(ctx, 1)) != ITSU_OK) return st;
+  if ((st = stage_count_then_write(ctx, itsu::launch_tracklets_count, itsu::launch_tracklets_write, itsu::kTracklets,
+                                   ensure_tracklets)) != ITSU_OK) {
+    return st;
+  }
+  ctx->stage = kTracklets;
+  return ITSU_OK;
+}
+
+itsu_status itsu_compute_layer_cells(itsu_context *ctx)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kTracklets, "itsu_compute_layer_cells")) != ITSU_OK) return st;
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((st = ensure_cells(ctx, 1)) != ITSU_OK) return st;
+  if ((st = stage_count_then_write(ctx, itsu::launch_cells_count, itsu::launch_cells_write, itsu::kCells, ensure_cells)) != ITSU_OK) {
+    return st;
+  }
+  ctx->stage = kCells;
+  return ITSU_OK;
+}
+
+itsu_status itsu_find_cells_neighbours(itsu_context *ctx)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kCells, "itsu_find_cells_neighbours")) != ITSU_OK) return st;
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((st = ensure_neighbours(ctx, 1)) != ITSU_OK) return st;
+  if ((st = stage_count_then_write(ctx, itsu::launch_neighbours_count, itsu::launch_neighbours_write, itsu::kNeighbours,
+                                   ensure_neighbours)) != ITSU_OK) {
+    return st;
+  }
+  ctx->stage = kNeighbours;
+  return ITSU_OK;
+}
+
+itsu_status itsu_find_tracks(itsu_context *ctx)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kNeighbours, "itsu_find_tracks")) != ITSU_OK) return st;
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((st = ensure_roads(ctx, 1)) != ITSU_OK) return st;
+  if ((st = stage_count_then_write(ctx, itsu::launch_roads_count, itsu::launch_roads_write, itsu::kRoads, ensure_roads)) != ITSU_OK) {
+    return st;
+  }
+  ctx->stage = kRoads;
+  return ITSU_OK;
+}
+
+itsu_status itsu_compute_montecarlo_labels(itsu_context *ctx)
+{
+  // The road kernel votes the labels of every road it writes (Moore's vote over the road's
+  // clusters), so the labels already exist once the roads do.
+  return require_stage(ctx, kRoads, "itsu_compute_montecarlo_labels");
+}
+
+itsu_status itsu_get_counts(itsu_context *ctx, int32_t event, itsu_counts *out)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kInitialized, "itsu_get_counts")) != ITSU_OK) return st;
+  if (!out) return fail(ctx, ITSU_ERR_INVALID, "null output");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  EventSegments s;
+  if ((st = event_segments(ctx, event, s)) != ITSU_OK) return st;
+  counts_from(ctx, s, out);
+  return ITSU_OK;
+}
+
+itsu_status itsu_copy_results(itsu_context *ctx, int32_t event, const itsu_results *out)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kInitialized, "itsu_copy_results")) != ITSU_OK) return st;
+  if (!out) return fail(ctx, ITSU_ERR_INVALID, "null output");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  EventSegments s;
+  if ((st = event_segments(ctx, event, s)) != ITSU_OK) return st;
+  itsu_counts n;
+  counts_from(ctx, s, &n);
+  for (int l = 0; l < ITSU_LAYERS; ++l) {
+    if ((st = copy_range(ctx, out->clusters[l], ctx->sorted + s.lo[l], n.clusters[l])) != ITSU_OK) return st;
+  }
+  for (int l = 0; l < ITSU_TRACKLET_LAYERS; ++l) {
+    if ((st = copy_range(ctx, out->index_tables[l], ctx->index_tables + ((int64_t)event * ITSU_TRACKLET_LAYERS + l) * ITSU_INDEX_TABLE_SIZE,
+                         ITSU_INDEX_TABLE_SIZE)) != ITSU_OK) {
+      return st;
+    }
+  }
+  if (ctx->stage >= kTracklets) {
+    for (int l = 0; l < ITSU_TRACKLET_LAYERS; ++l) {
+      if ((st = copy_range(ctx, out->tracklets[l], ctx->tracklets + s.ts[l], n.tracklets[l])) != ITSU_OK) return st;
+    }
+    for (int l = 0; l < ITSU_CELL_LAYERS; ++l) {
+      if ((st = copy_range(ctx, out->tracklets_lookup[l], ctx->trk_lookup + s.lo[l + 1], n.clusters[l + 1])) != ITSU_OK) return st;
+    }
+  } else {
+    for (int l = 0; l < ITSU_CELL_LAYERS; ++l) {
+      if (out->tracklets_lookup[l]) std::fill(out->tracklets_lookup[l], out->tracklets_lookup[l] + n.clusters[l + 1], ITSU_UNUSED_INDEX);
+    }
+  }
+  if (ctx->stage >= kCells) {
+    for (int l = 0; l < ITSU_CELL_LAYERS; ++l) {
+      if ((st = copy_range(ctx, out->cells[l], ctx->cells + s.cs[l], n.cells[l])) != ITSU_OK) return st;
+    }
+    for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {
+      if ((st = copy_range(ctx, out->cells_lookup[l], ctx->cell_lookup + s.ts[l + 1], n.tracklets[l + 1])) != ITSU_OK) return st;
+    }
+  }
+  if (ctx->stage >= kNeighbours) {
+    for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {
+      if ((st = copy_range(ctx, out->neighbour_offsets[l], ctx->nb_off + s.cs[l + 1], (int64_t)n.cells[l + 1] + 1)) != ITSU_OK) return st;
+      if ((st = copy_range(ctx, out->neighbours[l], ctx->nb + s.nbo[l + 1], n.neighbours[l])) != ITSU_OK) return st;
+    }
+  }
+  if (ctx->stage >= kRoads) {
+    if ((st = copy_range(ctx, out->roads, ctx->roads + s.rs[0], n.roads)) != ITSU_OK) return st;
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->stage >= kNeighbours) {
+    for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {  // rebase the CSR rows to this layer
+      if (out->neighbour_offsets[l]) {
+        for (int32_t k = 0; k <= n.cells[l + 1]; ++k) out->neighbour_offsets[l][k] -= s.nbo[l + 1];
+      }
+    }
+  }
+  return ITSU_OK;
+}
+
+itsu_status itsu_clusters_to_tracks(itsu_context *ctx, const itsu_cluster *const layers[ITSU_LAYERS],
+                                    const int32_t counts[ITSU_LAYERS], const float vertex[3], itsu_road *roads,
+                                    int32_t roads_capacity, int32_t *roads_count)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu_status st;
+  if ((st = upload_vertex(ctx, layers, counts, vertex)) != ITSU_OK) return st;
+  if ((st = ensure_outputs_for(ctx, ctx->n_clusters)) != ITSU_OK) return st;
+  if ((st = run_all(ctx)) != ITSU_OK) return st;
+  const int64_t total = ctx->h_status->total[itsu::kRoads];
+  if (roads_count) *roads_count = (int32_t)total;
+  if (roads) {
+    if (total > roads_capacity) return fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %d given", (long long)total, roads_capacity);
+    if ((st = copy_range(ctx, roads, (const itsu_road *)ctx->roads, total)) != ITSU_OK) return st;
+    ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return ITSU_OK;
+}
+
+static itsu_status set_batch(itsu_context *ctx, const itsu_batch *batch)
+{
+  if (!batch) return fail(ctx, ITSU_ERR_INVALID, "null batch");
+  if (batch->n_events < 0 || batch->n_clusters < 0 || batch->n_clusters > INT32_MAX) {
+    return fail(ctx, ITSU_ERR_INVALID, "bad batch size (%d events, %lld clusters)", batch->n_events, (long long)batch->n_clusters);
+  }
+  if (batch->n_events > 0 && (!batch->layer_offsets || !batch->vertices || (batch->n_clusters > 0 && !batch->clusters))) {
+    return fail(ctx, ITSU_ERR_INVALID, "null batch pointer");
+  }
+  itsu_status st;
+  if ((st = ensure_clusters(ctx, batch->n_clusters, batch->n_events)) != ITSU_OK) return st;
+  if ((st = ensure_outputs_for(ctx, batch->n_clusters)) != ITSU_OK) return st;
+  ctx->n_events = batch->n_events;
+  ctx->n_clusters = batch->n_clusters;
+  ctx->in_raw = batch->clusters;
+  ctx->in_layer_off = batch->layer_offsets;
+  ctx->in_vtx = batch->vertices;
+  ctx->h_layer_off.resize((size_t)batch->n_events * ITSU_LAYERS + 1);
+  if (batch->n_events > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_layer_off.data(), batch->layer_offsets, sizeof(int32_t) * ctx->h_layer_off.size(),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_layer_off[0] != 0 || ctx->h_layer_off.back() != batch->n_clusters) {
+      return fail(ctx, ITSU_ERR_INVALID, "layer offsets must start at 0 and end at n_clusters");
+    }
+    for (size_t k = 1; k < ctx->h_layer_off.size(); ++k) {
+      if (ctx->h_layer_off[k] < ctx->h_layer_off[k - 1]) return fail(ctx, ITSU_ERR_INVALID, "layer offsets decrease at %zu", k);
+    }
+  }
+  ctx->stage = kNone;
+  return ITSU_OK;
+}
+
+itsu_status itsu_batch_run(itsu_context *ctx, const itsu_batch *batch)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu_status st;
+  if ((st = set_batch(ctx, batch)) != ITSU_OK) return st;
+  return run_all(ctx);
+}
+
+itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu_status st;
+  const bool same = batch && ctx->stage != kNone && batch->clusters == ctx->in_raw && batch->layer_offsets == ctx->in_layer_off &&
+                    batch->vertices == ctx->in_vtx && batch->n_events == ctx->n_events && batch->n_clusters == ctx->n_clusters;
+  if (!same && (st = set_batch(ctx, batch)) != ITSU_OK) return st;
+  if ((st = launch_all(ctx)) != ITSU_OK) return st;
+  ctx->stage = kRoads;
+  return ITSU_OK;
+}
+
+itsu_status itsu_batch_status(itsu_context *ctx)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  itsu_status st;
+  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  if ((st = check_invalid(ctx)) != ITSU_OK) return st;
+  if (ctx->h_status->flags & itsu::kCapacityMask) {
+    ctx->stage = kNone;
+    return fail(ctx, ITSU_ERR_CAPACITY, "a result exceeded the arena; run itsu_batch_run once to size it");
+  }
+  return ITSU_OK;
+}
+
+itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, const int32_t **road_offsets)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kRoads, "itsu_batch_roads_device")) != ITSU_OK) return st;
+  if (roads) *roads = ctx->roads;
+  if (road_offsets) *road_offsets = ctx->road_seg;
+  return ITSU_OK;
+}
+
+itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
+                                const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
+                                int32_t *road_offsets)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  if (n_events < 0 || (n_events > 0 && (!layer_offsets || !vertices))) return fail(ctx, ITSU_ERR_INVALID, "bad batch arguments");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int64_t n_clusters = n_events > 0 ? layer_offsets[(int64_t)n_events * ITSU_LAYERS] : 0;
+  if (n_clusters > 0 && !clusters) return fail(ctx, ITSU_ERR_INVALID, "null clusters");
+  itsu_status st;
+  if ((st = ensure_clusters(ctx, n_clusters, n_events)) != ITSU_OK) return st;
+  if (n_clusters > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw, clusters, sizeof(itsu_cluster) * n_clusters, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->layer_off, layer_offsets, sizeof(int32_t) * ((int64_t)n_events * ITSU_LAYERS + 1),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, vertices, sizeof(float) * 3 * (int64_t)n_events, cudaMemcpyHostToDevice, ctx->stream));
+  itsu_batch b{};
+  b.clusters = ctx->raw;
+  b.layer_offsets = ctx->layer_off;
+  b.vertices = ctx->vtx;
+  b.n_events = n_events;
+  b.n_clusters = n_clusters;
+  if ((st = ensure_outputs_for(ctx, n_clusters)) != ITSU_OK) return st;
+  ctx->n_events = n_events;
+  ctx->n_clusters = n_clusters;
+  ctx->in_raw = b.clusters;
+  ctx->in_layer_off = b.layer_offsets;
+  ctx->in_vtx = b.vertices;
+  ctx->h_layer_off.assign(layer_offsets, layer_offsets + (int64_t)n_events * ITSU_LAYERS + 1);
+  if ((st = run_all(ctx)) != ITSU_OK) return st;
+  const int64_t total = ctx->h_status->total[itsu::kRoads];
+  if (road_offsets) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(road_offsets, ctx->road_seg, sizeof(int32_t) * ((int64_t)n_events + 1), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+  }
+  if (roads) {
+    if (total > roads_capacity) return fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %lld given", (long long)total, (long long)roads_capacity);
+    if ((st = copy_range(ctx, roads, (const itsu_road *)ctx->roads, total)) != ITSU_OK) return st;
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+int32_t itsu_kernels_per_run(void) { return itsu::kernels_per_run(); }
+
+itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_time *times, int32_t capacity, int32_t *count)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kRoads, "itsu_batch_profile")) != ITSU_OK) return st;
+  if (repeats < 1 || !times || capacity < 0) return fail(ctx, ITSU_ERR_INVALID, "bad profile arguments");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  int n = 0;
+  const itsu::KernelStep *steps = itsu::pipeline_steps(&n);
+  std::vector<cudaEvent_t> ev(n + 1, nullptr);
+  std::vector<double> total(n, 0.0);
+  for (auto &e : ev) {
+    ITSU_CUDA(ctx, cudaEventCreate(&e));
+  }
+  const Arena a = arena_of(ctx);
+  const Launch l = launch_of(ctx);
+  cudaError_t err = cudaSuccess;
+  for (int r = 0; r < repeats && err == cudaSuccess; ++r) {
+    cudaEventRecord(ev[0], ctx->stream);
+    for (int k = 0; k < n; ++k) {
+      steps[k].launch(a, l);
+      cudaEventRecord(ev[k + 1], ctx->stream);
+    }
+    err = cudaStreamSynchronize(ctx->stream);
+    for (int k = 0; k < n && err == cudaSuccess; ++k) {
+      float ms = 0.0f;
+      err = cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+      total[k] += ms;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  ITSU_CUDA(ctx, err);
+  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  if (ctx->h_status->flags) return fail(ctx, ITSU_ERR_CAPACITY, "profile run did not complete (flags %d)", ctx->h_status->flags);
+  const int m = std::min(n, (int)capacity);
+  for (int k = 0; k < m; ++k) {
+    std::memset(times[k].name, 0, sizeof times[k].name);
+    std::strncpy(times[k].name, steps[k].name, sizeof times[k].name - 1);
+    times[k].ms = (float)(total[k] / repeats);
+    times[k].launches = repeats;
+  }
+  if (count) *count = n;
+  return ITSU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// itsu_internal.h - device arena layout and kernel launchers shared by the C ABI layer.
+//
+// All results of a run live in flat, event-major device arrays; the single-vertex entry points
+// are a batch of one event. Layout (E events, NC clusters, T tracklets, C cells):
+//   layer_off[E*7+1]   cluster segment (event e, layer L) = [layer_off[7e+L], layer_off[7e+L+1])
+//   sorted/xyzr/phi    clusters of each segment, stably sorted by index-table bin
+//   index_tables       E*6 tables of 401 ints (table of layer L+1 at (6e+L)*401)
+//   trk_count/trk_off  tracklets per inner cluster and their exclusive scan (NC+1)
+//   trk_seg[E*6+1]     tracklet segment (e, L) = [trk_seg[6e+L], trk_seg[6e+L+1])
+//   cell_count/off     cells per first tracklet and their scan (T+1); cell_seg[E*5+1]
+//   nb_count/off       neighbours per next-layer cell and their scan (C+1): CSR over cells
+//   road_count/off     roads per root cell and their scan (C+1); road_seg[E+1]
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "itsu.h"
+
+namespace itsu {
+
+enum : int32_t {
+  kFlagInvalid = 1,
+  kFlagCapTracklets = 2,
+  kFlagCapCells = 4,
+  kFlagCapNeighbours = 8,
+  kFlagCapRoads = 16,
+  kFlagCountOverflow = 32,
+};
+constexpr int32_t kCapacityMask = kFlagCapTracklets | kFlagCapCells | kFlagCapNeighbours | kFlagCapRoads | kFlagCountOverflow;
+
+// Totals and requirements of a run, written by the device.
+struct DevStatus {
+  int32_t flags;
+  int32_t invalid_index;  // first offending flat cluster index, INT32_MAX if none
+  int32_t invalid_event;  // first event with a malformed vertex, INT32_MAX if none
+  int32_t pad_;
+  int64_t total[4];       // tracklets, cells, neighbours, roads
+};
+
+enum TotalIndex { kTracklets = 0, kCells = 1, kNeighbours = 2, kRoads = 3 };
+
+struct Arena {
+  int32_t n_events;
+  int32_t pad_;
+  int64_t n_clusters;
+  // inputs
+  const itsu_cluster *raw;
+  const int32_t *layer_off;
+  const float *vtx;
+  // clustering
+  itsu_cluster *sorted;
+  float4 *xyzr;
+  float *phi;
+  itsu_cluster *tmp;
+  int32_t *index_tables;
+  // tracklets
+  int32_t *trk_count;
+  int32_t *trk_off;
+  int32_t *trk_lookup;
+  int32_t *trk_seg;
+  itsu_tracklet *tracklets;
+  int32_t *trk_seg_id;
+  // cells
+  int32_t *cell_count;
+  int32_t *cell_off;
+  int32_t *cell_lookup;
+  int32_t *cell_seg;
+  itsu_cell *cells;
+  int32_t *cell_seg_id;
+  // neighbours, levels, roads
+  int32_t *nb_count;
+  int32_t *nb_off;
+  int32_t *nb_fill;
+  int32_t *nb;
+  int64_t *paths;
+  int32_t *road_count;
+  int32_t *road_off;
+  int32_t *road_seg;
+  itsu_road *roads;
+  // scan scratch and status
+  int64_t *scan_partials;
+  DevStatus *status;
+  // capacities of the growable outputs
+  int64_t cap_tracklets, cap_cells, cap_neighbours, cap_roads;
+};
+
+// Launch geometry shared by the grid-stride kernels.
+struct Launch {
+  cudaStream_t stream;
+  int num_sms;
+};
+
+// Stage launchers (asynchronous on l.stream).
+void launch_status_init(const Arena &a, const Launch &l);
+void launch_cluster_sort(const Arena &a, const Launch &l);
+void launch_tracklets_count(const Arena &a, const Launch &l);
+void launch_tracklets_write(const Arena &a, const Launch &l);
+void launch_cells_count(const Arena &a, const Launch &l);
+void launch_cells_write(const Arena &a, const Launch &l);
+void launch_neighbours_count(const Arena &a, const Launch &l);
+void launch_neighbours_write(const Arena &a, const Launch &l);
+void launch_roads_count(const Arena &a, const Launch &l);
+void launch_roads_write(const Arena &a, const Launch &l);
+
+// Every kernel of a run, in launch order, with its name (the instrumentation API times them
+// one by one). The stage launchers above enqueue consecutive ranges of this table.
+struct KernelStep {
+  const char *name;
+  void (*launch)(const Arena &, const Launch &);
+};
+const KernelStep *pipeline_steps(int *count);
+int kernels_per_run();
+
+}  // namespace itsu

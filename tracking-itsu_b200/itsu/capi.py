@@ -1,0 +1,273 @@
+"""ctypes binding of the C ABI (include/itsu.h) in lib/libitsu_b200.so.
+
+There is no fallback: if the library is missing or no B200 is visible, the calls raise.
+Results come back in the same canonical dict form as the oracle, so tests compare them field
+by field.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .gen import CLUSTER_DTYPE
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libitsu_b200.so")
+
+TRACKLET_DTYPE = np.dtype([("c1", "<i4"), ("c2", "<i4"), ("tan_lambda", "<f4"), ("phi", "<f4")])
+CELL_DTYPE = np.dtype(
+    [("c1", "<i4"), ("c2", "<i4"), ("c3", "<i4"), ("t1", "<i4"), ("t2", "<i4"), ("nx", "<f4"), ("ny", "<f4"),
+     ("nz", "<f4"), ("curvature", "<f4"), ("level", "<i4")]
+)
+ROAD_DTYPE = np.dtype([("cells", "<i4", (5,)), ("size", "<i4"), ("label", "<i4"), ("fake", "u1"), ("pad", "u1", (3,))])
+
+OK, ERR_INVALID, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NOMEM, ERR_STATE = range(7)
+FLAG_NO_GROW = 1
+
+
+class ItsuError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+STATUS_NAMES = {OK: "ITSU_OK", ERR_INVALID: "ITSU_ERR_INVALID", ERR_CAPACITY: "ITSU_ERR_CAPACITY",
+                ERR_TIMEOUT: "ITSU_ERR_TIMEOUT", ERR_CUDA: "ITSU_ERR_CUDA", ERR_NOMEM: "ITSU_ERR_NOMEM",
+                ERR_STATE: "ITSU_ERR_STATE"}
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("flags", ctypes.c_uint32), ("max_clusters", ctypes.c_int64),
+                ("max_tracklets", ctypes.c_int64), ("max_cells", ctypes.c_int64), ("max_neighbours", ctypes.c_int64),
+                ("max_roads", ctypes.c_int64), ("max_events", ctypes.c_int32), ("reserved_", ctypes.c_int32)]
+
+
+class Counts(ctypes.Structure):
+    _fields_ = [("clusters", ctypes.c_int32 * 7), ("tracklets", ctypes.c_int32 * 6), ("cells", ctypes.c_int32 * 5),
+                ("neighbours", ctypes.c_int32 * 4), ("roads", ctypes.c_int32)]
+
+
+class Results(ctypes.Structure):
+    _fields_ = [("clusters", ctypes.c_void_p * 7), ("index_tables", ctypes.c_void_p * 6), ("tracklets", ctypes.c_void_p * 6),
+                ("tracklets_lookup", ctypes.c_void_p * 5), ("cells", ctypes.c_void_p * 5), ("cells_lookup", ctypes.c_void_p * 4),
+                ("neighbour_offsets", ctypes.c_void_p * 4), ("neighbours", ctypes.c_void_p * 4), ("roads", ctypes.c_void_p)]
+
+
+class KernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 40), ("ms", ctypes.c_float), ("launches", ctypes.c_int32)]
+
+
+class Batch(ctypes.Structure):
+    _fields_ = [("clusters", ctypes.c_void_p), ("layer_offsets", ctypes.c_void_p), ("vertices", ctypes.c_void_p),
+                ("n_events", ctypes.c_int32), ("reserved_", ctypes.c_int32), ("n_clusters", ctypes.c_int64)]
+
+
+_lib = None
+
+# (name, restype, argtypes) of every entry point declared in include/itsu.h
+SIGNATURES = [
+    ("itsu_version", ctypes.c_char_p, []),
+    ("itsu_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("itsu_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("itsu_config_default", None, [ctypes.POINTER(Config)]),
+    ("itsu_context_create", ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]),
+    ("itsu_context_destroy", None, [ctypes.c_void_p]),
+    ("itsu_context_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("itsu_context_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("itsu_pvc_initialize", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("itsu_compute_layer_tracklets", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_compute_layer_cells", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_find_cells_neighbours", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_find_tracks", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_compute_montecarlo_labels", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_get_counts", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Counts)]),
+    ("itsu_copy_results", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Results)]),
+    ("itsu_clusters_to_tracks", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.POINTER(ctypes.c_int32)]),
+    ("itsu_batch_run", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Batch)]),
+    ("itsu_batch_run_host", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+      ctypes.c_void_p]),
+    ("itsu_batch_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Batch)]),
+    ("itsu_batch_status", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_batch_roads_device", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]),
+    ("itsu_kernels_per_run", ctypes.c_int32, []),
+    ("itsu_batch_profile", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+]
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise ImportError("libitsu_b200.so not found at %s: run `make -C tracking-itsu_b200`" % path)
+        L = ctypes.CDLL(path)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+class Context:
+    """One itsu_context: a device arena and stream."""
+
+    def __init__(self, device: int = 0, flags: int = 0, **caps):
+        self.lib = load()
+        cfg = Config()
+        self.lib.itsu_config_default(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.flags = flags
+        for k, v in caps.items():
+            setattr(cfg, k, v)
+        h = ctypes.c_void_p()
+        st = self.lib.itsu_context_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != OK:
+            raise ItsuError(st, self.lib.itsu_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.itsu_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != OK:
+            raise ItsuError(st, self.lib.itsu_last_error(self.h).decode())
+
+    def set_stream(self, stream_handle: int):
+        self._check(self.lib.itsu_context_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.itsu_context_stream(self.h) or 0
+
+    # ---- per vertex ----
+    @staticmethod
+    def _layer_args(layers, vertex):
+        layers = [np.ascontiguousarray(l, dtype=CLUSTER_DTYPE) for l in layers]
+        ptrs = (ctypes.c_void_p * 7)(*[l.ctypes.data if len(l) else None for l in layers])
+        counts = (ctypes.c_int32 * 7)(*[len(l) for l in layers])
+        v = (ctypes.c_float * 3)(*[float(x) for x in vertex])
+        return layers, ptrs, counts, v
+
+    def initialize(self, layers, vertex):
+        keep, ptrs, counts, v = self._layer_args(layers, vertex)
+        self._check(self.lib.itsu_pvc_initialize(self.h, ptrs, counts, v))
+
+    def run_stages(self, layers, vertex):
+        """PrimaryVertexContext::initialize then every Tracker stage, one call per stage."""
+        self.initialize(layers, vertex)
+        for fn in (self.lib.itsu_compute_layer_tracklets, self.lib.itsu_compute_layer_cells,
+                   self.lib.itsu_find_cells_neighbours, self.lib.itsu_find_tracks, self.lib.itsu_compute_montecarlo_labels):
+            self._check(fn(self.h))
+
+    def counts(self, event: int = 0) -> Counts:
+        c = Counts()
+        self._check(self.lib.itsu_get_counts(self.h, event, ctypes.byref(c)))
+        return c
+
+    def results(self, event: int = 0) -> dict:
+        """Host copies of every output of one event, in the oracle's canonical form."""
+        c = self.counts(event)
+        res = dict(
+            clusters=[np.zeros(c.clusters[l], CLUSTER_DTYPE) for l in range(7)],
+            index_tables=np.zeros((6, 401), np.int32),
+            tracklets=[np.zeros(c.tracklets[l], TRACKLET_DTYPE) for l in range(6)],
+            trk_lookup=[np.zeros(c.clusters[l + 1], np.int32) for l in range(5)],
+            cells=[np.zeros(c.cells[l], CELL_DTYPE) for l in range(5)],
+            cell_lookup=[np.zeros(c.tracklets[l + 1], np.int32) for l in range(4)],
+            nb_offsets=[np.zeros(c.cells[l + 1] + 1, np.int32) for l in range(4)],
+            nb=[np.zeros(c.neighbours[l], np.int32) for l in range(4)],
+            roads=np.zeros(c.roads, ROAD_DTYPE),
+        )
+        r = Results()
+        for l in range(7):
+            r.clusters[l] = res["clusters"][l].ctypes.data if c.clusters[l] else None
+        for l in range(6):
+            r.index_tables[l] = res["index_tables"][l].ctypes.data
+            r.tracklets[l] = res["tracklets"][l].ctypes.data if c.tracklets[l] else None
+        for l in range(5):
+            r.tracklets_lookup[l] = res["trk_lookup"][l].ctypes.data if len(res["trk_lookup"][l]) else None
+            r.cells[l] = res["cells"][l].ctypes.data if c.cells[l] else None
+        for l in range(4):
+            r.cells_lookup[l] = res["cell_lookup"][l].ctypes.data if len(res["cell_lookup"][l]) else None
+            r.neighbour_offsets[l] = res["nb_offsets"][l].ctypes.data
+            r.neighbours[l] = res["nb"][l].ctypes.data if c.neighbours[l] else None
+        r.roads = res["roads"].ctypes.data if c.roads else None
+        self._check(self.lib.itsu_copy_results(self.h, event, ctypes.byref(r)))
+        res["roads"]["pad"] = 0
+        return res
+
+    def run_vertex(self, layers, vertex) -> dict:
+        self.run_stages(layers, vertex)
+        return self.results(0)
+
+    def clusters_to_tracks(self, layers, vertex) -> np.ndarray:
+        """Whole path for one vertex in one call; returns its roads."""
+        keep, ptrs, counts, v = self._layer_args(layers, vertex)
+        n = ctypes.c_int32()
+        self._check(self.lib.itsu_clusters_to_tracks(self.h, ptrs, counts, v, None, 0, ctypes.byref(n)))
+        roads = np.zeros(n.value, ROAD_DTYPE)
+        self._check(self.lib.itsu_clusters_to_tracks(self.h, ptrs, counts, v, _ptr(roads), n.value, ctypes.byref(n)))
+        roads["pad"] = 0
+        return roads
+
+    # ---- batches ----
+    def batch_run_host(self, clusters, layer_offsets, vertices, roads_capacity=None):
+        """Host in / host out over a batch; returns (roads, road_offsets)."""
+        clusters = np.ascontiguousarray(clusters, CLUSTER_DTYPE)
+        layer_offsets = np.ascontiguousarray(layer_offsets, np.int32)
+        vertices = np.ascontiguousarray(vertices, np.float32)
+        n_events = (len(layer_offsets) - 1) // 7
+        offs = np.zeros(n_events + 1, np.int32)
+        if roads_capacity is None:
+            self._check(self.lib.itsu_batch_run_host(self.h, _ptr(clusters), _ptr(layer_offsets), _ptr(vertices), n_events,
+                                                     None, 0, _ptr(offs)))
+            roads_capacity = int(offs[-1])
+        roads = np.zeros(roads_capacity, ROAD_DTYPE)
+        self._check(self.lib.itsu_batch_run_host(self.h, _ptr(clusters), _ptr(layer_offsets), _ptr(vertices), n_events,
+                                                 _ptr(roads), roads_capacity, _ptr(offs)))
+        roads = roads[: offs[-1]].copy()
+        roads["pad"] = 0
+        return roads, offs
+
+    def batch_device(self, clusters_ptr, layer_offsets_ptr, vertices_ptr, n_events, n_clusters) -> Batch:
+        b = Batch()
+        b.clusters, b.layer_offsets, b.vertices = clusters_ptr, layer_offsets_ptr, vertices_ptr
+        b.n_events, b.n_clusters = n_events, n_clusters
+        return b
+
+    def batch_run(self, batch: Batch):
+        self._check(self.lib.itsu_batch_run(self.h, ctypes.byref(batch)))
+
+    def batch_launch(self, batch: Batch):
+        self._check(self.lib.itsu_batch_launch(self.h, ctypes.byref(batch)))
+
+    def batch_status(self):
+        self._check(self.lib.itsu_batch_status(self.h))
+
+    def profile(self, repeats: int = 5) -> list:
+        """(kernel name, mean ms) for every kernel of the last batch, timed one by one."""
+        n = self.lib.itsu_kernels_per_run()
+        arr = (KernelTime * n)()
+        cnt = ctypes.c_int32()
+        self._check(self.lib.itsu_batch_profile(self.h, repeats, arr, n, ctypes.byref(cnt)))
+        return [(arr[k].name.decode(), float(arr[k].ms)) for k in range(cnt.value)]

@@ -232,3 +232,23 @@ def pack_batch(events, vertex_index=None):
     clusters = np.concatenate([l for ev in events for l in ev.layers]) if counts else np.zeros(0, CLUSTER_DTYPE)
     vertices = np.stack([ev.vertices[vi] for ev, vi in zip(events, vertex_index)]).astype(np.float32)
     return clusters, offsets, vertices.reshape(-1)
+
+
+def write_binary_events(events, path: str) -> None:
+    """Binary event file "ITSUEVT1" read by the reference harness (oracle/ref_harness.cpp):
+    int32 n_events; per event int32 n_vertices, float32 xyz per vertex, int32 counts[7], then per
+    cluster float32 x, y, z, alpha and int32 mc, layer by layer (cluster ids are implied by order,
+    as in the reference's text loader)."""
+    rec = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("alpha", "<f4"), ("mc", "<i4")])
+    with open(path, "wb") as f:
+        f.write(b"ITSUEVT1")
+        f.write(np.array([len(events)], np.int32).tobytes())
+        for ev in events:
+            f.write(np.array([len(ev.vertices)], np.int32).tobytes())
+            f.write(np.ascontiguousarray(ev.vertices, np.float32).tobytes())
+            f.write(np.array([len(l) for l in ev.layers], np.int32).tobytes())
+            for l in ev.layers:
+                r = np.zeros(len(l), rec)
+                for k in ("x", "y", "z", "alpha", "mc"):
+                    r[k] = l[k]
+                f.write(r.tobytes())
