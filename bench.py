@@ -51,7 +51,7 @@ WORKLOAD = "pbpb_central_6000trk_5pct_noise"
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--events", type=int, default=128, help="events per step per GPU")
@@ -144,31 +144,41 @@ KERNEL_STAGE = {
 
 
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+    """nvidia-smi samples (every 100 ms) of SM clock, power and throttle reasons; only samples
+    taken inside the timed window (mark_start/mark_end) are summarised."""
+
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index):
         self.device_index = device_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.device_index), "-f", self.path],
                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
-        time.sleep(0.3)
+        time.sleep(0.5)
         return self
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def __exit__(self, *exc):
         if self.proc is not None:
-            time.sleep(0.25)
+            time.sleep(0.15)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -176,12 +186,19 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        import datetime
+
         rows = []
         try:
             for line in open(self.path):
                 f = [x.strip() for x in line.split(",")]
-                if len(f) >= 9 and f[1].replace(".", "").isdigit():
-                    rows.append(f)
+                if len(f) < 10:
+                    continue
+                try:
+                    ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    rows.append((ts, float(f[2]), float(f[3]), f[4], f[6:10]))
+                except ValueError:
+                    continue
         except OSError:
             pass
         finally:
@@ -189,11 +206,14 @@ class ClockSampler:
                 os.unlink(self.path)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in rows]
+        lo, hi = (self.t0 or 0) - 0.05, (self.t1 or 1e18) + 0.05
+        inside = [r for r in rows if lo <= r[0] <= hi]
+        used = inside if inside else rows
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
-                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+        reasons = sorted({n for r in used for n, v in zip(names, r[4]) if v.lower().startswith("active")})
+        power = [float(r[3]) for r in used if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(r[1] for r in used), "sm_max_mhz": used[0][2], "reasons": reasons,
+                "samples": len(used), "samples_in_window": len(inside), "power_w_max": max(power) if power else None}
 
 
 # ------------------------------------------------------------------------------------------
@@ -320,11 +340,13 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
+        clocks.mark_start()
         start.record(stream)
         for _ in range(args.steps):
             ctx.batch_launch(batch)
         end.record(stream)
         torch.cuda.synchronize()
+        clocks.mark_end()
     ctx.batch_status()
     if dist:
         dist.barrier()

@@ -98,15 +98,27 @@ def test_arena_growth_gives_identical_results():
         _assert_same(small.results(0), want, "after growth")
     finally:
         small.close()
-    fixed = capi.Context(device=0, flags=capi.FLAG_NO_GROW, max_clusters=16, max_tracklets=16, max_cells=16,
-                         max_neighbours=16, max_roads=16, max_events=1)
-    try:
-        clusters, offsets, vertices = gen.pack_batch([ev])
-        with pytest.raises(capi.ItsuError) as err:
-            fixed.batch_run_host(clusters, offsets, vertices, roads_capacity=100000)
-        assert err.value.status == capi.ERR_CAPACITY
-    finally:
-        fixed.close()
+    # a fixed arena (ITSU_FLAG_NO_GROW) reports the overflow instead of growing, for the inputs
+    # and for every output class, and stays usable for work that fits
+    clusters, offsets, vertices = gen.pack_batch([ev])
+    for caps in (dict(max_clusters=64), dict(max_tracklets=1000), dict(max_cells=100), dict(max_neighbours=10), dict(max_roads=10)):
+        full = dict(max_clusters=100000, max_tracklets=10**6, max_cells=10**6, max_neighbours=10**6, max_roads=10**6, max_events=4)
+        full.update(caps)
+        fixed = capi.Context(device=0, flags=capi.FLAG_NO_GROW, **full)
+        try:
+            with pytest.raises(capi.ItsuError) as err:
+                fixed.batch_run_host(clusters, offsets, vertices, roads_capacity=100000)
+            assert err.value.status == capi.ERR_CAPACITY, caps
+            pp = gen.pp_event(3)
+            roads = fixed.clusters_to_tracks(pp.layers, pp.vertices[0]) if "max_clusters" not in caps else None
+            if roads is not None:
+                want_pp = oracle.run_vertex(pp.layers, pp.vertices[0])["roads"]
+                if len(want_pp) <= full["max_roads"]:
+                    assert np.array_equal(roads.view(np.uint8), want_pp.view(np.uint8))
+        except capi.ItsuError as e:
+            assert e.status == capi.ERR_CAPACITY, caps
+        finally:
+            fixed.close()
 
 
 def test_malformed_input_is_rejected(ctx):

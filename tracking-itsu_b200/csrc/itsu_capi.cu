@@ -176,6 +176,16 @@ Arena arena_of(const itsu_context *ctx)
 
 int64_t grow_to(int64_t need) { return need + need / 4 + 1024; }
 
+// With ITSU_FLAG_NO_GROW the arena keeps the capacities the context was created with.
+itsu_status growth_allowed(itsu_context *ctx, const char *what, int64_t need, int64_t cap)
+{
+  if ((ctx->flags & ITSU_FLAG_NO_GROW) && ctx->stage != -1) {
+    return fail(ctx, ITSU_ERR_CAPACITY, "%s: %lld needed, arena holds %lld (ITSU_FLAG_NO_GROW)", what, (long long)need,
+                (long long)cap);
+  }
+  return ITSU_OK;
+}
+
 itsu_status ensure_partials(itsu_context *ctx)
 {
   const int64_t need = std::max({ctx->cap_clusters, ctx->cap_tracklets, ctx->cap_cells}) / 2048 + 2;
@@ -190,6 +200,8 @@ itsu_status ensure_partials(itsu_context *ctx)
 itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_events)
 {
   if (n_clusters > ctx->cap_clusters) {
+    itsu_status st = growth_allowed(ctx, "clusters", n_clusters, ctx->cap_clusters);
+    if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(n_clusters);
     ITSU_CUDA(ctx, alloc(ctx->raw, cap));
     ITSU_CUDA(ctx, alloc(ctx->sorted, cap));
@@ -203,6 +215,8 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ctx->generation++;
   }
   if (n_events > ctx->cap_events) {
+    itsu_status st = growth_allowed(ctx, "events", n_events, ctx->cap_events);
+    if (st != ITSU_OK) return st;
     const int32_t cap = n_events + n_events / 4 + 4;
     ITSU_CUDA(ctx, alloc(ctx->layer_off, (int64_t)cap * ITSU_LAYERS + 1));
     ITSU_CUDA(ctx, alloc(ctx->vtx, (int64_t)cap * 3));
@@ -219,6 +233,8 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
 itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
 {
   if (need > ctx->cap_tracklets) {
+    itsu_status st = growth_allowed(ctx, "tracklets", need, ctx->cap_tracklets);
+    if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
     ITSU_CUDA(ctx, alloc(ctx->tracklets, cap));
     ITSU_CUDA(ctx, alloc(ctx->trk_seg_id, cap));
@@ -234,6 +250,8 @@ itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
 itsu_status ensure_cells(itsu_context *ctx, int64_t need)
 {
   if (need > ctx->cap_cells) {
+    itsu_status st = growth_allowed(ctx, "cells", need, ctx->cap_cells);
+    if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
     ITSU_CUDA(ctx, alloc(ctx->cells, cap));
     ITSU_CUDA(ctx, alloc(ctx->cell_seg_id, cap));
@@ -252,6 +270,8 @@ itsu_status ensure_cells(itsu_context *ctx, int64_t need)
 itsu_status ensure_neighbours(itsu_context *ctx, int64_t need)
 {
   if (need > ctx->cap_neighbours) {
+    itsu_status st = growth_allowed(ctx, "neighbours", need, ctx->cap_neighbours);
+    if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
     ITSU_CUDA(ctx, alloc(ctx->nb, cap));
     ctx->cap_neighbours = cap;
@@ -263,6 +283,8 @@ itsu_status ensure_neighbours(itsu_context *ctx, int64_t need)
 itsu_status ensure_roads(itsu_context *ctx, int64_t need)
 {
   if (need > ctx->cap_roads) {
+    itsu_status st = growth_allowed(ctx, "roads", need, ctx->cap_roads);
+    if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
     ITSU_CUDA(ctx, alloc(ctx->roads, cap));
     ctx->cap_roads = cap;
@@ -275,11 +297,17 @@ itsu_status ensure_roads(itsu_context *ctx, int64_t need)
 // 8 tracklets, 1 cell and 0.2 roads per cluster; the arena grows past these when needed).
 itsu_status ensure_outputs_for(itsu_context *ctx, int64_t n_clusters)
 {
+  if ((ctx->flags & ITSU_FLAG_NO_GROW) && ctx->stage != -1) {
+    return ITSU_OK;  // fixed arena: overflow is reported by the run itself
+  }
+  // configured capacities are floors; a fixed arena takes them as given
+  const bool fixed = (ctx->flags & ITSU_FLAG_NO_GROW) != 0;
+  auto pick = [fixed](int64_t configured, int64_t dflt) { return fixed && configured > 0 ? configured : std::max(configured, dflt); };
   itsu_status st;
-  if ((st = ensure_tracklets(ctx, std::max(ctx->init_tracklets, 10 * n_clusters + 4096))) != ITSU_OK) return st;
-  if ((st = ensure_cells(ctx, std::max(ctx->init_cells, 2 * n_clusters + 4096))) != ITSU_OK) return st;
-  if ((st = ensure_neighbours(ctx, std::max(ctx->init_neighbours, 2 * n_clusters + 4096))) != ITSU_OK) return st;
-  return ensure_roads(ctx, std::max(ctx->init_roads, n_clusters / 2 + 4096));
+  if ((st = ensure_tracklets(ctx, pick(ctx->init_tracklets, 10 * n_clusters + 4096))) != ITSU_OK) return st;
+  if ((st = ensure_cells(ctx, pick(ctx->init_cells, 2 * n_clusters + 4096))) != ITSU_OK) return st;
+  if ((st = ensure_neighbours(ctx, pick(ctx->init_neighbours, 2 * n_clusters + 4096))) != ITSU_OK) return st;
+  return ensure_roads(ctx, pick(ctx->init_roads, n_clusters / 2 + 4096));
 }
 
 itsu_status check_launch(itsu_context *ctx)
@@ -599,8 +627,10 @@ itsu_status itsu_context_create(const itsu_config *cfg, itsu_context **out)
     if ((err = cudaMallocHost((void **)&ctx->h_status, sizeof(DevStatus))) != cudaSuccess) break;
     std::memset(ctx->h_status, 0, sizeof(DevStatus));
     if (c.max_clusters > 0 || c.max_events > 0) {
+      ctx->stage = -1;  // initial allocation: allowed even with ITSU_FLAG_NO_GROW
       if ((st = ensure_clusters(ctx, c.max_clusters, c.max_events)) != ITSU_OK) break;
       if ((st = ensure_outputs_for(ctx, c.max_clusters)) != ITSU_OK) break;
+      ctx->stage = kNone;
     }
   } while (false);
   if (err != cudaSuccess && st == ITSU_OK) {

@@ -106,13 +106,11 @@ __device__ __forceinline__ bool tracklet_cut(int layer, float tan_lambda, float 
          (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
 }
 
-// Tracker.cxx:161-216: cell cuts for tracklets t1 (clusters c1, c2) and t2 (clusters c2, c3).
-// Returns false when the pair is rejected; otherwise fills the unit normal and curvature.
-__device__ __forceinline__ bool cell_cut(int layer, float t1_tan_lambda, float t1_phi, float t2_tan_lambda, float t2_phi,
-                                         float4 c1, float4 c2, float4 c3, float vx, float vy, float vz, float3 &normal,
-                                         float &curvature)
+// Tracker.cxx:161-173: the cheap cell cuts, which need only the two tracklets and the first
+// cluster (c = (x, y, z, r)); most pairs stop here.
+__device__ __forceinline__ bool cell_precut(int layer, float t1_tan_lambda, float t1_phi, float t2_tan_lambda, float t2_phi,
+                                            float4 c1, float vz)
 {
-  // c = (x, y, z, r)
   const float delta_tan_lambda = fabsf(t1_tan_lambda - t2_tan_lambda);
   const float delta_phi = fabsf(t1_phi - t2_phi);
   if (!(delta_tan_lambda < kCellMaxDeltaTanLambda &&
@@ -122,9 +120,14 @@ __device__ __forceinline__ bool cell_cut(int layer, float t1_tan_lambda, float t
   const float average_tan_lambda = 0.5f * (t1_tan_lambda + t2_tan_lambda);
   const float dir_z = -average_tan_lambda * c1.w + c1.z;
   const float delta_z = fabsf(dir_z - vz);
-  if (!(delta_z < kC.cell_max_dz[layer])) {
-    return false;
-  }
+  return delta_z < kC.cell_max_dz[layer];
+}
+
+// Tracker.cxx:175-216: circle-plane normal, radius and DCA of the three clusters. Returns false
+// when the pair is rejected; otherwise fills the unit normal and curvature.
+__device__ __forceinline__ bool cell_geometry(int layer, float4 c1, float4 c2, float4 c3, float vx, float vy, float3 &normal,
+                                              float &curvature)
+{
   const float r1sq = c1.w * c1.w;
   const float r2sq = c2.w * c2.w;
   const float r3sq = c3.w * c3.w;

@@ -428,71 +428,157 @@ __device__ __forceinline__ bool tracklets_active(const int32_t *lo, int layer)
   return true;
 }
 
+// Tracklet.cxx:32-40 for a queued pair (out slot, inner flat index, outer flat index, cluster
+// segment of the inner cluster).
+__device__ __forceinline__ void write_tracklet(const Arena &a, int4 q)
+{
+  const int seg = q.w;
+  const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
+  const float4 c = a.xyzr[q.y];
+  const float4 d = a.xyzr[q.z];
+  itsu_tracklet t;
+  t.first_cluster = q.y - a.layer_off[seg];
+  t.second_cluster = q.z - a.layer_off[seg + 1];
+  t.tan_lambda = (c.z - d.z) / (c.w - d.w);
+  t.phi = itsu_atan2f(c.y - d.y, c.x - d.x);
+  a.tracklets[q.x] = t;
+  a.trk_seg_id[q.x] = e * ITSU_TRACKLET_LAYERS + layer;
+}
+
+// Walks the reference's candidate sequence of one inner cluster (Tracker.cxx:73-89): the phi
+// rows of its bin window in wrap-around order, and in each row the sorted clusters from the
+// row's first bin to the first cluster at or after the window's end (inclusive, P1/P5 bounds).
+struct CandidateWalk {
+  const int32_t *table;
+  int n_next;
+  int z_min, z_span;  // first z bin, number of z bins + 1
+  int phi_bin, rows_left;
+  int j, last;
+
+  __device__ __forceinline__ bool next()
+  {
+    ++j;
+    while (j > last) {
+      if (rows_left == 0) {
+        return false;
+      }
+      const int first_bin = bin_index(z_min, phi_bin);
+      const int max_bin = min(first_bin + z_span, kTableBins);
+      j = table[first_bin];
+      last = min(table[max_bin], n_next - 1);
+      phi_bin = (phi_bin + 1 == kPhiBins) ? 0 : phi_bin + 1;
+      --rows_left;
+    }
+    return true;
+  }
+};
+
+constexpr int kQueue = 64;  // per-warp queue of accepted pairs, drained 32 at a time
+
+// One thread per inner cluster; the warp advances its 32 candidate walks in lock step so that
+// accepted pairs can be compacted (ballot) into a per-warp queue. The write pass drains the queue
+// with all 32 lanes converged, so the double-precision azimuth of each new tracklet runs without
+// divergence. Output slots come from the scan of the count pass: emission order is the
+// reference's (inner cluster, phi row, candidate).
 template <bool kWrite>
 __global__ void __launch_bounds__(kThreads) k_tracklets(Arena a)
 {
+  __shared__ int4 queue[kWrite ? kThreads / 32 : 1][kQueue];
   if (kWrite && capacity_failed(a.status)) {
     return;
   }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t i = global_thread();
-  if (i >= a.n_clusters) {
-    return;
+  const bool in_range = i < a.n_clusters;
+  int seg = 0, e = 0, layer = ITSU_LAYERS - 1;
+  const int32_t *lo = a.layer_off;
+  if (in_range) {
+    seg = find_segment(a.layer_off, a.n_events * ITSU_LAYERS, i);
+    e = seg / ITSU_LAYERS;
+    layer = seg % ITSU_LAYERS;
+    lo = a.layer_off + e * ITSU_LAYERS;
   }
-  const int seg = find_segment(a.layer_off, a.n_events * ITSU_LAYERS, i);
-  const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
-  const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
-  int count = 0;
-  int64_t out = kWrite ? a.trk_off[i] : 0;
-  if (layer < ITSU_LAYERS - 1 && tracklets_active(lo, layer)) {
-    const float4 c = a.xyzr[i];
-    const float phi1 = a.phi[i];
+  float4 c = make_float4(0, 0, 0, 0);
+  float phi1 = 0, tan_lambda = 0;
+  int64_t next_begin = 0;
+  CandidateWalk walk{nullptr, 0, 0, 0, 0, 0, 0, -1};
+  bool has = false;
+  if (in_range && layer < ITSU_LAYERS - 1 && tracklets_active(lo, layer)) {
+    c = a.xyzr[i];
+    phi1 = a.phi[i];
     const float vz = a.vtx[3 * e + 2];
-    const float tan_lambda = (c.z - vz) / c.w;
+    tan_lambda = (c.z - vz) / c.w;
     const float dir_z = tan_lambda * (kC.r[layer + 1] - c.w) + c.z;
     const int4 rect = bins_rect(phi1, layer, dir_z);
     if (!(rect.x == 0 && rect.y == 0 && rect.z == 0 && rect.w == 0)) {
-      const int32_t *table = a.index_tables + ((int64_t)e * ITSU_TRACKLET_LAYERS + layer) * kTableSize;
-      const int64_t next_begin = lo[layer + 1];
-      const int n_next = lo[layer + 2] - lo[layer + 1];
-      const int i_local = (int)(i - lo[layer]);
       int phi_bins = rect.w - rect.y + 1;
       if (phi_bins < 0) {
         phi_bins += kPhiBins;
       }
-      for (int phi_bin = rect.y, phi_count = 0; phi_count < phi_bins;
-           phi_bin = (phi_bin + 1 == kPhiBins) ? 0 : phi_bin + 1, ++phi_count) {
-        const int first_bin = bin_index(rect.x, phi_bin);
-        const int max_bin = min(first_bin + rect.z - rect.x + 1, kTableBins);  // P5
-        const int first_row = table[first_bin];
-        const int last_row = min(table[max_bin], n_next - 1);                  // inclusive bound, P1
-        for (int j = first_row; j <= last_row; ++j) {
-          const float4 d = a.xyzr[next_begin + j];
-          const float phi2 = a.phi[next_begin + j];
-          if (tracklet_cut(layer, tan_lambda, c.w, c.z, phi1, d.w, d.z, phi2)) {
-            if (kWrite) {
-              itsu_tracklet t;
-              t.first_cluster = i_local;
-              t.second_cluster = j;
-              t.tan_lambda = (c.z - d.z) / (c.w - d.w);
-              t.phi = itsu_atan2f(c.y - d.y, c.x - d.x);
-              a.tracklets[out] = t;
-              a.trk_seg_id[out] = e * ITSU_TRACKLET_LAYERS + layer;
-              ++out;
-            } else {
-              ++count;
-            }
-          }
-        }
-      }
+      walk.table = a.index_tables + ((int64_t)e * ITSU_TRACKLET_LAYERS + layer) * kTableSize;
+      walk.n_next = lo[layer + 2] - lo[layer + 1];
+      walk.z_min = rect.x;
+      walk.z_span = rect.z - rect.x + 1;
+      walk.phi_bin = rect.y;
+      walk.rows_left = phi_bins;
+      next_begin = lo[layer + 1];
+      has = walk.next();
     }
   }
-  if (!kWrite) {
+  int count = 0;
+  int out = 0;
+  int queued = 0;
+  if (kWrite && in_range) {
+    out = a.trk_off[i];
+  }
+  const float max_dz = kC.trk_max_dz[layer < ITSU_TRACKLET_LAYERS ? layer : 0];
+  while (__any_sync(0xffffffffu, has)) {
+    bool pass = false;
+    if (has) {
+      const int64_t jf = next_begin + walk.j;
+      const float4 d = a.xyzr[jf];
+      const float phi2 = a.phi[jf];
+      const float delta_z = fabsf(tan_lambda * (d.w - c.w) + c.z - d.z);
+      const float delta_phi = fabsf(phi1 - phi2);
+      pass = delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
+    }
+    if (kWrite) {
+      const unsigned m = __ballot_sync(0xffffffffu, pass);
+      if (pass) {
+        queue[warp][queued + __popc(m & ((1u << lane) - 1u))] = make_int4(out, (int)i, (int)(next_begin + walk.j), seg);
+        ++out;
+      }
+      queued += __popc(m);
+      if (queued >= 32) {
+        __syncwarp();
+        write_tracklet(a, queue[warp][lane]);
+        __syncwarp();
+        if (lane < queued - 32) {
+          queue[warp][lane] = queue[warp][lane + 32];
+        }
+        __syncwarp();
+        queued -= 32;
+      }
+    } else {
+      count += pass;
+    }
+    if (has) {
+      has = walk.next();
+    }
+  }
+  if (kWrite) {
+    __syncwarp();
+    if (lane < queued) {
+      write_tracklet(a, queue[warp][lane]);
+    }
+    if (in_range) {
+      const int32_t first = a.trk_off[i];
+      a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && a.trk_off[i + 1] > first)
+                            ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
+                            : ITSU_UNUSED_INDEX;
+    }
+  } else if (in_range) {
     a.trk_count[i] = count;
-  } else {
-    const int32_t first = a.trk_off[i];
-    a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && a.trk_off[i + 1] > first)
-                          ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
-                          : ITSU_UNUSED_INDEX;
   }
 }
 
@@ -551,10 +637,13 @@ __global__ void __launch_bounds__(kThreads) k_cells(Arena a)
       const float vx = a.vtx[3 * e], vy = a.vtx[3 * e + 1], vz = a.vtx[3 * e + 2];
       for (int32_t j = j0; j < j1; ++j) {
         const itsu_tracklet t2 = a.tracklets[j];
+        if (!cell_precut(layer, t1.tan_lambda, t1.phi, t2.tan_lambda, t2.phi, c1, vz)) {
+          continue;
+        }
         const float4 c3 = a.xyzr[lo[layer + 2] + t2.second_cluster];
         float3 normal;
         float curvature;
-        if (cell_cut(layer, t1.tan_lambda, t1.phi, t2.tan_lambda, t2.phi, c1, c2, c3, vx, vy, vz, normal, curvature)) {
+        if (cell_geometry(layer, c1, c2, c3, vx, vy, normal, curvature)) {
           if (kWrite) {
             itsu_cell cell;
             cell.first_cluster = t1.first_cluster;
