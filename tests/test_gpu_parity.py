@@ -144,3 +144,34 @@ def test_stage_order_is_enforced():
         assert err.value.status == capi.ERR_STATE
     finally:
         fresh.close()
+
+
+def test_results_after_each_stage(ctx):
+    """The PrimaryVertexContext getters after each stage hold that stage's results and empty
+    later ones, like the reference between its Tracker stages (Tracker.cxx:253-259)."""
+    ev = gen.pp_event(9)
+    want = oracle.run_vertex(ev.layers, ev.vertices[0])
+    stages = [ctx.lib.itsu_compute_layer_tracklets, ctx.lib.itsu_compute_layer_cells, ctx.lib.itsu_find_cells_neighbours,
+              ctx.lib.itsu_find_tracks]
+    fresh = capi.Context(device=0)
+    try:
+        fresh.initialize(ev.layers, ev.vertices[0])
+        got = fresh.results(0)
+        for l in range(7):
+            assert np.array_equal(got["clusters"][l].view(np.uint8), want["clusters"][l].view(np.uint8))
+        assert np.array_equal(got["index_tables"], want["index_tables"])
+        assert all(len(t) == 0 for t in got["tracklets"]) and len(got["roads"]) == 0
+        assert all((lk == -1).all() for lk in got["trk_lookup"])
+        for k, stage in enumerate(stages):
+            fresh._check(stage(fresh.h))
+            got = fresh.results(0)
+            if k == 0:
+                for l in range(6):
+                    assert np.array_equal(got["tracklets"][l].view(np.uint8), want["tracklets"][l].view(np.uint8))
+                assert all(len(c) == 0 for c in got["cells"])
+            if k == 1:
+                for l in range(4):
+                    assert np.array_equal(got["cell_lookup"][l], want["cell_lookup"][l])
+        _assert_same(got, want, "all stages")
+    finally:
+        fresh.close()

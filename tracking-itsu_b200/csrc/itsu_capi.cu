@@ -536,15 +536,25 @@ struct EventSegments {
 itsu_status event_segments(itsu_context *ctx, int32_t e, EventSegments &seg)
 {
   if (e < 0 || e >= ctx->n_events) return fail(ctx, ITSU_ERR_INVALID, "event %d out of range", e);
+  // Only the segments of stages that have run exist: the others read as empty.
+  std::memset(&seg, 0, sizeof seg);
   std::memcpy(seg.lo, ctx->h_layer_off.data() + (int64_t)e * ITSU_LAYERS, sizeof seg.lo);
-  ITSU_CUDA(ctx, cudaMemcpyAsync(seg.ts, ctx->trk_seg + (int64_t)e * ITSU_TRACKLET_LAYERS, sizeof seg.ts, cudaMemcpyDeviceToHost, ctx->stream));
-  ITSU_CUDA(ctx, cudaMemcpyAsync(seg.cs, ctx->cell_seg + (int64_t)e * ITSU_CELL_LAYERS, sizeof seg.cs, cudaMemcpyDeviceToHost, ctx->stream));
-  ITSU_CUDA(ctx, cudaMemcpyAsync(seg.rs, ctx->road_seg + e, sizeof seg.rs, cudaMemcpyDeviceToHost, ctx->stream));
-  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (int l = 0; l <= ITSU_CELL_LAYERS; ++l) {
-    ITSU_CUDA(ctx, cudaMemcpyAsync(&seg.nbo[l], ctx->nb_off + seg.cs[l], sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->stage >= kTracklets) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(seg.ts, ctx->trk_seg + (int64_t)e * ITSU_TRACKLET_LAYERS, sizeof seg.ts, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (ctx->stage >= kCells) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(seg.cs, ctx->cell_seg + (int64_t)e * ITSU_CELL_LAYERS, sizeof seg.cs, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (ctx->stage >= kRoads) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(seg.rs, ctx->road_seg + e, sizeof seg.rs, cudaMemcpyDeviceToHost, ctx->stream));
   }
   ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->stage >= kNeighbours) {
+    for (int l = 0; l <= ITSU_CELL_LAYERS; ++l) {
+      ITSU_CUDA(ctx, cudaMemcpyAsync(&seg.nbo[l], ctx->nb_off + seg.cs[l], sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   return ITSU_OK;
 }
 
@@ -815,11 +825,19 @@ itsu_status itsu_copy_results(itsu_context *ctx, int32_t event, const itsu_resul
     for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {
       if ((st = copy_range(ctx, out->cells_lookup[l], ctx->cell_lookup + s.ts[l + 1], n.tracklets[l + 1])) != ITSU_OK) return st;
     }
+  } else {
+    for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {  // no cells yet: every lookup entry unused
+      if (out->cells_lookup[l]) std::fill(out->cells_lookup[l], out->cells_lookup[l] + n.tracklets[l + 1], ITSU_UNUSED_INDEX);
+    }
   }
   if (ctx->stage >= kNeighbours) {
     for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {
       if ((st = copy_range(ctx, out->neighbour_offsets[l], ctx->nb_off + s.cs[l + 1], (int64_t)n.cells[l + 1] + 1)) != ITSU_OK) return st;
       if ((st = copy_range(ctx, out->neighbours[l], ctx->nb + s.nbo[l + 1], n.neighbours[l])) != ITSU_OK) return st;
+    }
+  } else {
+    for (int l = 0; l < ITSU_NEIGHBOUR_LAYERS; ++l) {  // no neighbours yet: empty rows
+      if (out->neighbour_offsets[l]) std::fill(out->neighbour_offsets[l], out->neighbour_offsets[l] + n.cells[l + 1] + 1, 0);
     }
   }
   if (ctx->stage >= kRoads) {
