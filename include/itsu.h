@@ -217,6 +217,26 @@ int32_t itsu_kernels_per_run(void);
 itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_time *times, int32_t capacity,
                                int32_t *count);
 
+/* ---- clustering without any allocation ----
+ * No counterpart in the reference: its GPU backend allocates per call (gpu/Vector.h:97-122).
+ * For callers that cannot call cudaMalloc (a process whose memory pool owns the device's memory,
+ * or a latency-critical loop that cannot afford an allocation's implicit synchronisation), this
+ * runs the clustering stage of one primary vertex (PrimaryVertexContext::initialize,
+ * src/CA/PrimaryVertexContext.cxx:31-142) using only the caller's device buffers and a scratch
+ * array of fixed size compiled into the library; it allocates nothing.
+ *   clusters       device: n_clusters raw clusters, layer-major
+ *   layer_offsets  device: 8 offsets, layer L = [layer_offsets[L], layer_offsets[L+1])
+ *   vertex         device: x, y, z of the primary vertex
+ *   sorted         device out: n_clusters clusters, per layer sorted stably by bin
+ *   index_tables   device out: 6 x 401 ints (tables of layers 1..6)
+ * At most ITSU_NOALLOC_MAX_CLUSTERS clusters (ITSU_ERR_CAPACITY beyond). Runs on cuda_stream on
+ * the current device and waits for it; the first call on a device looks up the scratch array's
+ * address and should come before any stream capture. All calls share the scratch array: calls
+ * that overlap on the GPU race. Errors are reported through itsu_last_error(NULL). */
+#define ITSU_NOALLOC_MAX_CLUSTERS 65536
+itsu_status itsu_pvc_initialize_noalloc(const itsu_cluster *clusters, const int32_t *layer_offsets, const float *vertex,
+                                        int64_t n_clusters, itsu_cluster *sorted, int32_t *index_tables, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

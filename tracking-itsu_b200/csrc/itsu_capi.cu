@@ -32,6 +32,8 @@ enum Stage { kNone = 0, kInitialized, kTracklets, kCells, kNeighbours, kRoads };
 
 }  // namespace
 
+void itsu::set_thread_error(const char *message) { g_thread_error = message; }
+
 struct itsu_context {
   int device = 0;
   uint32_t flags = 0;

@@ -113,4 +113,7 @@ struct KernelStep {
 const KernelStep *pipeline_steps(int *count);
 int kernels_per_run();
 
+// Sets the calling thread's last error message (returned by itsu_last_error(NULL)).
+void set_thread_error(const char *message);
+
 }  // namespace itsu

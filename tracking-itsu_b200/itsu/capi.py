@@ -96,6 +96,8 @@ SIGNATURES = [
     ("itsu_batch_roads_device", ctypes.c_int,
      [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]),
     ("itsu_kernels_per_run", ctypes.c_int32, []),
+    ("itsu_pvc_initialize_noalloc", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("itsu_batch_profile", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
 ]
