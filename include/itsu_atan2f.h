@@ -12,9 +12,9 @@
  *
  * Method (a published one, restated here): Ziv's two-step rounding test.
  *  1. Fast path in binary64. With num = min(|x|,|y|), den = max(|x|,|y|), pick k = round(32 t)
- *     for t = num/den and reduce with atan(t) = atan(k/32) + atan(u),
+ *     for t = num/den (from a binary32 quotient) and reduce with atan(t) = atan(k/32) + atan(u),
  *     u = (num - (k/32) den) / (den + (k/32) num). The numerator is exact (both products have
- *     <= 30 significant bits and the operands are within a factor of two), |u| <= 1/64, and
+ *     <= 30 significant bits and their exponents are at most two apart), |u| <= 1/64 + 2^-20, and
  *     atan(u) is a 6-term Taylor polynomial. Octant reconstruction uses pi/2 - a and pi - a.
  *     The relative error is below 2^-48; the result is returned when the interval
  *     [a - 2^-44 a, a + 2^-44 a] does not contain a binary32 rounding boundary.
@@ -46,6 +46,10 @@
 #define ITSU_DDIV(a, b) __ddiv_rn((a), (b))
 #define ITSU_D2F(a) __double2float_rn(a)
 #define ITSU_D2I_RZ(a) __double2int_rz(a)
+#define ITSU_FDIV(a, b) __fdiv_rn((a), (b))
+#define ITSU_FMUL(a, b) __fmul_rn((a), (b))
+#define ITSU_FADD(a, b) __fadd_rn((a), (b))
+#define ITSU_F2I_RZ(a) __float2int_rz(a)
 #else
 #define ITSU_DADD(a, b) ((a) + (b))
 #define ITSU_DSUB(a, b) ((a) - (b))
@@ -53,6 +57,10 @@
 #define ITSU_DDIV(a, b) ((a) / (b))
 #define ITSU_D2F(a) ((float)(a))
 #define ITSU_D2I_RZ(a) ((int)(a))
+#define ITSU_FDIV(a, b) ((a) / (b))
+#define ITSU_FMUL(a, b) ((a) * (b))
+#define ITSU_FADD(a, b) ((a) + (b))
+#define ITSU_F2I_RZ(a) ((int)(a))
 #endif
 
 /* atan(k/32), k = 0..32, as (hi, lo) pairs. */
@@ -297,11 +305,15 @@ ITSU_CR_FN float itsu_atan2f(float y, float x)
   }
 
   {
-    const double ax = (double)itsu_cr_u2f(axb), ay = (double)itsu_cr_u2f(ayb);
-    const int swap = ay > ax;
-    const double num = swap ? ax : ay, den = swap ? ay : ax;
-    const double t = ITSU_DDIV(num, den);
-    const int k = ITSU_D2I_RZ(ITSU_DADD(ITSU_DMUL(t, 32.0), 0.5));
+    const float axf = itsu_cr_u2f(axb), ayf = itsu_cr_u2f(ayb);
+    const int swap = ayf > axf;
+    const float numf = swap ? axf : ayf, denf = swap ? ayf : axf;
+    const double num = (double)numf, den = (double)denf;
+    /* k = round(32 t) from a binary32 quotient: |32 t - k| <= 1/2 + 2^-19, which keeps |u| within
+     * 1/64 + 2^-20 and the numerator below exact (both products have <= 30 significant bits and
+     * exponents at most two apart). */
+    const float tf = ITSU_FDIV(numf, denf);
+    const int k = ITSU_F2I_RZ(ITSU_FADD(ITSU_FMUL(tf, 32.0f), 0.5f));
     const double c = ITSU_DMUL((double)k, 0.03125);
     const double nn = ITSU_DSUB(num, ITSU_DMUL(c, den)); /* exact */
     const double cn = ITSU_DMUL(c, num);                 /* exact */

@@ -52,12 +52,20 @@ struct itsu_context {
   float4 *xyzr = nullptr;
   float *phi = nullptr;
   int32_t *trk_count = nullptr, *trk_off = nullptr, *trk_lookup = nullptr;
+  float *zs_z = nullptr;
+  int32_t *zs_j = nullptr;
+  int32_t *trk_slots = nullptr;
   // event class
+  float2 *seg_rrange = nullptr;
+  int32_t *seg_regular = nullptr;
   int32_t *layer_off = nullptr, *index_tables = nullptr, *trk_seg = nullptr, *cell_seg = nullptr, *road_seg = nullptr;
   float *vtx = nullptr;
   // tracklet class
   itsu_tracklet *tracklets = nullptr;
   int32_t *trk_seg_id = nullptr, *cell_count = nullptr, *cell_off = nullptr, *cell_lookup = nullptr;
+  unsigned long long *cell_mask = nullptr;
+  float *trk_tl = nullptr, *tl_key = nullptr;
+  uint8_t *tl_perm = nullptr;
   // cell class
   itsu_cell *cells = nullptr;
   int32_t *cell_seg_id = nullptr, *nb_count = nullptr, *nb_off = nullptr, *nb_fill = nullptr, *road_count = nullptr,
@@ -146,13 +154,22 @@ Arena arena_of(const itsu_context *ctx)
   a.phi = ctx->phi;
   a.tmp = ctx->tmp;
   a.index_tables = ctx->index_tables;
+  a.zs_z = ctx->zs_z;
+  a.zs_j = ctx->zs_j;
+  a.seg_rrange = ctx->seg_rrange;
+  a.seg_regular = ctx->seg_regular;
   a.trk_count = ctx->trk_count;
+  a.trk_slots = ctx->trk_slots;
   a.trk_off = ctx->trk_off;
   a.trk_lookup = ctx->trk_lookup;
   a.trk_seg = ctx->trk_seg;
   a.tracklets = ctx->tracklets;
   a.trk_seg_id = ctx->trk_seg_id;
+  a.trk_tl = ctx->trk_tl;
+  a.tl_key = ctx->tl_key;
+  a.tl_perm = ctx->tl_perm;
   a.cell_count = ctx->cell_count;
+  a.cell_mask = ctx->cell_mask;
   a.cell_off = ctx->cell_off;
   a.cell_lookup = ctx->cell_lookup;
   a.cell_seg = ctx->cell_seg;
@@ -213,6 +230,9 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ITSU_CUDA(ctx, alloc(ctx->trk_count, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->trk_off, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->trk_lookup, cap));
+    ITSU_CUDA(ctx, alloc(ctx->zs_z, cap));
+    ITSU_CUDA(ctx, alloc(ctx->zs_j, cap));
+    ITSU_CUDA(ctx, alloc(ctx->trk_slots, cap * itsu::kTrackletSlotsPerCluster));
     ctx->cap_clusters = cap;
     ctx->generation++;
   }
@@ -226,6 +246,8 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ITSU_CUDA(ctx, alloc(ctx->trk_seg, (int64_t)cap * ITSU_TRACKLET_LAYERS + 1));
     ITSU_CUDA(ctx, alloc(ctx->cell_seg, (int64_t)cap * ITSU_CELL_LAYERS + 1));
     ITSU_CUDA(ctx, alloc(ctx->road_seg, (int64_t)cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->seg_rrange, (int64_t)cap * ITSU_LAYERS));
+    ITSU_CUDA(ctx, alloc(ctx->seg_regular, (int64_t)cap * ITSU_LAYERS));
     ctx->cap_events = cap;
     ctx->generation++;
   }
@@ -241,6 +263,10 @@ itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
     ITSU_CUDA(ctx, alloc(ctx->tracklets, cap));
     ITSU_CUDA(ctx, alloc(ctx->trk_seg_id, cap));
     ITSU_CUDA(ctx, alloc(ctx->cell_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx->cell_mask, cap));
+    ITSU_CUDA(ctx, alloc(ctx->trk_tl, cap));
+    ITSU_CUDA(ctx, alloc(ctx->tl_key, cap));
+    ITSU_CUDA(ctx, alloc(ctx->tl_perm, cap));
     ITSU_CUDA(ctx, alloc(ctx->cell_off, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->cell_lookup, cap));
     ctx->cap_tracklets = cap;
@@ -665,10 +691,11 @@ void itsu_context_destroy(itsu_context *ctx)
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graph(ctx);
   release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
-  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup);
+  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs_z); release(ctx->zs_j); release(ctx->trk_slots);
+  release(ctx->seg_rrange); release(ctx->seg_regular);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
-  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_off); release(ctx->cell_lookup);
+  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->trk_tl); release(ctx->tl_key); release(ctx->tl_perm); release(ctx->cell_off); release(ctx->cell_lookup);
   release(ctx->cells); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);

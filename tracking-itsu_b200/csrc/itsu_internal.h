@@ -28,6 +28,7 @@ enum : int32_t {
   kFlagCapRoads = 16,
   kFlagCountOverflow = 32,
 };
+constexpr int kTrackletSlotsPerCluster = 48;  // outer clusters the tracklet count pass keeps per inner cluster
 constexpr int32_t kCapacityMask = kFlagCapTracklets | kFlagCapCells | kFlagCapNeighbours | kFlagCapRoads | kFlagCountOverflow;
 
 // Totals and requirements of a run, written by the device.
@@ -55,15 +56,26 @@ struct Arena {
   float *phi;
   itsu_cluster *tmp;
   int32_t *index_tables;
+  // candidate-pruning index (null: not built): per bin, the bin's clusters sorted by (z, index);
+  // per (event, layer) the r range of its clusters and whether all its bins are regular
+  float *zs_z;
+  int32_t *zs_j;
+  float2 *seg_rrange;
+  int32_t *seg_regular;
   // tracklets
   int32_t *trk_count;
+  int32_t *trk_slots;  // per inner cluster, the first outer clusters of its tracklets (count pass)
   int32_t *trk_off;
   int32_t *trk_lookup;
   int32_t *trk_seg;
   itsu_tracklet *tracklets;
   int32_t *trk_seg_id;
+  float *trk_tl;     // tan(lambda) of each tracklet, compact
+  float *tl_key;     // per cluster, its outgoing tracklets' tan(lambda) sorted (cell pruning index)
+  uint8_t *tl_perm;  // ... and each one's position in the cluster's outgoing range
   // cells
   int32_t *cell_count;
+  unsigned long long *cell_mask;  // per first tracklet: which outgoing tracklets make cells
   int32_t *cell_off;
   int32_t *cell_lookup;
   int32_t *cell_seg;

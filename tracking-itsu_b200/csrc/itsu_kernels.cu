@@ -31,6 +31,7 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr float kMaxAbsCoordinate = 1.0e6f;
+constexpr int kMaxPruneBin = 64;  // larger bins disable pruning for their layer
 
 __device__ __forceinline__ bool capacity_failed(const DevStatus *s) { return (*(volatile const int32_t *)&s->flags & kCapacityMask) != 0; }
 
@@ -412,6 +413,61 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
       store_sorted(a, begin + i, a.tmp[begin + i]);
     }
   }
+
+  // Pass 5: the tracklet stage's candidate-pruning index. A layer is regular when every cluster
+  // has a z bin and a phi bin inside the 20 x 20 table (then a bin's column is its clusters' z
+  // bin) and no bin holds more than kMaxPruneBin clusters; for regular layers, each bin's
+  // clusters are listed again sorted by (z, sorted index), with the layer's r range beside.
+  if (a.zs_z == nullptr || layer == 0) {
+    return;  // no index wanted, or layer 0 (never the outer layer of a tracklet)
+  }
+  __shared__ int s_irregular;
+  __shared__ int s_rmin, s_rmax;  // float bits; r >= 0 orders like its bits
+  if (tid == 0) {
+    s_irregular = m > 0 || bucket_total[kBuckets - 1] > 0;  // negative bins or bin 400
+    s_rmin = 0x7f800000;
+    s_rmax = 0;
+  }
+  __syncthreads();
+  int irregular = 0, rmin = 0x7f800000, rmax = 0;
+  for (int i = tid; i < n; i += kSortThreads) {
+    const float4 c = a.xyzr[begin + i];
+    const int zb = z_bin_index(layer, c.z);
+    const int pb = phi_bin_index(a.phi[begin + i]);
+    irregular |= zb < 0 || zb >= kZBins || pb < 0 || pb >= kPhiBins;
+    rmin = min(rmin, __float_as_int(c.w));
+    rmax = max(rmax, __float_as_int(c.w));
+  }
+  if (irregular) {
+    atomicOr(&s_irregular, 1);
+  }
+  atomicMin(&s_rmin, rmin);
+  atomicMax(&s_rmax, rmax);
+  for (int b = tid; b < kTableBins; b += kSortThreads) {
+    const int cnt = bucket_total[b + 1], st = bucket_base[b + 1];
+    if (cnt > kMaxPruneBin) {
+      atomicOr(&s_irregular, 1);
+      continue;
+    }
+    float *zz = a.zs_z + begin + st;
+    int32_t *jj = a.zs_j + begin + st;
+    for (int k = 0; k < cnt; ++k) {  // insertion by (z, index): equal z keep index order
+      const float z = a.xyzr[begin + st + k].z;
+      int p = k;
+      while (p > 0 && zz[p - 1] > z) {
+        zz[p] = zz[p - 1];
+        jj[p] = jj[p - 1];
+        --p;
+      }
+      zz[p] = z;
+      jj[p] = st + k;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    a.seg_regular[seg] = !s_irregular;
+    a.seg_rrange[seg] = make_float2(__int_as_float(s_rmin), __int_as_float(s_rmax));
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -428,157 +484,300 @@ __device__ __forceinline__ bool tracklets_active(const int32_t *lo, int layer)
   return true;
 }
 
-// Tracklet.cxx:32-40 for a queued pair (out slot, inner flat index, outer flat index, cluster
-// segment of the inner cluster).
-__device__ __forceinline__ void write_tracklet(const Arena &a, int4 q)
+// Tracklet.cxx:32-40: the tracklet from inner cluster i_flat to outer cluster j_flat.
+__device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t i_flat, int64_t j_flat, int seg)
 {
-  const int seg = q.w;
   const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
-  const float4 c = a.xyzr[q.y];
-  const float4 d = a.xyzr[q.z];
+  const float4 c = a.xyzr[i_flat];
+  const float4 d = a.xyzr[j_flat];
   itsu_tracklet t;
-  t.first_cluster = q.y - a.layer_off[seg];
-  t.second_cluster = q.z - a.layer_off[seg + 1];
+  t.first_cluster = (int32_t)(i_flat - a.layer_off[seg]);
+  t.second_cluster = (int32_t)(j_flat - a.layer_off[seg + 1]);
   t.tan_lambda = (c.z - d.z) / (c.w - d.w);
   t.phi = itsu_atan2f(c.y - d.y, c.x - d.x);
-  a.tracklets[q.x] = t;
-  a.trk_seg_id[q.x] = e * ITSU_TRACKLET_LAYERS + layer;
+  a.tracklets[out] = t;
+  a.trk_seg_id[out] = e * ITSU_TRACKLET_LAYERS + layer;
+  a.trk_tl[out] = t.tan_lambda;
 }
 
-// Walks the reference's candidate sequence of one inner cluster (Tracker.cxx:73-89): the phi
-// rows of its bin window in wrap-around order, and in each row the sorted clusters from the
-// row's first bin to the first cluster at or after the window's end (inclusive, P1/P5 bounds).
-struct CandidateWalk {
-  const int32_t *table;
-  int n_next;
-  int z_min, z_span;  // first z bin, number of z bins + 1
-  int phi_bin, rows_left;
-  int j, last;
+constexpr int kColHits = 16;        // hits of one z-pruned column sorted back into index order
+constexpr int kTrackletSlots = kTrackletSlotsPerCluster;
+constexpr int kMaxMaskedOut = 64;  // out-degrees up to this are evaluated pair-parallel with a pass mask
 
-  __device__ __forceinline__ bool next()
+// The reference's candidate sequence of one inner cluster (Tracker.cxx:73-113), calling
+// on_pass(j) for every next-layer cluster j that passes the cut, in emission order: the phi
+// rows of the bin window in wrap-around order and, in each row, the sorted clusters from the
+// row's first bin through the first cluster at or after the window's end (inclusive bound, with
+// the P1/P5 guards).
+//
+// On a regular next layer the row is walked through the pruning index instead, which is exact:
+// a pass needs |P - z2| < dz with P = (tanL (r2 - r1) + z1) in binary32, P is monotone in r2, so
+// every passing z2 lies within [P(rmin) - dz, P(rmax) + dz] (widened by 1e-3 cm for the rounding
+// of the bounds); only the z bins of the row that meet that interval can hold passes, and in each
+// such bin only the clusters listed there between the two z values. Their passes are put back
+// into index order before on_pass. The row's last candidate (the inclusive bound, past the
+// window's z bins) is always evaluated. Irregular layers take the reference walk.
+struct TrackletProbe {
+  float4 c;      // inner cluster (x, y, z, r)
+  float phi1, tan_lambda, max_dz;
+  const float4 *xyzr;  // next layer
+  const float *phi;
+
+  __device__ __forceinline__ bool pass(int j) const
   {
-    ++j;
-    while (j > last) {
-      if (rows_left == 0) {
-        return false;
-      }
-      const int first_bin = bin_index(z_min, phi_bin);
-      const int max_bin = min(first_bin + z_span, kTableBins);
-      j = table[first_bin];
-      last = min(table[max_bin], n_next - 1);
-      phi_bin = (phi_bin + 1 == kPhiBins) ? 0 : phi_bin + 1;
-      --rows_left;
-    }
-    return true;
+    const float4 d = xyzr[j];
+    const float phi2 = phi[j];
+    const float delta_z = fabsf(tan_lambda * (d.w - c.w) + c.z - d.z);
+    const float delta_phi = fabsf(phi1 - phi2);
+    return delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
   }
 };
 
-constexpr int kQueue = 64;  // per-warp queue of accepted pairs, drained 32 at a time
-
-// One thread per inner cluster; the warp advances its 32 candidate walks in lock step so that
-// accepted pairs can be compacted (ballot) into a per-warp queue. The write pass drains the queue
-// with all 32 lanes converged, so the double-precision azimuth of each new tracklet runs without
-// divergence. Output slots come from the scan of the count pass: emission order is the
-// reference's (inner cluster, phi row, candidate).
-template <bool kWrite>
-__global__ void __launch_bounds__(kThreads) k_tracklets(Arena a)
+template <typename OnPass>
+__device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next, int4 rect, int layer, const TrackletProbe &probe,
+                                                bool prune, float zlo, float zhi, const float *zs_z, const int32_t *zs_j,
+                                                OnPass &&on_pass)
 {
-  __shared__ int4 queue[kWrite ? kThreads / 32 : 1][kQueue];
-  if (kWrite && capacity_failed(a.status)) {
-    return;
+  int phi_bins = rect.w - rect.y + 1;
+  if (phi_bins < 0) {
+    phi_bins += kPhiBins;
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t i = global_thread();
-  const bool in_range = i < a.n_clusters;
-  int seg = 0, e = 0, layer = ITSU_LAYERS - 1;
-  const int32_t *lo = a.layer_off;
-  if (in_range) {
-    seg = find_segment(a.layer_off, a.n_events * ITSU_LAYERS, i);
-    e = seg / ITSU_LAYERS;
-    layer = seg % ITSU_LAYERS;
-    lo = a.layer_off + e * ITSU_LAYERS;
-  }
-  float4 c = make_float4(0, 0, 0, 0);
-  float phi1 = 0, tan_lambda = 0;
-  int64_t next_begin = 0;
-  CandidateWalk walk{nullptr, 0, 0, 0, 0, 0, 0, -1};
-  bool has = false;
-  if (in_range && layer < ITSU_LAYERS - 1 && tracklets_active(lo, layer)) {
-    c = a.xyzr[i];
-    phi1 = a.phi[i];
-    const float vz = a.vtx[3 * e + 2];
-    tan_lambda = (c.z - vz) / c.w;
-    const float dir_z = tan_lambda * (kC.r[layer + 1] - c.w) + c.z;
-    const int4 rect = bins_rect(phi1, layer, dir_z);
-    if (!(rect.x == 0 && rect.y == 0 && rect.z == 0 && rect.w == 0)) {
-      int phi_bins = rect.w - rect.y + 1;
-      if (phi_bins < 0) {
-        phi_bins += kPhiBins;
-      }
-      walk.table = a.index_tables + ((int64_t)e * ITSU_TRACKLET_LAYERS + layer) * kTableSize;
-      walk.n_next = lo[layer + 2] - lo[layer + 1];
-      walk.z_min = rect.x;
-      walk.z_span = rect.z - rect.x + 1;
-      walk.phi_bin = rect.y;
-      walk.rows_left = phi_bins;
-      next_begin = lo[layer + 1];
-      has = walk.next();
-    }
-  }
-  int count = 0;
-  int out = 0;
-  int queued = 0;
-  if (kWrite && in_range) {
-    out = a.trk_off[i];
-  }
-  const float max_dz = kC.trk_max_dz[layer < ITSU_TRACKLET_LAYERS ? layer : 0];
-  while (__any_sync(0xffffffffu, has)) {
-    bool pass = false;
-    if (has) {
-      const int64_t jf = next_begin + walk.j;
-      const float4 d = a.xyzr[jf];
-      const float phi2 = a.phi[jf];
-      const float delta_z = fabsf(tan_lambda * (d.w - c.w) + c.z - d.z);
-      const float delta_phi = fabsf(phi1 - phi2);
-      pass = delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
-    }
-    if (kWrite) {
-      const unsigned m = __ballot_sync(0xffffffffu, pass);
-      if (pass) {
-        queue[warp][queued + __popc(m & ((1u << lane) - 1u))] = make_int4(out, (int)i, (int)(next_begin + walk.j), seg);
-        ++out;
-      }
-      queued += __popc(m);
-      if (queued >= 32) {
-        __syncwarp();
-        write_tracklet(a, queue[warp][lane]);
-        __syncwarp();
-        if (lane < queued - 32) {
-          queue[warp][lane] = queue[warp][lane + 32];
+  const int zb_lo = prune ? max(rect.x, z_bin_index(layer + 1, zlo)) : 0;
+  const int zb_hi = prune ? min(rect.z, z_bin_index(layer + 1, zhi)) : -1;
+  for (int phi_bin = rect.y, phi_count = 0; phi_count < phi_bins;
+       phi_bin = (phi_bin + 1 == kPhiBins) ? 0 : phi_bin + 1, ++phi_count) {
+    const int first_bin = bin_index(rect.x, phi_bin);
+    const int max_bin = min(first_bin + rect.z - rect.x + 1, kTableBins);  // P5
+    if (prune && phi_bin < kPhiBins) {
+      for (int col = zb_lo; col <= zb_hi; ++col) {
+        const int bin = phi_bin * kPhiBins + col;
+        const int k0 = table[bin], k1 = table[bin + 1];
+        int lo = k0, hi = k1;  // first listed cluster with z >= zlo
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (zs_z[mid] < zlo) {
+            lo = mid + 1;
+          } else {
+            hi = mid;
+          }
         }
-        __syncwarp();
-        queued -= 32;
+        int hits[kColHits];
+        int h = 0;
+        bool overflow = false;
+        for (int k = lo; k < k1 && zs_z[k] <= zhi; ++k) {
+          const int j = zs_j[k];
+          if (probe.pass(j)) {
+            if (h == kColHits) {
+              overflow = true;
+              break;
+            }
+            int q = h++;
+            while (q > 0 && hits[q - 1] > j) {
+              hits[q] = hits[q - 1];
+              --q;
+            }
+            hits[q] = j;
+          }
+        }
+        if (!overflow) {
+          for (int q = 0; q < h; ++q) {
+            on_pass(hits[q]);
+          }
+        } else {
+          for (int j = k0; j < k1; ++j) {  // a crowded column: walk it in index order
+            if (probe.pass(j)) {
+              on_pass(j);
+            }
+          }
+        }
+      }
+      const int x = table[max_bin];  // the inclusive bound's candidate (P1: inside the layer)
+      if (x < n_next && probe.pass(x)) {
+        on_pass(x);
       }
     } else {
-      count += pass;
-    }
-    if (has) {
-      has = walk.next();
+      const int first_row = table[first_bin];
+      const int last_row = min(table[max_bin], n_next - 1);  // inclusive bound, P1
+      for (int j = first_row; j <= last_row; ++j) {
+        if (probe.pass(j)) {
+          on_pass(j);
+        }
+      }
     }
   }
-  if (kWrite) {
-    __syncwarp();
-    if (lane < queued) {
-      write_tracklet(a, queue[warp][lane]);
+}
+
+// The walk state of one inner cluster i (flat index): whether its layer runs the tracklet
+// stage, and the probe, window and pruning bounds of its candidate walk.
+struct InnerCluster {
+  bool walk;
+  int seg, e, layer;
+  int4 rect;
+  TrackletProbe probe;
+  bool prune;
+  float zlo, zhi;
+  const int32_t *table;
+  int n_next;
+  int64_t next_begin;
+};
+
+__device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
+{
+  InnerCluster s;
+  s.walk = false;
+  s.seg = find_segment(a.layer_off, a.n_events * ITSU_LAYERS, i);
+  s.e = s.seg / ITSU_LAYERS;
+  s.layer = s.seg % ITSU_LAYERS;
+  const int32_t *lo = a.layer_off + s.e * ITSU_LAYERS;
+  if (s.layer >= ITSU_LAYERS - 1 || !tracklets_active(lo, s.layer)) {
+    return s;
+  }
+  s.probe.c = a.xyzr[i];
+  s.probe.phi1 = a.phi[i];
+  const float vz = a.vtx[3 * s.e + 2];
+  s.probe.tan_lambda = (s.probe.c.z - vz) / s.probe.c.w;
+  const float dir_z = s.probe.tan_lambda * (kC.r[s.layer + 1] - s.probe.c.w) + s.probe.c.z;
+  s.rect = bins_rect(s.probe.phi1, s.layer, dir_z);
+  if (s.rect.x == 0 && s.rect.y == 0 && s.rect.z == 0 && s.rect.w == 0) {
+    return s;
+  }
+  s.walk = true;
+  s.next_begin = lo[s.layer + 1];
+  s.probe.xyzr = a.xyzr + s.next_begin;
+  s.probe.phi = a.phi + s.next_begin;
+  s.probe.max_dz = kC.trk_max_dz[s.layer];
+  const int next_seg = s.seg + 1;
+  s.prune = a.seg_regular[next_seg] != 0;
+  s.zlo = s.zhi = 0;
+  if (s.prune) {
+    const float2 rr = a.seg_rrange[next_seg];
+    const float p1 = s.probe.tan_lambda * (rr.x - s.probe.c.w) + s.probe.c.z;
+    const float p2 = s.probe.tan_lambda * (rr.y - s.probe.c.w) + s.probe.c.z;
+    s.zlo = fminf(p1, p2) - s.probe.max_dz - 1e-3f;
+    s.zhi = fmaxf(p1, p2) + s.probe.max_dz + 1e-3f;
+    s.prune = isfinite(s.zlo) && isfinite(s.zhi);
+  }
+  s.table = a.index_tables + ((int64_t)s.e * ITSU_TRACKLET_LAYERS + s.layer) * kTableSize;
+  s.n_next = lo[s.layer + 2] - lo[s.layer + 1];
+  return s;
+}
+
+template <typename OnPass>
+__device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s, OnPass &&on_pass)
+{
+  walk_candidates(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, a.zs_z + s.next_begin,
+                  a.zs_j + s.next_begin, on_pass);
+}
+
+// Count pass, one thread per inner cluster: the number of tracklets, and the outer clusters of
+// the first kTrackletSlots of them in emission order.
+__global__ void __launch_bounds__(kThreads) k_tracklets_count(Arena a)
+{
+  const int64_t i = global_thread();
+  if (i >= a.n_clusters) {
+    return;
+  }
+  const InnerCluster s = inner_cluster(a, i);
+  int count = 0;
+  if (s.walk) {
+    int32_t *slots = a.trk_slots + i * kTrackletSlots;
+    walk_inner(a, s, [&](int j) {
+      if (count < kTrackletSlots) {
+        slots[count] = j;
+      }
+      ++count;
+    });
+  }
+  a.trk_count[i] = count;
+}
+
+// Write pass, one thread per tracklet: its inner cluster is the last one whose scanned offset is
+// at or below the tracklet's slot, its outer cluster comes from the count pass's slots. All
+// tracklets of a warp compute their binary64 azimuth together. Tracklets of inner clusters with
+// more than kTrackletSlots are written by k_tracklets_tail instead.
+__global__ void __launch_bounds__(kThreads) k_tracklets_write(Arena a)
+{
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int64_t n = a.status->total[kTracklets];
+  const int nc = (int)a.n_clusters;
+  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
+    int lo = 0, hi = nc;  // trk_off[lo] <= k < trk_off[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (a.trk_off[mid] <= k) {
+        lo = mid;
+      } else {
+        hi = mid;
+      }
     }
-    if (in_range) {
-      const int32_t first = a.trk_off[i];
-      a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && a.trk_off[i + 1] > first)
-                            ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
-                            : ITSU_UNUSED_INDEX;
+    const int64_t i = lo;
+    if (a.trk_count[i] > kTrackletSlots) {
+      continue;
     }
-  } else if (in_range) {
-    a.trk_count[i] = count;
+    const int r = (int)(k - a.trk_off[i]);
+    const int seg_t = find_segment(a.trk_seg, a.n_events * ITSU_TRACKLET_LAYERS, k);
+    const int seg = seg_t + seg_t / ITSU_TRACKLET_LAYERS;  // (e, L) as a cluster segment: 7e + L
+    write_tracklet(a, (int)k, i, a.layer_off[seg + 1] + a.trk_slots[i * kTrackletSlots + r], seg);
+  }
+}
+
+// Per inner cluster: its entry of the tracklets lookup table (Tracker.cxx:102-108) and, for the
+// rare clusters with more than kTrackletSlots tracklets, the tracklets themselves, walked again
+// and written in order.
+__global__ void __launch_bounds__(kThreads) k_tracklets_tail(Arena a)
+{
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int64_t i = global_thread();
+  if (i >= a.n_clusters) {
+    return;
+  }
+  const int32_t first = a.trk_off[i], count = a.trk_off[i + 1] - first;
+  const int seg = find_segment(a.layer_off, a.n_events * ITSU_LAYERS, i);
+  const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
+  a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && count > 0)
+                        ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
+                        : ITSU_UNUSED_INDEX;
+  if (count > kTrackletSlots) {
+    const InnerCluster s = inner_cluster(a, i);
+    int out = first;
+    walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, seg); });
+  }
+}
+
+// The cell stage's pruning index: the outgoing tracklets of each cluster (at most kMaxMaskedOut)
+// sorted by tan(lambda), with each one's position in the cluster's range. NaN slopes (two
+// clusters at equal r) sort last; they never pass a cut.
+__device__ __forceinline__ bool tl_before(float a, float b) { return a < b || (!isnan(a) && isnan(b)); }
+
+__global__ void __launch_bounds__(kThreads) k_tracklet_index(Arena a)
+{
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int64_t n = a.status->total[kTracklets];
+  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
+    // the cluster whose outgoing range holds tracklet k is its first cluster
+    const int sid = a.trk_seg_id[k];
+    const int seg = sid + sid / ITSU_TRACKLET_LAYERS;
+    const int64_t c = a.layer_off[seg] + a.tracklets[k].first_cluster;
+    const int32_t j0 = a.trk_off[c];
+    const int cnt = a.trk_off[c + 1] - j0;
+    if (cnt > kMaxMaskedOut) {
+      continue;
+    }
+    const int q = (int)(k - j0);
+    const float v = a.trk_tl[k];
+    int rank = 0;  // slopes before this one, ties in range order
+    for (int p = 0; p < cnt; ++p) {
+      const float w = a.trk_tl[j0 + p];
+      rank += tl_before(w, v) || (!tl_before(v, w) && p < q);
+    }
+    a.tl_key[j0 + rank] = v;
+    a.tl_perm[j0 + rank] = (uint8_t)q;
   }
 }
 
@@ -614,64 +813,299 @@ __device__ __forceinline__ bool cells_active(const int32_t *ts, int layer)
   return true;
 }
 
-template <bool kWrite>
-__global__ void __launch_bounds__(kThreads) k_cells(Arena a)
+constexpr int kCellQueue = 64;
+
+// Per-lane state of the warp-parallel cell stage: lane l owns first tracklet k = base + l.
+struct CellLane {
+  int64_t k;
+  int layer, e;
+  float t1_tan_lambda, t1_phi;
+  float4 c1, c2;
+  float vx, vy, vz;
+  int32_t j0, n_out;     // the outgoing tracklets of the tracklet's outer cluster: [j0, j0 + n_out)
+  int64_t c3_base;       // first cluster of layer L + 2
+  int32_t t1_local, t1_first, t2_base;  // tracklet index in its layer, its first cluster, first tracklet of layer L + 1
+};
+
+__device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t n)
+{
+  CellLane s;
+  s.k = k;
+  s.n_out = 0;
+  s.layer = ITSU_CELL_LAYERS;
+  s.e = 0;
+  if (k >= n) {
+    return s;
+  }
+  const int sid = a.trk_seg_id[k];
+  s.e = sid / ITSU_TRACKLET_LAYERS;
+  s.layer = sid % ITSU_TRACKLET_LAYERS;
+  const int32_t *ts = a.trk_seg + s.e * ITSU_TRACKLET_LAYERS;
+  if (s.layer >= ITSU_CELL_LAYERS || !cells_active(ts, s.layer)) {
+    s.layer = ITSU_CELL_LAYERS;
+    return s;
+  }
+  const int32_t *lo = a.layer_off + s.e * ITSU_LAYERS;
+  const itsu_tracklet t1 = a.tracklets[k];
+  s.t1_tan_lambda = t1.tan_lambda;
+  s.t1_phi = t1.phi;
+  s.t1_first = t1.first_cluster;
+  s.c1 = a.xyzr[lo[s.layer] + t1.first_cluster];
+  const int64_t c2i = lo[s.layer + 1] + t1.second_cluster;
+  s.c2 = a.xyzr[c2i];
+  s.j0 = a.trk_off[c2i];
+  s.n_out = a.trk_off[c2i + 1] - s.j0;
+  s.vx = a.vtx[3 * s.e];
+  s.vy = a.vtx[3 * s.e + 1];
+  s.vz = a.vtx[3 * s.e + 2];
+  s.c3_base = lo[s.layer + 2];
+  s.t1_local = (int32_t)(k - ts[s.layer]);
+  s.t2_base = ts[s.layer + 1];
+  return s;
+}
+
+__device__ __forceinline__ float4 shfl4(float4 v, int src)
+{
+  return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                     __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+
+// Owner lane of flattened item t given the lanes' exclusive prefix sums: the last lane whose
+// prefix is <= t (for t < total this lane holds item t). All lanes must call it together.
+__device__ __forceinline__ int owner_of(int excl, int t)
+{
+  int owner = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    const int v = __shfl_sync(0xffffffffu, excl, owner + step);
+    if (v <= t) {
+      owner += step;
+    }
+  }
+  return owner;
+}
+
+__device__ __forceinline__ int warp_exclusive_sum(int v, int &total)
+{
+  const int lane = threadIdx.x & 31;
+  int inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) {
+      inc += t;
+    }
+  }
+  total = __shfl_sync(0xffffffffu, inc, 31);
+  return inc - v;
+}
+
+__device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const CellLane &s, const itsu_tracklet &t2, int32_t j,
+                                           float3 normal, float curvature)
+{
+  itsu_cell cell;
+  cell.first_cluster = s.t1_first;
+  cell.second_cluster = t2.first_cluster;
+  cell.third_cluster = t2.second_cluster;
+  cell.first_tracklet = s.t1_local;
+  cell.second_tracklet = j - s.t2_base;
+  cell.nx = normal.x;
+  cell.ny = normal.y;
+  cell.nz = normal.z;
+  cell.curvature = curvature;
+  cell.level = 1;
+  a.cells[out] = cell;
+  a.cell_seg_id[out] = s.e * ITSU_CELL_LAYERS + s.layer;
+}
+
+// Count pass: for each first tracklet, a mask of which of its (<= 64) outgoing tracklets make a
+// cell, and their number. The warp flattens its 32 tracklets' pairs across lanes (Tracker.cxx:
+// 155-158 iterates them per tracklet); pairs that pass the cheap cuts queue up so the circle
+// geometry runs with all 32 lanes converged.
+__global__ void __launch_bounds__(kThreads) k_cells_count(Arena a)
+{
+  __shared__ int4 queue[kThreads / 32][kCellQueue];             // (owner lane, pair bit, c3 flat, -)
+  __shared__ unsigned long long masks[kThreads / 32][32];
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t n = a.status->total[kTracklets];
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
+    const CellLane s = cell_lane(a, base + lane, n);
+    const bool big = s.n_out > kMaxMaskedOut;
+    // Only outgoing tracklets with |dtanL| < 0.025 can pass (Tracker.cxx:161-166): |fl(t1 - t2)|
+    // < 0.025f implies |t1 - t2| < 0.025f exactly, so the window is read off the slope-sorted
+    // index with binary64 bounds (widened by 1e-12).
+    int q0 = 0, q1 = 0;
+    if (!big && s.n_out > 0 && isfinite(s.t1_tan_lambda)) {
+      const float *key = a.tl_key + s.j0;
+      const double lo_d = (double)s.t1_tan_lambda - (double)kCellMaxDeltaTanLambda - 1e-12;
+      const double hi_d = (double)s.t1_tan_lambda + (double)kCellMaxDeltaTanLambda + 1e-12;
+      // the keys are sorted (NaN last): count those below the window and those inside it with
+      // independent loads rather than a chain of dependent binary-search steps
+      for (int q = 0; q < s.n_out; ++q) {
+        const double v = (double)key[q];
+        q0 += v < lo_d;
+        q1 += v <= hi_d;
+      }
+    }
+    masks[warp][lane] = 0ull;
+    int total = 0;
+    const int excl = warp_exclusive_sum(q1 - q0, total);
+    __syncwarp();
+    int queued = 0;
+    auto drain = [&](int count) {
+      const int4 q = queue[warp][lane < count ? lane : 0];
+      const int owner = q.x;
+      const float4 c1 = shfl4(s.c1, owner), c2 = shfl4(s.c2, owner);
+      const float vx = __shfl_sync(0xffffffffu, s.vx, owner), vy = __shfl_sync(0xffffffffu, s.vy, owner);
+      const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
+      if (lane < count) {
+        float3 normal;
+        float curvature;
+        if (cell_geometry(layer, c1, c2, a.xyzr[q.z], vx, vy, normal, curvature)) {
+          atomicOr(&masks[warp][owner], 1ull << q.y);
+        }
+      }
+    };
+    for (int p0 = 0; p0 < total; p0 += 32) {
+      const int p = p0 + lane;
+      const int owner = owner_of(excl, p);
+      const int q = __shfl_sync(0xffffffffu, q0, owner) + p - __shfl_sync(0xffffffffu, excl, owner);
+      const float tl = __shfl_sync(0xffffffffu, s.t1_tan_lambda, owner);
+      const float ph = __shfl_sync(0xffffffffu, s.t1_phi, owner);
+      const float4 c1 = shfl4(s.c1, owner);
+      const float vz = __shfl_sync(0xffffffffu, s.vz, owner);
+      const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
+      const int32_t j0 = __shfl_sync(0xffffffffu, s.j0, owner);
+      const int64_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
+      bool pre = false;
+      int64_t c3 = 0;
+      int b = 0;
+      if (p < total) {
+        b = a.tl_perm[j0 + q];
+        const itsu_tracklet t2 = a.tracklets[j0 + b];
+        pre = cell_precut(layer, tl, ph, t2.tan_lambda, t2.phi, c1, vz);
+        c3 = c3_base + t2.second_cluster;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, pre);
+      if (pre) {
+        queue[warp][queued + __popc(m & ((1u << lane) - 1u))] = make_int4(owner, b, (int)c3, 0);
+      }
+      queued += __popc(m);
+      if (queued >= 32) {
+        __syncwarp();
+        drain(32);
+        __syncwarp();
+        if (lane < queued - 32) {
+          queue[warp][lane] = queue[warp][lane + 32];
+        }
+        __syncwarp();
+        queued -= 32;
+      }
+    }
+    __syncwarp();
+    if (queued > 0) {
+      drain(queued);
+    }
+    __syncwarp();
+    int count = __popcll(masks[warp][lane]);
+    if (big) {  // a crowded outer cluster: this lane evaluates its pairs in order
+      count = 0;
+      for (int b = 0; b < s.n_out; ++b) {
+        const itsu_tracklet t2 = a.tracklets[s.j0 + b];
+        float3 normal;
+        float curvature;
+        count += cell_precut(s.layer, s.t1_tan_lambda, s.t1_phi, t2.tan_lambda, t2.phi, s.c1, s.vz) &&
+                 cell_geometry(s.layer, s.c1, s.c2, a.xyzr[s.c3_base + t2.second_cluster], s.vx, s.vy, normal, curvature);
+      }
+    }
+    if (s.k < n) {
+      a.cell_count[s.k] = count;
+      a.cell_mask[s.k] = big ? 0ull : masks[warp][lane];
+    }
+    __syncwarp();
+  }
+}
+
+// Write pass: the cells of each first tracklet at its scanned slot, in outgoing-tracklet order
+// (the mask's bit order). The warp flattens its tracklets' cells across lanes.
+__global__ void __launch_bounds__(kThreads) k_cells_write(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
   }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t n = a.status->total[kTracklets];
-  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
-    const int sid = a.trk_seg_id[k];
-    const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
-    const int32_t *ts = a.trk_seg + e * ITSU_TRACKLET_LAYERS;
-    int count = 0;
-    int64_t out = kWrite ? a.cell_off[k] : 0;
-    if (layer < ITSU_CELL_LAYERS && cells_active(ts, layer)) {
-      const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
-      const itsu_tracklet t1 = a.tracklets[k];
-      const float4 c1 = a.xyzr[lo[layer] + t1.first_cluster];
-      const int64_t c2i = lo[layer + 1] + t1.second_cluster;
-      const float4 c2 = a.xyzr[c2i];
-      const int32_t j0 = a.trk_off[c2i], j1 = a.trk_off[c2i + 1];
-      const float vx = a.vtx[3 * e], vy = a.vtx[3 * e + 1], vz = a.vtx[3 * e + 2];
-      for (int32_t j = j0; j < j1; ++j) {
-        const itsu_tracklet t2 = a.tracklets[j];
-        if (!cell_precut(layer, t1.tan_lambda, t1.phi, t2.tan_lambda, t2.phi, c1, vz)) {
-          continue;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
+    const int64_t k = base + lane;
+    unsigned long long mask = 0;
+    int32_t first = 0;
+    bool has = false;
+    if (k < n) {
+      mask = a.cell_mask[k];
+      first = a.cell_off[k];
+      has = a.cell_off[k + 1] > first;
+    }
+    // lanes with cells load their tracklet state; the others keep n_out = 0
+    CellLane s = cell_lane(a, has ? k : n, n);
+    s.k = k;
+    const bool big = s.n_out > kMaxMaskedOut;
+    int total = 0;
+    const int excl = warp_exclusive_sum(big ? 0 : __popcll(mask), total);
+    for (int p0 = 0; p0 < total; p0 += 32) {
+      const int p = p0 + lane;
+      const int owner = owner_of(excl, p);
+      const int r = p - __shfl_sync(0xffffffffu, excl, owner);
+      const unsigned long long m = __shfl_sync(0xffffffffu, mask, owner);
+      const float4 c1 = shfl4(s.c1, owner), c2 = shfl4(s.c2, owner);
+      const float vx = __shfl_sync(0xffffffffu, s.vx, owner), vy = __shfl_sync(0xffffffffu, s.vy, owner);
+      const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
+      const int32_t j0 = __shfl_sync(0xffffffffu, s.j0, owner);
+      const int32_t out0 = __shfl_sync(0xffffffffu, first, owner);
+      CellLane o;
+      o.e = __shfl_sync(0xffffffffu, s.e, owner);
+      o.layer = layer;
+      o.t1_local = __shfl_sync(0xffffffffu, s.t1_local, owner);
+      o.t1_first = __shfl_sync(0xffffffffu, s.t1_first, owner);
+      o.t2_base = __shfl_sync(0xffffffffu, s.t2_base, owner);
+      const int64_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
+      if (p < total) {
+        // the r-th (from 0) set bit of the owner's mask
+        unsigned long long rest = m;
+        for (int q = 0; q < r; ++q) {
+          rest &= rest - 1ull;
         }
-        const float4 c3 = a.xyzr[lo[layer + 2] + t2.second_cluster];
+        const int b = __ffsll((long long)rest) - 1;
+        const int32_t j = j0 + b;
+        const itsu_tracklet t2 = a.tracklets[j];
         float3 normal;
         float curvature;
-        if (cell_geometry(layer, c1, c2, c3, vx, vy, normal, curvature)) {
-          if (kWrite) {
-            itsu_cell cell;
-            cell.first_cluster = t1.first_cluster;
-            cell.second_cluster = t2.first_cluster;
-            cell.third_cluster = t2.second_cluster;
-            cell.first_tracklet = (int32_t)(k - ts[layer]);
-            cell.second_tracklet = j - ts[layer + 1];
-            cell.nx = normal.x;
-            cell.ny = normal.y;
-            cell.nz = normal.z;
-            cell.curvature = curvature;
-            cell.level = 1;
-            a.cells[out] = cell;
-            a.cell_seg_id[out] = e * ITSU_CELL_LAYERS + layer;
-            ++out;
-          } else {
-            ++count;
-          }
+        cell_geometry(layer, c1, c2, a.xyzr[c3_base + t2.second_cluster], vx, vy, normal, curvature);
+        write_cell(a, out0 + r, o, t2, j, normal, curvature);
+      }
+    }
+    if (big && has) {  // a crowded outer cluster: in order, on this lane
+      int64_t out = first;
+      for (int b = 0; b < s.n_out; ++b) {
+        const int32_t j = s.j0 + b;
+        const itsu_tracklet t2 = a.tracklets[j];
+        float3 normal;
+        float curvature;
+        if (cell_precut(s.layer, s.t1_tan_lambda, s.t1_phi, t2.tan_lambda, t2.phi, s.c1, s.vz) &&
+            cell_geometry(s.layer, s.c1, s.c2, a.xyzr[s.c3_base + t2.second_cluster], s.vx, s.vy, normal, curvature)) {
+          write_cell(a, out++, s, t2, j, normal, curvature);
         }
       }
     }
-    if (!kWrite) {
-      a.cell_count[k] = count;
-    } else {
-      const int32_t first = a.cell_off[k];
-      a.cell_lookup[k] = (layer >= 1 && layer < ITSU_CELL_LAYERS && a.cell_off[k + 1] > first)
-                             ? first - a.cell_seg[e * ITSU_CELL_LAYERS + layer]
-                             : ITSU_UNUSED_INDEX;
+    if (k < n) {
+      const int sid = a.trk_seg_id[k];
+      const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
+      a.cell_lookup[k] = (layer >= 1 && layer < ITSU_CELL_LAYERS && has) ? first - a.cell_seg[e * ITSU_CELL_LAYERS + layer]
+                                                                         : ITSU_UNUSED_INDEX;
     }
   }
 }
@@ -935,22 +1369,34 @@ void step_cluster_sort(const Arena &a, const Launch &l)
   }
 }
 
-template <bool kWrite>
-void step_tracklets(const Arena &a, const Launch &l)
+void step_tracklets_count(const Arena &a, const Launch &l)
 {
   const int64_t blocks = (a.n_clusters + kThreads - 1) / kThreads;
   if (blocks > 0) {
-    k_tracklets<kWrite><<<(unsigned)blocks, kThreads, 0, l.stream>>>(a);
+    k_tracklets_count<<<(unsigned)blocks, kThreads, 0, l.stream>>>(a);
   }
 }
+
+void step_tracklets_write(const Arena &a, const Launch &l) { k_tracklets_write<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+
+void step_tracklets_tail(const Arena &a, const Launch &l)
+{
+  const int64_t blocks = (a.n_clusters + kThreads - 1) / kThreads;
+  if (blocks > 0) {
+    k_tracklets_tail<<<(unsigned)blocks, kThreads, 0, l.stream>>>(a);
+  }
+}
+
+void step_tracklet_index(const Arena &a, const Launch &l) { k_tracklet_index<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
 
 void step_tracklet_segments(const Arena &a, const Launch &l)
 {
   k_tracklet_segments<<<(a.n_events * ITSU_TRACKLET_LAYERS + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
 }
 
-template <bool kWrite>
-void step_cells(const Arena &a, const Launch &l) { k_cells<kWrite><<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+void step_cells_count(const Arena &a, const Launch &l) { k_cells_count<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+
+void step_cells_write(const Arena &a, const Launch &l) { k_cells_write<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
 
 void step_cell_segments(const Arena &a, const Launch &l)
 {
@@ -978,18 +1424,20 @@ void step_roads(const Arena &a, const Launch &l) { k_roads<<<fixed_grid(l), kThr
 const KernelStep kSteps[] = {
     {"status_init", step_status_init},                   // 0
     {"cluster_sort", step_cluster_sort},                 // 1  (a)
-    {"tracklets_count", step_tracklets<false>},          // 2  (b)
+    {"tracklets_count", step_tracklets_count},           // 2  (b)
     {"scan_reduce_tracklets", step_scan_reduce<0>},      // 3
     {"scan_partials_tracklets", step_scan_partials<0>},  // 4
     {"scan_apply_tracklets", step_scan_apply<0>},        // 5
     {"tracklet_segments", step_tracklet_segments},       // 6
-    {"tracklets_write", step_tracklets<true>},           // 7
-    {"cells_count", step_cells<false>},                  // 8  (c)
+    {"tracklets_write", step_tracklets_write},           // 7
+    {"tracklets_tail", step_tracklets_tail},             // 8
+    {"tracklet_index", step_tracklet_index},             // 9
+    {"cells_count", step_cells_count},                     // 8  (c)
     {"scan_reduce_cells", step_scan_reduce<1>},          // 9
     {"scan_partials_cells", step_scan_partials<1>},      // 10
     {"scan_apply_cells", step_scan_apply<1>},            // 11
     {"cell_segments", step_cell_segments},               // 12
-    {"cells_write", step_cells<true>},                   // 13
+    {"cells_write", step_cells_write},                    // 13
     {"neighbour_reset", step_neighbour_reset},           // 14 (d)
     {"neighbours_count", step_neighbours<false>},        // 15
     {"scan_reduce_neighbours", step_scan_reduce<2>},     // 16
@@ -1027,13 +1475,13 @@ const KernelStep *pipeline_steps(int *count)
 void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l); }
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
-void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 7, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(8, 12, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(13, 13, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(14, 19, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(20, 24, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(25, 28, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(29, 29, a, l); }
+void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 9, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(10, 14, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 15, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
 
 int kernels_per_run() { return kNumSteps; }
 
