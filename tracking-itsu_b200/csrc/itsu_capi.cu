@@ -64,8 +64,7 @@ struct itsu_context {
   itsu_tracklet *tracklets = nullptr;
   int32_t *trk_seg_id = nullptr, *cell_count = nullptr, *cell_off = nullptr, *cell_lookup = nullptr;
   unsigned long long *cell_mask = nullptr;
-  float *trk_tl = nullptr, *tl_key = nullptr;
-  uint8_t *tl_perm = nullptr;
+  float *trk_tl = nullptr;
   // cell class
   itsu_cell *cells = nullptr;
   int32_t *cell_seg_id = nullptr, *nb_count = nullptr, *nb_off = nullptr, *nb_fill = nullptr, *road_count = nullptr,
@@ -160,14 +159,13 @@ Arena arena_of(const itsu_context *ctx)
   a.seg_regular = ctx->seg_regular;
   a.trk_count = ctx->trk_count;
   a.trk_slots = ctx->trk_slots;
+  a.slot_stride = ctx->cap_clusters;
   a.trk_off = ctx->trk_off;
   a.trk_lookup = ctx->trk_lookup;
   a.trk_seg = ctx->trk_seg;
   a.tracklets = ctx->tracklets;
   a.trk_seg_id = ctx->trk_seg_id;
   a.trk_tl = ctx->trk_tl;
-  a.tl_key = ctx->tl_key;
-  a.tl_perm = ctx->tl_perm;
   a.cell_count = ctx->cell_count;
   a.cell_mask = ctx->cell_mask;
   a.cell_off = ctx->cell_off;
@@ -265,8 +263,6 @@ itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
     ITSU_CUDA(ctx, alloc(ctx->cell_count, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->cell_mask, cap));
     ITSU_CUDA(ctx, alloc(ctx->trk_tl, cap));
-    ITSU_CUDA(ctx, alloc(ctx->tl_key, cap));
-    ITSU_CUDA(ctx, alloc(ctx->tl_perm, cap));
     ITSU_CUDA(ctx, alloc(ctx->cell_off, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->cell_lookup, cap));
     ctx->cap_tracklets = cap;
@@ -695,7 +691,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->seg_rrange); release(ctx->seg_regular);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
-  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->trk_tl); release(ctx->tl_key); release(ctx->tl_perm); release(ctx->cell_off); release(ctx->cell_lookup);
+  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->trk_tl); release(ctx->cell_off); release(ctx->cell_lookup);
   release(ctx->cells); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);

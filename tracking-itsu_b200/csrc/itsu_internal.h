@@ -64,15 +64,14 @@ struct Arena {
   int32_t *seg_regular;
   // tracklets
   int32_t *trk_count;
-  int32_t *trk_slots;  // per inner cluster, the first outer clusters of its tracklets (count pass)
+  int32_t *trk_slots;  // slot n of inner cluster i at n * slot_stride + i: the outer clusters of its first tracklets
+  int64_t slot_stride;
   int32_t *trk_off;
   int32_t *trk_lookup;
   int32_t *trk_seg;
   itsu_tracklet *tracklets;
   int32_t *trk_seg_id;
-  float *trk_tl;     // tan(lambda) of each tracklet, compact
-  float *tl_key;     // per cluster, its outgoing tracklets' tan(lambda) sorted (cell pruning index)
-  uint8_t *tl_perm;  // ... and each one's position in the cluster's outgoing range
+  float *trk_tl;     // tan(lambda) of each tracklet, compact (the cell stage's slope window)
   // cells
   int32_t *cell_count;
   unsigned long long *cell_mask;  // per first tracklet: which outgoing tracklets make cells

@@ -444,24 +444,28 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   atomicMin(&s_rmin, rmin);
   atomicMax(&s_rmax, rmax);
   for (int b = tid; b < kTableBins; b += kSortThreads) {
-    const int cnt = bucket_total[b + 1], st = bucket_base[b + 1];
-    if (cnt > kMaxPruneBin) {
+    if (bucket_total[b + 1] > kMaxPruneBin) {
       atomicOr(&s_irregular, 1);
+    }
+  }
+  // each cluster's rank in its bin by (z, sorted index)
+  for (int i = tid; i < n; i += kSortThreads) {
+    const int bin = a.sorted[begin + i].bin;
+    if (bin < 0 || bin >= kTableBins) {
       continue;
     }
-    float *zz = a.zs_z + begin + st;
-    int32_t *jj = a.zs_j + begin + st;
-    for (int k = 0; k < cnt; ++k) {  // insertion by (z, index): equal z keep index order
-      const float z = a.xyzr[begin + st + k].z;
-      int p = k;
-      while (p > 0 && zz[p - 1] > z) {
-        zz[p] = zz[p - 1];
-        jj[p] = jj[p - 1];
-        --p;
-      }
-      zz[p] = z;
-      jj[p] = st + k;
+    const int st = bucket_base[bin + 1], cnt = bucket_total[bin + 1];
+    if (cnt > kMaxPruneBin) {
+      continue;
     }
+    const float z = a.xyzr[begin + i].z;
+    int rank = 0;
+    for (int k = 0; k < cnt; ++k) {
+      const float zk = a.xyzr[begin + st + k].z;
+      rank += zk < z || (zk == z && st + k < i);
+    }
+    a.zs_z[begin + st + rank] = z;
+    a.zs_j[begin + st + rank] = i;
   }
   __syncthreads();
   if (tid == 0) {
@@ -680,10 +684,9 @@ __global__ void __launch_bounds__(kThreads) k_tracklets_count(Arena a)
   const InnerCluster s = inner_cluster(a, i);
   int count = 0;
   if (s.walk) {
-    int32_t *slots = a.trk_slots + i * kTrackletSlots;
     walk_inner(a, s, [&](int j) {
       if (count < kTrackletSlots) {
-        slots[count] = j;
+        a.trk_slots[count * a.slot_stride + i] = j;
       }
       ++count;
     });
@@ -719,7 +722,7 @@ __global__ void __launch_bounds__(kThreads) k_tracklets_write(Arena a)
     const int r = (int)(k - a.trk_off[i]);
     const int seg_t = find_segment(a.trk_seg, a.n_events * ITSU_TRACKLET_LAYERS, k);
     const int seg = seg_t + seg_t / ITSU_TRACKLET_LAYERS;  // (e, L) as a cluster segment: 7e + L
-    write_tracklet(a, (int)k, i, a.layer_off[seg + 1] + a.trk_slots[i * kTrackletSlots + r], seg);
+    write_tracklet(a, (int)k, i, a.layer_off[seg + 1] + a.trk_slots[r * a.slot_stride + i], seg);
   }
 }
 
@@ -745,39 +748,6 @@ __global__ void __launch_bounds__(kThreads) k_tracklets_tail(Arena a)
     const InnerCluster s = inner_cluster(a, i);
     int out = first;
     walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, seg); });
-  }
-}
-
-// The cell stage's pruning index: the outgoing tracklets of each cluster (at most kMaxMaskedOut)
-// sorted by tan(lambda), with each one's position in the cluster's range. NaN slopes (two
-// clusters at equal r) sort last; they never pass a cut.
-__device__ __forceinline__ bool tl_before(float a, float b) { return a < b || (!isnan(a) && isnan(b)); }
-
-__global__ void __launch_bounds__(kThreads) k_tracklet_index(Arena a)
-{
-  if (capacity_failed(a.status)) {
-    return;
-  }
-  const int64_t n = a.status->total[kTracklets];
-  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
-    // the cluster whose outgoing range holds tracklet k is its first cluster
-    const int sid = a.trk_seg_id[k];
-    const int seg = sid + sid / ITSU_TRACKLET_LAYERS;
-    const int64_t c = a.layer_off[seg] + a.tracklets[k].first_cluster;
-    const int32_t j0 = a.trk_off[c];
-    const int cnt = a.trk_off[c + 1] - j0;
-    if (cnt > kMaxMaskedOut) {
-      continue;
-    }
-    const int q = (int)(k - j0);
-    const float v = a.trk_tl[k];
-    int rank = 0;  // slopes before this one, ties in range order
-    for (int p = 0; p < cnt; ++p) {
-      const float w = a.trk_tl[j0 + p];
-      rank += tl_before(w, v) || (!tl_before(v, w) && p < q);
-    }
-    a.tl_key[j0 + rank] = v;
-    a.tl_perm[j0 + rank] = (uint8_t)q;
   }
 }
 
@@ -864,6 +834,15 @@ __device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t
   return s;
 }
 
+// Position of the r-th (from 0) set bit of m (m has more than r set bits).
+__device__ __forceinline__ int nth_set_bit(unsigned long long m, int r)
+{
+  for (int q = 0; q < r; ++q) {
+    m &= m - 1ull;
+  }
+  return __ffsll((long long)m) - 1;
+}
+
 __device__ __forceinline__ float4 shfl4(float4 v, int src)
 {
   return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
@@ -936,24 +915,21 @@ __global__ void __launch_bounds__(kThreads) k_cells_count(Arena a)
     const CellLane s = cell_lane(a, base + lane, n);
     const bool big = s.n_out > kMaxMaskedOut;
     // Only outgoing tracklets with |dtanL| < 0.025 can pass (Tracker.cxx:161-166): |fl(t1 - t2)|
-    // < 0.025f implies |t1 - t2| < 0.025f exactly, so the window is read off the slope-sorted
-    // index with binary64 bounds (widened by 1e-12).
-    int q0 = 0, q1 = 0;
+    // < 0.025f implies |t1 - t2| < 0.025f exactly. The lane marks its window with binary64 bounds
+    // (widened by 1e-12) from the compact slopes, one independent load per outgoing tracklet.
+    unsigned long long window = 0;
     if (!big && s.n_out > 0 && isfinite(s.t1_tan_lambda)) {
-      const float *key = a.tl_key + s.j0;
+      const float *tl = a.trk_tl + s.j0;
       const double lo_d = (double)s.t1_tan_lambda - (double)kCellMaxDeltaTanLambda - 1e-12;
       const double hi_d = (double)s.t1_tan_lambda + (double)kCellMaxDeltaTanLambda + 1e-12;
-      // the keys are sorted (NaN last): count those below the window and those inside it with
-      // independent loads rather than a chain of dependent binary-search steps
       for (int q = 0; q < s.n_out; ++q) {
-        const double v = (double)key[q];
-        q0 += v < lo_d;
-        q1 += v <= hi_d;
+        const double v = (double)tl[q];
+        window |= (unsigned long long)(v >= lo_d && v <= hi_d) << q;
       }
     }
     masks[warp][lane] = 0ull;
     int total = 0;
-    const int excl = warp_exclusive_sum(q1 - q0, total);
+    const int excl = warp_exclusive_sum(__popcll(window), total);
     __syncwarp();
     int queued = 0;
     auto drain = [&](int count) {
@@ -973,7 +949,8 @@ __global__ void __launch_bounds__(kThreads) k_cells_count(Arena a)
     for (int p0 = 0; p0 < total; p0 += 32) {
       const int p = p0 + lane;
       const int owner = owner_of(excl, p);
-      const int q = __shfl_sync(0xffffffffu, q0, owner) + p - __shfl_sync(0xffffffffu, excl, owner);
+      const int r = p - __shfl_sync(0xffffffffu, excl, owner);
+      const unsigned long long wmask = __shfl_sync(0xffffffffu, window, owner);
       const float tl = __shfl_sync(0xffffffffu, s.t1_tan_lambda, owner);
       const float ph = __shfl_sync(0xffffffffu, s.t1_phi, owner);
       const float4 c1 = shfl4(s.c1, owner);
@@ -985,7 +962,7 @@ __global__ void __launch_bounds__(kThreads) k_cells_count(Arena a)
       int64_t c3 = 0;
       int b = 0;
       if (p < total) {
-        b = a.tl_perm[j0 + q];
+        b = nth_set_bit(wmask, r);
         const itsu_tracklet t2 = a.tracklets[j0 + b];
         pre = cell_precut(layer, tl, ph, t2.tan_lambda, t2.phi, c1, vz);
         c3 = c3_base + t2.second_cluster;
@@ -1074,12 +1051,7 @@ __global__ void __launch_bounds__(kThreads) k_cells_write(Arena a)
       o.t2_base = __shfl_sync(0xffffffffu, s.t2_base, owner);
       const int64_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
       if (p < total) {
-        // the r-th (from 0) set bit of the owner's mask
-        unsigned long long rest = m;
-        for (int q = 0; q < r; ++q) {
-          rest &= rest - 1ull;
-        }
-        const int b = __ffsll((long long)rest) - 1;
+        const int b = nth_set_bit(m, r);
         const int32_t j = j0 + b;
         const itsu_tracklet t2 = a.tracklets[j];
         float3 normal;
@@ -1387,8 +1359,6 @@ void step_tracklets_tail(const Arena &a, const Launch &l)
   }
 }
 
-void step_tracklet_index(const Arena &a, const Launch &l) { k_tracklet_index<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
-
 void step_tracklet_segments(const Arena &a, const Launch &l)
 {
   k_tracklet_segments<<<(a.n_events * ITSU_TRACKLET_LAYERS + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
@@ -1431,7 +1401,6 @@ const KernelStep kSteps[] = {
     {"tracklet_segments", step_tracklet_segments},       // 6
     {"tracklets_write", step_tracklets_write},           // 7
     {"tracklets_tail", step_tracklets_tail},             // 8
-    {"tracklet_index", step_tracklet_index},             // 9
     {"cells_count", step_cells_count},                     // 8  (c)
     {"scan_reduce_cells", step_scan_reduce<1>},          // 9
     {"scan_partials_cells", step_scan_partials<1>},      // 10
@@ -1475,13 +1444,13 @@ const KernelStep *pipeline_steps(int *count)
 void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l); }
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
-void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 9, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(10, 14, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 15, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
+void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 13, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 14, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(15, 20, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(21, 25, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(26, 29, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(30, 30, a, l); }
 
 int kernels_per_run() { return kNumSteps; }
 
