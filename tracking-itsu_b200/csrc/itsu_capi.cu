@@ -65,6 +65,7 @@ struct itsu_context {
   int32_t *trk_seg_id = nullptr, *cell_count = nullptr, *cell_off = nullptr, *cell_lookup = nullptr;
   unsigned long long *cell_mask = nullptr;
   float *trk_tl = nullptr;
+  int32_t *trk_owner = nullptr;
   // cell class
   itsu_cell *cells = nullptr;
   int32_t *cell_seg_id = nullptr, *nb_count = nullptr, *nb_off = nullptr, *nb_fill = nullptr, *road_count = nullptr,
@@ -166,6 +167,7 @@ Arena arena_of(const itsu_context *ctx)
   a.tracklets = ctx->tracklets;
   a.trk_seg_id = ctx->trk_seg_id;
   a.trk_tl = ctx->trk_tl;
+  a.trk_owner = ctx->trk_owner;
   a.cell_count = ctx->cell_count;
   a.cell_mask = ctx->cell_mask;
   a.cell_off = ctx->cell_off;
@@ -263,6 +265,7 @@ itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
     ITSU_CUDA(ctx, alloc(ctx->cell_count, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->cell_mask, cap));
     ITSU_CUDA(ctx, alloc(ctx->trk_tl, cap));
+    ITSU_CUDA(ctx, alloc(ctx->trk_owner, cap));
     ITSU_CUDA(ctx, alloc(ctx->cell_off, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->cell_lookup, cap));
     ctx->cap_tracklets = cap;
@@ -691,7 +694,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->seg_rrange); release(ctx->seg_regular);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
-  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->trk_tl); release(ctx->cell_off); release(ctx->cell_lookup);
+  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->trk_tl); release(ctx->trk_owner); release(ctx->cell_off); release(ctx->cell_lookup);
   release(ctx->cells); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);

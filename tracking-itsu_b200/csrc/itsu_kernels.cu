@@ -694,41 +694,10 @@ __global__ void __launch_bounds__(kThreads) k_tracklets_count(Arena a)
   a.trk_count[i] = count;
 }
 
-// Write pass, one thread per tracklet: its inner cluster is the last one whose scanned offset is
-// at or below the tracklet's slot, its outer cluster comes from the count pass's slots. All
-// tracklets of a warp compute their binary64 azimuth together. Tracklets of inner clusters with
-// more than kTrackletSlots are written by k_tracklets_tail instead.
-__global__ void __launch_bounds__(kThreads) k_tracklets_write(Arena a)
-{
-  if (capacity_failed(a.status)) {
-    return;
-  }
-  const int64_t n = a.status->total[kTracklets];
-  const int nc = (int)a.n_clusters;
-  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
-    int lo = 0, hi = nc;  // trk_off[lo] <= k < trk_off[hi]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (a.trk_off[mid] <= k) {
-        lo = mid;
-      } else {
-        hi = mid;
-      }
-    }
-    const int64_t i = lo;
-    if (a.trk_count[i] > kTrackletSlots) {
-      continue;
-    }
-    const int r = (int)(k - a.trk_off[i]);
-    const int seg_t = find_segment(a.trk_seg, a.n_events * ITSU_TRACKLET_LAYERS, k);
-    const int seg = seg_t + seg_t / ITSU_TRACKLET_LAYERS;  // (e, L) as a cluster segment: 7e + L
-    write_tracklet(a, (int)k, i, a.layer_off[seg + 1] + a.trk_slots[r * a.slot_stride + i], seg);
-  }
-}
-
-// Per inner cluster: its entry of the tracklets lookup table (Tracker.cxx:102-108) and, for the
-// rare clusters with more than kTrackletSlots tracklets, the tracklets themselves, walked again
-// and written in order.
+// Per inner cluster, before the write pass: its entry of the tracklets lookup table
+// (Tracker.cxx:102-108) and, for each of its tracklet slots, the owner cluster and segment the
+// write pass reads. Clusters with more than kTrackletSlots tracklets (rare) walk their candidates
+// again here and write their tracklets in order.
 __global__ void __launch_bounds__(kThreads) k_tracklets_tail(Arena a)
 {
   if (capacity_failed(a.status)) {
@@ -744,10 +713,37 @@ __global__ void __launch_bounds__(kThreads) k_tracklets_tail(Arena a)
   a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && count > 0)
                         ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
                         : ITSU_UNUSED_INDEX;
+  // every slot gets its owner (the write pass reads it for every tracklet)
+  const int sid = e * ITSU_TRACKLET_LAYERS + layer;
+  for (int r = 0; r < count; ++r) {
+    a.trk_owner[first + r] = (int32_t)i;
+    a.trk_seg_id[first + r] = sid;
+  }
   if (count > kTrackletSlots) {
     const InnerCluster s = inner_cluster(a, i);
     int out = first;
     walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, seg); });
+  }
+}
+
+// Write pass, one thread per tracklet (owner and segment filled in by k_tracklets_tail, outer
+// cluster kept by the count pass): all tracklets of a warp compute their binary64 azimuth
+// together. Tracklets of crowded clusters were written by k_tracklets_tail.
+__global__ void __launch_bounds__(kThreads) k_tracklets_write(Arena a)
+{
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int64_t n = a.status->total[kTracklets];
+  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
+    const int64_t i = a.trk_owner[k];
+    const int32_t first = a.trk_off[i];
+    if (a.trk_off[i + 1] - first > kTrackletSlots) {
+      continue;
+    }
+    const int sid = a.trk_seg_id[k];
+    const int seg = sid + sid / ITSU_TRACKLET_LAYERS;  // (e, L) as a cluster segment: 7e + L
+    write_tracklet(a, (int)k, i, a.layer_off[seg + 1] + a.trk_slots[(k - first) * a.slot_stride + i], seg);
   }
 }
 
@@ -1399,8 +1395,8 @@ const KernelStep kSteps[] = {
     {"scan_partials_tracklets", step_scan_partials<0>},  // 4
     {"scan_apply_tracklets", step_scan_apply<0>},        // 5
     {"tracklet_segments", step_tracklet_segments},       // 6
-    {"tracklets_write", step_tracklets_write},           // 7
-    {"tracklets_tail", step_tracklets_tail},             // 8
+    {"tracklets_tail", step_tracklets_tail},             // 7
+    {"tracklets_write", step_tracklets_write},           // 8
     {"cells_count", step_cells_count},                     // 8  (c)
     {"scan_reduce_cells", step_scan_reduce<1>},          // 9
     {"scan_partials_cells", step_scan_partials<1>},      // 10
