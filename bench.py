@@ -54,7 +54,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--events", type=int, default=128, help="events per step per GPU")
+    ap.add_argument("--events", type=int, default=128, help="events per step per GPU (pbpb, uneven)")
+    ap.add_argument("--workload", choices=("pbpb", "uneven", "pileup"), default="pbpb",
+                    help="pbpb: central Pb-Pb-like events, 6000 tracks (the headline); uneven: log-uniform "
+                         "20-8000 tracks; pileup: frames of 5 collisions of ~1500 tracks, 10%% noise")
+    ap.add_argument("--frames", type=int, default=32, help="pile-up frames per step per GPU")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -109,6 +113,13 @@ def sum_over_ranks(dist, value, device=None):
 
 def make_events(n, seed):
     return [gen.pbpb_event(seed * 100000 + i, TRACKS) for i in range(n)]
+
+
+WORKLOADS = {
+    "pbpb": "pbpb_central_6000trk_5pct_noise",
+    "uneven": "uneven_batch_loguniform_20_8000trk_5pct_noise",
+    "pileup": "pileup_frames_5x1500trk_10pct_noise",
+}
 
 
 def algorithmic_bytes(counts) -> dict:
@@ -310,8 +321,19 @@ def run_ours(args):
     device = torch.device("cuda", local)
     from itsu import capi
 
-    events = make_events(args.events, args.seed + 7919 * rank)
-    clusters, offsets, vertices = gen.pack_batch(events)
+    seed = args.seed + 7919 * rank
+    frames = None
+    if args.workload == "pileup":
+        frames = gen.pileup_stream(seed, args.frames, collisions=5, n_tracks=1500)
+        events = [ev for ev in frames for _ in ev.vertices]
+        f_clusters, f_offsets, f_vertices, f_vertex_frame = gen.pack_frames(frames)
+        clusters, offsets, vertices = gen.pack_batch(events, [iv for ev in frames for iv in range(len(ev.vertices))])
+    elif args.workload == "uneven":
+        events = gen.batch_events(seed, n_events=args.events)
+        clusters, offsets, vertices = gen.pack_batch(events)
+    else:
+        events = make_events(args.events, seed)
+        clusters, offsets, vertices = gen.pack_batch(events)
     n_events, n_clusters = len(events), len(clusters)
 
     # device-resident inputs (torch owns the memory; the library only reads it)
@@ -322,7 +344,13 @@ def run_ours(args):
     ctx = capi.Context(device=local)
     ctx.set_stream(stream.cuda_stream)
     batch = ctx.batch_device(d_clusters.data_ptr(), d_offsets.data_ptr(), d_vertices.data_ptr(), n_events, n_clusters)
-    ctx.batch_run(batch)  # sizes the arena, validates the inputs, captures the graph
+    if frames is not None:
+        # frames: the raw clusters of a frame are resident once and shared by its vertices
+        ctx.frames_run_host(f_clusters, f_offsets, f_vertices, f_vertex_frame)
+        launch = ctx.relaunch
+    else:
+        ctx.batch_run(batch)  # sizes the arena, validates the inputs, captures the graph
+        launch = lambda: ctx.batch_launch(batch)  # noqa: E731
     counts = []
     for e in range(n_events):
         c = ctx.counts(e)
@@ -330,7 +358,7 @@ def run_ours(args):
     total_roads = sum(c["R"] for c in counts)
 
     for _ in range(args.warmup):
-        ctx.batch_launch(batch)
+        launch()
     stream.synchronize()
     kernels = ctx.lib.itsu_kernels_per_run()
 
@@ -343,7 +371,7 @@ def run_ours(args):
         clocks.mark_start()
         start.record(stream)
         for _ in range(args.steps):
-            ctx.batch_launch(batch)
+            launch()
         end.record(stream)
         torch.cuda.synchronize()
         clocks.mark_end()
@@ -371,6 +399,24 @@ def run_ours(args):
                                          ctypes.c_void_p(h_vertices.data_ptr()), n_events, ctypes.c_void_p(h_roads.data_ptr()),
                                          roads_cap, ctypes.c_void_p(h_road_off.data_ptr()))
         ctx._check(st)
+
+    if frames is not None:
+        from itsu.capi import Frames
+
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).pin_memory()  # noqa: E731
+        hf = [pin(f_clusters), pin(f_offsets), pin(f_vertices), pin(f_vertex_frame)]
+        fr = Frames()
+        fr.clusters, fr.frame_offsets, fr.vertices, fr.vertex_frame = (t.data_ptr() for t in hf)
+        fr.n_frames, fr.n_vertices = len(frames), n_events
+        h_clusters = hf[0]
+        h2d_bytes = sum(t.numel() for t in hf)
+
+        def host_run():  # noqa: F811
+            st = ctx.lib.itsu_frames_run_host(ctx.h, ctypes.byref(fr), ctypes.c_void_p(h_roads.data_ptr()), roads_cap,
+                                              ctypes.c_void_p(h_road_off.data_ptr()))
+            ctx._check(st)
+    else:
+        h2d_bytes = int(clusters.nbytes + offsets.nbytes + vertices.nbytes)
 
     for _ in range(max(1, args.warmup)):
         host_run()
@@ -410,6 +456,19 @@ def run_ours(args):
     except (OSError, ValueError):
         pass
 
+    # plain path, one vertex per call (itsu_clusters_to_tracks, host in / host out, synchronous),
+    # the way the reference's Tracker::clustersToTracks is driven event by event
+    single = events[: min(16, len(events))]
+    ctx1 = capi.Context(device=local)
+    ctx1.set_stream(stream.cuda_stream)
+    for ev in single[:2]:
+        ctx1.clusters_to_tracks(ev.layers, ev.vertices[0])
+    t0 = time.perf_counter()
+    for ev in single:
+        ctx1.clusters_to_tracks(ev.layers, ev.vertices[0])
+    single_eps = len(single) / (time.perf_counter() - t0)
+    ctx1.close()
+
     total_events = sum_over_ranks(dist, n_events * args.steps, device)
     value = total_events / (ms * 1e-3)
     e2e_value = total_events / (e2e_ms * 1e-3)
@@ -432,26 +491,32 @@ def run_ours(args):
             "dtype": "f32",
             "data": "synthetic (seeded helix generator, reference geometry; no public dataset)",
             "config": {
-                "workload": WORKLOAD,
+                "workload": WORKLOADS[args.workload],
                 "events_per_step_per_gpu": n_events,
-                "tracks_per_event": TRACKS,
+                "tracks_per_event": TRACKS if args.workload == "pbpb" else ("log-uniform 20-8000" if args.workload == "uneven" else "5 collisions x 1050-1950"),
+                "frames_per_step_per_gpu": len(frames) if frames is not None else None,
                 "clusters_per_step_per_gpu": n_clusters,
                 "tracklets_per_step_per_gpu": int(sum(sum(c["T"]) for c in counts)),
                 "cells_per_step_per_gpu": int(sum(sum(c["C"]) for c in counts)),
                 "roads_per_step_per_gpu": int(total_roads),
-                "mode": "batched plain path, one CUDA graph per step",
+                "mode": "batched plain path, one CUDA graph per step" + ("; frames: raw clusters resident once per frame" if frames is not None else ""),
                 "parallelism": "event shards, one rank per GPU" if world > 1 else "single GPU",
                 "l2": "inputs larger than L2 (%.0f MB raw clusters, %.0f MB tracklets per step), no flush" % (
                     clusters.nbytes / 1e6, 16 * sum(sum(c["T"]) for c in counts) / 1e6),
             },
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(clusters.nbytes + offsets.nbytes + vertices.nbytes),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d_bytes),
                     "d2h_bytes_per_step": int(32 * total_roads + 4 * (n_events + 1)),
-                    "api": "itsu_batch_run_host (pinned host buffers)"},
+                    "api": ("itsu_frames_run_host" if frames is not None else "itsu_batch_run_host") + " (pinned host buffers)"},
             "gpu_launches": kernels * args.steps,
             "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "algorithmic_bytes_per_launch": step_bytes.get(stage), "launch_ms": top_ms,
                          "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_src if peak_src == "measured" else "fallback 6.65 TB/s"},
+            "modes": {
+                "batched_plain_events_per_s": value,
+                "plain_single_event_events_per_s": single_eps,
+                "plain_single_event_note": "itsu_clusters_to_tracks, one vertex per synchronous call, host in/out, wall clock",
+            },
             "kernel_ms": {name: round(t, 4) for name, t in prof},
             "algorithmic_bytes_per_step": step_bytes.get("event"),
             "achieved_gbs_whole_step": step_bytes.get("event") / (ms / args.steps * 1e-3) / 1e9,

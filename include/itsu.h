@@ -201,6 +201,28 @@ itsu_status itsu_batch_status(itsu_context *ctx);
 /* Device pointer to the roads of the last batch (event-major) and to road_offsets[n_events+1]. */
 itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, const int32_t **road_offsets);
 
+/* ---- pile-up frames: several primary vertices over the same clusters ----
+ * The reference tracks every vertex of an event over all of the event's clusters, running the
+ * whole per-vertex sequence once per vertex (Tracker<IsGPU>::clustersToTracks, Tracker.cxx:251-262;
+ * the pile-up merger of benchmarks/scripts/root/generatePileUpData.cxx builds such events).
+ * Here each frame's clusters are uploaded once and every vertex becomes one run of the batch:
+ * run v tracks vertex v over frame vertex_frame[v]. Host in / host out; per-run results through
+ * itsu_get_counts / itsu_copy_results with event = v. */
+typedef struct itsu_frames {
+  const itsu_cluster *clusters; /* host: raw clusters, frame-major then layer-major */
+  const int32_t *frame_offsets; /* host: n_frames*7 + 1 offsets into clusters */
+  const float *vertices;        /* host: n_vertices*3 */
+  const int32_t *vertex_frame;  /* host: n_vertices frame indices */
+  int32_t n_frames;
+  int32_t n_vertices;
+} itsu_frames;
+itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, itsu_road *roads, int64_t roads_capacity,
+                                 int32_t *road_offsets);
+
+/* Replays the whole sequence of the last run (any entry point) on the inputs already in device
+ * memory, without waiting; itsu_batch_status waits and reports. */
+itsu_status itsu_relaunch(itsu_context *ctx);
+
 /* ---- instrumentation (no counterpart in the reference beyond its clock() stage timers,
  *      src/CA/Tracker.cxx:655-684) ---- */
 typedef struct itsu_kernel_time {

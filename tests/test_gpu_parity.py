@@ -175,3 +175,26 @@ def test_results_after_each_stage(ctx):
         _assert_same(got, want, "all stages")
     finally:
         fresh.close()
+
+
+def test_pileup_frames_share_their_clusters(ctx):
+    """Frames API: every vertex of a frame runs over the frame's clusters uploaded once; each run
+    equals the oracle on that vertex and the roads equal the duplicated-batch path's."""
+    frames = gen.pileup_stream(17, n_frames=3, collisions=3, n_tracks=250)
+    clusters, offsets, vertices, vertex_frame = gen.pack_frames(frames)
+    roads, road_off = ctx.frames_run_host(clusters, offsets, vertices, vertex_frame)
+    runs = [(ev, iv) for ev in frames for iv in range(len(ev.vertices))]
+    assert len(road_off) == len(runs) + 1
+    for v, (ev, iv) in enumerate(runs):
+        want = oracle.run_vertex(ev.layers, ev.vertices[iv])
+        _assert_same(ctx.results(v), want, "frame run %d" % v)
+    b_clusters, b_offsets, b_vertices = gen.pack_batch([ev for ev, _ in runs], [iv for _, iv in runs])
+    b_roads, b_off = ctx.batch_run_host(b_clusters, b_offsets, b_vertices)
+    assert np.array_equal(b_off, road_off)
+    assert np.array_equal(b_roads.view(np.uint8), roads.view(np.uint8))
+    # the device-resident replay of the same frames gives the same roads
+    ctx.frames_run_host(clusters, offsets, vertices, vertex_frame)
+    ctx.relaunch()
+    ctx.batch_status()
+    again = ctx.results(len(runs) - 1)
+    _assert_same(again, oracle.run_vertex(runs[-1][0].layers, runs[-1][0].vertices[runs[-1][1]]), "replay")

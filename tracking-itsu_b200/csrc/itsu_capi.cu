@@ -83,7 +83,9 @@ struct itsu_context {
   int64_t n_clusters = 0;
   std::vector<int32_t> h_layer_off;
   const itsu_cluster *in_raw = nullptr;
+  const int32_t *in_raw_off = nullptr;
   const int32_t *in_layer_off = nullptr;
+  int32_t *raw_off = nullptr;  // arena copy of a frames run's raw offsets (event class)
   const float *in_vtx = nullptr;
   int stage = kNone;
 
@@ -91,7 +93,7 @@ struct itsu_context {
   cudaGraphExec_t graph = nullptr;
   uint64_t graph_generation = 0;
   uint64_t generation = 1;  // bumped whenever a buffer is reallocated
-  const void *graph_key[3] = {nullptr, nullptr, nullptr};
+  const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t graph_events = -1;
   int64_t graph_clusters = -1;
 
@@ -147,6 +149,7 @@ Arena arena_of(const itsu_context *ctx)
   a.n_events = ctx->n_events;
   a.n_clusters = ctx->n_clusters;
   a.raw = ctx->in_raw;
+  a.raw_off = ctx->in_raw_off;
   a.layer_off = ctx->in_layer_off;
   a.vtx = ctx->in_vtx;
   a.sorted = ctx->sorted;
@@ -248,6 +251,7 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ITSU_CUDA(ctx, alloc(ctx->road_seg, (int64_t)cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->seg_rrange, (int64_t)cap * ITSU_LAYERS));
     ITSU_CUDA(ctx, alloc(ctx->seg_regular, (int64_t)cap * ITSU_LAYERS));
+    ITSU_CUDA(ctx, alloc(ctx->raw_off, (int64_t)cap * ITSU_LAYERS));
     ctx->cap_events = cap;
     ctx->generation++;
   }
@@ -408,6 +412,7 @@ itsu_status launch_all(itsu_context *ctx)
 {
   const bool same = ctx->graph && ctx->graph_generation == ctx->generation && ctx->graph_key[0] == ctx->in_raw &&
                     ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
+                    ctx->graph_key[3] == ctx->in_raw_off &&
                     ctx->graph_events == ctx->n_events && ctx->graph_clusters == ctx->n_clusters;
   if (!same) {
     drop_graph(ctx);
@@ -431,6 +436,7 @@ itsu_status launch_all(itsu_context *ctx)
     ctx->graph_key[0] = ctx->in_raw;
     ctx->graph_key[1] = ctx->in_layer_off;
     ctx->graph_key[2] = ctx->in_vtx;
+    ctx->graph_key[3] = ctx->in_raw_off;
     ctx->graph_events = ctx->n_events;
     ctx->graph_clusters = ctx->n_clusters;
   }
@@ -537,6 +543,7 @@ itsu_status upload_vertex(itsu_context *ctx, const itsu_cluster *const layers[IT
   ctx->n_clusters = off[ITSU_LAYERS];
   ctx->h_layer_off = off;
   ctx->in_raw = ctx->raw;
+  ctx->in_raw_off = nullptr;
   ctx->in_layer_off = ctx->layer_off;
   ctx->in_vtx = ctx->vtx;
   ctx->stage = kNone;
@@ -691,7 +698,7 @@ void itsu_context_destroy(itsu_context *ctx)
   drop_graph(ctx);
   release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
   release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs_z); release(ctx->zs_j); release(ctx->trk_slots);
-  release(ctx->seg_rrange); release(ctx->seg_regular);
+  release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
   release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->trk_tl); release(ctx->trk_owner); release(ctx->cell_off); release(ctx->cell_lookup);
@@ -917,6 +924,7 @@ static itsu_status set_batch(itsu_context *ctx, const itsu_batch *batch)
   ctx->n_events = batch->n_events;
   ctx->n_clusters = batch->n_clusters;
   ctx->in_raw = batch->clusters;
+  ctx->in_raw_off = nullptr;
   ctx->in_layer_off = batch->layer_offsets;
   ctx->in_vtx = batch->vertices;
   ctx->h_layer_off.resize((size_t)batch->n_events * ITSU_LAYERS + 1);
@@ -949,7 +957,8 @@ itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch)
   if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
   itsu_status st;
-  const bool same = batch && ctx->stage != kNone && batch->clusters == ctx->in_raw && batch->layer_offsets == ctx->in_layer_off &&
+  const bool same = batch && ctx->stage != kNone && !ctx->in_raw_off && batch->clusters == ctx->in_raw &&
+                    batch->layer_offsets == ctx->in_layer_off &&
                     batch->vertices == ctx->in_vtx && batch->n_events == ctx->n_events && batch->n_clusters == ctx->n_clusters;
   if (!same && (st = set_batch(ctx, batch)) != ITSU_OK) return st;
   if ((st = launch_all(ctx)) != ITSU_OK) return st;
@@ -1006,6 +1015,7 @@ itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters,
   ctx->n_events = n_events;
   ctx->n_clusters = n_clusters;
   ctx->in_raw = b.clusters;
+  ctx->in_raw_off = nullptr;
   ctx->in_layer_off = b.layer_offsets;
   ctx->in_vtx = b.vertices;
   ctx->h_layer_off.assign(layer_offsets, layer_offsets + (int64_t)n_events * ITSU_LAYERS + 1);
@@ -1021,6 +1031,78 @@ itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters,
   }
   ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ITSU_OK;
+}
+
+itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, itsu_road *roads, int64_t roads_capacity,
+                                 int32_t *road_offsets)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
+  if (!frames || frames->n_frames < 0 || frames->n_vertices < 0) return fail(ctx, ITSU_ERR_INVALID, "bad frames");
+  const int32_t nf = frames->n_frames, nv = frames->n_vertices;
+  if ((nf > 0 && !frames->frame_offsets) || (nv > 0 && (!frames->vertices || !frames->vertex_frame))) {
+    return fail(ctx, ITSU_ERR_INVALID, "null frames pointer");
+  }
+  const int32_t *fo = frames->frame_offsets;
+  const int64_t frame_clusters = nf > 0 ? fo[(int64_t)nf * ITSU_LAYERS] : 0;
+  if (nf > 0 && fo[0] != 0) return fail(ctx, ITSU_ERR_INVALID, "frame offsets must start at 0");
+  for (int64_t k = 1; k <= (int64_t)nf * ITSU_LAYERS; ++k) {
+    if (fo[k] < fo[k - 1]) return fail(ctx, ITSU_ERR_INVALID, "frame offsets decrease at %lld", (long long)k);
+  }
+  if (frame_clusters > 0 && !frames->clusters) return fail(ctx, ITSU_ERR_INVALID, "null clusters");
+  // one run per vertex over its frame's clusters: output layout per run, raw input shared
+  std::vector<int32_t> run_off((size_t)nv * ITSU_LAYERS + 1, 0), raw_off((size_t)nv * ITSU_LAYERS, 0);
+  int64_t total = 0;
+  for (int32_t v = 0; v < nv; ++v) {
+    const int32_t f = frames->vertex_frame[v];
+    if (f < 0 || f >= nf) return fail(ctx, ITSU_ERR_INVALID, "vertex %d names frame %d of %d", v, f, nf);
+    for (int l = 0; l < ITSU_LAYERS; ++l) {
+      const int64_t k = (int64_t)v * ITSU_LAYERS + l;
+      raw_off[k] = fo[(int64_t)f * ITSU_LAYERS + l];
+      run_off[k] = (int32_t)total;
+      total += fo[(int64_t)f * ITSU_LAYERS + l + 1] - fo[(int64_t)f * ITSU_LAYERS + l];
+      if (total > INT32_MAX) return fail(ctx, ITSU_ERR_INVALID, "too many clusters over all vertices");
+    }
+  }
+  run_off[(size_t)nv * ITSU_LAYERS] = (int32_t)total;
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu_status st;
+  if ((st = ensure_clusters(ctx, std::max(total, frame_clusters), nv)) != ITSU_OK) return st;
+  if ((st = ensure_outputs_for(ctx, total)) != ITSU_OK) return st;
+  if (frame_clusters > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw, frames->clusters, sizeof(itsu_cluster) * frame_clusters, cudaMemcpyHostToDevice,
+                                   ctx->stream));
+  }
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->layer_off, run_off.data(), sizeof(int32_t) * run_off.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if (nv > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw_off, raw_off.data(), sizeof(int32_t) * raw_off.size(), cudaMemcpyHostToDevice, ctx->stream));
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, frames->vertices, sizeof(float) * 3 * (int64_t)nv, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->n_events = nv;
+  ctx->n_clusters = total;
+  ctx->in_raw = ctx->raw;
+  ctx->in_raw_off = ctx->raw_off;
+  ctx->in_layer_off = ctx->layer_off;
+  ctx->in_vtx = ctx->vtx;
+  ctx->h_layer_off = run_off;
+  if ((st = run_all(ctx)) != ITSU_OK) return st;
+  const int64_t n_roads = ctx->h_status->total[itsu::kRoads];
+  if (road_offsets) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(road_offsets, ctx->road_seg, sizeof(int32_t) * ((int64_t)nv + 1), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (roads) {
+    if (n_roads > roads_capacity) return fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %lld given", (long long)n_roads, (long long)roads_capacity);
+    if ((st = copy_range(ctx, roads, (const itsu_road *)ctx->roads, n_roads)) != ITSU_OK) return st;
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+itsu_status itsu_relaunch(itsu_context *ctx)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kRoads, "itsu_relaunch")) != ITSU_OK) return st;
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  return launch_all(ctx);
 }
 
 int32_t itsu_kernels_per_run(void) { return itsu::kernels_per_run(); }

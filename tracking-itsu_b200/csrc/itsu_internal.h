@@ -48,6 +48,7 @@ struct Arena {
   int64_t n_clusters;
   // inputs
   const itsu_cluster *raw;
+  const int32_t *raw_off;  // per (run, layer): start of its raw clusters; null = same as layer_off
   const int32_t *layer_off;
   const float *vtx;
   // clustering

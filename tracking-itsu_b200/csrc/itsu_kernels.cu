@@ -283,6 +283,7 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
   const int64_t begin = a.layer_off[seg];
   const int n = (int)(a.layer_off[seg + 1] - begin);
+  const int64_t raw_begin = a.raw_off ? a.raw_off[seg] : begin;  // frames share raw clusters
   const float vx = a.vtx[3 * e], vy = a.vtx[3 * e + 1], vz = a.vtx[3 * e + 2];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   const int chunk = (n + kSortWarps - 1) / kSortWarps;
   const int wb = min(n, warp * chunk), we = min(n, wb + chunk);
   for (int i = wb + lane; i < we; i += 32) {
-    itsu_cluster c = a.raw[begin + i];
+    itsu_cluster c = a.raw[raw_begin + i];
     const Transformed t = transform_cluster(layer, c.x, c.y, c.z, vx, vy);
     c.phi = t.phi;
     c.r = t.r;

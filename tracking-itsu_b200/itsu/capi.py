@@ -59,6 +59,11 @@ class KernelTime(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 40), ("ms", ctypes.c_float), ("launches", ctypes.c_int32)]
 
 
+class Frames(ctypes.Structure):
+    _fields_ = [("clusters", ctypes.c_void_p), ("frame_offsets", ctypes.c_void_p), ("vertices", ctypes.c_void_p),
+                ("vertex_frame", ctypes.c_void_p), ("n_frames", ctypes.c_int32), ("n_vertices", ctypes.c_int32)]
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("clusters", ctypes.c_void_p), ("layer_offsets", ctypes.c_void_p), ("vertices", ctypes.c_void_p),
                 ("n_events", ctypes.c_int32), ("reserved_", ctypes.c_int32), ("n_clusters", ctypes.c_int64)]
@@ -95,6 +100,9 @@ SIGNATURES = [
     ("itsu_batch_status", ctypes.c_int, [ctypes.c_void_p]),
     ("itsu_batch_roads_device", ctypes.c_int,
      [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]),
+    ("itsu_frames_run_host", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(Frames), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
+    ("itsu_relaunch", ctypes.c_int, [ctypes.c_void_p]),
     ("itsu_kernels_per_run", ctypes.c_int32, []),
     ("itsu_pvc_initialize_noalloc", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -273,3 +281,26 @@ class Context:
         cnt = ctypes.c_int32()
         self._check(self.lib.itsu_batch_profile(self.h, repeats, arr, n, ctypes.byref(cnt)))
         return [(arr[k].name.decode(), float(arr[k].ms)) for k in range(cnt.value)]
+
+    def frames_run_host(self, clusters, frame_offsets, vertices, vertex_frame, roads_capacity=None):
+        """Pile-up frames: each frame's clusters once, one run per vertex; returns (roads, road_offsets)."""
+        clusters = np.ascontiguousarray(clusters, CLUSTER_DTYPE)
+        frame_offsets = np.ascontiguousarray(frame_offsets, np.int32)
+        vertices = np.ascontiguousarray(vertices, np.float32)
+        vertex_frame = np.ascontiguousarray(vertex_frame, np.int32)
+        f = Frames()
+        f.clusters, f.frame_offsets, f.vertices, f.vertex_frame = (_ptr(clusters).value, _ptr(frame_offsets).value,
+                                                                   _ptr(vertices).value, _ptr(vertex_frame).value)
+        f.n_frames, f.n_vertices = (len(frame_offsets) - 1) // 7, len(vertex_frame)
+        offs = np.zeros(f.n_vertices + 1, np.int32)
+        if roads_capacity is None:
+            self._check(self.lib.itsu_frames_run_host(self.h, ctypes.byref(f), None, 0, _ptr(offs)))
+            roads_capacity = int(offs[-1])
+        roads = np.zeros(roads_capacity, ROAD_DTYPE)
+        self._check(self.lib.itsu_frames_run_host(self.h, ctypes.byref(f), _ptr(roads), roads_capacity, _ptr(offs)))
+        roads = roads[: offs[-1]].copy()
+        roads["pad"] = 0
+        return roads, offs
+
+    def relaunch(self):
+        self._check(self.lib.itsu_relaunch(self.h))

@@ -252,3 +252,28 @@ def write_binary_events(events, path: str) -> None:
                 for k in ("x", "y", "z", "alpha", "mc"):
                     r[k] = l[k]
                 f.write(r.tobytes())
+
+
+def pack_frames(frames):
+    """Flatten pile-up frames for itsu_frames_run_host: clusters frame-major then layer-major,
+    frame_offsets[n_frames*7+1], vertices[n_vertices*3] and each vertex's frame index."""
+    counts = []
+    for ev in frames:
+        counts.extend(len(l) for l in ev.layers)
+    offsets = np.zeros(len(counts) + 1, np.int32)
+    np.cumsum(counts, out=offsets[1:])
+    clusters = np.concatenate([l for ev in frames for l in ev.layers]) if counts else np.zeros(0, CLUSTER_DTYPE)
+    vertices = np.concatenate([ev.vertices for ev in frames]).astype(np.float32).reshape(-1)
+    vertex_frame = np.concatenate([np.full(len(ev.vertices), f, np.int32) for f, ev in enumerate(frames)])
+    return clusters, offsets, vertices, vertex_frame
+
+
+def pileup_stream(seed: int, n_frames: int, collisions: int = 5, n_tracks: int = 1500, spread: float = 0.3) -> list:
+    """Pile-up frames of uneven size: each collision's multiplicity is drawn uniformly within
+    +-spread of n_tracks."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for f in range(n_frames):
+        m = int(rng.integers(int(n_tracks * (1 - spread)), int(n_tracks * (1 + spread)) + 1))
+        out.append(make_event(seed * 1000003 + f, m, pt_mean=0.6, noise=0.10, n_vertices=collisions))
+    return out
