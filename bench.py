@@ -62,6 +62,7 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     return ap.parse_args()
 
 
@@ -351,6 +352,10 @@ def run_ours(args):
     else:
         ctx.batch_run(batch)  # sizes the arena, validates the inputs, captures the graph
         launch = lambda: ctx.batch_launch(batch)  # noqa: E731
+    tune = None
+    if not args.no_autotune:
+        # the batched form's autotuner: launch shape for this multiplicity band (untimed)
+        tune = ctx.autotune(repeats=2)
     counts = []
     for e in range(n_events):
         c = ctx.counts(e)
@@ -500,6 +505,7 @@ def run_ours(args):
                 "cells_per_step_per_gpu": int(sum(sum(c["C"]) for c in counts)),
                 "roads_per_step_per_gpu": int(total_roads),
                 "mode": "batched plain path, one CUDA graph per step" + ("; frames: raw clusters resident once per frame" if frames is not None else ""),
+                "launch_shape": tune if tune is not None else "default (256 threads, 8 blocks/SM, pruning on)",
                 "parallelism": "event shards, one rank per GPU" if world > 1 else "single GPU",
                 "l2": "inputs larger than L2 (%.0f MB raw clusters, %.0f MB tracklets per step), no flush" % (
                     clusters.nbytes / 1e6, 16 * sum(sum(c["T"]) for c in counts) / 1e6),

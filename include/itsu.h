@@ -223,6 +223,27 @@ itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, i
  * memory, without waiting; itsu_batch_status waits and reports. */
 itsu_status itsu_relaunch(itsu_context *ctx);
 
+/* ---- launch-shape autotuner for batches (no counterpart in the reference) ----
+ * Runs are grouped in multiplicity bands: band = floor(log2(mean clusters per event)). For the
+ * band of the last run, itsu_autotune times every candidate launch shape (threads per block of
+ * the per-item kernels 128/256/512, resident blocks per SM of the grid-stride kernels 4/8/16, the
+ * tracklet candidate index on/off) on the inputs already resident, `repeats` times each, and
+ * keeps the fastest for that band; later runs in the band use it. Results never depend on the
+ * launch shape. itsu_get_tune / itsu_set_tune read and restore a band's entry (to persist a
+ * tuned table). */
+typedef struct itsu_tune {
+  int32_t band;
+  int32_t threads_per_block;
+  int32_t blocks_per_sm;
+  int32_t prune;  /* tracklet candidate pruning index on (1) or off (0) */
+  float ms;       /* best time of one run of the tuned inputs, 0 if untuned */
+  int32_t reserved_;
+} itsu_tune;
+int32_t itsu_multiplicity_band(int64_t n_clusters, int32_t n_events);
+itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best);
+itsu_status itsu_get_tune(itsu_context *ctx, int32_t band, itsu_tune *out);
+itsu_status itsu_set_tune(itsu_context *ctx, const itsu_tune *in);
+
 /* ---- instrumentation (no counterpart in the reference beyond its clock() stage timers,
  *      src/CA/Tracker.cxx:655-684) ---- */
 typedef struct itsu_kernel_time {

@@ -198,3 +198,26 @@ def test_pileup_frames_share_their_clusters(ctx):
     ctx.batch_status()
     again = ctx.results(len(runs) - 1)
     _assert_same(again, oracle.run_vertex(runs[-1][0].layers, runs[-1][0].vertices[runs[-1][1]]), "replay")
+
+
+def test_launch_shapes_and_autotuner_keep_results(ctx):
+    """The batch results do not depend on the launch shape; the autotuner's pick neither."""
+    events = gen.batch_events(5, n_events=6)
+    clusters, offsets, vertices = gen.pack_batch(events)
+    base_roads, base_off = ctx.batch_run_host(clusters, offsets, vertices)
+    want = [ctx.results(e) for e in range(len(events))]
+    band = ctx.lib.itsu_multiplicity_band(len(clusters), len(events))
+    try:
+        for block, per_sm, prune in [(128, 4, 0), (512, 16, 1), (64, 2, 1)]:
+            ctx.set_tune(band, block, per_sm, prune)
+            assert ctx.get_tune(band)["threads_per_block"] == block
+            roads, off = ctx.batch_run_host(clusters, offsets, vertices)
+            assert np.array_equal(off, base_off) and np.array_equal(roads.view(np.uint8), base_roads.view(np.uint8))
+            for e in range(len(events)):
+                _assert_same(ctx.results(e), want[e], "shape %d/%d/%d event %d" % (block, per_sm, prune, e))
+        best = ctx.autotune(repeats=1)
+        assert best["band"] == band and best["threads_per_block"] in (128, 256, 512) and best["ms"] > 0
+        roads, off = ctx.batch_run_host(clusters, offsets, vertices)
+        assert np.array_equal(roads.view(np.uint8), base_roads.view(np.uint8))
+    finally:
+        ctx.set_tune(band, 256, 8, 1)

@@ -34,6 +34,29 @@ enum Stage { kNone = 0, kInitialized, kTracklets, kCells, kNeighbours, kRoads };
 
 void itsu::set_thread_error(const char *message) { g_thread_error = message; }
 
+namespace {
+// Launch shape of a run; tuned per multiplicity band (itsu_autotune).
+struct Tune {
+  int block = 256;
+  int blocks_per_sm = 8;
+  int prune = 1;
+  float ms = 0.0f;
+  bool set = false;
+};
+constexpr int kBands = 32;
+
+// Band of a run: log2 of its mean cluster count per event.
+int band_of(int64_t n_clusters, int32_t n_events)
+{
+  const int64_t mean = n_clusters / (n_events > 0 ? n_events : 1);
+  int band = 0;
+  while (band + 1 < kBands && (int64_t(1) << (band + 1)) <= mean) {
+    ++band;
+  }
+  return band;
+}
+}  // namespace
+
 struct itsu_context {
   int device = 0;
   uint32_t flags = 0;
@@ -97,6 +120,12 @@ struct itsu_context {
   int32_t graph_events = -1;
   int64_t graph_clusters = -1;
 
+  // launch shapes per multiplicity band, and the candidate under test while tuning
+  Tune tunes[kBands];
+  Tune override_tune;
+  bool tuning = false;
+  int graph_tune[3] = {0, 0, -1};
+
   std::string error;
 };
 
@@ -141,7 +170,20 @@ cudaError_t alloc(T *&p, int64_t count)
   return cudaMalloc((void **)&p, (size_t)std::max<int64_t>(count, 1) * sizeof(T));
 }
 
-Launch launch_of(const itsu_context *ctx) { return Launch{ctx->stream, ctx->num_sms}; }
+Tune current_tune(const itsu_context *ctx)
+{
+  if (ctx->tuning) {
+    return ctx->override_tune;
+  }
+  const Tune &t = ctx->tunes[band_of(ctx->n_clusters, ctx->n_events)];
+  return t.set ? t : Tune{};
+}
+
+Launch launch_of(const itsu_context *ctx)
+{
+  const Tune t = current_tune(ctx);
+  return Launch{ctx->stream, ctx->num_sms, t.block, t.blocks_per_sm};
+}
 
 Arena arena_of(const itsu_context *ctx)
 {
@@ -161,6 +203,7 @@ Arena arena_of(const itsu_context *ctx)
   a.zs_j = ctx->zs_j;
   a.seg_rrange = ctx->seg_rrange;
   a.seg_regular = ctx->seg_regular;
+  a.prune_tracklets = current_tune(ctx).prune;
   a.trk_count = ctx->trk_count;
   a.trk_slots = ctx->trk_slots;
   a.slot_stride = ctx->cap_clusters;
@@ -410,7 +453,10 @@ void drop_graph(itsu_context *ctx)
 // sizes or arena buffers change.
 itsu_status launch_all(itsu_context *ctx)
 {
+  const Tune tune = current_tune(ctx);
   const bool same = ctx->graph && ctx->graph_generation == ctx->generation && ctx->graph_key[0] == ctx->in_raw &&
+                    ctx->graph_tune[0] == tune.block && ctx->graph_tune[1] == tune.blocks_per_sm &&
+                    ctx->graph_tune[2] == tune.prune &&
                     ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
                     ctx->graph_key[3] == ctx->in_raw_off &&
                     ctx->graph_events == ctx->n_events && ctx->graph_clusters == ctx->n_clusters;
@@ -437,6 +483,9 @@ itsu_status launch_all(itsu_context *ctx)
     ctx->graph_key[1] = ctx->in_layer_off;
     ctx->graph_key[2] = ctx->in_vtx;
     ctx->graph_key[3] = ctx->in_raw_off;
+    ctx->graph_tune[0] = tune.block;
+    ctx->graph_tune[1] = tune.blocks_per_sm;
+    ctx->graph_tune[2] = tune.prune;
     ctx->graph_events = ctx->n_events;
     ctx->graph_clusters = ctx->n_clusters;
   }
@@ -1106,6 +1155,98 @@ itsu_status itsu_relaunch(itsu_context *ctx)
 }
 
 int32_t itsu_kernels_per_run(void) { return itsu::kernels_per_run(); }
+
+int32_t itsu_multiplicity_band(int64_t n_clusters, int32_t n_events) { return band_of(n_clusters, n_events); }
+
+itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kRoads, "itsu_autotune")) != ITSU_OK) return st;
+  if (repeats < 1) return fail(ctx, ITSU_ERR_INVALID, "repeats must be positive");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  int n = 0;
+  const itsu::KernelStep *steps = itsu::pipeline_steps(&n);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ITSU_CUDA(ctx, cudaEventCreate(&e0));
+  ITSU_CUDA(ctx, cudaEventCreate(&e1));
+  Tune winner;
+  winner.ms = 1e30f;
+  const int blocks[] = {128, 256, 512}, per_sm[] = {4, 8, 16}, prunes[] = {1, 0};
+  ctx->tuning = true;
+  cudaError_t err = cudaSuccess;
+  for (int b : blocks) {
+    for (int m : per_sm) {
+      for (int p : prunes) {
+        ctx->override_tune = Tune{b, m, p, 0.0f, true};
+        const Arena a = arena_of(ctx);
+        const Launch l = launch_of(ctx);
+        float best_ms = 1e30f;
+        for (int r = 0; r <= repeats && err == cudaSuccess; ++r) {  // the first pass warms up
+          cudaEventRecord(e0, ctx->stream);
+          for (int k = 0; k < n; ++k) steps[k].launch(a, l);
+          cudaEventRecord(e1, ctx->stream);
+          err = cudaStreamSynchronize(ctx->stream);
+          float ms = 0;
+          if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+          if (r > 0) best_ms = std::min(best_ms, ms);
+        }
+        if (err != cudaSuccess) break;
+        if ((st = sync_status(ctx)) != ITSU_OK) break;
+        if (ctx->h_status->flags == 0 && best_ms < winner.ms) {
+          winner = ctx->override_tune;
+          winner.ms = best_ms;
+        }
+      }
+    }
+  }
+  ctx->tuning = false;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ITSU_CUDA(ctx, err);
+  if (st != ITSU_OK) return st;
+  if (winner.ms >= 1e30f) return fail(ctx, ITSU_ERR_CAPACITY, "no candidate launch shape completed");
+  const int band = band_of(ctx->n_clusters, ctx->n_events);
+  ctx->tunes[band] = winner;
+  drop_graph(ctx);
+  // leave the arena holding this shape's results of the last run
+  if ((st = run_all(ctx)) != ITSU_OK) return st;
+  if (best) {
+    best->band = band;
+    best->threads_per_block = winner.block;
+    best->blocks_per_sm = winner.blocks_per_sm;
+    best->prune = winner.prune;
+    best->ms = winner.ms;
+  }
+  return ITSU_OK;
+}
+
+itsu_status itsu_get_tune(itsu_context *ctx, int32_t band, itsu_tune *out)
+{
+  if (!ctx || !out) return fail(ctx, ITSU_ERR_INVALID, "null argument");
+  if (band < 0 || band >= kBands) return fail(ctx, ITSU_ERR_INVALID, "band %d out of range", band);
+  const Tune &t = ctx->tunes[band];
+  const Tune d;
+  out->band = band;
+  out->threads_per_block = t.set ? t.block : d.block;
+  out->blocks_per_sm = t.set ? t.blocks_per_sm : d.blocks_per_sm;
+  out->prune = t.set ? t.prune : d.prune;
+  out->ms = t.set ? t.ms : 0.0f;
+  return ITSU_OK;
+}
+
+itsu_status itsu_set_tune(itsu_context *ctx, const itsu_tune *in)
+{
+  if (!ctx || !in) return fail(ctx, ITSU_ERR_INVALID, "null argument");
+  if (in->band < 0 || in->band >= kBands) return fail(ctx, ITSU_ERR_INVALID, "band %d out of range", in->band);
+  if (in->threads_per_block < 64 || in->threads_per_block > 512 || in->threads_per_block % 32 != 0 || in->blocks_per_sm < 1 ||
+      in->blocks_per_sm > 32) {
+    return fail(ctx, ITSU_ERR_INVALID, "launch shape %d threads x %d blocks/SM out of range", in->threads_per_block,
+                in->blocks_per_sm);
+  }
+  ctx->tunes[in->band] = Tune{in->threads_per_block, in->blocks_per_sm, in->prune ? 1 : 0, in->ms, true};
+  drop_graph(ctx);
+  return ITSU_OK;
+}
 
 itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_time *times, int32_t capacity, int32_t *count)
 {

@@ -63,6 +63,7 @@ struct Arena {
   int32_t *zs_j;
   float2 *seg_rrange;
   int32_t *seg_regular;
+  int32_t prune_tracklets;  // use the index (tuning knob; results are identical either way)
   // tracklets
   int32_t *trk_count;
   int32_t *trk_slots;  // slot n of inner cluster i at n * slot_stride + i: the outer clusters of its first tracklets
@@ -103,6 +104,8 @@ struct Arena {
 struct Launch {
   cudaStream_t stream;
   int num_sms;
+  int block;          // threads per block of the per-item kernels (64..512, a multiple of 32)
+  int blocks_per_sm;  // grid of the grid-stride kernels, in blocks per SM
 };
 
 // Stage launchers (asynchronous on l.stream).

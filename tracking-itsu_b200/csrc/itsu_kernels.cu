@@ -23,7 +23,8 @@
 namespace itsu {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;     // threads per block of the fixed-shape helper kernels
+constexpr int kMaxThreads = 512;  // upper bound of the tunable per-item kernels' block size
 constexpr int kSortThreads = 512;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kBuckets = kTableSize + 1;  // bucket 0: negative bins; bucket b+1: bin b
@@ -652,7 +653,7 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
   s.probe.phi = a.phi + s.next_begin;
   s.probe.max_dz = kC.trk_max_dz[s.layer];
   const int next_seg = s.seg + 1;
-  s.prune = a.seg_regular[next_seg] != 0;
+  s.prune = a.prune_tracklets && a.seg_regular[next_seg] != 0;
   s.zlo = s.zhi = 0;
   if (s.prune) {
     const float2 rr = a.seg_rrange[next_seg];
@@ -676,7 +677,7 @@ __device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s
 
 // Count pass, one thread per inner cluster: the number of tracklets, and the outer clusters of
 // the first kTrackletSlots of them in emission order.
-__global__ void __launch_bounds__(kThreads) k_tracklets_count(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
 {
   const int64_t i = global_thread();
   if (i >= a.n_clusters) {
@@ -699,7 +700,7 @@ __global__ void __launch_bounds__(kThreads) k_tracklets_count(Arena a)
 // (Tracker.cxx:102-108) and, for each of its tracklet slots, the owner cluster and segment the
 // write pass reads. Clusters with more than kTrackletSlots tracklets (rare) walk their candidates
 // again here and write their tracklets in order.
-__global__ void __launch_bounds__(kThreads) k_tracklets_tail(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_tracklets_tail(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -730,7 +731,7 @@ __global__ void __launch_bounds__(kThreads) k_tracklets_tail(Arena a)
 // Write pass, one thread per tracklet (owner and segment filled in by k_tracklets_tail, outer
 // cluster kept by the count pass): all tracklets of a warp compute their binary64 azimuth
 // together. Tracklets of crowded clusters were written by k_tracklets_tail.
-__global__ void __launch_bounds__(kThreads) k_tracklets_write(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_tracklets_write(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -898,10 +899,10 @@ __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const Ce
 // cell, and their number. The warp flattens its 32 tracklets' pairs across lanes (Tracker.cxx:
 // 155-158 iterates them per tracklet); pairs that pass the cheap cuts queue up so the circle
 // geometry runs with all 32 lanes converged.
-__global__ void __launch_bounds__(kThreads) k_cells_count(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
 {
-  __shared__ int4 queue[kThreads / 32][kCellQueue];             // (owner lane, pair bit, c3 flat, -)
-  __shared__ unsigned long long masks[kThreads / 32][32];
+  __shared__ int4 queue[kMaxThreads / 32][kCellQueue];             // (owner lane, pair bit, c3 flat, -)
+  __shared__ unsigned long long masks[kMaxThreads / 32][32];
   if (capacity_failed(a.status)) {
     return;
   }
@@ -1006,7 +1007,7 @@ __global__ void __launch_bounds__(kThreads) k_cells_count(Arena a)
 
 // Write pass: the cells of each first tracklet at its scanned slot, in outgoing-tracklet order
 // (the mask's bit order). The warp flattens its tracklets' cells across lanes.
-__global__ void __launch_bounds__(kThreads) k_cells_write(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_cells_write(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -1103,7 +1104,7 @@ __global__ void k_cell_segments(Arena a)
 // (d) neighbours and CA levels: Tracker<IsGPU>::findCellsNeighbours (Tracker.cxx:417-474)
 
 // Per-cell state of the neighbour and road stages, reset so that the stage can be re-run.
-__global__ void __launch_bounds__(kThreads) k_neighbour_reset(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_neighbour_reset(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -1118,7 +1119,7 @@ __global__ void __launch_bounds__(kThreads) k_neighbour_reset(Arena a)
 }
 
 template <bool kWrite>
-__global__ void __launch_bounds__(kThreads) k_neighbours(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_neighbours(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -1159,7 +1160,7 @@ __global__ void k_neighbour_check(Arena a)
 // Rows of layer `layer` cells: sort ascending (the reference pushes in cell order), then the
 // level (Tracker.cxx:463-468: 1 + the highest neighbour level) and the number of
 // level-decreasing chains down to layer 0 (the roads a level-5 cell starts, Tracker.cxx:477-571).
-__global__ void __launch_bounds__(kThreads) k_levels(Arena a, int layer)
+__global__ void __launch_bounds__(kMaxThreads) k_levels(Arena a, int layer)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -1238,7 +1239,7 @@ __device__ __forceinline__ int32_t cluster_mc(const Arena &a, const int32_t *lo,
   return a.sorted[lo[layer] + idx].mc_id;
 }
 
-__global__ void __launch_bounds__(kThreads) k_roads(Arena a)
+__global__ void __launch_bounds__(kMaxThreads) k_roads(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -1327,7 +1328,9 @@ __global__ void __launch_bounds__(kThreads) k_roads(Arena a)
   }
 }
 
-int fixed_grid(const Launch &l) { return l.num_sms * 8; }
+// Grid of the grid-stride kernels: the tuned number of resident blocks per SM, scaled to the
+// block size so that the number of resident threads stays comparable.
+int fixed_grid(const Launch &l) { return l.num_sms * l.blocks_per_sm; }
 
 void step_status_init(const Arena &a, const Launch &l) { k_status_init<<<1, 1, 0, l.stream>>>(a.status); }
 
@@ -1340,19 +1343,19 @@ void step_cluster_sort(const Arena &a, const Launch &l)
 
 void step_tracklets_count(const Arena &a, const Launch &l)
 {
-  const int64_t blocks = (a.n_clusters + kThreads - 1) / kThreads;
+  const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
   if (blocks > 0) {
-    k_tracklets_count<<<(unsigned)blocks, kThreads, 0, l.stream>>>(a);
+    k_tracklets_count<<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
   }
 }
 
-void step_tracklets_write(const Arena &a, const Launch &l) { k_tracklets_write<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+void step_tracklets_write(const Arena &a, const Launch &l) { k_tracklets_write<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
 void step_tracklets_tail(const Arena &a, const Launch &l)
 {
-  const int64_t blocks = (a.n_clusters + kThreads - 1) / kThreads;
+  const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
   if (blocks > 0) {
-    k_tracklets_tail<<<(unsigned)blocks, kThreads, 0, l.stream>>>(a);
+    k_tracklets_tail<<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
   }
 }
 
@@ -1361,31 +1364,31 @@ void step_tracklet_segments(const Arena &a, const Launch &l)
   k_tracklet_segments<<<(a.n_events * ITSU_TRACKLET_LAYERS + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
 }
 
-void step_cells_count(const Arena &a, const Launch &l) { k_cells_count<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+void step_cells_count(const Arena &a, const Launch &l) { k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
-void step_cells_write(const Arena &a, const Launch &l) { k_cells_write<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+void step_cells_write(const Arena &a, const Launch &l) { k_cells_write<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
 void step_cell_segments(const Arena &a, const Launch &l)
 {
   k_cell_segments<<<(a.n_events * ITSU_CELL_LAYERS + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
 }
 
-void step_neighbour_reset(const Arena &a, const Launch &l) { k_neighbour_reset<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+void step_neighbour_reset(const Arena &a, const Launch &l) { k_neighbour_reset<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
 template <bool kWrite>
-void step_neighbours(const Arena &a, const Launch &l) { k_neighbours<kWrite><<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+void step_neighbours(const Arena &a, const Launch &l) { k_neighbours<kWrite><<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
 void step_neighbour_check(const Arena &a, const Launch &l) { k_neighbour_check<<<1, 32, 0, l.stream>>>(a); }
 
 template <int kLayer>
-void step_levels(const Arena &a, const Launch &l) { k_levels<<<fixed_grid(l), kThreads, 0, l.stream>>>(a, kLayer); }
+void step_levels(const Arena &a, const Launch &l) { k_levels<<<fixed_grid(l), l.block, 0, l.stream>>>(a, kLayer); }
 
 void step_road_segments(const Arena &a, const Launch &l)
 {
   k_road_segments<<<(a.n_events + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
 }
 
-void step_roads(const Arena &a, const Launch &l) { k_roads<<<fixed_grid(l), kThreads, 0, l.stream>>>(a); }
+void step_roads(const Arena &a, const Launch &l) { k_roads<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
 // The whole run, kernel by kernel, in launch order.
 const KernelStep kSteps[] = {

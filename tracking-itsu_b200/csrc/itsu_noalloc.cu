@@ -114,7 +114,7 @@ extern "C" itsu_status itsu_pvc_initialize_noalloc(const itsu_cluster *clusters,
   a.tmp = reinterpret_cast<itsu_cluster *>(scratch + kTmpOff);
   a.xyzr = reinterpret_cast<float4 *>(scratch + kXyzrOff);
   a.phi = reinterpret_cast<float *>(scratch + kPhiOff);
-  const itsu::Launch l{stream, 0};
+  const itsu::Launch l{stream, 0, 256, 8};
   itsu::launch_status_init(a, l);
   itsu::launch_cluster_sort(a, l);
   if ((err = cudaGetLastError()) != cudaSuccess) {

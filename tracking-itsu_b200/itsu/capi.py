@@ -64,6 +64,11 @@ class Frames(ctypes.Structure):
                 ("vertex_frame", ctypes.c_void_p), ("n_frames", ctypes.c_int32), ("n_vertices", ctypes.c_int32)]
 
 
+class Tune(ctypes.Structure):
+    _fields_ = [("band", ctypes.c_int32), ("threads_per_block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("prune", ctypes.c_int32), ("ms", ctypes.c_float), ("reserved_", ctypes.c_int32)]
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("clusters", ctypes.c_void_p), ("layer_offsets", ctypes.c_void_p), ("vertices", ctypes.c_void_p),
                 ("n_events", ctypes.c_int32), ("reserved_", ctypes.c_int32), ("n_clusters", ctypes.c_int64)]
@@ -104,6 +109,10 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.POINTER(Frames), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     ("itsu_relaunch", ctypes.c_int, [ctypes.c_void_p]),
     ("itsu_kernels_per_run", ctypes.c_int32, []),
+    ("itsu_multiplicity_band", ctypes.c_int32, [ctypes.c_int64, ctypes.c_int32]),
+    ("itsu_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Tune)]),
+    ("itsu_get_tune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Tune)]),
+    ("itsu_set_tune", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tune)]),
     ("itsu_pvc_initialize_noalloc", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("itsu_batch_profile", ctypes.c_int,
@@ -304,3 +313,18 @@ class Context:
 
     def relaunch(self):
         self._check(self.lib.itsu_relaunch(self.h))
+
+    def autotune(self, repeats: int = 3) -> dict:
+        """Tune the launch shape for the band of the last run; returns the chosen entry."""
+        t = Tune()
+        self._check(self.lib.itsu_autotune(self.h, repeats, ctypes.byref(t)))
+        return dict(band=t.band, threads_per_block=t.threads_per_block, blocks_per_sm=t.blocks_per_sm, prune=t.prune, ms=t.ms)
+
+    def set_tune(self, band: int, threads_per_block: int, blocks_per_sm: int, prune: int = 1):
+        t = Tune(band, threads_per_block, blocks_per_sm, prune, 0.0, 0)
+        self._check(self.lib.itsu_set_tune(self.h, ctypes.byref(t)))
+
+    def get_tune(self, band: int) -> dict:
+        t = Tune()
+        self._check(self.lib.itsu_get_tune(self.h, band, ctypes.byref(t)))
+        return dict(band=t.band, threads_per_block=t.threads_per_block, blocks_per_sm=t.blocks_per_sm, prune=t.prune, ms=t.ms)
