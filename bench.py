@@ -63,6 +63,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter mode")
+    ap.add_argument("--prefilter", default=os.path.join(PKG, "weights", "prefilter_pbpb.itsumlp"),
+                    help="checkpoint of the learned prefilter")
     return ap.parse_args()
 
 
@@ -108,6 +111,18 @@ def sum_over_ranks(dist, value, device=None):
     return float(t.item())
 
 
+def shard_seed(seed, rank):
+    """Each rank's events come from its own seed (independent event shards, weak scaling)."""
+    return seed + 7919 * rank
+
+
+def whole_job_rate(dist, units_local, ms_local, device=None):
+    """Units of all ranks / the slowest rank's time: (units per second, max ms, total units)."""
+    ms = max_over_ranks(dist, ms_local, device)
+    units = sum_over_ranks(dist, units_local, device)
+    return units / (ms * 1e-3), ms, units
+
+
 # ------------------------------------------------------------------------------------------
 # workload
 
@@ -143,8 +158,10 @@ KERNEL_STAGE = {
     "cluster_sort": "cluster_sort",
     "tracklets_count": "tracklets",
     "tracklets_write": "tracklets",
+    "tracklets_tail": "tracklets",
     "cells_count": "cells",
-    "cells_write": "cells",
+    "cells_scatter": "cells",
+    "cells_lookup": "cells",
     "neighbours_count": "neighbours",
     "neighbours_write": "neighbours",
     "roads_write": "roads",
@@ -322,7 +339,7 @@ def run_ours(args):
     device = torch.device("cuda", local)
     from itsu import capi
 
-    seed = args.seed + 7919 * rank
+    seed = shard_seed(args.seed, rank)
     frames = None
     if args.workload == "pileup":
         frames = gen.pileup_stream(seed, args.frames, collisions=5, n_tracks=1500)
@@ -384,7 +401,7 @@ def run_ours(args):
     if dist:
         dist.barrier()
     ms_local = start.elapsed_time(end)
-    ms = max_over_ranks(dist, ms_local, device)
+    value, ms, total_events = whole_job_rate(dist, n_events * args.steps, ms_local, device)
     clock_summary = clocks.summary()
 
     # ---- e2e: host in / host out through the C ABI ----
@@ -437,6 +454,14 @@ def run_ours(args):
     e2e_ms = max_over_ranks(dist, e_start.elapsed_time(e_end), device)
     assert int(h_road_off[-1]) == total_roads, "host path road count differs from the device path"
 
+    # ---- learned-prefilter form: same inputs, same timing rules ----
+    learned = None
+    if not args.no_prefilter and os.path.exists(args.prefilter):
+        l_ms, l_cmp, l_prof, l_thr = learned_mode(ctx, launch, args, stream, dist, device)
+        learned = dict(ms=l_ms, cmp=l_cmp, prof=l_prof, threshold=l_thr)
+        launch()  # back to the plain graph (the profile below times the plain kernels)
+        ctx.batch_status()
+
     # ---- live per-kernel timing for the roofline ----
     prof = ctx.profile(repeats=3)
     step_bytes = {}
@@ -474,8 +499,6 @@ def run_ours(args):
     single_eps = len(single) / (time.perf_counter() - t0)
     ctx1.close()
 
-    total_events = sum_over_ranks(dist, n_events * args.steps, device)
-    value = total_events / (ms * 1e-3)
     e2e_value = total_events / (e2e_ms * 1e-3)
     line = None
     if rank == 0:
@@ -522,6 +545,21 @@ def run_ours(args):
                 "batched_plain_events_per_s": value,
                 "plain_single_event_events_per_s": single_eps,
                 "plain_single_event_note": "itsu_clusters_to_tracks, one vertex per synchronous call, host in/out, wall clock",
+                "learned_prefilter": None if learned is None else {
+                    "events_per_s": total_events / (learned["ms"] * 1e-3),
+                    "ms_per_step": learned["ms"] / args.steps,
+                    "vs_batched_plain": (total_events / (learned["ms"] * 1e-3)) / value,
+                    "road_reproduction": learned["cmp"]["road_reproduction"],
+                    "plain_roads": learned["cmp"]["plain_roads"],
+                    "learned_roads": learned["cmp"]["learned_roads"],
+                    "extra_roads": learned["cmp"]["extra"],
+                    "extra_fakes": learned["cmp"]["extra_fakes"],
+                    "cells_kept": learned["cmp"]["cells_kept"],
+                    "logit_threshold": learned["threshold"],
+                    "checkpoint": os.path.relpath(args.prefilter, ROOT),
+                    "kernel_ms": {name: round(t, 4) for name, t in learned["prof"]},
+                    "note": "same resident batch and timing as the plain value; fused BF16 MLP (mma.sync) in the cell stage",
+                },
             },
             "kernel_ms": {name: round(t, 4) for name, t in prof},
             "algorithmic_bytes_per_step": step_bytes.get("event"),
@@ -535,6 +573,45 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+def learned_mode(ctx, launch, args, stream, dist, device):
+    """The learned-prefilter form on the same resident inputs: K timed graph replays (max over
+    ranks), and its roads against the plain run's (exported just before)."""
+    import torch
+
+    from itsu import capi, prefilter
+
+    plain_keys, plain_fake = prefilter.export_roads(ctx, device)
+    plain_cells = ctx.prefilter_export()[0]
+    model = capi.prefilter_load(args.prefilter)
+    ctx.prefilter_set_model(model)
+    ctx.prefilter_enable(True)
+    try:
+        launch()  # captures the learned graph
+        ctx.batch_status()
+        learned_cells = ctx.prefilter_export()[0]
+        keys, fake = prefilter.export_roads(ctx, device)
+        for _ in range(args.warmup):
+            launch()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            launch()
+        end.record(stream)
+        torch.cuda.synchronize()
+        ctx.batch_status()
+        ms = max_over_ranks(dist, start.elapsed_time(end), device)
+        prof = ctx.profile(repeats=3)
+    finally:
+        ctx.prefilter_enable(False)
+    cmp = prefilter.compare_roads(plain_keys, plain_fake, keys, fake)
+    cmp["road_reproduction"] = cmp["reproduced"] / max(cmp["plain_roads"], 1)
+    cmp["cells_kept"] = learned_cells / max(plain_cells, 1)
+    return ms, cmp, prof, float(model.logit_threshold)
 
 
 # ------------------------------------------------------------------------------------------

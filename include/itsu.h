@@ -252,13 +252,96 @@ typedef struct itsu_kernel_time {
   int32_t launches;
 } itsu_kernel_time;
 
-/* Number of kernels one whole-path or batch run launches. */
+/* Number of kernels one plain whole-path or batch run launches (the learned-prefilter form
+ * launches one more, its scoring kernel). */
 int32_t itsu_kernels_per_run(void);
 /* Re-runs the last batch `repeats` times with every kernel launched on its own and bracketed by
- * CUDA events on the context stream; fills up to `capacity` entries in launch order. Call after
- * itsu_batch_run (or itsu_batch_run_host) has sized the arena for that batch. */
+ * CUDA events on the context stream; fills up to `capacity` entries in launch order and sets
+ * *count to the number of kernels of the context's form. Call after itsu_batch_run (or
+ * itsu_batch_run_host) has sized the arena for that batch. */
 itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_time *times, int32_t capacity,
                                int32_t *count);
+
+/* ---- learned tracklet-pair prefilter (no counterpart in the reference) ----
+ * A small MLP (8 -> 64 -> 64 -> 1, GELU, sigmoid output; BF16 weights and activations, FP32
+ * accumulation) scores, inside the cell stage (the seam of TrackerTraits::computeLayerCells,
+ * src/CA/Tracker.cxx:120-235), each tracklet pair that passes the exact cell cuts; a pair whose
+ * logit is below the model's threshold does not become a cell. Its features, per pair: dphi, dz
+ * and dtanL of the cell cuts (Tracker.cxx:161-171), the signed curvature of each tracklet's
+ * circle through the primary vertex, the pair's DCA (Tracker.cxx:203-210), the inner layer
+ * index and the first cluster's radius. The plain path is unchanged and stays the judge: a
+ * learned run's cells are a subset of the plain run's, so its roads are plain roads. Training
+ * labels come from plain runs (1 = the cell is on a found road). */
+#define ITSU_MLP_INPUTS 8
+#define ITSU_MLP_HIDDEN 64
+/* trainable parameters: w1, b1, w2, b2, w3, b3, contiguous at the start of itsu_prefilter_model */
+#define ITSU_MLP_PARAMS (ITSU_MLP_HIDDEN * ITSU_MLP_INPUTS + ITSU_MLP_HIDDEN + ITSU_MLP_HIDDEN * ITSU_MLP_HIDDEN + \
+                         ITSU_MLP_HIDDEN + ITSU_MLP_HIDDEN + 1)
+/* The FP32 master copy of a model; the device computes with BF16 copies of w1, w2, w3. */
+typedef struct itsu_prefilter_model {
+  float w1[ITSU_MLP_HIDDEN][ITSU_MLP_INPUTS]; /* [out][in] */
+  float b1[ITSU_MLP_HIDDEN];
+  float w2[ITSU_MLP_HIDDEN][ITSU_MLP_HIDDEN]; /* [out][in] */
+  float b2[ITSU_MLP_HIDDEN];
+  float w3[ITSU_MLP_HIDDEN];
+  float b3;
+  float mean[ITSU_MLP_INPUTS];    /* the network sees (feature - mean) * inv_std */
+  float inv_std[ITSU_MLP_INPUTS];
+  float logit_threshold;          /* a pair is kept unless its logit is below this */
+} itsu_prefilter_model;
+
+/* Device buffers that itsu_prefilter_export fills; every array may be NULL (then not written). */
+typedef struct itsu_prefilter_samples {
+  float *features;       /* [capacity][8]: the pair features of each cell of the last run */
+  uint8_t *labels;       /* [capacity]: 1 if a found road uses the cell */
+  int64_t capacity;      /* rows available; the export fails with ITSU_ERR_CAPACITY below n_cells */
+  int32_t *road_cells;   /* [road_capacity][5]: each road's cells as sample rows, layers 0..4 */
+  int32_t *road_keys;    /* [road_capacity][8]: each road's event and the layer-local sorted indices
+                            of its 7 clusters, layers 0..6 */
+  uint8_t *road_fake;    /* [road_capacity]: the road's fake flag (Moore vote, Tracker.cxx:574-652) */
+  int64_t road_capacity;
+  int64_t n_cells;       /* out: cells of the last run (rows in event, layer, cell order) */
+  int64_t n_roads;       /* out: roads of the last run (in road order) */
+} itsu_prefilter_samples;
+
+typedef struct itsu_train_config {
+  int64_t steps;          /* Adam steps */
+  int32_t batch;          /* samples per step, a multiple of 32, drawn with replacement */
+  int32_t reserved_;
+  float lr;               /* peak learning rate; cosine decay to lr_final over the steps */
+  float lr_final;
+  float beta1, beta2, eps;
+  float weight_decay;     /* decoupled, on the weight matrices only */
+  float pos_weight;       /* loss weight of label-1 samples */
+  uint64_t seed;          /* minibatch sampling */
+} itsu_train_config;
+
+/* Deterministic fresh model (host only): scaled-uniform weights from seed, zero biases, identity
+ * standardisation, threshold 0 (probability 0.5). */
+void itsu_prefilter_init(itsu_prefilter_model *model, uint64_t seed);
+void itsu_train_config_default(itsu_train_config *cfg);
+/* Checkpoint file: magic, sizes, the FP32 master model, the BF16 copies of its weights and a
+ * 64-bit FNV-1a checksum. Loading verifies all of them (ITSU_ERR_INVALID on any mismatch). */
+itsu_status itsu_prefilter_save(const itsu_prefilter_model *model, const char *path);
+itsu_status itsu_prefilter_load(const char *path, itsu_prefilter_model *model);
+/* The context's model (used by the learned form, the scorer and training). */
+itsu_status itsu_prefilter_set_model(itsu_context *ctx, const itsu_prefilter_model *model);
+itsu_status itsu_prefilter_get_model(itsu_context *ctx, itsu_prefilter_model *model);
+/* Learned form on (1) or off (0) for later whole-path, batch and frames runs. Needs a model. */
+itsu_status itsu_prefilter_enable(itsu_context *ctx, int32_t enable);
+/* Training samples and road keys of the last whole-path / batch / frames run (after its roads). */
+itsu_status itsu_prefilter_export(itsu_context *ctx, itsu_prefilter_samples *samples);
+/* Logits of n feature rows (device pointers), with the same kernel code as the learned form. */
+itsu_status itsu_prefilter_score(itsu_context *ctx, const float *features, int64_t n, float *logits);
+/* Trains the context's model in place: cfg->steps Adam steps of binary cross-entropy on
+ * minibatches of the n device samples (rows with non-finite features must be left out by the
+ * caller). losses (host, may be NULL) receives each step's minibatch loss. */
+itsu_status itsu_prefilter_train(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
+                                 const itsu_train_config *cfg, float *losses);
+/* Mean loss and its gradient over all n device samples at the current model (host outputs:
+ * grad[ITSU_MLP_PARAMS] in itsu_prefilter_model order). */
+itsu_status itsu_prefilter_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
+                                    float pos_weight, float *grad, float *loss);
 
 /* ---- clustering without any allocation ----
  * No counterpart in the reference: its GPU backend allocates per call (gpu/Vector.h:97-122).

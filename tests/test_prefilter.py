@@ -1,0 +1,134 @@
+"""Host-side parts of the learned prefilter (no GPU): the checkpoint format, the seeded
+initialisation, the numpy restatements the GPU tests compare against, threshold calibration and
+road-set comparison."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from itsu import capi, gen, prefilter
+from oracle import oracle
+
+
+def test_model_layout_matches_the_header():
+    assert ctypes.sizeof(capi.PrefilterModel) == 4 * (capi.MLP_PARAMS + 2 * 8 + 1)
+    assert capi.MLP_PARAMS == 4801
+    assert ctypes.sizeof(capi.PrefilterSamples) == 72
+    assert ctypes.sizeof(capi.TrainConfig) == 56
+
+
+def test_init_is_seeded():
+    a, b, c = capi.prefilter_init(1), capi.prefilter_init(1), capi.prefilter_init(2)
+    assert bytes(a) == bytes(b) and bytes(a) != bytes(c)
+    p = a.params()
+    assert np.all(np.abs(p[:512]) <= np.sqrt(6 / 72) + 1e-7)
+    assert np.all(p[512:576] == 0) and a.logit_threshold == 0.0
+    assert list(a.inv_std) == [1.0] * 8
+
+
+def test_checkpoint_round_trip_and_corruption(tmp_path):
+    m = capi.prefilter_init(9)
+    m.logit_threshold = -1.25
+    m.mean[3] = 0.5
+    path = str(tmp_path / "m.itsumlp")
+    capi.prefilter_save(m, path)
+    assert bytes(capi.prefilter_load(path)) == bytes(m)
+    raw = bytearray(open(path, "rb").read())
+    # a flipped byte anywhere fails the checksum
+    bad = bytearray(raw)
+    bad[100] ^= 1
+    open(path, "wb").write(bytes(bad))
+    with pytest.raises(capi.ItsuError) as e:
+        capi.prefilter_load(path)
+    assert e.value.status == capi.ERR_INVALID and "checksum" in str(e.value)
+    # truncated
+    open(path, "wb").write(bytes(raw[:-9]))
+    with pytest.raises(capi.ItsuError):
+        capi.prefilter_load(path)
+    # master weights edited and the checksum recomputed: the BF16 copies no longer match
+    bad = bytearray(raw[:-8])
+    off = 24  # header: 8-byte magic + 4 uint32
+    w = np.frombuffer(bytes(bad[off:off + 4]), np.float32)[0]
+    bad[off:off + 4] = np.float32(w + 0.5).tobytes()
+    h = 0xcbf29ce484222325
+    for byte in bad:
+        h = ((h ^ byte) * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    open(path, "wb").write(bytes(bad) + h.to_bytes(8, "little"))
+    with pytest.raises(capi.ItsuError) as e:
+        capi.prefilter_load(path)
+    assert "BF16" in str(e.value)
+    with pytest.raises(capi.ItsuError):
+        capi.prefilter_load(str(tmp_path / "missing"))
+
+
+def test_committed_checkpoint_loads():
+    if not os.path.exists(prefilter.CHECKPOINT):
+        pytest.skip("no trained checkpoint")
+    m = capi.prefilter_load(prefilter.CHECKPOINT)
+    assert np.isfinite(m.params()).all() and np.isfinite(m.logit_threshold)
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, 1.0 + 2 ** -9, -2.5, 3.0e38], np.float32)
+    got = prefilter.bf16_round(x)
+    assert list(got[:5]) == [1.0, 1.0, 1.0 + 2 ** -6, 1.0, -2.5]  # ties to even, exact values kept
+    assert np.isfinite(got[5])
+
+
+def test_numpy_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    m = capi.prefilter_init(3).arrays()
+    m["b1"], m["b2"], m["b3"] = rng.normal(0, 0.1, 64), rng.normal(0, 0.1, 64), 0.1
+    f = rng.normal(0, 1, (64, 8)).astype(np.float32)
+    y = (rng.random(64) < 0.6).astype(np.float64)
+    g, _ = prefilter.mlp_gradient(m, f, y, 1.5, rounding=False)
+    flat = np.concatenate([m["w1"].ravel(), m["b1"], m["w2"].ravel(), m["b2"], m["w3"], [m["b3"]]]).astype(np.float64)
+    shapes = (("w1", (64, 8)), ("b1", (64,)), ("w2", (64, 64)), ("b2", (64,)), ("w3", (64,)), ("b3", ()))
+
+    def loss_at(v):
+        mm, o = dict(m), 0
+        for k, shp in shapes:
+            n = int(np.prod(shp)) if shp else 1
+            mm[k] = v[o:o + n].reshape(shp) if shp else v[o]
+            o += n
+        return prefilter.mlp_gradient(mm, f, y, 1.5, rounding=False)[1]
+
+    for i in list(rng.choice(len(flat), 30, replace=False)) + [0, 512, 600, 4700, 4750, 4800]:
+        up, dn = flat.copy(), flat.copy()
+        up[i] += 1e-6
+        dn[i] -= 1e-6
+        assert abs((loss_at(up) - loss_at(dn)) / 2e-6 - g[i]) < 1e-7 + 1e-5 * abs(g[i])
+
+
+def test_pair_features_of_oracle_cells():
+    """Features of the plain path's cells respect the cuts that made them."""
+    ev = gen.pbpb_event(5, n_tracks=800)
+    res = oracle.run_vertex(ev.layers, ev.vertices[0])
+    f = prefilter.pair_features(res)
+    assert len(f) == sum(len(c) for c in res["cells"]) > 0 and np.isfinite(f).all()
+    layer = f[:, 6].astype(int)
+    assert np.all(f[:, 0] < 0.14) and np.all(f[:, 2] < 0.025)
+    assert np.all(f[:, 1] < np.array([0.2, 0.4, 0.5, 0.6, 3.0], np.float32)[layer])
+    assert np.all(f[:, 5] <= prefilter.CELL_MAX_DCA[layer])
+    rows = prefilter.road_cells(res)
+    assert np.all(f[rows, 6] == np.arange(5)[None, :])
+
+
+def test_calibrate_keeps_the_target_fraction_of_roads():
+    rng = np.random.default_rng(1)
+    logits = rng.normal(0, 1, 5000).astype(np.float32)
+    logits[7] = np.nan  # NaN keeps its cell
+    rows = rng.integers(0, 5000, (997, 5))
+    for target in (0.9, 0.995, 1.0):
+        thr = prefilter.calibrate(logits, rows, target)
+        kept = ~(logits < thr)
+        assert kept[rows].all(axis=1).mean() >= target
+    assert prefilter.calibrate(logits, rows[:0], 0.99) == float("-inf")
+
+
+def test_compare_roads():
+    p = np.array([[0, 1, 2, 3, 4, 5, 6, 7], [1, 1, 2, 3, 4, 5, 6, 7], [1, 2, 2, 3, 4, 5, 6, 7]], np.int32)
+    l = np.array([[1, 1, 2, 3, 4, 5, 6, 7], [2, 0, 0, 0, 0, 0, 0, 0]], np.int32)
+    c = prefilter.compare_roads(p, np.array([0, 1, 0]), l, np.array([1, 1]))
+    assert c == dict(plain_roads=3, learned_roads=2, reproduced=1, extra=1, extra_fakes=1, plain_fakes=1, learned_fakes=2)

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +20,7 @@
 
 #include "itsu.h"
 #include "itsu_internal.h"
+#include "itsu_mlp.cuh"
 
 using itsu::Arena;
 using itsu::DevStatus;
@@ -91,6 +93,8 @@ struct itsu_context {
   int32_t *trk_owner = nullptr;
   // cell class
   itsu_cell *cells = nullptr;
+  itsu::CellEntry *cell_entries = nullptr;
+  int64_t cap_cell_entries = 0;
   int32_t *cell_seg_id = nullptr, *nb_count = nullptr, *nb_off = nullptr, *nb_fill = nullptr, *road_count = nullptr,
           *road_off = nullptr;
   int64_t *paths = nullptr;
@@ -125,6 +129,13 @@ struct itsu_context {
   Tune override_tune;
   bool tuning = false;
   int graph_tune[3] = {0, 0, -1};
+  bool graph_prefilter = false;
+
+  // learned prefilter: FP32 master model and the device model the kernels read
+  itsu_prefilter_model *d_master = nullptr;
+  itsu::MlpDevice *d_mlp = nullptr;
+  bool has_model = false;
+  bool prefilter = false;
 
   std::string error;
 };
@@ -221,6 +232,8 @@ Arena arena_of(const itsu_context *ctx)
   a.cell_seg = ctx->cell_seg;
   a.cells = ctx->cells;
   a.cell_seg_id = ctx->cell_seg_id;
+  a.cell_entries = ctx->cell_entries;
+  a.cap_cell_entries = ctx->cap_cell_entries;
   a.nb_count = ctx->nb_count;
   a.nb_off = ctx->nb_off;
   a.nb_fill = ctx->nb_fill;
@@ -230,6 +243,7 @@ Arena arena_of(const itsu_context *ctx)
   a.road_off = ctx->road_off;
   a.road_seg = ctx->road_seg;
   a.roads = ctx->roads;
+  a.mlp = ctx->prefilter ? ctx->d_mlp : nullptr;
   a.scan_partials = ctx->scan_partials;
   a.status = ctx->d_status;
   a.cap_tracklets = ctx->cap_tracklets;
@@ -321,6 +335,29 @@ itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
   return ensure_partials(ctx);
 }
 
+// Entries the cell count pass may reserve beyond the cells it finds: every warp of its grid can
+// leave part of one chunk unused. Sized for the larger of the current launch shape and the
+// largest shape the autotuner tries (16 blocks of 512 threads per SM).
+int64_t cell_entry_slack(const itsu_context *ctx)
+{
+  const Tune t = current_tune(ctx);
+  const int64_t warps = std::max<int64_t>((int64_t)t.blocks_per_sm * (t.block / 32), 16 * (512 / 32));
+  return (int64_t)ctx->num_sms * warps * itsu::kCellChunk;
+}
+
+itsu_status ensure_cell_entries(itsu_context *ctx, int64_t need)
+{
+  if (need > ctx->cap_cell_entries) {
+    itsu_status st = growth_allowed(ctx, "cell entries", need, ctx->cap_cell_entries);
+    if (st != ITSU_OK) return st;
+    const int64_t cap = grow_to(need);
+    ITSU_CUDA(ctx, alloc(ctx->cell_entries, cap));
+    ctx->cap_cell_entries = cap;
+    ctx->generation++;
+  }
+  return ITSU_OK;
+}
+
 itsu_status ensure_cells(itsu_context *ctx, int64_t need)
 {
   if (need > ctx->cap_cells) {
@@ -338,6 +375,8 @@ itsu_status ensure_cells(itsu_context *ctx, int64_t need)
     ctx->cap_cells = cap;
     ctx->generation++;
   }
+  itsu_status st = ensure_cell_entries(ctx, ctx->cap_cells + cell_entry_slack(ctx));
+  if (st != ITSU_OK) return st;
   return ensure_partials(ctx);
 }
 
@@ -456,7 +495,7 @@ itsu_status launch_all(itsu_context *ctx)
   const Tune tune = current_tune(ctx);
   const bool same = ctx->graph && ctx->graph_generation == ctx->generation && ctx->graph_key[0] == ctx->in_raw &&
                     ctx->graph_tune[0] == tune.block && ctx->graph_tune[1] == tune.blocks_per_sm &&
-                    ctx->graph_tune[2] == tune.prune &&
+                    ctx->graph_tune[2] == tune.prune && ctx->graph_prefilter == ctx->prefilter &&
                     ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
                     ctx->graph_key[3] == ctx->in_raw_off &&
                     ctx->graph_events == ctx->n_events && ctx->graph_clusters == ctx->n_clusters;
@@ -486,6 +525,7 @@ itsu_status launch_all(itsu_context *ctx)
     ctx->graph_tune[0] = tune.block;
     ctx->graph_tune[1] = tune.blocks_per_sm;
     ctx->graph_tune[2] = tune.prune;
+    ctx->graph_prefilter = ctx->prefilter;
     ctx->graph_events = ctx->n_events;
     ctx->graph_clusters = ctx->n_clusters;
   }
@@ -521,6 +561,9 @@ itsu_status run_all(itsu_context *ctx)
       if ((st = ensure_roads(ctx, (int64_t)(ctx->cap_roads * f))) != ITSU_OK) return st;
     }
     if ((s.flags & itsu::kFlagCapCells) && (st = ensure_cells(ctx, s.total[1])) != ITSU_OK) return st;
+    if ((s.flags & itsu::kFlagCapScratch) && (st = ensure_cell_entries(ctx, s.cell_entries + cell_entry_slack(ctx))) != ITSU_OK) {
+      return st;
+    }
     if ((s.flags & itsu::kFlagCapNeighbours) && (st = ensure_neighbours(ctx, s.total[2])) != ITSU_OK) return st;
     if ((s.flags & itsu::kFlagCapRoads) && (st = ensure_roads(ctx, s.total[3])) != ITSU_OK) return st;
   }
@@ -532,10 +575,18 @@ itsu_status stage_count_then_write(itsu_context *ctx, void (*count)(const Arena 
                                    itsu_status (*ensure)(itsu_context *, int64_t))
 {
   itsu_status st;
-  if ((st = clear_flags(ctx)) != ITSU_OK) return st;
-  count(arena_of(ctx), launch_of(ctx));
-  if ((st = check_launch(ctx)) != ITSU_OK) return st;
-  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  for (int attempt = 0;; ++attempt) {
+    if ((st = clear_flags(ctx)) != ITSU_OK) return st;
+    ITSU_CUDA(ctx, cudaMemsetAsync(&ctx->d_status->cell_entries, 0, sizeof(int64_t), ctx->stream));
+    count(arena_of(ctx), launch_of(ctx));
+    if ((st = check_launch(ctx)) != ITSU_OK) return st;
+    if ((st = sync_status(ctx)) != ITSU_OK) return st;
+    // the cell count pass keeps its entries for the write: if they overflowed their scratch,
+    // grow it and count again
+    if (!(ctx->h_status->flags & itsu::kFlagCapScratch) || (ctx->h_status->flags & itsu::kFlagCountOverflow)) break;
+    if (attempt == 4) return fail(ctx, ITSU_ERR_CAPACITY, "cell entry scratch growth did not converge");
+    if ((st = ensure_cell_entries(ctx, ctx->h_status->cell_entries + cell_entry_slack(ctx))) != ITSU_OK) return st;
+  }
   const DevStatus &s = *ctx->h_status;
   if (s.flags & itsu::kFlagCountOverflow) return count_overflow(ctx);
   if (s.flags & itsu::kCapacityMask) {
@@ -751,9 +802,10 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
   release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->trk_tl); release(ctx->trk_owner); release(ctx->cell_off); release(ctx->cell_lookup);
-  release(ctx->cells); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
+  release(ctx->cells); release(ctx->cell_entries); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
+  release(ctx->d_master); release(ctx->d_mlp);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -1254,8 +1306,13 @@ itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_t
   if ((st = require_stage(ctx, kRoads, "itsu_batch_profile")) != ITSU_OK) return st;
   if (repeats < 1 || !times || capacity < 0) return fail(ctx, ITSU_ERR_INVALID, "bad profile arguments");
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
-  int n = 0;
-  const itsu::KernelStep *steps = itsu::pipeline_steps(&n);
+  int n_all = 0;
+  const itsu::KernelStep *all = itsu::pipeline_steps(&n_all);
+  std::vector<itsu::KernelStep> steps;  // the steps that launch a kernel in this context's form
+  for (int k = 0; k < n_all; ++k) {
+    if (!all[k].learned_only || ctx->prefilter) steps.push_back(all[k]);
+  }
+  const int n = (int)steps.size();
   std::vector<cudaEvent_t> ev(n + 1, nullptr);
   std::vector<double> total(n, 0.0);
   for (auto &e : ev) {
@@ -1289,6 +1346,327 @@ itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_t
     times[k].launches = repeats;
   }
   if (count) *count = n;
+  return ITSU_OK;
+}
+
+}  // extern "C"
+
+// ---- learned prefilter ----
+
+namespace {
+
+uint64_t host_splitmix64(uint64_t &state)
+{
+  uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// binary32 -> bfloat16, round to nearest even (NaN stays a quiet NaN)
+uint16_t host_bf16(float f)
+{
+  uint32_t u;
+  std::memcpy(&u, &f, sizeof u);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+uint64_t fnv1a64(const unsigned char *p, size_t n, uint64_t h = 0xcbf29ce484222325ull)
+{
+  for (size_t i = 0; i < n; ++i) {
+    h ^= p[i];
+    h *= 0x100000001b3ull;
+  }
+  return h;
+}
+
+constexpr char kCheckpointMagic[8] = {'I', 'T', 'S', 'U', 'M', 'L', 'P', '1'};
+constexpr uint32_t kCheckpointVersion = 1;
+constexpr uint32_t kBf16Weights = ITSU_MLP_HIDDEN * ITSU_MLP_INPUTS + ITSU_MLP_HIDDEN * ITSU_MLP_HIDDEN + ITSU_MLP_HIDDEN;
+
+struct CheckpointHeader {
+  char magic[8];
+  uint32_t version, n_params, model_bytes, n_bf16;
+};
+
+// The BF16 copies of w1, w2, w3 in that order.
+std::vector<uint16_t> bf16_weights(const itsu_prefilter_model &m)
+{
+  std::vector<uint16_t> out;
+  out.reserve(kBf16Weights);
+  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
+    for (int i = 0; i < ITSU_MLP_INPUTS; ++i) out.push_back(host_bf16(m.w1[o][i]));
+  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
+    for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) out.push_back(host_bf16(m.w2[o][i]));
+  for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) out.push_back(host_bf16(m.w3[i]));
+  return out;
+}
+
+template <typename T>
+struct DeviceScratch {  // a temporary device allocation freed on scope exit
+  T *p = nullptr;
+  ~DeviceScratch() { if (p) cudaFree(p); }
+};
+
+itsu_status require_model(itsu_context *ctx, const char *what)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "%s: null context", what);
+  if (!ctx->has_model) return fail(ctx, ITSU_ERR_STATE, "%s: no prefilter model set", what);
+  return ITSU_OK;
+}
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+static_assert(sizeof(itsu_prefilter_model) == sizeof(float) * (ITSU_MLP_PARAMS + 2 * ITSU_MLP_INPUTS + 1), "model layout");
+static_assert(ITSU_MLP_PARAMS == itsu::kMlpParams, "parameter count");
+
+void itsu_prefilter_init(itsu_prefilter_model *model, uint64_t seed)
+{
+  if (!model) return;
+  std::memset(model, 0, sizeof *model);
+  uint64_t state = seed;
+  auto uniform = [&](float limit) {
+    const double u = (double)(host_splitmix64(state) >> 11) * (1.0 / 9007199254740992.0);  // [0, 1)
+    return (float)((2.0 * u - 1.0) * limit);
+  };
+  // Glorot-uniform limits sqrt(6 / (fan_in + fan_out))
+  const float l1 = (float)std::sqrt(6.0 / (ITSU_MLP_INPUTS + ITSU_MLP_HIDDEN));
+  const float l2 = (float)std::sqrt(6.0 / (2 * ITSU_MLP_HIDDEN));
+  const float l3 = (float)std::sqrt(6.0 / (ITSU_MLP_HIDDEN + 1));
+  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
+    for (int i = 0; i < ITSU_MLP_INPUTS; ++i) model->w1[o][i] = uniform(l1);
+  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
+    for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) model->w2[o][i] = uniform(l2);
+  for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) model->w3[i] = uniform(l3);
+  for (int i = 0; i < ITSU_MLP_INPUTS; ++i) model->inv_std[i] = 1.0f;
+  model->logit_threshold = 0.0f;
+}
+
+void itsu_train_config_default(itsu_train_config *cfg)
+{
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof *cfg);
+  cfg->steps = 20000;
+  cfg->batch = 8192;
+  cfg->lr = 2e-3f;
+  cfg->lr_final = 1e-4f;
+  cfg->beta1 = 0.9f;
+  cfg->beta2 = 0.999f;
+  cfg->eps = 1e-8f;
+  cfg->weight_decay = 0.0f;
+  cfg->pos_weight = 1.0f;
+  cfg->seed = 1;
+}
+
+itsu_status itsu_prefilter_save(const itsu_prefilter_model *model, const char *path)
+{
+  if (!model || !path) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_save: null argument");
+  CheckpointHeader h;
+  std::memcpy(h.magic, kCheckpointMagic, sizeof h.magic);
+  h.version = kCheckpointVersion;
+  h.n_params = ITSU_MLP_PARAMS;
+  h.model_bytes = sizeof(itsu_prefilter_model);
+  h.n_bf16 = kBf16Weights;
+  const std::vector<uint16_t> bf = bf16_weights(*model);
+  std::vector<unsigned char> buf(sizeof h + sizeof *model + sizeof(uint16_t) * bf.size());
+  std::memcpy(buf.data(), &h, sizeof h);
+  std::memcpy(buf.data() + sizeof h, model, sizeof *model);
+  std::memcpy(buf.data() + sizeof h + sizeof *model, bf.data(), sizeof(uint16_t) * bf.size());
+  const uint64_t sum = fnv1a64(buf.data(), buf.size());
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_save: cannot open %s", path);
+  const bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size() && std::fwrite(&sum, sizeof sum, 1, f) == 1;
+  if (std::fclose(f) != 0 || !ok) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_save: write to %s failed", path);
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_load(const char *path, itsu_prefilter_model *model)
+{
+  if (!model || !path) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: null argument");
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: cannot open %s", path);
+  const size_t body = sizeof(CheckpointHeader) + sizeof(itsu_prefilter_model) + sizeof(uint16_t) * kBf16Weights;
+  std::vector<unsigned char> buf(body + sizeof(uint64_t) + 1);
+  const size_t got = std::fread(buf.data(), 1, buf.size(), f);
+  std::fclose(f);
+  if (got != body + sizeof(uint64_t)) {
+    return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s has %zu bytes, a checkpoint has %zu", path, got,
+                body + sizeof(uint64_t));
+  }
+  CheckpointHeader h;
+  std::memcpy(&h, buf.data(), sizeof h);
+  if (std::memcmp(h.magic, kCheckpointMagic, sizeof h.magic) != 0 || h.version != kCheckpointVersion ||
+      h.n_params != ITSU_MLP_PARAMS || h.model_bytes != sizeof(itsu_prefilter_model) || h.n_bf16 != kBf16Weights) {
+    return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s is not a version-%u prefilter checkpoint", path,
+                kCheckpointVersion);
+  }
+  uint64_t sum;
+  std::memcpy(&sum, buf.data() + body, sizeof sum);
+  if (fnv1a64(buf.data(), body) != sum) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s: checksum mismatch", path);
+  itsu_prefilter_model m;
+  std::memcpy(&m, buf.data() + sizeof h, sizeof m);
+  const std::vector<uint16_t> bf = bf16_weights(m);
+  if (std::memcmp(bf.data(), buf.data() + sizeof h + sizeof m, sizeof(uint16_t) * bf.size()) != 0) {
+    return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s: BF16 weights do not match the FP32 master", path);
+  }
+  *model = m;
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_set_model(itsu_context *ctx, const itsu_prefilter_model *model)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_set_model: null context");
+  if (!model) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_set_model: null model");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->d_master) ITSU_CUDA(ctx, cudaMalloc((void **)&ctx->d_master, sizeof(itsu_prefilter_model)));
+  if (!ctx->d_mlp) ITSU_CUDA(ctx, cudaMalloc((void **)&ctx->d_mlp, itsu::mlp_device_bytes()));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->d_master, model, sizeof *model, cudaMemcpyHostToDevice, ctx->stream));
+  itsu::launch_mlp_publish(ctx->d_master, ctx->d_mlp, ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->has_model = true;
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_get_model(itsu_context *ctx, itsu_prefilter_model *model)
+{
+  itsu_status st;
+  if ((st = require_model(ctx, "itsu_prefilter_get_model")) != ITSU_OK) return st;
+  if (!model) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_get_model: null model");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(model, ctx->d_master, sizeof *model, cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_enable(itsu_context *ctx, int32_t enable)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_enable: null context");
+  if (enable && !ctx->has_model) return fail(ctx, ITSU_ERR_STATE, "itsu_prefilter_enable: no prefilter model set");
+  if (enable) {
+    ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+    ITSU_CUDA(ctx, itsu::prepare_learned_kernels());
+  }
+  ctx->prefilter = enable != 0;
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_export(itsu_context *ctx, itsu_prefilter_samples *samples)
+{
+  itsu_status st;
+  if ((st = require_stage(ctx, kRoads, "itsu_prefilter_export")) != ITSU_OK) return st;
+  if (!samples) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_export: null samples");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  const int64_t n_cells = ctx->h_status->total[itsu::kCells], n_roads = ctx->h_status->total[itsu::kRoads];
+  samples->n_cells = n_cells;
+  samples->n_roads = n_roads;
+  if ((samples->features || samples->labels) && samples->capacity < n_cells) {
+    return fail(ctx, ITSU_ERR_CAPACITY, "itsu_prefilter_export: %lld cells, room for %lld", (long long)n_cells,
+                (long long)samples->capacity);
+  }
+  if ((samples->road_cells || samples->road_keys || samples->road_fake) && samples->road_capacity < n_roads) {
+    return fail(ctx, ITSU_ERR_CAPACITY, "itsu_prefilter_export: %lld roads, room for %lld", (long long)n_roads,
+                (long long)samples->road_capacity);
+  }
+  if (samples->features && !aligned16(samples->features)) {
+    return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_export: features must be 16-byte aligned");
+  }
+  itsu::launch_prefilter_export(arena_of(ctx), *samples, ctx->num_sms, ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_score(itsu_context *ctx, const float *features, int64_t n, float *logits)
+{
+  itsu_status st;
+  if ((st = require_model(ctx, "itsu_prefilter_score")) != ITSU_OK) return st;
+  if (n < 0 || (n > 0 && (!features || !logits))) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_score: bad arguments");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu::launch_mlp_score(ctx->d_mlp, features, n, logits, ctx->num_sms, ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_train(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
+                                 const itsu_train_config *cfg, float *losses)
+{
+  itsu_status st;
+  if ((st = require_model(ctx, "itsu_prefilter_train")) != ITSU_OK) return st;
+  if (!cfg || !features || !labels || n <= 0) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_train: bad arguments");
+  if (cfg->steps < 0 || cfg->batch <= 0 || cfg->batch % 32 != 0 || !(cfg->lr >= 0.0f) || !(cfg->lr_final >= 0.0f) ||
+      !(cfg->beta1 >= 0.0f && cfg->beta1 < 1.0f) || !(cfg->beta2 >= 0.0f && cfg->beta2 < 1.0f) || !(cfg->eps > 0.0f)) {
+    return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_train: bad configuration");
+  }
+  if (!aligned16(features)) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_train: features must be 16-byte aligned");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int blocks = itsu::mlp_gradient_blocks(cfg->batch);
+  DeviceScratch<float> partials, m, v, loss;
+  ITSU_CUDA(ctx, cudaMalloc((void **)&partials.p, sizeof(float) * blocks * ITSU_MLP_PARAMS));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&m.p, sizeof(float) * ITSU_MLP_PARAMS));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&v.p, sizeof(float) * ITSU_MLP_PARAMS));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&loss.p, sizeof(float) * std::max<int64_t>(cfg->steps, 1)));
+  ITSU_CUDA(ctx, cudaMemsetAsync(m.p, 0, sizeof(float) * ITSU_MLP_PARAMS, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemsetAsync(v.p, 0, sizeof(float) * ITSU_MLP_PARAMS, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemsetAsync(loss.p, 0, sizeof(float) * std::max<int64_t>(cfg->steps, 1), ctx->stream));
+  double b1t = 1.0, b2t = 1.0;
+  for (int64_t step = 0; step < cfg->steps; ++step) {
+    // cosine decay from lr to lr_final
+    const double frac = cfg->steps > 1 ? (double)step / (double)(cfg->steps - 1) : 0.0;
+    const float lr = (float)(cfg->lr_final + 0.5 * (cfg->lr - cfg->lr_final) * (1.0 + std::cos(3.14159265358979323846 * frac)));
+    b1t *= cfg->beta1;
+    b2t *= cfg->beta2;
+    itsu::launch_mlp_gradient(ctx->d_mlp, features, labels, n, cfg->batch, false, cfg->seed, step, cfg->pos_weight, partials.p,
+                              loss.p + step, ctx->stream);
+    itsu::launch_mlp_adam(ctx->d_master, partials.p, blocks, m.p, v.p, lr, cfg->beta1, cfg->beta2, cfg->eps, cfg->weight_decay,
+                          (float)(1.0 - b1t), (float)(1.0 - b2t), ctx->d_mlp, ctx->stream);
+    if ((step & 1023) == 0) ITSU_CUDA(ctx, cudaGetLastError());
+  }
+  ITSU_CUDA(ctx, cudaGetLastError());
+  if (losses && cfg->steps > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(losses, loss.p, sizeof(float) * cfg->steps, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
+                                    float pos_weight, float *grad, float *loss_out)
+{
+  itsu_status st;
+  if ((st = require_model(ctx, "itsu_prefilter_gradient")) != ITSU_OK) return st;
+  if (!features || !labels || !grad || n <= 0 || n > INT32_MAX - 31) {
+    return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_gradient: bad arguments");
+  }
+  if (!aligned16(features)) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_gradient: features must be 16-byte aligned");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int32_t batch = (int32_t)n;
+  const int blocks = itsu::mlp_gradient_blocks(batch);
+  DeviceScratch<float> partials, loss;
+  ITSU_CUDA(ctx, cudaMalloc((void **)&partials.p, sizeof(float) * blocks * ITSU_MLP_PARAMS));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&loss.p, sizeof(float)));
+  ITSU_CUDA(ctx, cudaMemsetAsync(loss.p, 0, sizeof(float), ctx->stream));
+  itsu::launch_mlp_gradient(ctx->d_mlp, features, labels, n, batch, true, 0, 0, pos_weight, partials.p, loss.p, ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  std::vector<float> h((size_t)blocks * ITSU_MLP_PARAMS);
+  float l = 0.0f;
+  ITSU_CUDA(ctx, cudaMemcpyAsync(h.data(), partials.p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(&l, loss.p, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < ITSU_MLP_PARAMS; ++i) {
+    double sum = 0.0;
+    for (int b = 0; b < blocks; ++b) sum += h[(size_t)b * ITSU_MLP_PARAMS + i];
+    grad[i] = (float)sum;
+  }
+  if (loss_out) *loss_out = l;
   return ITSU_OK;
 }
 

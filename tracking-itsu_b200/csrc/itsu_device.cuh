@@ -124,10 +124,12 @@ __device__ __forceinline__ bool cell_precut(int layer, float t1_tan_lambda, floa
 }
 
 // Tracker.cxx:175-216: circle-plane normal, radius and DCA of the three clusters. Returns false
-// when the pair is rejected; otherwise fills the unit normal and curvature.
+// when the pair is rejected; otherwise fills the unit normal and curvature. dca_out receives the
+// DCA whenever it is computed (-1 when the clusters give no plane).
 __device__ __forceinline__ bool cell_geometry(int layer, float4 c1, float4 c2, float4 c3, float vx, float vy, float3 &normal,
-                                              float &curvature)
+                                              float &curvature, float &dca_out)
 {
+  dca_out = -1.0f;
   const float r1sq = c1.w * c1.w;
   const float r2sq = c2.w * c2.w;
   const float r3sq = c3.w * c3.w;
@@ -150,12 +152,20 @@ __device__ __forceinline__ bool cell_geometry(int layer, float4 c1, float4 c2, f
   const float ccx = -0.5f * unx / unz;
   const float ccy = -0.5f * uny / unz;
   const float dca = fabsf(radius - sqrtf(ccx * ccx + ccy * ccy));
+  dca_out = dca;
   if (dca > kC.cell_max_dca[layer]) {
     return false;
   }
   normal = make_float3(unx, uny, unz);
   curvature = 1.0f / radius;
   return true;
+}
+
+__device__ __forceinline__ bool cell_geometry(int layer, float4 c1, float4 c2, float4 c3, float vx, float vy, float3 &normal,
+                                              float &curvature)
+{
+  float dca;
+  return cell_geometry(layer, c1, c2, c3, vx, vy, normal, curvature, dca);
 }
 
 // Tracker.cxx:448-459: neighbour cut between a cell and a next-layer cell.

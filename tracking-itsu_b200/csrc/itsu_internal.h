@@ -20,6 +20,8 @@
 
 namespace itsu {
 
+struct MlpDevice;  // the prefilter model (itsu_mlp.cuh)
+
 enum : int32_t {
   kFlagInvalid = 1,
   kFlagCapTracklets = 2,
@@ -27,9 +29,12 @@ enum : int32_t {
   kFlagCapNeighbours = 8,
   kFlagCapRoads = 16,
   kFlagCountOverflow = 32,
+  kFlagCapScratch = 64,  // the cell entries of the count pass exceed their scratch
 };
 constexpr int kTrackletSlotsPerCluster = 48;  // outer clusters the tracklet count pass keeps per inner cluster
-constexpr int32_t kCapacityMask = kFlagCapTracklets | kFlagCapCells | kFlagCapNeighbours | kFlagCapRoads | kFlagCountOverflow;
+constexpr int32_t kCapacityMask =
+    kFlagCapTracklets | kFlagCapCells | kFlagCapNeighbours | kFlagCapRoads | kFlagCountOverflow | kFlagCapScratch;
+constexpr int kCellChunk = 64;  // cell entries a warp of the cell count pass reserves at a time
 
 // Totals and requirements of a run, written by the device.
 struct DevStatus {
@@ -38,7 +43,21 @@ struct DevStatus {
   int32_t invalid_event;  // first event with a malformed vertex, INT32_MAX if none
   int32_t pad_;
   int64_t total[4];       // tracklets, cells, neighbours, roads
+  int64_t cell_entries;   // cell entries reserved by the cell count pass (may exceed the scratch)
 };
+
+// A cell as the count pass finds it: its first and second tracklets (flat), the outgoing-tracklet
+// bit it came from, and what its geometry gave. The write pass scatters each entry whose bit
+// survived to cell_off[t1] + (its rank among the tracklet's set bits); t1 < 0 marks an unused
+// slot. The learned prefilter scores entries in place (the DCA is one of its features).
+struct __align__(16) CellEntry {
+  int32_t t1;
+  int32_t bit;
+  int32_t t2;
+  float dca;
+  float nx, ny, nz, curvature;
+};
+static_assert(sizeof(CellEntry) == 32, "cell entry layout");
 
 enum TotalIndex { kTracklets = 0, kCells = 1, kNeighbours = 2, kRoads = 3 };
 
@@ -83,6 +102,8 @@ struct Arena {
   int32_t *cell_seg;
   itsu_cell *cells;
   int32_t *cell_seg_id;
+  CellEntry *cell_entries;  // scratch of the cell count pass
+  int64_t cap_cell_entries;
   // neighbours, levels, roads
   int32_t *nb_count;
   int32_t *nb_off;
@@ -93,6 +114,8 @@ struct Arena {
   int32_t *road_off;
   int32_t *road_seg;
   itsu_road *roads;
+  // learned prefilter of the cell stage (null: the plain path)
+  const MlpDevice *mlp;
   // scan scratch and status
   int64_t *scan_partials;
   DevStatus *status;
@@ -125,9 +148,35 @@ void launch_roads_write(const Arena &a, const Launch &l);
 struct KernelStep {
   const char *name;
   void (*launch)(const Arena &, const Launch &);
+  bool learned_only;  // launches a kernel only in the learned-prefilter form
 };
 const KernelStep *pipeline_steps(int *count);
-int kernels_per_run();
+int kernels_per_run();  // kernels one plain run launches (the learned form adds the learned_only steps)
+
+// Opts the learned cell-count kernel in to the shared memory it needs (current device).
+cudaError_t prepare_learned_kernels();
+
+// Learned prefilter (itsu_prefilter.cu), all asynchronous on `stream`.
+// The FP32 master parameters (itsu_prefilter_model) -> the device model (BF16 weights).
+void launch_mlp_publish(const itsu_prefilter_model *master, MlpDevice *model, cudaStream_t stream);
+// One training sample per cell of the last run: its pair features and whether a found road uses
+// it; per road, its 5 cells as sample rows and its key (event, 7 layer-local cluster indices).
+void launch_prefilter_export(const Arena &a, const itsu_prefilter_samples &out, int num_sms, cudaStream_t stream);
+void launch_mlp_score(const MlpDevice *model, const float *features, int64_t n, float *logits, int num_sms, cudaStream_t stream);
+// Mean-loss gradient of one minibatch: each block writes its partial sum of the gradient to
+// grad_partials[block][kMlpParams] (mlp_gradient_blocks(batch) blocks) and adds the batch loss
+// to *loss. With sequential set the batch is samples 0..batch-1; otherwise `batch` samples drawn
+// with replacement from n by (seed, step). features: 16-byte aligned rows of 8 floats.
+void launch_mlp_gradient(const MlpDevice *model, const float *features, const uint8_t *labels, int64_t n, int32_t batch,
+                         bool sequential, uint64_t seed, int64_t step, float pos_weight, float *grad_partials, float *loss,
+                         cudaStream_t stream);
+int mlp_gradient_blocks(int32_t batch);
+int mlp_max_gradient_blocks();
+// One Adam step on the master parameters from the summed partials, then publishes the device model.
+void launch_mlp_adam(itsu_prefilter_model *master, const float *grad_partials, int blocks, float *m, float *v, float lr,
+                     float beta1, float beta2, float eps, float weight_decay, float bias1, float bias2, MlpDevice *model,
+                     cudaStream_t stream);
+size_t mlp_device_bytes();
 
 // Sets the calling thread's last error message (returned by itsu_last_error(NULL)).
 void set_thread_error(const char *message);

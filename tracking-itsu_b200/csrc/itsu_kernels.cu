@@ -19,6 +19,7 @@
 
 #include "itsu_device.cuh"
 #include "itsu_internal.h"
+#include "itsu_mlp.cuh"
 
 namespace itsu {
 namespace {
@@ -65,6 +66,7 @@ __global__ void k_status_init(DevStatus *s)
   for (int k = 0; k < 4; ++k) {
     s->total[k] = 0;
   }
+  s->cell_entries = 0;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -792,7 +794,7 @@ struct CellLane {
   float vx, vy, vz;
   int32_t j0, n_out;     // the outgoing tracklets of the tracklet's outer cluster: [j0, j0 + n_out)
   int64_t c3_base;       // first cluster of layer L + 2
-  int32_t t1_local, t1_first, t2_base;  // tracklet index in its layer, its first cluster, first tracklet of layer L + 1
+  int32_t t1_local, t1_first, t1_second, t2_base;  // tracklet index in its layer, its clusters, first tracklet of layer L + 1
 };
 
 __device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t n)
@@ -818,6 +820,7 @@ __device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t
   s.t1_tan_lambda = t1.tan_lambda;
   s.t1_phi = t1.phi;
   s.t1_first = t1.first_cluster;
+  s.t1_second = t1.second_cluster;
   s.c1 = a.xyzr[lo[s.layer] + t1.first_cluster];
   const int64_t c2i = lo[s.layer + 1] + t1.second_cluster;
   s.c2 = a.xyzr[c2i];
@@ -898,10 +901,12 @@ __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const Ce
 // Count pass: for each first tracklet, a mask of which of its (<= 64) outgoing tracklets make a
 // cell, and their number. The warp flattens its 32 tracklets' pairs across lanes (Tracker.cxx:
 // 155-158 iterates them per tracklet); pairs that pass the cheap cuts queue up so the circle
-// geometry runs with all 32 lanes converged.
+// geometry runs with all 32 lanes converged. Each pair that passes becomes a cell entry (its
+// tracklets, normal, curvature and DCA) in the warp's current chunk of the entry scratch, so the
+// write pass needs no geometry.
 __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
 {
-  __shared__ int4 queue[kMaxThreads / 32][kCellQueue];             // (owner lane, pair bit, c3 flat, -)
+  __shared__ int4 queue[kMaxThreads / 32][kCellQueue];             // (owner lane, pair bit, c3 flat, t2 flat)
   __shared__ unsigned long long masks[kMaxThreads / 32][32];
   if (capacity_failed(a.status)) {
     return;
@@ -909,20 +914,19 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t n = a.status->total[kTracklets];
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  int64_t chunk_pos = 0, chunk_end = 0;  // this warp's reserved cell entries (warp-uniform)
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
     const CellLane s = cell_lane(a, base + lane, n);
     const bool big = s.n_out > kMaxMaskedOut;
-    // Only outgoing tracklets with |dtanL| < 0.025 can pass (Tracker.cxx:161-166): |fl(t1 - t2)|
-    // < 0.025f implies |t1 - t2| < 0.025f exactly. The lane marks its window with binary64 bounds
-    // (widened by 1e-12) from the compact slopes, one independent load per outgoing tracklet.
+    // Only outgoing tracklets with |dtanL| < 0.025 can pass (Tracker.cxx:161-166). The lane
+    // evaluates that first cut term exactly as cell_precut does, on the compact slopes (one
+    // independent 4-byte load per outgoing tracklet), and queues only the pairs it keeps.
     unsigned long long window = 0;
-    if (!big && s.n_out > 0 && isfinite(s.t1_tan_lambda)) {
+    if (!big && s.n_out > 0) {
       const float *tl = a.trk_tl + s.j0;
-      const double lo_d = (double)s.t1_tan_lambda - (double)kCellMaxDeltaTanLambda - 1e-12;
-      const double hi_d = (double)s.t1_tan_lambda + (double)kCellMaxDeltaTanLambda + 1e-12;
+#pragma unroll 4
       for (int q = 0; q < s.n_out; ++q) {
-        const double v = (double)tl[q];
-        window |= (unsigned long long)(v >= lo_d && v <= hi_d) << q;
+        window |= (unsigned long long)(fabsf(s.t1_tan_lambda - tl[q]) < kCellMaxDeltaTanLambda) << q;
       }
     }
     masks[warp][lane] = 0ull;
@@ -936,12 +940,40 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
       const float4 c1 = shfl4(s.c1, owner), c2 = shfl4(s.c2, owner);
       const float vx = __shfl_sync(0xffffffffu, s.vx, owner), vy = __shfl_sync(0xffffffffu, s.vy, owner);
       const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
+      bool pass = false;
+      float3 normal = make_float3(0.0f, 0.0f, 0.0f);
+      float curvature = 0.0f, dca = 0.0f;
       if (lane < count) {
-        float3 normal;
-        float curvature;
-        if (cell_geometry(layer, c1, c2, a.xyzr[q.z], vx, vy, normal, curvature)) {
+        pass = cell_geometry(layer, c1, c2, a.xyzr[q.z], vx, vy, normal, curvature, dca);
+        if (pass) {
           atomicOr(&masks[warp][owner], 1ull << q.y);
         }
+      }
+      // entries: the passing lanes' slots, contiguous in the warp's chunk
+      const unsigned m = __ballot_sync(0xffffffffu, pass);
+      const int need = __popc(m);
+      const int rank = __popc(m & ((1u << lane) - 1u));
+      int64_t slot = chunk_pos + rank;
+      if (need > chunk_end - chunk_pos) {
+        const int room = (int)(chunk_end - chunk_pos);
+        unsigned long long fresh = 0;
+        if (lane == 0) {
+          fresh = atomicAdd(reinterpret_cast<unsigned long long *>(&a.status->cell_entries), (unsigned long long)kCellChunk);
+          if ((int64_t)fresh + kCellChunk > a.cap_cell_entries) {
+            atomicOr(&a.status->flags, kFlagCapScratch);
+          }
+        }
+        const int64_t fresh_base = (int64_t)__shfl_sync(0xffffffffu, fresh, 0);
+        slot = rank < room ? chunk_pos + rank : fresh_base + (rank - room);
+        chunk_pos = fresh_base + (need - room);
+        chunk_end = fresh_base + kCellChunk;
+      } else {
+        chunk_pos += need;
+      }
+      if (pass && slot < a.cap_cell_entries) {
+        int4 *dst = reinterpret_cast<int4 *>(a.cell_entries + slot);
+        dst[0] = make_int4((int)(base + owner), q.y, q.w, __float_as_int(dca));
+        dst[1] = make_int4(__float_as_int(normal.x), __float_as_int(normal.y), __float_as_int(normal.z), __float_as_int(curvature));
       }
     };
     for (int p0 = 0; p0 < total; p0 += 32) {
@@ -967,7 +999,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
       }
       const unsigned m = __ballot_sync(0xffffffffu, pre);
       if (pre) {
-        queue[warp][queued + __popc(m & ((1u << lane) - 1u))] = make_int4(owner, b, (int)c3, 0);
+        queue[warp][queued + __popc(m & ((1u << lane) - 1u))] = make_int4(owner, b, (int)c3, j0 + b);
       }
       queued += __popc(m);
       if (queued >= 32) {
@@ -1003,62 +1035,122 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
     }
     __syncwarp();
   }
+  // the unused rest of the last chunk is marked empty
+  for (int64_t i = chunk_pos + lane; i < chunk_end && i < a.cap_cell_entries; i += 32) {
+    a.cell_entries[i].t1 = -1;
+  }
 }
 
-// Write pass: the cells of each first tracklet at its scanned slot, in outgoing-tracklet order
-// (the mask's bit order). The warp flattens its tracklets' cells across lanes.
-__global__ void __launch_bounds__(kMaxThreads) k_cells_write(Arena a)
+// Learned prefilter: scores the count pass's cell entries, 32 per warp on the tensor cores, and
+// drops those whose logit is below the model's threshold from their tracklet's mask and count
+// before the scan. The score and the exact cuts are combined with AND, so scoring only the pairs
+// that passed the cuts (whose geometry also gave the DCA feature) keeps the same cells as scoring
+// every candidate first. A NaN logit keeps its cell. The pairs of a tracklet with more than
+// kMaxMaskedOut outgoing tracklets are counted in order on one lane and are kept unscored.
+constexpr int kPrefilterThreads = 256;
+
+__global__ void __launch_bounds__(kPrefilterThreads) k_cells_prefilter(Arena a)
 {
+  __shared__ MlpSmem mlp;
+  __shared__ __align__(16) __nv_bfloat16 rows[kPrefilterThreads / 32][32][kRowPitch];
+  load_mlp(mlp, *a.mlp);
+  __syncthreads();
   if (capacity_failed(a.status)) {
     return;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t n = a.status->total[kTracklets];
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
-    const int64_t k = base + lane;
-    unsigned long long mask = 0;
-    int32_t first = 0;
-    bool has = false;
-    if (k < n) {
-      mask = a.cell_mask[k];
-      first = a.cell_off[k];
-      has = a.cell_off[k + 1] > first;
+  const int64_t reserved = a.status->cell_entries;
+  const int64_t n = reserved < a.cap_cell_entries ? reserved : a.cap_cell_entries;
+  const int64_t tiles = (n + 31) / 32;
+  for (int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; tile < tiles; tile += (int64_t)gridDim.x * (blockDim.x >> 5)) {
+    const int64_t i = tile * 32 + lane;
+    int4 h = make_int4(-1, 0, 0, 0);
+    if (i < n) {
+      h = reinterpret_cast<const int4 *>(a.cell_entries + i)[0];
     }
-    // lanes with cells load their tracklet state; the others keep n_out = 0
-    CellLane s = cell_lane(a, has ? k : n, n);
-    s.k = k;
-    const bool big = s.n_out > kMaxMaskedOut;
-    int total = 0;
-    const int excl = warp_exclusive_sum(big ? 0 : __popcll(mask), total);
-    for (int p0 = 0; p0 < total; p0 += 32) {
-      const int p = p0 + lane;
-      const int owner = owner_of(excl, p);
-      const int r = p - __shfl_sync(0xffffffffu, excl, owner);
-      const unsigned long long m = __shfl_sync(0xffffffffu, mask, owner);
-      const float4 c1 = shfl4(s.c1, owner), c2 = shfl4(s.c2, owner);
-      const float vx = __shfl_sync(0xffffffffu, s.vx, owner), vy = __shfl_sync(0xffffffffu, s.vy, owner);
-      const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
-      const int32_t j0 = __shfl_sync(0xffffffffu, s.j0, owner);
-      const int32_t out0 = __shfl_sync(0xffffffffu, first, owner);
-      CellLane o;
-      o.e = __shfl_sync(0xffffffffu, s.e, owner);
-      o.layer = layer;
-      o.t1_local = __shfl_sync(0xffffffffu, s.t1_local, owner);
-      o.t1_first = __shfl_sync(0xffffffffu, s.t1_first, owner);
-      o.t2_base = __shfl_sync(0xffffffffu, s.t2_base, owner);
-      const int64_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
-      if (p < total) {
-        const int b = nth_set_bit(m, r);
-        const int32_t j = j0 + b;
-        const itsu_tracklet t2 = a.tracklets[j];
-        float3 normal;
-        float curvature;
-        cell_geometry(layer, c1, c2, a.xyzr[c3_base + t2.second_cluster], vx, vy, normal, curvature);
-        write_cell(a, out0 + r, o, t2, j, normal, curvature);
+    float f[kMlpIn];
+    if (h.x >= 0) {
+      const int t1k = h.x;
+      const int sid = a.trk_seg_id[t1k];
+      const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
+      const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
+      const itsu_tracklet t1 = a.tracklets[t1k];
+      const itsu_tracklet t2 = a.tracklets[h.z];
+      const float4 c1 = a.xyzr[lo[layer] + t1.first_cluster];
+      const float4 c2 = a.xyzr[lo[layer + 1] + t1.second_cluster];
+      const float4 c3 = a.xyzr[lo[layer + 2] + t2.second_cluster];
+      pair_features(layer, t1.tan_lambda, t1.phi, t2.tan_lambda, t2.phi, c1, c2, c3, a.vtx[3 * e], a.vtx[3 * e + 1],
+                    a.vtx[3 * e + 2], __int_as_float(h.w), f);
+    } else {
+      for (int k = 0; k < kMlpIn; ++k) {
+        f[k] = mlp.mean[k];
       }
     }
-    if (big && has) {  // a crowded outer cluster: in order, on this lane
+    feature_row(mlp.mean, mlp.inv_std, f, rows[warp][lane]);
+    __syncwarp();
+    const float logit = mlp_logits_warp<false>(mlp, rows[warp], nullptr);
+    if (h.x >= 0 && logit < mlp.threshold) {
+      atomicAnd(&a.cell_mask[h.x], ~(1ull << h.y));
+      atomicSub(&a.cell_count[h.x], 1);
+    }
+    __syncwarp();
+  }
+}
+
+// Write pass, part 1: every cell entry whose bit survived goes to its scanned slot, in
+// outgoing-tracklet order within its first tracklet (the rank of its bit in the mask).
+__global__ void __launch_bounds__(kMaxThreads) k_cells_scatter(Arena a)
+{
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int64_t reserved = a.status->cell_entries;
+  const int64_t n = reserved < a.cap_cell_entries ? reserved : a.cap_cell_entries;
+  for (int64_t i = global_thread(); i < n; i += grid_threads()) {
+    const int4 *src = reinterpret_cast<const int4 *>(a.cell_entries + i);
+    const int4 h = src[0];
+    if (h.x < 0) {
+      continue;
+    }
+    const unsigned long long m = a.cell_mask[h.x];
+    if (!((m >> h.y) & 1ull)) {
+      continue;  // removed by the learned prefilter
+    }
+    const int32_t out = a.cell_off[h.x] + __popcll(m & ((1ull << h.y) - 1ull));
+    const int sid = a.trk_seg_id[h.x];
+    const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
+    const int32_t *ts = a.trk_seg + e * ITSU_TRACKLET_LAYERS;
+    const itsu_tracklet t1 = a.tracklets[h.x];
+    const itsu_tracklet t2 = a.tracklets[h.z];
+    const int4 g = src[1];
+    int2 *dst = reinterpret_cast<int2 *>(a.cells + out);
+    dst[0] = make_int2(t1.first_cluster, t1.second_cluster);
+    dst[1] = make_int2(t2.second_cluster, h.x - ts[layer]);
+    dst[2] = make_int2(h.z - ts[layer + 1], g.x);
+    dst[3] = make_int2(g.y, g.z);
+    dst[4] = make_int2(g.w, 1);
+    a.cell_seg_id[out] = e * ITSU_CELL_LAYERS + layer;
+  }
+}
+
+// Write pass, part 2: the cells lookup of every tracklet, and the cells of the tracklets whose
+// outer cluster was too crowded for the pair-parallel count (their mask is empty), in order on
+// one lane.
+__global__ void __launch_bounds__(kMaxThreads) k_cells_lookup(Arena a)
+{
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int64_t n = a.status->total[kTracklets];
+  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
+    const int32_t first = a.cell_off[k];
+    const bool has = a.cell_off[k + 1] > first;
+    const int sid = a.trk_seg_id[k];
+    const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
+    a.cell_lookup[k] = (layer >= 1 && layer < ITSU_CELL_LAYERS && has) ? first - a.cell_seg[e * ITSU_CELL_LAYERS + layer]
+                                                                       : ITSU_UNUSED_INDEX;
+    if (has && a.cell_mask[k] == 0ull) {
+      const CellLane s = cell_lane(a, k, n);
       int64_t out = first;
       for (int b = 0; b < s.n_out; ++b) {
         const int32_t j = s.j0 + b;
@@ -1070,12 +1162,6 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_write(Arena a)
           write_cell(a, out++, s, t2, j, normal, curvature);
         }
       }
-    }
-    if (k < n) {
-      const int sid = a.trk_seg_id[k];
-      const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
-      a.cell_lookup[k] = (layer >= 1 && layer < ITSU_CELL_LAYERS && has) ? first - a.cell_seg[e * ITSU_CELL_LAYERS + layer]
-                                                                         : ITSU_UNUSED_INDEX;
     }
   }
 }
@@ -1366,7 +1452,17 @@ void step_tracklet_segments(const Arena &a, const Launch &l)
 
 void step_cells_count(const Arena &a, const Launch &l) { k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
-void step_cells_write(const Arena &a, const Launch &l) { k_cells_write<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
+// Launches only in the learned form (a.mlp set).
+void step_cells_prefilter(const Arena &a, const Launch &l)
+{
+  if (a.mlp) {
+    k_cells_prefilter<<<l.num_sms * 3, kPrefilterThreads, 0, l.stream>>>(a);  // one wave (3 blocks per SM by registers)
+  }
+}
+
+void step_cells_scatter(const Arena &a, const Launch &l) { k_cells_scatter<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
+
+void step_cells_lookup(const Arena &a, const Launch &l) { k_cells_lookup<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
 void step_cell_segments(const Arena &a, const Launch &l)
 {
@@ -1401,28 +1497,30 @@ const KernelStep kSteps[] = {
     {"tracklet_segments", step_tracklet_segments},       // 6
     {"tracklets_tail", step_tracklets_tail},             // 7
     {"tracklets_write", step_tracklets_write},           // 8
-    {"cells_count", step_cells_count},                     // 8  (c)
-    {"scan_reduce_cells", step_scan_reduce<1>},          // 9
-    {"scan_partials_cells", step_scan_partials<1>},      // 10
-    {"scan_apply_cells", step_scan_apply<1>},            // 11
-    {"cell_segments", step_cell_segments},               // 12
-    {"cells_write", step_cells_write},                    // 13
-    {"neighbour_reset", step_neighbour_reset},           // 14 (d)
-    {"neighbours_count", step_neighbours<false>},        // 15
-    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 16
-    {"scan_partials_neighbours", step_scan_partials<2>}, // 17
-    {"scan_apply_neighbours", step_scan_apply<2>},       // 18
-    {"neighbour_check", step_neighbour_check},           // 19
-    {"neighbours_write", step_neighbours<true>},         // 20
-    {"levels_1", step_levels<1>},                        // 21
-    {"levels_2", step_levels<2>},                        // 22
-    {"levels_3", step_levels<3>},                        // 23
-    {"levels_4", step_levels<4>},                        // 24
-    {"scan_reduce_roads", step_scan_reduce<3>},          // 25 (e)
-    {"scan_partials_roads", step_scan_partials<3>},      // 26
-    {"scan_apply_roads", step_scan_apply<3>},            // 27
-    {"road_segments", step_road_segments},               // 28
-    {"roads_write", step_roads},                         // 29
+    {"cells_count", step_cells_count},                   // 9  (c)
+    {"cells_prefilter", step_cells_prefilter, true},     // 10 (learned form only)
+    {"scan_reduce_cells", step_scan_reduce<1>},          // 11
+    {"scan_partials_cells", step_scan_partials<1>},      // 12
+    {"scan_apply_cells", step_scan_apply<1>},            // 13
+    {"cell_segments", step_cell_segments},               // 14
+    {"cells_scatter", step_cells_scatter},               // 15
+    {"cells_lookup", step_cells_lookup},                 // 16
+    {"neighbour_reset", step_neighbour_reset},           // 17 (d)
+    {"neighbours_count", step_neighbours<false>},        // 18
+    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 19
+    {"scan_partials_neighbours", step_scan_partials<2>}, // 20
+    {"scan_apply_neighbours", step_scan_apply<2>},       // 21
+    {"neighbour_check", step_neighbour_check},           // 22
+    {"neighbours_write", step_neighbours<true>},         // 23
+    {"levels_1", step_levels<1>},                        // 24
+    {"levels_2", step_levels<2>},                        // 25
+    {"levels_3", step_levels<3>},                        // 26
+    {"levels_4", step_levels<4>},                        // 27
+    {"scan_reduce_roads", step_scan_reduce<3>},          // 28 (e)
+    {"scan_partials_roads", step_scan_partials<3>},      // 29
+    {"scan_apply_roads", step_scan_apply<3>},            // 30
+    {"road_segments", step_road_segments},               // 31
+    {"roads_write", step_roads},                         // 32
 };
 constexpr int kNumSteps = sizeof(kSteps) / sizeof(kSteps[0]);
 
@@ -1435,6 +1533,9 @@ void run_steps(int first, int last, const Arena &a, const Launch &l)
 
 }  // namespace
 
+// The learned kernels fit the default shared-memory limit: nothing to opt in to.
+cudaError_t prepare_learned_kernels() { return cudaSuccess; }
+
 const KernelStep *pipeline_steps(int *count)
 {
   *count = kNumSteps;
@@ -1445,13 +1546,20 @@ void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l)
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
 void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 13, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 14, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(15, 20, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(21, 25, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(26, 29, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(30, 30, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 14, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 16, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(17, 22, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(23, 27, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(28, 31, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(32, 32, a, l); }
 
-int kernels_per_run() { return kNumSteps; }
+int kernels_per_run()
+{
+  int n = 0;
+  for (const KernelStep &k : kSteps) {
+    n += k.learned_only ? 0 : 1;
+  }
+  return n;
+}
 
 }  // namespace itsu

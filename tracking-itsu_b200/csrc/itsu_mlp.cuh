@@ -1,0 +1,287 @@
+// itsu_mlp.cuh - the learned tracklet-pair prefilter: pair features and the 8-64-64-1 MLP.
+//
+// The prefilter scores the tracklet pairs that pass the cell cuts of Tracker.cxx:161-216 before
+// they become cells; a pair is dropped when its logit is below the model's threshold. Its 8
+// features are the pair's dphi, dz and dtanL (the cut variables of Tracker.cxx:161-171), the
+// curvature of each tracklet's circle through the primary vertex (the reference Tracklet,
+// Tracklet.h:33-36, has none: this build defines them), the pair's DCA to the vertex (Tracker.cxx:
+// 203-210), the inner layer index and the first cluster's radius. The network is 8 -> 64 -> 64 ->
+// 1 with GELU (tanh form, Hendrycks & Gimpel 2016) and a sigmoid output, BF16 weights and
+// activations, FP32 accumulation and biases. It runs on the tensor cores as warp MMAs
+// (mma.sync m16n8k16, BF16 in, FP32 accumulate) over 32 pairs at a time; each layer's FP32
+// accumulators are re-packed in registers as the next layer's BF16 A operand. Thresholding the
+// logit is thresholding the sigmoid output at sigmoid(threshold).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+namespace itsu {
+
+constexpr int kMlpIn = 8;
+constexpr int kMlpHidden = 64;
+constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1;
+// Offsets of the trainable parameters in the flat FP32 master array (itsu_prefilter_model order).
+constexpr int kOffW1 = 0;
+constexpr int kOffB1 = kOffW1 + kMlpHidden * kMlpIn;
+constexpr int kOffW2 = kOffB1 + kMlpHidden;
+constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;
+constexpr int kOffW3 = kOffB2 + kMlpHidden;
+constexpr int kOffB3 = kOffW3 + kMlpHidden;
+static_assert(kOffB3 + 1 == kMlpParams, "parameter layout");
+
+// Row pitches (in BF16 elements) of the shared-memory operands, padded so that the 8 rows one
+// MMA fragment load touches fall in distinct banks.
+constexpr int kRowPitch = 24;  // feature rows and W1 rows (16 used)
+constexpr int kHidPitch = 72;  // W2 / W3 rows and hidden-activation rows (64 used)
+constexpr int kSmpPitch = 40;  // transposed [unit][sample] operands (32 used)
+
+// The model as the device keeps it in global memory.
+struct MlpDevice {
+  __nv_bfloat16 w1[kMlpHidden][kMlpIn];       // [out][in]
+  __nv_bfloat16 w2[kMlpHidden][kMlpHidden];   // [out][in]
+  __nv_bfloat16 w3[kMlpHidden];
+  float b1[kMlpHidden];
+  float b2[kMlpHidden];
+  float b3;
+  float threshold;
+  float mean[kMlpIn];
+  float inv_std[kMlpIn];
+};
+
+// The model staged in shared memory in MMA-friendly, zero-padded form.
+struct __align__(16) MlpSmem {
+  __nv_bfloat16 w1[kMlpHidden][kRowPitch];  // columns 8.. are zero (the first MMA has K = 16)
+  __nv_bfloat16 w2[kMlpHidden][kHidPitch];
+  __nv_bfloat16 w3[8][kHidPitch];           // row 0 holds the output weights, rows 1..7 are zero (N = 8)
+  float b1[kMlpHidden];
+  float b2[kMlpHidden];
+  float b3;
+  float threshold;
+  float mean[kMlpIn];
+  float inv_std[kMlpIn];
+};
+
+// Block-cooperative copy of the model into shared memory (the caller synchronises the block).
+__device__ __forceinline__ void load_mlp(MlpSmem &s, const MlpDevice &g)
+{
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+  for (int i = threadIdx.x; i < kMlpHidden * kRowPitch; i += blockDim.x) {
+    const int r = i / kRowPitch, c = i % kRowPitch;
+    s.w1[r][c] = c < kMlpIn ? g.w1[r][c] : zero;
+  }
+  for (int i = threadIdx.x; i < kMlpHidden * kHidPitch; i += blockDim.x) {
+    const int r = i / kHidPitch, c = i % kHidPitch;
+    s.w2[r][c] = c < kMlpHidden ? g.w2[r][c] : zero;
+  }
+  for (int i = threadIdx.x; i < 8 * kHidPitch; i += blockDim.x) {
+    const int r = i / kHidPitch, c = i % kHidPitch;
+    s.w3[r][c] = (r == 0 && c < kMlpHidden) ? g.w3[c] : zero;
+  }
+  for (int i = threadIdx.x; i < kMlpHidden; i += blockDim.x) {
+    s.b1[i] = g.b1[i];
+    s.b2[i] = g.b2[i];
+  }
+  for (int i = threadIdx.x; i < kMlpIn; i += blockDim.x) {
+    s.mean[i] = g.mean[i];
+    s.inv_std[i] = g.inv_std[i];
+  }
+  if (threadIdx.x == 0) {
+    s.b3 = g.b3;
+    s.threshold = g.threshold;
+  }
+}
+
+constexpr float kGeluC = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float kGeluA = 0.044715f;
+
+__device__ __forceinline__ float tanh_approx(float x)
+{
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ float gelu(float x)
+{
+  const float u = kGeluC * (x + kGeluA * (x * x * x));
+  return 0.5f * x * (1.0f + tanh_approx(u));
+}
+
+__device__ __forceinline__ float gelu_grad(float x)
+{
+  const float x2 = x * x;
+  const float th = tanh_approx(kGeluC * (x + kGeluA * (x2 * x)));
+  return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * kGeluC * (1.0f + 3.0f * kGeluA * x2);
+}
+
+// Signed curvature (1/R) of the circle through three points of the transverse plane; 0 when
+// they are collinear or coincide.
+__device__ __forceinline__ float circle_curvature(float ax, float ay, float bx, float by, float cx, float cy)
+{
+  const float ux = bx - ax, uy = by - ay, vx = cx - ax, vy = cy - ay, wx = cx - bx, wy = cy - by;
+  const float cross = ux * vy - uy * vx;
+  const float d = sqrtf((ux * ux + uy * uy) * (vx * vx + vy * vy) * (wx * wx + wy * wy));
+  return d > 0.0f ? 2.0f * cross / d : 0.0f;
+}
+
+// The 8 raw features of a pair (t1 from cluster c1 to c2, t2 from c2 to c3; c = (x, y, z, r)).
+__device__ __forceinline__ void pair_features(int layer, float t1_tan_lambda, float t1_phi, float t2_tan_lambda, float t2_phi,
+                                              float4 c1, float4 c2, float4 c3, float vx, float vy, float vz, float dca,
+                                              float f[kMlpIn])
+{
+  const float delta_phi = fabsf(t1_phi - t2_phi);
+  f[0] = fminf(delta_phi, fabsf(delta_phi - 6.28318530717958647692f));
+  f[1] = fabsf(-(0.5f * (t1_tan_lambda + t2_tan_lambda)) * c1.w + c1.z - vz);
+  f[2] = fabsf(t1_tan_lambda - t2_tan_lambda);
+  f[3] = circle_curvature(vx, vy, c1.x, c1.y, c2.x, c2.y);
+  f[4] = circle_curvature(vx, vy, c2.x, c2.y, c3.x, c3.y);
+  f[5] = dca;
+  f[6] = (float)layer;
+  f[7] = c1.w;
+}
+
+// Standardised features as one BF16 row of the first MMA's A operand (columns 8..15 zero).
+__device__ __forceinline__ void feature_row(const float *mean, const float *inv_std, const float f[kMlpIn],
+                                            __nv_bfloat16 *row)
+{
+#pragma unroll
+  for (int k = 0; k < kMlpIn; ++k) {
+    row[k] = __float2bfloat16_rn((f[k] - mean[k]) * inv_std[k]);
+  }
+#pragma unroll
+  for (int k = kMlpIn; k < 16; ++k) {
+    row[k] = __float2bfloat16_rn(0.0f);
+  }
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+// D += A * B for one m16n8k16 tile (A row-major 16x16, B column-major 16x8, BF16; D FP32).
+__device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], uint32_t b0, uint32_t b1)
+{
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Fragment layout of m16n8k16 (g = lane / 4, t = lane % 4): A registers hold (row g, k 2t..2t+1),
+// (row g+8, k 2t..), (row g, k 2t+8..), (row g+8, k 2t+8..); B registers hold (k 2t..2t+1, col g)
+// and (k 2t+8.., col g); D holds (row g, col 2t), (row g, col 2t+1), (row g+8, col 2t), (row g+8,
+// col 2t+1).
+
+// Where the training pass keeps a 32-sample tile's intermediate values.
+struct MlpTrace {
+  float (*a1)[kMlpHidden + 1];  // [sample][unit] layer-1 pre-activations
+  float (*a2)[kMlpHidden + 1];  // [sample][unit] layer-2 pre-activations
+  __nv_bfloat16 (*h1t)[kSmpPitch];  // [unit][sample] layer-1 activations (BF16, as the next MMA sees them)
+};
+
+// Forward pass of rows 16 mt .. 16 mt + 15 of a 32-row tile; returns the logits of rows g and
+// g + 8 of the tile in lo / hi (valid in lanes with t == 0). All lanes of the warp take part.
+template <bool kTrace>
+__device__ __forceinline__ void mlp_forward_m16(const MlpSmem &m, const __nv_bfloat16 (*rows)[kRowPitch], int mt, float &lo,
+                                                float &hi, const MlpTrace *trace)
+{
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = mt * 16 + g, r1 = r0 + 8;
+  uint32_t a[4];
+  a[0] = ld32(&rows[r0][2 * t]);
+  a[1] = ld32(&rows[r1][2 * t]);
+  a[2] = ld32(&rows[r0][2 * t + 8]);
+  a[3] = ld32(&rows[r1][2 * t + 8]);
+  // layer 1: [16 x 16] x [16 x 64] -> GELU -> BF16 A fragments of layer 2 (hk[kk] covers k 16kk..)
+  uint32_t hk[4][4];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    mma_bf16(c, a, ld32(&m.w1[nt * 8 + g][2 * t]), ld32(&m.w1[nt * 8 + g][2 * t + 8]));
+    const int col = nt * 8 + 2 * t;
+    c[0] += m.b1[col];
+    c[1] += m.b1[col + 1];
+    c[2] += m.b1[col];
+    c[3] += m.b1[col + 1];
+    const uint32_t top = pack_bf16(gelu(c[0]), gelu(c[1])), bottom = pack_bf16(gelu(c[2]), gelu(c[3]));
+    hk[nt >> 1][(nt & 1) * 2 + 0] = top;
+    hk[nt >> 1][(nt & 1) * 2 + 1] = bottom;
+    if constexpr (kTrace) {
+      trace->a1[r0][col] = c[0];
+      trace->a1[r0][col + 1] = c[1];
+      trace->a1[r1][col] = c[2];
+      trace->a1[r1][col + 1] = c[3];
+      const __nv_bfloat162 tv = *reinterpret_cast<const __nv_bfloat162 *>(&top);
+      const __nv_bfloat162 bv = *reinterpret_cast<const __nv_bfloat162 *>(&bottom);
+      trace->h1t[col][r0] = tv.x;
+      trace->h1t[col + 1][r0] = tv.y;
+      trace->h1t[col][r1] = bv.x;
+      trace->h1t[col + 1][r1] = bv.y;
+    }
+  }
+  // layer 2: [16 x 64] x [64 x 64]
+  float h2[8][4];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.0f;
+  }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      mma_bf16(h2[nt], hk[kk], ld32(&m.w2[nt * 8 + g][16 * kk + 2 * t]), ld32(&m.w2[nt * 8 + g][16 * kk + 2 * t + 8]));
+    }
+  }
+  // layer 3: [16 x 64] x [64 x 8], column 0 real
+  float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    uint32_t ak[4];
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int nt = 2 * kk + half;
+      const int col = nt * 8 + 2 * t;
+      const float v0 = h2[nt][0] + m.b2[col], v1 = h2[nt][1] + m.b2[col + 1];
+      const float v2 = h2[nt][2] + m.b2[col], v3 = h2[nt][3] + m.b2[col + 1];
+      if constexpr (kTrace) {
+        trace->a2[r0][col] = v0;
+        trace->a2[r0][col + 1] = v1;
+        trace->a2[r1][col] = v2;
+        trace->a2[r1][col + 1] = v3;
+      }
+      ak[half * 2 + 0] = pack_bf16(gelu(v0), gelu(v1));
+      ak[half * 2 + 1] = pack_bf16(gelu(v2), gelu(v3));
+    }
+    mma_bf16(o, ak, ld32(&m.w3[g][16 * kk + 2 * t]), ld32(&m.w3[g][16 * kk + 2 * t + 8]));
+  }
+  lo = o[0] + m.b3;
+  hi = o[2] + m.b3;
+}
+
+// Logits of the 32 rows of a tile; lane l gets row l's. All lanes of the warp take part.
+template <bool kTrace>
+__device__ __forceinline__ float mlp_logits_warp(const MlpSmem &m, const __nv_bfloat16 (*rows)[kRowPitch], const MlpTrace *trace)
+{
+  const int lane = threadIdx.x & 31;
+  float mine = 0.0f;
+#pragma unroll 1
+  for (int mt = 0; mt < 2; ++mt) {
+    float lo, hi;
+    mlp_forward_m16<kTrace>(m, rows, mt, lo, hi, trace);
+    // row r of this m-tile sits in lane 4 (r mod 8), in lo for r < 8 and hi otherwise
+    const int src = (lane & 7) << 2;
+    lo = __shfl_sync(0xffffffffu, lo, src);
+    hi = __shfl_sync(0xffffffffu, hi, src);
+    if ((lane >> 4) == mt) {
+      mine = (lane & 8) ? hi : lo;
+    }
+  }
+  return mine;
+}
+
+}  // namespace itsu

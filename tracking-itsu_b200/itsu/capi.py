@@ -74,6 +74,40 @@ class Batch(ctypes.Structure):
                 ("n_events", ctypes.c_int32), ("reserved_", ctypes.c_int32), ("n_clusters", ctypes.c_int64)]
 
 
+MLP_INPUTS, MLP_HIDDEN = 8, 64
+MLP_PARAMS = MLP_HIDDEN * MLP_INPUTS + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
+
+
+class PrefilterModel(ctypes.Structure):
+    _fields_ = [("w1", (ctypes.c_float * MLP_INPUTS) * MLP_HIDDEN), ("b1", ctypes.c_float * MLP_HIDDEN),
+                ("w2", (ctypes.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b2", ctypes.c_float * MLP_HIDDEN),
+                ("w3", ctypes.c_float * MLP_HIDDEN), ("b3", ctypes.c_float), ("mean", ctypes.c_float * MLP_INPUTS),
+                ("inv_std", ctypes.c_float * MLP_INPUTS), ("logit_threshold", ctypes.c_float)]
+
+    def params(self) -> np.ndarray:
+        """The trainable parameters as one float32 array (w1, b1, w2, b2, w3, b3)."""
+        return np.frombuffer(bytes(self), np.float32, MLP_PARAMS).copy()
+
+    def arrays(self) -> dict:
+        return dict(w1=np.ctypeslib.as_array(self.w1).copy(), b1=np.ctypeslib.as_array(self.b1).copy(),
+                    w2=np.ctypeslib.as_array(self.w2).copy(), b2=np.ctypeslib.as_array(self.b2).copy(),
+                    w3=np.ctypeslib.as_array(self.w3).copy(), b3=float(self.b3),
+                    mean=np.ctypeslib.as_array(self.mean).copy(), inv_std=np.ctypeslib.as_array(self.inv_std).copy(),
+                    logit_threshold=float(self.logit_threshold))
+
+
+class PrefilterSamples(ctypes.Structure):
+    _fields_ = [("features", ctypes.c_void_p), ("labels", ctypes.c_void_p), ("capacity", ctypes.c_int64),
+                ("road_cells", ctypes.c_void_p), ("road_keys", ctypes.c_void_p), ("road_fake", ctypes.c_void_p),
+                ("road_capacity", ctypes.c_int64), ("n_cells", ctypes.c_int64), ("n_roads", ctypes.c_int64)]
+
+
+class TrainConfig(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int64), ("batch", ctypes.c_int32), ("reserved_", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("lr_final", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("weight_decay", ctypes.c_float), ("pos_weight", ctypes.c_float), ("seed", ctypes.c_uint64)]
+
+
 _lib = None
 
 # (name, restype, argtypes) of every entry point declared in include/itsu.h
@@ -117,7 +151,52 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("itsu_batch_profile", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    ("itsu_prefilter_init", None, [ctypes.POINTER(PrefilterModel), ctypes.c_uint64]),
+    ("itsu_train_config_default", None, [ctypes.POINTER(TrainConfig)]),
+    ("itsu_prefilter_save", ctypes.c_int, [ctypes.POINTER(PrefilterModel), ctypes.c_char_p]),
+    ("itsu_prefilter_load", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(PrefilterModel)]),
+    ("itsu_prefilter_set_model", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PrefilterModel)]),
+    ("itsu_prefilter_get_model", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PrefilterModel)]),
+    ("itsu_prefilter_enable", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("itsu_prefilter_export", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PrefilterSamples)]),
+    ("itsu_prefilter_score", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
+    ("itsu_prefilter_train", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(TrainConfig), ctypes.c_void_p]),
+    ("itsu_prefilter_gradient", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p,
+      ctypes.POINTER(ctypes.c_float)]),
 ]
+
+
+def prefilter_init(seed: int) -> PrefilterModel:
+    """A fresh seeded model (host only)."""
+    m = PrefilterModel()
+    load().itsu_prefilter_init(ctypes.byref(m), seed)
+    return m
+
+
+def train_config(**kw) -> TrainConfig:
+    cfg = TrainConfig()
+    load().itsu_train_config_default(ctypes.byref(cfg))
+    for k, v in kw.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def prefilter_save(model: PrefilterModel, path: str):
+    L = load()
+    st = L.itsu_prefilter_save(ctypes.byref(model), path.encode())
+    if st != OK:
+        raise ItsuError(st, L.itsu_last_error(None).decode())
+
+
+def prefilter_load(path: str) -> PrefilterModel:
+    L = load()
+    m = PrefilterModel()
+    st = L.itsu_prefilter_load(path.encode(), ctypes.byref(m))
+    if st != OK:
+        raise ItsuError(st, L.itsu_last_error(None).decode())
+    return m
 
 
 def load(path: str = LIB_PATH):
@@ -285,11 +364,11 @@ class Context:
 
     def profile(self, repeats: int = 5) -> list:
         """(kernel name, mean ms) for every kernel of the last batch, timed one by one."""
-        n = self.lib.itsu_kernels_per_run()
+        n = self.lib.itsu_kernels_per_run() + 8  # the learned form launches more
         arr = (KernelTime * n)()
         cnt = ctypes.c_int32()
         self._check(self.lib.itsu_batch_profile(self.h, repeats, arr, n, ctypes.byref(cnt)))
-        return [(arr[k].name.decode(), float(arr[k].ms)) for k in range(cnt.value)]
+        return [(arr[k].name.decode(), float(arr[k].ms)) for k in range(min(cnt.value, n))]
 
     def frames_run_host(self, clusters, frame_offsets, vertices, vertex_frame, roads_capacity=None):
         """Pile-up frames: each frame's clusters once, one run per vertex; returns (roads, road_offsets)."""
@@ -328,3 +407,40 @@ class Context:
         t = Tune()
         self._check(self.lib.itsu_get_tune(self.h, band, ctypes.byref(t)))
         return dict(band=t.band, threads_per_block=t.threads_per_block, blocks_per_sm=t.blocks_per_sm, prune=t.prune, ms=t.ms)
+
+    # ---- learned prefilter ----
+
+    def prefilter_set_model(self, model: PrefilterModel):
+        self._check(self.lib.itsu_prefilter_set_model(self.h, ctypes.byref(model)))
+
+    def prefilter_get_model(self) -> PrefilterModel:
+        m = PrefilterModel()
+        self._check(self.lib.itsu_prefilter_get_model(self.h, ctypes.byref(m)))
+        return m
+
+    def prefilter_enable(self, enable: bool = True):
+        self._check(self.lib.itsu_prefilter_enable(self.h, 1 if enable else 0))
+
+    def prefilter_export(self, features=0, labels=0, capacity=0, road_cells=0, road_keys=0, road_fake=0, road_capacity=0):
+        """Device pointers (ints) of the buffers to fill; returns (n_cells, n_roads)."""
+        s = PrefilterSamples()
+        s.features, s.labels, s.capacity = features or None, labels or None, capacity
+        s.road_cells, s.road_keys, s.road_fake, s.road_capacity = road_cells or None, road_keys or None, road_fake or None, road_capacity
+        self._check(self.lib.itsu_prefilter_export(self.h, ctypes.byref(s)))
+        return s.n_cells, s.n_roads
+
+    def prefilter_score(self, features_ptr: int, n: int, logits_ptr: int):
+        self._check(self.lib.itsu_prefilter_score(self.h, ctypes.c_void_p(features_ptr), n, ctypes.c_void_p(logits_ptr)))
+
+    def prefilter_train(self, features_ptr: int, labels_ptr: int, n: int, cfg: TrainConfig) -> np.ndarray:
+        losses = np.zeros(max(int(cfg.steps), 1), np.float32)
+        self._check(self.lib.itsu_prefilter_train(self.h, ctypes.c_void_p(features_ptr), ctypes.c_void_p(labels_ptr), n,
+                                                  ctypes.byref(cfg), _ptr(losses)))
+        return losses[:int(cfg.steps)]
+
+    def prefilter_gradient(self, features_ptr: int, labels_ptr: int, n: int, pos_weight: float = 1.0):
+        grad = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        self._check(self.lib.itsu_prefilter_gradient(self.h, ctypes.c_void_p(features_ptr), ctypes.c_void_p(labels_ptr), n,
+                                                     pos_weight, _ptr(grad), ctypes.byref(loss)))
+        return grad, loss.value

@@ -1,0 +1,389 @@
+"""The learned tracklet-pair prefilter: training pipeline, threshold calibration, evaluation, and
+numpy restatements of its arithmetic (the tests' references).
+
+The model (include/itsu.h, itsu_prefilter_model) scores, inside the cell stage, each tracklet
+pair that passes the exact cell cuts; a pair whose logit is below the model's threshold does not
+become a cell. Everything below runs through the C ABI on one GPU:
+
+1. ``collect``: plain batched runs over seeded central Pb-Pb-like events (6000 tracks, 5% noise);
+   ``itsu_prefilter_export`` gives one sample per cell (its 8 pair features; label 1 when a
+   found road uses the cell) and each road's 5 cells as sample rows.
+2. ``train``: feature standardisation from the training samples, then ``itsu_prefilter_train``
+   (hand-written CUDA forward/backward on the tensor cores, Adam on FP32 master weights).
+3. ``calibrate``: the largest logit threshold that keeps all 5 cells of at least ``target`` of
+   the training roads (a plain road survives the learned form iff all its cells are kept).
+4. ``evaluate``: learned and plain batched runs over held-out events; the fraction of plain
+   roads the learned runs reproduce, and the learned roads that the plain runs lack (zero by
+   construction: a learned run's cells are a subset of the plain run's, and roads are the
+   complete 5-cell chains of the cell graph).
+
+Run ``python -m itsu.prefilter --out <checkpoint>`` (from tracking-itsu_b200/) on a GPU machine.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing
+import os
+import time
+
+import numpy as np
+
+from . import capi, gen
+
+TRAIN_SEED0 = 7_000_000  # training events: seeds TRAIN_SEED0 .. + n_train - 1
+EVAL_SEED0 = 8_000_000   # held-out events
+CHECKPOINT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights", "prefilter_pbpb.itsumlp")
+TWO_PI_F = np.float32(6.28318530717958647692)
+CELL_MAX_DCA = np.array([0.05, 0.04, 0.05, 0.2, 0.4], np.float32)
+
+# ---------------------------------------------------------------------------------------------
+# numpy restatements (float32 ops in the device's order; BF16 by round-to-nearest-even)
+
+
+def bf16_round(x) -> np.ndarray:
+    """float32 -> nearest bfloat16 (ties to even), returned as float32."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16 << 16
+    return u.astype(np.uint32).view(np.float32)
+
+
+def gelu(x):
+    x = np.asarray(x, np.float64)
+    return 0.5 * x * (1.0 + np.tanh(0.7978845608028654 * (x + 0.044715 * x ** 3)))
+
+
+def gelu_grad(x):
+    x = np.asarray(x, np.float64)
+    th = np.tanh(0.7978845608028654 * (x + 0.044715 * x ** 3))
+    return 0.5 * (1.0 + th) + 0.5 * x * (1.0 - th * th) * 0.7978845608028654 * (1.0 + 3.0 * 0.044715 * x * x)
+
+
+def mlp_forward(m: dict, features, rounding: bool = True):
+    """Logits as the device computes them (BF16 inputs, weights and activations; wide
+    accumulation). rounding=False gives the same network in plain float64."""
+    rnd = (lambda a: bf16_round(np.asarray(a, np.float32)).astype(np.float64)) if rounding else (lambda a: np.asarray(a, np.float64))
+    f = np.asarray(features, np.float32)
+    x = rnd((f - m["mean"].astype(np.float32)) * m["inv_std"].astype(np.float32))
+    w1, w2, w3 = (rnd(m[k]) for k in ("w1", "w2", "w3"))
+    a1 = x @ w1.T + m["b1"]
+    h1 = rnd(gelu(a1))
+    a2 = h1 @ w2.T + m["b2"]
+    h2 = rnd(gelu(a2))
+    z = h2 @ w3 + m["b3"]
+    return dict(x=x, a1=a1, h1=h1, a2=a2, h2=h2, z=z, w2=w2, w3=w3)
+
+
+def mlp_gradient(m: dict, features, labels, pos_weight: float = 1.0, rounding: bool = True):
+    """Mean weighted binary cross-entropy and its gradient (itsu_prefilter_model parameter order),
+    in float64 through the forward values (straight-through for the BF16 rounding)."""
+    fw = mlp_forward(m, features, rounding)
+    y = np.asarray(labels, np.float64)
+    n = len(y)
+    w = np.where(y > 0, pos_weight, 1.0)
+    z = fw["z"]
+    loss = float(np.sum(w * (np.maximum(z, 0) - z * y + np.log1p(np.exp(-np.abs(z))))) / n)
+    dz = w * (1.0 / (1.0 + np.exp(-z)) - y) / n
+    g_w3 = fw["h2"].T @ dz
+    g_b3 = dz.sum()
+    d2 = dz[:, None] * fw["w3"][None, :] * gelu_grad(fw["a2"])
+    g_w2 = d2.T @ fw["h1"]
+    g_b2 = d2.sum(0)
+    d1 = (d2 @ fw["w2"]) * gelu_grad(fw["a1"])
+    g_w1 = d1.T @ fw["x"]
+    g_b1 = d1.sum(0)
+    grad = np.concatenate([g_w1.ravel(), g_b1, g_w2.ravel(), g_b2, g_w3, [g_b3]])
+    return grad, loss
+
+
+def _curvature(ax, ay, bx, by, cx, cy):
+    ux, uy, vx, vy, wx, wy = bx - ax, by - ay, cx - ax, cy - ay, cx - bx, cy - by
+    cross = ux * vy - uy * vx
+    d = np.sqrt((ux * ux + uy * uy) * (vx * vx + vy * vy) * (wx * wx + wy * wy))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(d > 0, np.float32(2.0) * cross / d, np.float32(0.0)).astype(np.float32)
+
+
+def _dca(layer, c1, c2, c3, vx, vy):
+    """Tracker.cxx:175-210 in float32: the DCA of the circle through three clusters."""
+    f = np.float32
+    r1sq, r2sq, r3sq = c1["r"] * c1["r"], c2["r"] * c2["r"], c3["r"] * c3["r"]
+    d1x, d1y, d1z = c2["x"] - c1["x"], c2["y"] - c1["y"], r2sq - r1sq
+    d2x, d2y, d2z = c3["x"] - c1["x"], c3["y"] - c1["y"], r3sq - r1sq
+    nx = (d1y * d2z) - (d1z * d2y)
+    ny = (d1z * d2x) - (d1x * d2z)
+    nz = (d1x * d2y) - (d1y * d2x)
+    with np.errstate(all="ignore"):
+        norm = np.sqrt(nx * nx + ny * ny + nz * nz)
+        inv = f(1.0) / norm
+        unx, uny, unz = nx * inv, ny * inv, nz * inv
+        plane_d = -unx * (c2["x"] - vx) - (uny * c2["y"] - vy) - unz * r2sq
+        nzsq = unz * unz
+        radius = np.sqrt((f(1.0) - nzsq - f(4.0) * plane_d * unz) / (f(4.0) * nzsq))
+        ccx = f(-0.5) * unx / unz
+        ccy = f(-0.5) * uny / unz
+        return np.abs(radius - np.sqrt(ccx * ccx + ccy * ccy)).astype(np.float32)
+
+
+def pair_features(res: dict) -> np.ndarray:
+    """The 8 features of every cell of one vertex's results (oracle canonical form), in the
+    export's row order (layer by layer, cells in order)."""
+    out = []
+    vx, vy, vz = (np.float32(v) for v in res["vertex"])
+    for layer in range(5):
+        cells = res["cells"][layer]
+        if len(cells) == 0:
+            continue
+        t1 = res["tracklets"][layer][cells["t1"]]
+        t2 = res["tracklets"][layer + 1][cells["t2"]]
+        c1 = res["clusters"][layer][cells["c1"]]
+        c2 = res["clusters"][layer + 1][cells["c2"]]
+        c3 = res["clusters"][layer + 2][cells["c3"]]
+        f = np.zeros((len(cells), 8), np.float32)
+        dphi = np.abs(t1["phi"] - t2["phi"])
+        f[:, 0] = np.minimum(dphi, np.abs(dphi - TWO_PI_F))
+        f[:, 1] = np.abs(-(np.float32(0.5) * (t1["tan_lambda"] + t2["tan_lambda"])) * c1["r"] + c1["z"] - vz)
+        f[:, 2] = np.abs(t1["tan_lambda"] - t2["tan_lambda"])
+        f[:, 3] = _curvature(vx, vy, c1["x"], c1["y"], c2["x"], c2["y"])
+        f[:, 4] = _curvature(vx, vy, c2["x"], c2["y"], c3["x"], c3["y"])
+        f[:, 5] = _dca(layer, c1, c2, c3, vx, vy)
+        f[:, 6] = np.float32(layer)
+        f[:, 7] = c1["r"]
+        out.append(f)
+    return np.concatenate(out) if out else np.zeros((0, 8), np.float32)
+
+
+def road_cells(res: dict) -> np.ndarray:
+    """Each road's 5 cells as rows of pair_features(res)."""
+    base = np.concatenate([[0], np.cumsum([len(c) for c in res["cells"]])])[:5]
+    return res["roads"]["cells"].astype(np.int64) + base[None, :]
+
+
+def calibrate(logits: np.ndarray, road_rows: np.ndarray, target: float) -> float:
+    """Largest threshold t such that at least `target` of the roads keep all their cells
+    (logit >= t; NaN logits keep their cell)."""
+    lg = np.where(np.isnan(logits), np.inf, logits.astype(np.float64))
+    road_min = lg[road_rows].min(axis=1) if len(road_rows) else np.zeros(0)
+    if len(road_min) == 0:
+        return float("-inf")
+    s = np.sort(road_min)
+    k = int(math.floor((1.0 - target) * len(s)))
+    k = min(max(k, 0), len(s) - 1)
+    return float(np.float32(s[k]))
+
+
+def compare_roads(plain_keys, plain_fake, learned_keys, learned_fake) -> dict:
+    """Road sets of a plain and a learned run of the same events, keyed by (event, 7 clusters)."""
+    p = {bytes(r) for r in np.ascontiguousarray(plain_keys, np.int32)}
+    lk = np.ascontiguousarray(learned_keys, np.int32)
+    reproduced = extra = extra_fakes = 0
+    for r, fk in zip(lk, learned_fake):
+        if bytes(r) in p:
+            reproduced += 1
+        else:
+            extra += 1
+            extra_fakes += int(fk != 0)
+    return dict(plain_roads=len(plain_keys), learned_roads=len(learned_keys), reproduced=reproduced, extra=extra,
+                extra_fakes=extra_fakes, plain_fakes=int(np.count_nonzero(plain_fake)),
+                learned_fakes=int(np.count_nonzero(learned_fake)))
+
+
+# ---------------------------------------------------------------------------------------------
+# pipeline (GPU)
+
+
+def make_events(seeds, workers: int | None = None) -> list:
+    """Central Pb-Pb-like events (6000 tracks, 5% noise) for the given seeds, generated in
+    parallel worker processes (spawned, so that no CUDA state is forked)."""
+    seeds = list(seeds)
+    workers = workers or min(32, os.cpu_count() or 1)
+    if workers <= 1 or len(seeds) < 8:
+        return [gen.pbpb_event(s) for s in seeds]
+    with multiprocessing.get_context("spawn").Pool(workers) as pool:
+        return pool.map(gen.pbpb_event, seeds, chunksize=max(1, len(seeds) // (4 * workers)))
+
+
+class DeviceBatch:
+    """A batch of events resident on the device (torch owns the memory)."""
+
+    def __init__(self, ctx, events, device):
+        import torch
+
+        clusters, offsets, vertices = gen.pack_batch(events)
+        self.clusters = torch.from_numpy(clusters.view(np.uint8)).to(device)
+        self.offsets = torch.from_numpy(offsets).to(device)
+        self.vertices = torch.from_numpy(vertices).to(device)
+        self.batch = ctx.batch_device(self.clusters.data_ptr(), self.offsets.data_ptr(), self.vertices.data_ptr(), len(events),
+                                      len(clusters))
+
+
+def export_samples(ctx, device):
+    """Samples and road rows of the context's last run, as device tensors."""
+    import torch
+
+    n_cells, n_roads = ctx.prefilter_export()
+    feats = torch.empty((max(n_cells, 1), 8), dtype=torch.float32, device=device)
+    labels = torch.empty(max(n_cells, 1), dtype=torch.uint8, device=device)
+    rcells = torch.empty((max(n_roads, 1), 5), dtype=torch.int32, device=device)
+    ctx.prefilter_export(features=feats.data_ptr(), labels=labels.data_ptr(), capacity=n_cells, road_cells=rcells.data_ptr(),
+                         road_capacity=n_roads)
+    return feats[:n_cells], labels[:n_cells], rcells[:n_roads]
+
+
+def export_roads(ctx, device):
+    import torch
+
+    _, n_roads = ctx.prefilter_export()
+    keys = torch.empty((max(n_roads, 1), 8), dtype=torch.int32, device=device)
+    fake = torch.empty(max(n_roads, 1), dtype=torch.uint8, device=device)
+    ctx.prefilter_export(road_keys=keys.data_ptr(), road_fake=fake.data_ptr(), road_capacity=n_roads)
+    return keys[:n_roads].cpu().numpy(), fake[:n_roads].cpu().numpy()
+
+
+def collect(ctx, seeds, device, chunk: int = 100, workers: int | None = None, log=print) -> dict:
+    """Plain runs over the events of `seeds`; all their samples, concatenated on the device."""
+    import torch
+
+    feats, labels, rows = [], [], []
+    base = 0
+    seeds = list(seeds)
+    for k in range(0, len(seeds), chunk):
+        events = make_events(seeds[k:k + chunk], workers)
+        b = DeviceBatch(ctx, events, device)
+        ctx.prefilter_enable(False)
+        ctx.batch_run(b.batch)
+        f, l, r = export_samples(ctx, device)
+        feats.append(f.clone())
+        labels.append(l.clone())
+        rows.append(r.to(torch.int64) + base)
+        base += len(f)
+        log("collect: events %d..%d, %d cells, %d roads" % (k, k + len(events) - 1, len(f), len(r)))
+    return dict(features=torch.cat(feats), labels=torch.cat(labels), road_rows=torch.cat(rows))
+
+
+def standardisation(features) -> tuple:
+    import torch
+
+    ok = torch.isfinite(features).all(dim=1)
+    f = features[ok].double()
+    mean = f.mean(dim=0)
+    std = f.std(dim=0)
+    std = torch.where(std > 0, std, torch.ones_like(std))
+    return mean.float().cpu().numpy(), (1.0 / std).float().cpu().numpy()
+
+
+def score(ctx, features, device):
+    import torch
+
+    n = len(features)
+    logits = torch.empty(max(n, 1), dtype=torch.float32, device=device)
+    ctx.prefilter_score(features.data_ptr(), n, logits.data_ptr())
+    return logits[:n]
+
+
+def train(ctx, data: dict, device, seed: int = 1, target: float = 0.997, log=print, **train_kw) -> tuple:
+    """Trains a model on `data` (from collect) and calibrates its threshold; returns
+    (model, report dict)."""
+    import torch
+
+    model = capi.prefilter_init(seed)
+    mean, inv_std = standardisation(data["features"])
+    for k in range(8):
+        model.mean[k], model.inv_std[k] = float(mean[k]), float(inv_std[k])
+    ctx.prefilter_set_model(model)
+    ok = torch.isfinite(data["features"]).all(dim=1)
+    f = data["features"][ok].contiguous()
+    y = data["labels"][ok].contiguous()
+    cfg = capi.train_config(**train_kw)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = ctx.prefilter_train(f.data_ptr(), y.data_ptr(), len(f), cfg)
+    train_s = time.perf_counter() - t0
+    model = ctx.prefilter_get_model()
+    logits = score(ctx, data["features"], device).cpu().numpy()
+    rows = data["road_rows"].cpu().numpy()
+    thr = calibrate(logits, rows, target)
+    model.logit_threshold = thr
+    ctx.prefilter_set_model(model)
+    labels = data["labels"].cpu().numpy()
+    kept = ~(logits < thr)
+    report = dict(
+        samples=int(len(f)), positives=int(y.sum().item()), steps=int(cfg.steps), batch=int(cfg.batch), lr=float(cfg.lr),
+        lr_final=float(cfg.lr_final), train_seconds=train_s, loss_first=float(np.mean(losses[:100])) if len(losses) else None,
+        loss_last=float(np.mean(losses[-100:])) if len(losses) else None, threshold=thr, calibration_target=target,
+        train_cells_kept=float(kept.mean()), train_positive_cells_kept=float(kept[labels == 1].mean()),
+        train_negative_cells_kept=float(kept[labels == 0].mean()),
+        train_road_reproduction=float((np.where(np.isnan(logits), np.inf, logits)[rows].min(axis=1) >= thr).mean()),
+    )
+    log("train: %s" % json.dumps(report))
+    return model, report
+
+
+def evaluate(ctx, model, seeds, device, chunk: int = 100, workers: int | None = None, log=print) -> dict:
+    """Learned vs plain batched runs over the events of `seeds`."""
+    ctx.prefilter_set_model(model)
+    tot = dict(plain_roads=0, learned_roads=0, reproduced=0, extra=0, extra_fakes=0, plain_fakes=0, learned_fakes=0,
+               plain_cells=0, learned_cells=0, events=0)
+    seeds = list(seeds)
+    for k in range(0, len(seeds), chunk):
+        events = make_events(seeds[k:k + chunk], workers)
+        b = DeviceBatch(ctx, events, device)
+        ctx.prefilter_enable(False)
+        ctx.batch_run(b.batch)
+        plain_cells, _ = ctx.prefilter_export()
+        pk, pf = export_roads(ctx, device)
+        ctx.prefilter_enable(True)
+        ctx.batch_run(b.batch)
+        learned_cells, _ = ctx.prefilter_export()
+        lk, lf = export_roads(ctx, device)
+        ctx.prefilter_enable(False)
+        c = compare_roads(pk, pf, lk, lf)
+        for key in c:
+            tot[key] += c[key]
+        tot["plain_cells"] += plain_cells
+        tot["learned_cells"] += learned_cells
+        tot["events"] += len(events)
+        log("evaluate: events %d..%d %s" % (k, k + len(events) - 1, json.dumps(c)))
+    tot["road_reproduction"] = tot["reproduced"] / max(tot["plain_roads"], 1)
+    tot["cells_kept"] = tot["learned_cells"] / max(tot["plain_cells"], 1)
+    return tot
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description="Train, calibrate and evaluate the learned prefilter on one GPU.")
+    p.add_argument("--out", default=CHECKPOINT, help="checkpoint to write")
+    p.add_argument("--report", default=None, help="JSON report (default: the checkpoint path with .json)")
+    p.add_argument("--train-events", type=int, default=2000)
+    p.add_argument("--eval-events", type=int, default=500)
+    p.add_argument("--steps", type=int, default=20000)
+    p.add_argument("--batch", type=int, default=8192)
+    p.add_argument("--lr", type=float, default=2e-3)
+    p.add_argument("--target", type=float, default=0.997, help="road reproduction the threshold keeps on the training events")
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--chunk", type=int, default=100)
+    args = p.parse_args(argv)
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    ctx = capi.Context(device=0)
+    t0 = time.perf_counter()
+    data = collect(ctx, range(TRAIN_SEED0, TRAIN_SEED0 + args.train_events), device, chunk=args.chunk)
+    collect_s = time.perf_counter() - t0
+    model, report = train(ctx, data, device, seed=args.seed, target=args.target, steps=args.steps, batch=args.batch, lr=args.lr)
+    del data
+    ev = evaluate(ctx, model, range(EVAL_SEED0, EVAL_SEED0 + args.eval_events), device, chunk=args.chunk)
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    capi.prefilter_save(model, args.out)
+    full = dict(train_events=args.train_events, train_seeds=[TRAIN_SEED0, TRAIN_SEED0 + args.train_events - 1],
+                eval_events=args.eval_events, eval_seeds=[EVAL_SEED0, EVAL_SEED0 + args.eval_events - 1],
+                collect_seconds=collect_s, train=report, evaluation=ev)
+    with open(args.report or os.path.splitext(args.out)[0] + ".json", "w") as fh:
+        json.dump(full, fh, indent=1)
+    print(json.dumps(full))
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
