@@ -504,8 +504,9 @@ __device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t 
   t.tan_lambda = (c.z - d.z) / (c.w - d.w);
   t.phi = itsu_atan2f(c.y - d.y, c.x - d.x);
   a.tracklets[out] = t;
-  a.trk_seg_id[out] = e * ITSU_TRACKLET_LAYERS + layer;
   a.trk_tl[out] = t.tan_lambda;
+  (void)e;
+  (void)layer;
 }
 
 constexpr int kColHits = 16;        // hits of one z-pruned column sorted back into index order
@@ -739,15 +740,43 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_write(Arena a)
     return;
   }
   const int64_t n = a.status->total[kTracklets];
-  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
-    const int64_t i = a.trk_owner[k];
-    const int32_t first = a.trk_off[i];
-    if (a.trk_off[i + 1] - first > kTrackletSlots) {
-      continue;
+  const int64_t stride = grid_threads();
+  constexpr int kPer = 2;  // tracklets per thread per round, their gathers in flight together
+  for (int64_t k0 = global_thread(); k0 < n; k0 += kPer * stride) {
+    int64_t owner[kPer];
+    int sid[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int64_t k = k0 + u * stride;
+      owner[u] = -1;
+      if (k < n) {
+        owner[u] = a.trk_owner[k];
+        sid[u] = a.trk_seg_id[k];
+      }
     }
-    const int sid = a.trk_seg_id[k];
-    const int seg = sid + sid / ITSU_TRACKLET_LAYERS;  // (e, L) as a cluster segment: 7e + L
-    write_tracklet(a, (int)k, i, a.layer_off[seg + 1] + a.trk_slots[(k - first) * a.slot_stride + i], seg);
+    int32_t first[kPer], slot[kPer];
+    bool go[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      go[u] = false;
+      if (owner[u] >= 0) {
+        first[u] = a.trk_off[owner[u]];
+        go[u] = a.trk_off[owner[u] + 1] - first[u] <= kTrackletSlots;  // else the tail wrote it
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      if (go[u]) {
+        slot[u] = a.trk_slots[(k0 + u * stride - first[u]) * a.slot_stride + owner[u]];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      if (go[u]) {
+        const int seg = sid[u] + sid[u] / ITSU_TRACKLET_LAYERS;  // (e, L) as a cluster segment: 7e + L
+        write_tracklet(a, (int)(k0 + u * stride), owner[u], a.layer_off[seg + 1] + slot[u], seg);
+      }
+    }
   }
 }
 
@@ -807,7 +836,9 @@ __device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t
   if (k >= n) {
     return s;
   }
+  // both loads first: neither depends on the other
   const int sid = a.trk_seg_id[k];
+  const itsu_tracklet t1 = a.tracklets[k];
   s.e = sid / ITSU_TRACKLET_LAYERS;
   s.layer = sid % ITSU_TRACKLET_LAYERS;
   const int32_t *ts = a.trk_seg + s.e * ITSU_TRACKLET_LAYERS;
@@ -816,7 +847,6 @@ __device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t
     return s;
   }
   const int32_t *lo = a.layer_off + s.e * ITSU_LAYERS;
-  const itsu_tracklet t1 = a.tracklets[k];
   s.t1_tan_lambda = t1.tan_lambda;
   s.t1_phi = t1.phi;
   s.t1_first = t1.first_cluster;
@@ -1106,30 +1136,50 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_scatter(Arena a)
   }
   const int64_t reserved = a.status->cell_entries;
   const int64_t n = reserved < a.cap_cell_entries ? reserved : a.cap_cell_entries;
-  for (int64_t i = global_thread(); i < n; i += grid_threads()) {
-    const int4 *src = reinterpret_cast<const int4 *>(a.cell_entries + i);
-    const int4 h = src[0];
-    if (h.x < 0) {
-      continue;
+  const int64_t stride = grid_threads();
+  constexpr int kPer = 4;  // entries per thread per round, their loads in flight together
+  for (int64_t i0 = global_thread(); i0 < n; i0 += kPer * stride) {
+    int4 h[kPer], g[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int64_t i = i0 + u * stride;
+      h[u] = make_int4(-1, 0, 0, 0);
+      if (i < n) {
+        const int4 *src = reinterpret_cast<const int4 *>(a.cell_entries + i);
+        h[u] = src[0];
+        g[u] = src[1];
+      }
     }
-    const unsigned long long m = a.cell_mask[h.x];
-    if (!((m >> h.y) & 1ull)) {
-      continue;  // removed by the learned prefilter
+    unsigned long long m[kPer];
+    int32_t off[kPer];
+    int sid[kPer];
+    itsu_tracklet t1[kPer], t2[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      if (h[u].x >= 0) {
+        m[u] = a.cell_mask[h[u].x];
+        off[u] = a.cell_off[h[u].x];
+        sid[u] = a.trk_seg_id[h[u].x];
+        t1[u] = a.tracklets[h[u].x];
+        t2[u] = a.tracklets[h[u].z];
+      }
     }
-    const int32_t out = a.cell_off[h.x] + __popcll(m & ((1ull << h.y) - 1ull));
-    const int sid = a.trk_seg_id[h.x];
-    const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
-    const int32_t *ts = a.trk_seg + e * ITSU_TRACKLET_LAYERS;
-    const itsu_tracklet t1 = a.tracklets[h.x];
-    const itsu_tracklet t2 = a.tracklets[h.z];
-    const int4 g = src[1];
-    int2 *dst = reinterpret_cast<int2 *>(a.cells + out);
-    dst[0] = make_int2(t1.first_cluster, t1.second_cluster);
-    dst[1] = make_int2(t2.second_cluster, h.x - ts[layer]);
-    dst[2] = make_int2(h.z - ts[layer + 1], g.x);
-    dst[3] = make_int2(g.y, g.z);
-    dst[4] = make_int2(g.w, 1);
-    a.cell_seg_id[out] = e * ITSU_CELL_LAYERS + layer;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      if (h[u].x < 0 || !((m[u] >> h[u].y) & 1ull)) {
+        continue;  // an unused slot, or a pair removed by the learned prefilter
+      }
+      const int32_t out = off[u] + __popcll(m[u] & ((1ull << h[u].y) - 1ull));
+      const int e = sid[u] / ITSU_TRACKLET_LAYERS, layer = sid[u] % ITSU_TRACKLET_LAYERS;
+      const int32_t *ts = a.trk_seg + e * ITSU_TRACKLET_LAYERS;
+      int2 *dst = reinterpret_cast<int2 *>(a.cells + out);
+      dst[0] = make_int2(t1[u].first_cluster, t1[u].second_cluster);
+      dst[1] = make_int2(t2[u].second_cluster, h[u].x - ts[layer]);
+      dst[2] = make_int2(h[u].z - ts[layer + 1], g[u].x);
+      dst[3] = make_int2(g[u].y, g[u].z);
+      dst[4] = make_int2(g[u].w, 1);
+      a.cell_seg_id[out] = e * ITSU_CELL_LAYERS + layer;
+    }
   }
 }
 
@@ -1142,24 +1192,46 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_lookup(Arena a)
     return;
   }
   const int64_t n = a.status->total[kTracklets];
-  for (int64_t k = global_thread(); k < n; k += grid_threads()) {
-    const int32_t first = a.cell_off[k];
-    const bool has = a.cell_off[k + 1] > first;
-    const int sid = a.trk_seg_id[k];
-    const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
-    a.cell_lookup[k] = (layer >= 1 && layer < ITSU_CELL_LAYERS && has) ? first - a.cell_seg[e * ITSU_CELL_LAYERS + layer]
-                                                                       : ITSU_UNUSED_INDEX;
-    if (has && a.cell_mask[k] == 0ull) {
-      const CellLane s = cell_lane(a, k, n);
-      int64_t out = first;
-      for (int b = 0; b < s.n_out; ++b) {
-        const int32_t j = s.j0 + b;
-        const itsu_tracklet t2 = a.tracklets[j];
-        float3 normal;
-        float curvature;
-        if (cell_precut(s.layer, s.t1_tan_lambda, s.t1_phi, t2.tan_lambda, t2.phi, s.c1, s.vz) &&
-            cell_geometry(s.layer, s.c1, s.c2, a.xyzr[s.c3_base + t2.second_cluster], s.vx, s.vy, normal, curvature)) {
-          write_cell(a, out++, s, t2, j, normal, curvature);
+  const int64_t stride = grid_threads();
+  constexpr int kPer = 4;  // tracklets per thread per round, their loads in flight together
+  for (int64_t k0 = global_thread(); k0 < n; k0 += kPer * stride) {
+    int32_t first[kPer], last[kPer];
+    int sid[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int64_t k = k0 + u * stride;
+      first[u] = last[u] = 0;
+      sid[u] = 0;
+      if (k < n) {
+        first[u] = a.cell_off[k];
+        last[u] = a.cell_off[k + 1];
+        sid[u] = a.trk_seg_id[k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int64_t k = k0 + u * stride;
+      if (k >= n) {
+        continue;
+      }
+      const bool has = last[u] > first[u];
+      const int e = sid[u] / ITSU_TRACKLET_LAYERS, layer = sid[u] % ITSU_TRACKLET_LAYERS;
+      a.cell_lookup[k] = (layer >= 1 && layer < ITSU_CELL_LAYERS && has) ? first[u] - a.cell_seg[e * ITSU_CELL_LAYERS + layer]
+                                                                         : ITSU_UNUSED_INDEX;
+      if (has && a.cell_mask[k] == 0ull) {
+        // a tracklet whose outer cluster was too crowded for the pair-parallel count: its cells
+        // in order, on this lane
+        const CellLane s = cell_lane(a, k, n);
+        int64_t out = first[u];
+        for (int b = 0; b < s.n_out; ++b) {
+          const int32_t j = s.j0 + b;
+          const itsu_tracklet t2 = a.tracklets[j];
+          float3 normal;
+          float curvature;
+          if (cell_precut(s.layer, s.t1_tan_lambda, s.t1_phi, t2.tan_lambda, t2.phi, s.c1, s.vz) &&
+              cell_geometry(s.layer, s.c1, s.c2, a.xyzr[s.c3_base + t2.second_cluster], s.vx, s.vy, normal, curvature)) {
+            write_cell(a, out++, s, t2, j, normal, curvature);
+          }
         }
       }
     }
