@@ -81,6 +81,10 @@ typedef enum itsu_status {
 
 /* Flags of itsu_config.flags */
 #define ITSU_FLAG_NO_GROW 1u /* report ITSU_ERR_CAPACITY instead of growing and re-running */
+/* itsu_batch_run_host streams: the batch runs as consecutive chunks of events, each chunk's
+ * upload overlapping the work on the one before; only the roads and road offsets are kept
+ * (the per-event results API then reports ITSU_ERR_STATE until the next run). */
+#define ITSU_FLAG_STREAM_HOST 2u
 
 typedef struct itsu_config {
   int32_t device;          /* CUDA device ordinal */
@@ -91,7 +95,7 @@ typedef struct itsu_config {
   int64_t max_neighbours;
   int64_t max_roads;
   int32_t max_events;
-  int32_t reserved_;
+  int32_t stream_chunk_clusters; /* ITSU_FLAG_STREAM_HOST: clusters per chunk (0 = 1,500,000) */
 } itsu_config;
 
 /* Per-vertex result sizes. */
@@ -190,7 +194,9 @@ itsu_status itsu_clusters_to_tracks(itsu_context *ctx, const itsu_cluster *const
  * when a result overflowed (unless ITSU_FLAG_NO_GROW). */
 itsu_status itsu_batch_run(itsu_context *ctx, const itsu_batch *batch);
 /* Host in / host out: copies the batch to the device, runs it, and copies back the roads
- * (event-major) and road_offsets[n_events+1]. roads may be NULL to query the total. */
+ * (event-major) and road_offsets[n_events+1]. roads may be NULL to query the total. With
+ * ITSU_FLAG_STREAM_HOST the copies of later events overlap the work on earlier ones (pinned
+ * host buffers make the copies asynchronous). */
 itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
                                 const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
                                 int32_t *road_offsets);

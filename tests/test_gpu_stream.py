@@ -1,0 +1,120 @@
+"""Streamed host batches (ITSU_FLAG_STREAM_HOST): the batch runs as consecutive chunks of events
+whose uploads overlap the work on earlier chunks. The roads and road offsets must be the ones of
+the one-pass run, byte for byte; the per-event intermediates are not kept."""
+import numpy as np
+import pytest
+
+from itsu import capi, gen
+
+pytestmark = pytest.mark.gpu
+
+
+def _pinned(a):
+    import torch
+
+    t = torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).pin_memory()
+    return t.numpy().view(a.dtype)
+
+
+def _both(events, chunk, prefilter=None):
+    clusters, offsets, vertices = gen.pack_batch(events)
+    one = capi.Context(device=0)
+    streamed = capi.Context(device=0, flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=chunk)
+    try:
+        if prefilter is not None:
+            for c in (one, streamed):
+                c.prefilter_set_model(prefilter)
+                c.prefilter_enable(True)
+        want = one.batch_run_host(clusters, offsets, vertices)
+        got = streamed.batch_run_host(_pinned(clusters), _pinned(offsets), _pinned(vertices))
+        got_again = streamed.batch_run_host(clusters, offsets, vertices)  # pageable buffers, arena reused
+        with pytest.raises(capi.ItsuError) as e:
+            streamed.results(0)
+        assert e.value.status == capi.ERR_STATE
+        return want, got, got_again
+    finally:
+        one.close()
+        streamed.close()
+
+
+def _same(a, b):
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(a[0].view(np.uint8), b[0].view(np.uint8))
+
+
+def test_streamed_pbpb_batch_equals_one_pass():
+    import torch
+
+    torch.cuda.init()
+    events = [gen.pbpb_event(s, n_tracks=2000) for s in range(60, 66)]
+    want, got, again = _both(events, chunk=30000)
+    assert want[1][-1] > 0
+    _same(want, got)
+    _same(want, again)
+
+
+def test_streamed_uneven_batch_equals_one_pass():
+    events = gen.batch_events(61, n_events=24, hi=4000)
+    want, got, again = _both(events, chunk=20000)
+    _same(want, got)
+    _same(want, again)
+
+
+def test_streamed_learned_batch_equals_one_pass():
+    events = [gen.pbpb_event(s, n_tracks=2000) for s in range(70, 74)]
+    model = capi.prefilter_init(4)
+    model.logit_threshold = -0.5
+    want, got, _ = _both(events, chunk=30000, prefilter=model)
+    _same(want, got)
+
+
+def test_streamed_malformed_cluster_reports_its_batch_index():
+    events = [gen.pbpb_event(s, n_tracks=800) for s in range(80, 86)]
+    clusters, offsets, vertices = gen.pack_batch(events)
+    bad = int(offsets[4 * 7 + 2]) + 3  # a cluster of event 4, layer 2: in a later chunk
+    clusters = clusters.copy()
+    clusters["x"][bad] = np.nan
+    ctx = capi.Context(device=0, flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=8000)
+    try:
+        with pytest.raises(capi.ItsuError) as e:
+            ctx.batch_run_host(clusters, offsets, vertices)
+        assert e.value.status == capi.ERR_INVALID
+        assert "cluster %d " % bad in str(e.value)
+    finally:
+        ctx.close()
+
+
+def test_streamed_roads_into_pinned_host_buffer():
+    """Pinned host buffers in and out (the benchmark's e2e call): same bytes as the one-pass run,
+    and a too small road buffer is reported."""
+    import ctypes
+
+    import torch
+
+    events = [gen.pbpb_event(s, n_tracks=2000) for s in range(90, 96)]
+    clusters, offsets, vertices = gen.pack_batch(events)
+    one = capi.Context(device=0)
+    ctx = capi.Context(device=0, flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=30000)
+    try:
+        want = one.batch_run_host(clusters, offsets, vertices)
+        cap = len(want[0]) + 16
+        h_roads = torch.zeros(cap * capi.ROAD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+        h_off = torch.zeros(len(events) + 1, dtype=torch.int32).pin_memory()
+        hc, ho, hv = _pinned(clusters), _pinned(offsets), _pinned(vertices)
+        st = ctx.lib.itsu_batch_run_host(ctx.h, hc.ctypes.data_as(ctypes.c_void_p), ho.ctypes.data_as(ctypes.c_void_p),
+                                         hv.ctypes.data_as(ctypes.c_void_p), len(events), ctypes.c_void_p(h_roads.data_ptr()), cap,
+                                         ctypes.c_void_p(h_off.data_ptr()))
+        assert st == capi.OK, ctx.lib.itsu_last_error(ctx.h)
+        got_off = h_off.numpy().copy()
+        got = h_roads.numpy().view(capi.ROAD_DTYPE)[: got_off[-1]].copy()
+        got["pad"] = 0
+        assert np.array_equal(got_off, want[1])
+        assert np.array_equal(got.view(np.uint8), want[0].view(np.uint8))
+        # too small a pinned buffer: the call reports the shortfall
+        st = ctx.lib.itsu_batch_run_host(ctx.h, hc.ctypes.data_as(ctypes.c_void_p), ho.ctypes.data_as(ctypes.c_void_p),
+                                         hv.ctypes.data_as(ctypes.c_void_p), len(events), ctypes.c_void_p(h_roads.data_ptr()),
+                                         len(want[0]) // 2, ctypes.c_void_p(h_off.data_ptr()))
+        assert st == capi.ERR_CAPACITY
+    finally:
+        one.close()
+        ctx.close()

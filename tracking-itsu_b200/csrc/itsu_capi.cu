@@ -131,6 +131,21 @@ struct itsu_context {
   int graph_tune[3] = {0, 0, -1};
   bool graph_prefilter = false;
 
+  // streamed host runs (ITSU_FLAG_STREAM_HOST): upload stream, per-chunk events, batch-wide roads
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t chunk_ready[16] = {};
+  int32_t *chunk_off = nullptr;   // each chunk's layer offsets, rebased to the chunk
+  int64_t cap_chunk_off = 0;
+  int32_t *h_chunk_off = nullptr;  // pinned staging of chunk_off
+  int64_t cap_h_chunk_off = 0;
+  int64_t chunk_clusters = 0;
+  itsu_road *roads_all = nullptr;
+  int64_t cap_roads_all = 0;
+  int32_t *road_off_all = nullptr;
+  int64_t cap_road_off_all = 0;
+  DevStatus *chunk_status = nullptr;  // 16 snapshots
+  DevStatus *h_chunk_status = nullptr;
+
   // learned prefilter: FP32 master model and the device model the kernels read
   itsu_prefilter_model *d_master = nullptr;
   itsu::MlpDevice *d_mlp = nullptr;
@@ -755,6 +770,11 @@ itsu_status itsu_context_create(const itsu_config *cfg, itsu_context **out)
   ctx->init_cells = c.max_cells;
   ctx->init_neighbours = c.max_neighbours;
   ctx->init_roads = c.max_roads;
+  if (c.stream_chunk_clusters < 0) {
+    delete ctx;
+    return fail(nullptr, ITSU_ERR_INVALID, "itsu_context_create: negative stream chunk size");
+  }
+  ctx->chunk_clusters = c.stream_chunk_clusters;
   itsu_status st = ITSU_OK;
   do {
     if ((err = cudaSetDevice(c.device)) != cudaSuccess) break;
@@ -806,6 +826,13 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
   release(ctx->d_master); release(ctx->d_mlp);
+  release(ctx->chunk_off); release(ctx->roads_all); release(ctx->road_off_all); release(ctx->chunk_status);
+  if (ctx->h_chunk_status) cudaFreeHost(ctx->h_chunk_status);
+  if (ctx->h_chunk_off) cudaFreeHost(ctx->h_chunk_off);
+  for (cudaEvent_t &e : ctx->chunk_ready) {
+    if (e) cudaEventDestroy(e);
+  }
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -1089,6 +1116,158 @@ itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, 
   return ITSU_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+constexpr int kMaxChunks = 16;
+constexpr int64_t kChunkClusters = 1500000;  // default clusters per streamed chunk (about 34 central Pb-Pb-like events)
+
+template <typename T>
+itsu_status grow_buffer(itsu_context *ctx, T *&p, int64_t &cap, int64_t need)
+{
+  if (need > cap) {
+    const int64_t c = grow_to(need);
+    ITSU_CUDA(ctx, alloc(p, c));
+    cap = c;
+  }
+  return ITSU_OK;
+}
+
+// itsu_batch_run_host with ITSU_FLAG_STREAM_HOST: consecutive chunks of events, each one's
+// upload (copy stream) overlapping the work on the one before (context stream). Sets *done to
+// false, with nothing reported, when the batch is too small to split or a chunk outgrew the
+// arena: the caller then runs the batch in one pass (which grows the arena).
+itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets, const float *vertices,
+                              int32_t n_events, int64_t n_clusters, itsu_road *roads, int64_t roads_capacity,
+                              int32_t *road_offsets, bool *done)
+{
+  *done = false;
+  const int64_t per_chunk = ctx->chunk_clusters > 0 ? ctx->chunk_clusters : kChunkClusters;
+  const int k_chunks = (int)std::min<int64_t>(std::min<int64_t>(kMaxChunks - 1, n_events), (n_clusters + per_chunk - 1) / per_chunk);
+  if (k_chunks < 2) return ITSU_OK;
+  // chunk boundaries (events) with about equal cluster counts
+  std::vector<int32_t> ev(k_chunks + 1, 0);
+  ev[k_chunks] = n_events;
+  for (int c = 1, e = 0; c < k_chunks; ++c) {
+    const int64_t target = n_clusters * c / k_chunks;
+    while (e < n_events && layer_offsets[(int64_t)e * ITSU_LAYERS] < target) ++e;
+    ev[c] = std::max(e, ev[c - 1] + 1);
+  }
+  for (int c = 1; c <= k_chunks; ++c) {
+    if (ev[c] <= ev[c - 1]) return ITSU_OK;  // degenerate split: one pass instead
+  }
+  int64_t max_chunk = 0;
+  for (int c = 0; c < k_chunks; ++c) {
+    max_chunk = std::max<int64_t>(max_chunk, layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS] - layer_offsets[(int64_t)ev[c] * ITSU_LAYERS]);
+  }
+  itsu_status st;
+  if ((st = ensure_clusters(ctx, n_clusters, n_events)) != ITSU_OK) return st;
+  if ((st = ensure_outputs_for(ctx, max_chunk)) != ITSU_OK) return st;
+  if ((st = grow_buffer(ctx, ctx->chunk_off, ctx->cap_chunk_off, (int64_t)n_events * ITSU_LAYERS + k_chunks)) != ITSU_OK) return st;
+  if ((st = grow_buffer(ctx, ctx->roads_all, ctx->cap_roads_all, std::max<int64_t>(ctx->cap_roads, n_clusters / 2 + 4096))) != ITSU_OK) {
+    return st;
+  }
+  if ((st = grow_buffer(ctx, ctx->road_off_all, ctx->cap_road_off_all, (int64_t)n_events + 1)) != ITSU_OK) return st;
+  if (!ctx->chunk_status) ITSU_CUDA(ctx, cudaMalloc((void **)&ctx->chunk_status, sizeof(DevStatus) * kMaxChunks));
+  if (!ctx->h_chunk_status) ITSU_CUDA(ctx, cudaMallocHost((void **)&ctx->h_chunk_status, sizeof(DevStatus) * kMaxChunks));
+  if (!ctx->copy_stream) ITSU_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  for (int c = 0; c < k_chunks; ++c) {
+    if (!ctx->chunk_ready[c]) ITSU_CUDA(ctx, cudaEventCreateWithFlags(&ctx->chunk_ready[c], cudaEventDisableTiming));
+  }
+  // each chunk's layer offsets, rebased (chunk c at 7 ev[c] + c), staged in pinned memory so that
+  // their upload is asynchronous
+  const int64_t n_off = (int64_t)n_events * ITSU_LAYERS + k_chunks;
+  if (n_off > ctx->cap_h_chunk_off) {
+    if (ctx->h_chunk_off) cudaFreeHost(ctx->h_chunk_off);
+    ctx->h_chunk_off = nullptr;
+    ctx->cap_h_chunk_off = 0;
+    ITSU_CUDA(ctx, cudaMallocHost((void **)&ctx->h_chunk_off, sizeof(int32_t) * grow_to(n_off)));
+    ctx->cap_h_chunk_off = grow_to(n_off);
+  }
+  // the previous call finished with a synchronisation: the staging buffer is free to refill
+  for (int c = 0; c < k_chunks; ++c) {
+    const int32_t base = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS];
+    for (int64_t k = (int64_t)ev[c] * ITSU_LAYERS; k <= (int64_t)ev[c + 1] * ITSU_LAYERS; ++k) {
+      ctx->h_chunk_off[k + c] = layer_offsets[k] - base;
+    }
+  }
+  // All uploads go on the copy stream, the small ones first: host-to-device copies share the copy
+  // engine in submission order, so a small copy queued behind the clusters would hold up the
+  // first chunk's work. The copy stream first waits for any earlier work of the context.
+  cudaEvent_t start = ctx->chunk_ready[kMaxChunks - 1];
+  if (!start) {
+    ITSU_CUDA(ctx, cudaEventCreateWithFlags(&ctx->chunk_ready[kMaxChunks - 1], cudaEventDisableTiming));
+    start = ctx->chunk_ready[kMaxChunks - 1];
+  }
+  ITSU_CUDA(ctx, cudaEventRecord(start, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, start, 0));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->chunk_off, ctx->h_chunk_off, sizeof(int32_t) * n_off, cudaMemcpyHostToDevice, ctx->copy_stream));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, vertices, sizeof(float) * 3 * (int64_t)n_events, cudaMemcpyHostToDevice, ctx->copy_stream));
+  for (int c = 0; c < k_chunks; ++c) {
+    const int64_t a = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS], b = layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS];
+    if (b > a) {
+      ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw + a, clusters + a, sizeof(itsu_cluster) * (b - a), cudaMemcpyHostToDevice,
+                                     ctx->copy_stream));
+    }
+    ITSU_CUDA(ctx, cudaEventRecord(ctx->chunk_ready[c], ctx->copy_stream));
+  }
+  // the work: per chunk (after its upload, which follows the offsets and vertices), the whole
+  // sequence, then its roads appended to the batch-wide output
+  ITSU_CUDA(ctx, cudaMemsetAsync(ctx->road_off_all, 0, sizeof(int32_t) * ((int64_t)n_events + 1), ctx->stream));
+  for (int c = 0; c < k_chunks; ++c) {
+    const int64_t a = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS], b = layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS];
+    ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_ready[c], 0));
+    ctx->n_events = ev[c + 1] - ev[c];
+    ctx->n_clusters = b - a;
+    ctx->in_raw = ctx->raw + a;
+    ctx->in_raw_off = nullptr;
+    ctx->in_layer_off = ctx->chunk_off + (int64_t)ev[c] * ITSU_LAYERS + c;
+    ctx->in_vtx = ctx->vtx + 3 * (int64_t)ev[c];
+    enqueue_all(ctx);
+    itsu::launch_append_roads(arena_of(ctx), launch_of(ctx), ctx->roads_all, ctx->road_off_all, ev[c], ctx->cap_roads_all,
+                              ctx->chunk_status + c);
+    ITSU_CUDA(ctx, cudaGetLastError());
+  }
+  ctx->stage = kNone;  // the arena holds only the last chunk's intermediate results
+  ctx->n_events = 0;
+  ctx->n_clusters = 0;
+  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_chunk_status, ctx->chunk_status, sizeof(DevStatus) * k_chunks, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+  int32_t total32 = 0;
+  ITSU_CUDA(ctx, cudaMemcpyAsync(&total32, ctx->road_off_all + n_events, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int c = 0; c < k_chunks; ++c) {
+    const DevStatus &s = ctx->h_chunk_status[c];
+    if (s.flags & itsu::kFlagInvalid) {
+      if (s.invalid_event != INT32_MAX) {
+        return fail(ctx, ITSU_ERR_INVALID, "primary vertex of event %d is not finite or beyond 1e6 cm", ev[c] + s.invalid_event);
+      }
+      return fail(ctx, ITSU_ERR_INVALID, "cluster %lld is malformed: a coordinate is not finite or beyond 1e6 cm, or it sits on the beam line at the vertex z (r == 0 and z == vertex z)",
+                  (long long)layer_offsets[(int64_t)ev[c] * ITSU_LAYERS] + s.invalid_index);
+    }
+    if (s.flags & itsu::kCapacityMask) return ITSU_OK;  // *done stays false: one pass, which grows the arena
+  }
+  const int64_t total = total32;
+  if (road_offsets) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(road_offsets, ctx->road_off_all, sizeof(int32_t) * ((int64_t)n_events + 1), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+  }
+  if (roads) {
+    if (total > roads_capacity) return fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %lld given", (long long)total, (long long)roads_capacity);
+    if (total > 0) {
+      ITSU_CUDA(ctx, cudaMemcpyAsync(roads, ctx->roads_all, sizeof(itsu_road) * total, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *done = true;
+  return ITSU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
                                 const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
                                 int32_t *road_offsets)
@@ -1098,7 +1277,19 @@ itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters,
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
   const int64_t n_clusters = n_events > 0 ? layer_offsets[(int64_t)n_events * ITSU_LAYERS] : 0;
   if (n_clusters > 0 && !clusters) return fail(ctx, ITSU_ERR_INVALID, "null clusters");
+  if (layer_offsets && layer_offsets[0] != 0) return fail(ctx, ITSU_ERR_INVALID, "layer offsets must start at 0");
+  for (int64_t k = 1; n_events > 0 && k <= (int64_t)n_events * ITSU_LAYERS; ++k) {
+    if (layer_offsets[k] < layer_offsets[k - 1]) return fail(ctx, ITSU_ERR_INVALID, "layer offsets decrease at %lld", (long long)k);
+  }
   itsu_status st;
+  if (ctx->flags & ITSU_FLAG_STREAM_HOST) {
+    bool done = false;
+    if ((st = run_host_streamed(ctx, clusters, layer_offsets, vertices, n_events, n_clusters, roads, roads_capacity, road_offsets,
+                                &done)) != ITSU_OK) {
+      return st;
+    }
+    if (done) return ITSU_OK;
+  }
   if ((st = ensure_clusters(ctx, n_clusters, n_events)) != ITSU_OK) return st;
   if (n_clusters > 0) {
     ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw, clusters, sizeof(itsu_cluster) * n_clusters, cudaMemcpyHostToDevice, ctx->stream));

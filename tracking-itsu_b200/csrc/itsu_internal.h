@@ -143,6 +143,11 @@ void launch_neighbours_write(const Arena &a, const Launch &l);
 void launch_roads_count(const Arena &a, const Launch &l);
 void launch_roads_write(const Arena &a, const Launch &l);
 
+// Streamed host runs: append the last run's roads and road offsets at event e0 of the batch-wide
+// output, and snapshot its status.
+void launch_append_roads(const Arena &a, const Launch &l, itsu_road *dst, int32_t *dst_off, int32_t e0, int64_t cap,
+                         DevStatus *snap);
+
 // Every kernel of a run, in launch order, with its name (the instrumentation API times them
 // one by one). The stage launchers above enqueue consecutive ranges of this table.
 struct KernelStep {

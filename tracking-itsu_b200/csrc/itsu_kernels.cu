@@ -1605,6 +1605,44 @@ void run_steps(int first, int last, const Arena &a, const Launch &l)
 
 }  // namespace
 
+// Streamed host runs: appends the last run's roads and road offsets to the batch-wide output at
+// event e0. The chunk's first road index is dst_off[e0], written by the previous chunk (or zeroed
+// by the host); a chunk that overflowed or does not fit leaves its roads out and passes its base
+// on, so the next chunk stays in bounds. The run's status goes to *snap for the host.
+__global__ void k_append_roads(Arena a, itsu_road *dst, int32_t *dst_off, int32_t e0, int64_t cap, DevStatus *snap)
+{
+  const bool ok = !capacity_failed(a.status);
+  int64_t base = dst_off[e0];
+  base = base < 0 ? 0 : base;
+  const int64_t total = ok ? a.status->total[kRoads] : 0;
+  const bool fits = base + total <= cap;
+  const int64_t tid = global_thread(), threads = grid_threads();
+  if (ok && fits) {
+    for (int64_t r = tid; r < total; r += threads) {
+      dst[base + r] = a.roads[r];
+    }
+    for (int64_t e = tid + 1; e <= a.n_events; e += threads) {
+      dst_off[e0 + e] = (int32_t)(base + a.road_seg[e]);
+    }
+  } else {
+    for (int64_t e = tid + 1; e <= a.n_events; e += threads) {
+      dst_off[e0 + e] = (int32_t)base;
+    }
+  }
+  if (tid == 0) {
+    DevStatus st = *a.status;
+    if (ok && !fits) {
+      st.flags |= kFlagCapRoads;
+    }
+    *snap = st;
+  }
+}
+
+void launch_append_roads(const Arena &a, const Launch &l, itsu_road *dst, int32_t *dst_off, int32_t e0, int64_t cap, DevStatus *snap)
+{
+  k_append_roads<<<l.num_sms * 2, 256, 0, l.stream>>>(a, dst, dst_off, e0, cap, snap);
+}
+
 // The learned kernels fit the default shared-memory limit: nothing to opt in to.
 cudaError_t prepare_learned_kernels() { return cudaSuccess; }
 

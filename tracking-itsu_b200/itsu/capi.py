@@ -25,6 +25,7 @@ ROAD_DTYPE = np.dtype([("cells", "<i4", (5,)), ("size", "<i4"), ("label", "<i4")
 
 OK, ERR_INVALID, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NOMEM, ERR_STATE = range(7)
 FLAG_NO_GROW = 1
+FLAG_STREAM_HOST = 2
 
 
 class ItsuError(RuntimeError):
@@ -41,7 +42,7 @@ STATUS_NAMES = {OK: "ITSU_OK", ERR_INVALID: "ITSU_ERR_INVALID", ERR_CAPACITY: "I
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("flags", ctypes.c_uint32), ("max_clusters", ctypes.c_int64),
                 ("max_tracklets", ctypes.c_int64), ("max_cells", ctypes.c_int64), ("max_neighbours", ctypes.c_int64),
-                ("max_roads", ctypes.c_int64), ("max_events", ctypes.c_int32), ("reserved_", ctypes.c_int32)]
+                ("max_roads", ctypes.c_int64), ("max_events", ctypes.c_int32), ("stream_chunk_clusters", ctypes.c_int32)]
 
 
 class Counts(ctypes.Structure):
