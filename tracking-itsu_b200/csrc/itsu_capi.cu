@@ -77,8 +77,7 @@ struct itsu_context {
   float4 *xyzr = nullptr;
   float *phi = nullptr;
   int32_t *trk_count = nullptr, *trk_off = nullptr, *trk_lookup = nullptr;
-  float *zs_z = nullptr;
-  int32_t *zs_j = nullptr;
+  float4 *zs = nullptr;
   int32_t *trk_slots = nullptr;
   // event class
   float2 *seg_rrange = nullptr;
@@ -225,8 +224,7 @@ Arena arena_of(const itsu_context *ctx)
   a.phi = ctx->phi;
   a.tmp = ctx->tmp;
   a.index_tables = ctx->index_tables;
-  a.zs_z = ctx->zs_z;
-  a.zs_j = ctx->zs_j;
+  a.zs = ctx->zs;
   a.seg_rrange = ctx->seg_rrange;
   a.seg_regular = ctx->seg_regular;
   a.prune_tracklets = current_tune(ctx).prune;
@@ -305,8 +303,7 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ITSU_CUDA(ctx, alloc(ctx->trk_count, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->trk_off, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx->trk_lookup, cap));
-    ITSU_CUDA(ctx, alloc(ctx->zs_z, cap));
-    ITSU_CUDA(ctx, alloc(ctx->zs_j, cap));
+    ITSU_CUDA(ctx, alloc(ctx->zs, cap));
     ITSU_CUDA(ctx, alloc(ctx->trk_slots, cap * itsu::kTrackletSlotsPerCluster));
     ctx->cap_clusters = cap;
     ctx->generation++;
@@ -817,7 +814,7 @@ void itsu_context_destroy(itsu_context *ctx)
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graph(ctx);
   release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
-  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs_z); release(ctx->zs_j); release(ctx->trk_slots);
+  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->trk_slots);
   release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);

@@ -76,10 +76,10 @@ struct Arena {
   float *phi;
   itsu_cluster *tmp;
   int32_t *index_tables;
-  // candidate-pruning index (null: not built): per bin, the bin's clusters sorted by (z, index);
+  // candidate-pruning index (null: not built): per bin, the bin's clusters sorted by (z, index),
+  // each with its r and phi for the cut;
   // per (event, layer) the r range of its clusters and whether all its bins are regular
-  float *zs_z;
-  int32_t *zs_j;
+  float4 *zs;  // (z, r, phi, sorted index as int bits)
   float2 *seg_rrange;
   int32_t *seg_regular;
   int32_t prune_tracklets;  // use the index (tuning knob; results are identical either way)

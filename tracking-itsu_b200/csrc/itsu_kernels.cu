@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   // has a z bin and a phi bin inside the 20 x 20 table (then a bin's column is its clusters' z
   // bin) and no bin holds more than kMaxPruneBin clusters; for regular layers, each bin's
   // clusters are listed again sorted by (z, sorted index), with the layer's r range beside.
-  if (a.zs_z == nullptr || layer == 0) {
+  if (a.zs == nullptr || layer == 0) {
     return;  // no index wanted, or layer 0 (never the outer layer of a tracklet)
   }
   __shared__ int s_irregular;
@@ -462,14 +462,13 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
     if (cnt > kMaxPruneBin) {
       continue;
     }
-    const float z = a.xyzr[begin + i].z;
+    const float4 c = a.xyzr[begin + i];
     int rank = 0;
     for (int k = 0; k < cnt; ++k) {
       const float zk = a.xyzr[begin + st + k].z;
-      rank += zk < z || (zk == z && st + k < i);
+      rank += zk < c.z || (zk == c.z && st + k < i);
     }
-    a.zs_z[begin + st + rank] = z;
-    a.zs_j[begin + st + rank] = i;
+    a.zs[begin + st + rank] = make_float4(c.z, c.w, a.phi[begin + i], __int_as_float(i));
   }
   __syncthreads();
   if (tid == 0) {
@@ -532,20 +531,24 @@ struct TrackletProbe {
   const float4 *xyzr;  // next layer
   const float *phi;
 
+  // Tracker.cxx:93-100 for a next-layer cluster at z2, r2, phi2
+  __device__ __forceinline__ bool pass(float z2, float r2, float phi2) const
+  {
+    const float delta_z = fabsf(tan_lambda * (r2 - c.w) + c.z - z2);
+    const float delta_phi = fabsf(phi1 - phi2);
+    return delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
+  }
+
   __device__ __forceinline__ bool pass(int j) const
   {
     const float4 d = xyzr[j];
-    const float phi2 = phi[j];
-    const float delta_z = fabsf(tan_lambda * (d.w - c.w) + c.z - d.z);
-    const float delta_phi = fabsf(phi1 - phi2);
-    return delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
+    return pass(d.z, d.w, phi[j]);
   }
 };
 
 template <typename OnPass>
 __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next, int4 rect, int layer, const TrackletProbe &probe,
-                                                bool prune, float zlo, float zhi, const float *zs_z, const int32_t *zs_j,
-                                                OnPass &&on_pass)
+                                                bool prune, float zlo, float zhi, const float4 *zs, OnPass &&on_pass)
 {
   int phi_bins = rect.w - rect.y + 1;
   if (phi_bins < 0) {
@@ -564,7 +567,7 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
         int lo = k0, hi = k1;  // first listed cluster with z >= zlo
         while (lo < hi) {
           const int mid = (lo + hi) >> 1;
-          if (zs_z[mid] < zlo) {
+          if (zs[mid].x < zlo) {
             lo = mid + 1;
           } else {
             hi = mid;
@@ -573,9 +576,13 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
         int hits[kColHits];
         int h = 0;
         bool overflow = false;
-        for (int k = lo; k < k1 && zs_z[k] <= zhi; ++k) {
-          const int j = zs_j[k];
-          if (probe.pass(j)) {
+        for (int k = lo; k < k1; ++k) {
+          const float4 q = zs[k];  // z, r, phi and the sorted index of the k-th cluster by z
+          if (!(q.x <= zhi)) {
+            break;
+          }
+          const int j = __float_as_int(q.w);
+          if (probe.pass(q.x, q.y, q.z)) {
             if (h == kColHits) {
               overflow = true;
               break;
@@ -674,8 +681,7 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
 template <typename OnPass>
 __device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s, OnPass &&on_pass)
 {
-  walk_candidates(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, a.zs_z + s.next_begin,
-                  a.zs_j + s.next_begin, on_pass);
+  walk_candidates(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, a.zs + s.next_begin, on_pass);
 }
 
 // Count pass, one thread per inner cluster: the number of tracklets, and the outer clusters of
