@@ -1737,10 +1737,6 @@ itsu_status itsu_prefilter_enable(itsu_context *ctx, int32_t enable)
 {
   if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_enable: null context");
   if (enable && !ctx->has_model) return fail(ctx, ITSU_ERR_STATE, "itsu_prefilter_enable: no prefilter model set");
-  if (enable) {
-    ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
-    ITSU_CUDA(ctx, itsu::prepare_learned_kernels());
-  }
   ctx->prefilter = enable != 0;
   return ITSU_OK;
 }

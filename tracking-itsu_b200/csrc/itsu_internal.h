@@ -158,9 +158,6 @@ struct KernelStep {
 const KernelStep *pipeline_steps(int *count);
 int kernels_per_run();  // kernels one plain run launches (the learned form adds the learned_only steps)
 
-// Opts the learned cell-count kernel in to the shared memory it needs (current device).
-cudaError_t prepare_learned_kernels();
-
 // Learned prefilter (itsu_prefilter.cu), all asynchronous on `stream`.
 // The FP32 master parameters (itsu_prefilter_model) -> the device model (BF16 weights).
 void launch_mlp_publish(const itsu_prefilter_model *master, MlpDevice *model, cudaStream_t stream);

@@ -1,20 +1,26 @@
 // itsu_kernels.cu - sm_100a kernels of the ITS CA track finder.
 //
 // Every stage is a deterministic count -> exclusive scan -> write sequence over flat,
-// event-major arrays, so the output order is the reference's emission order with no atomics on
-// the output path (the only atomics fill neighbour rows, which are then sorted):
+// event-major arrays, so the output order is the reference's emission order (where a count pass
+// uses atomics, to reserve scratch or fill neighbour rows, the write pass restores the order):
 //   clustering   one CTA per (event, layer): vertex-relative transform, stable counting sort by
-//                bin (per-warp histograms, warp-match ranks), index table (PVC.cxx:31-142)
-//   tracklets    one thread per inner cluster walking the reference's bin window (Tracker.cxx:45-117)
-//   cells        one thread per tracklet walking the next-layer tracklets of its outer cluster
-//                (Tracker.cxx:120-235)
+//                bin (per-warp histograms, warp-match ranks), index table, z-sorted bin lists
+//                for the tracklet pruning (PVC.cxx:31-142)
+//   tracklets    count: one thread per inner cluster walking the reference's bin window,
+//                z-pruned (Tracker.cxx:45-117); tail: lookup, owners, crowded clusters; write:
+//                a map over tracklets (slope and correctly rounded azimuth)
+//   cells        count: a warp per 32 first tracklets, their outgoing-tracklet pairs flattened
+//                over the lanes, exact cuts, one 32-byte entry per found cell (Tracker.cxx:
+//                120-235); learned form: the prefilter scores the entries; write: the entries
+//                scattered to their scanned slots, then the lookup table
 //   neighbours   one thread per cell walking the next-layer cells of its outer tracklet; rows
 //                keyed by the next-layer cell, sorted ascending (Tracker.cxx:417-474)
 //   levels       layer-ordered longest-chain DP plus the number of level-decreasing chains
 //   roads        one thread per level-5 cell: depth-first enumeration in the reference's order,
 //                Moore-vote labels (Tracker.cxx:477-652)
-// Capacity overflow never writes out of bounds: the write passes check the scanned totals
-// against the arena capacities, record the requirement and skip; the host grows and re-runs.
+// Capacity overflow never writes out of bounds: the passes check the scanned totals and scratch
+// reservations against the arena capacities, record the requirement and skip; the host grows
+// and re-runs.
 #include <climits>
 
 #include "itsu_device.cuh"
@@ -1648,9 +1654,6 @@ void launch_append_roads(const Arena &a, const Launch &l, itsu_road *dst, int32_
 {
   k_append_roads<<<l.num_sms * 2, 256, 0, l.stream>>>(a, dst, dst_off, e0, cap, snap);
 }
-
-// The learned kernels fit the default shared-memory limit: nothing to opt in to.
-cudaError_t prepare_learned_kernels() { return cudaSuccess; }
 
 const KernelStep *pipeline_steps(int *count)
 {

@@ -1,9 +1,10 @@
 // itsu_prefilter.cu - the learned prefilter's training-side kernels: sample export, scoring,
 // minibatch gradients and the Adam step.
 //
-// The fused inference lives in the cell stage (k_cells_count<true>, itsu_kernels.cu); the scorer
-// here runs the same device code (mlp_logits_warp) on exported feature rows, so that the two give
-// the same logit for the same pair. Training is binary cross-entropy on the sigmoid output with
+// Inference lives in the cell stage (k_cells_prefilter, itsu_kernels.cu: each cell entry's
+// features, the three layers and the threshold in one pass, no feature rows in memory); the
+// scorer here runs the same device code (pair_features, mlp_logits_warp) on exported feature
+// rows, so that the two give the same logit for the same pair. Training is binary cross-entropy on the sigmoid output with
 // the forward pass exactly as inference computes it (BF16 inputs, weights and activations, FP32
 // accumulation) and the backward pass on the tensor cores too: the gradients with respect to the
 // pre-activations are rounded to BF16 for the three backward MMAs (dW2, dh1, dW1), accumulated in
