@@ -64,9 +64,13 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter mode")
-    ap.add_argument("--prefilter", default=os.path.join(PKG, "weights", "prefilter_pbpb.itsumlp"),
-                    help="checkpoint of the learned prefilter")
-    return ap.parse_args()
+    ap.add_argument("--prefilter", default=None,
+                    help="checkpoint of the learned prefilter (default: the one trained for the workload)")
+    args = ap.parse_args()
+    if args.prefilter is None:
+        own = os.path.join(PKG, "weights", "prefilter_%s.itsumlp" % args.workload)
+        args.prefilter = own if os.path.exists(own) else os.path.join(PKG, "weights", "prefilter_pbpb.itsumlp")
+    return args
 
 
 # ------------------------------------------------------------------------------------------

@@ -205,3 +205,15 @@ def test_committed_checkpoint_reproduces_plain_roads(ctx, torch_dev):
     assert res["extra"] == 0
     assert res["road_reproduction"] >= 0.995, res
     assert res["cells_kept"] < 1.0
+
+
+@pytest.mark.skipif(not os.path.exists(prefilter.CHECKPOINTS["pileup"]), reason="no trained pile-up checkpoint")
+def test_committed_pileup_checkpoint_reproduces_plain_roads(ctx, torch_dev):
+    """Held-out pile-up frames (5 collisions each, every vertex a run): at least 99.5% of the plain
+    roads, and no road the plain path lacks."""
+    model = capi.prefilter_load(prefilter.CHECKPOINTS["pileup"])
+    seeds = range(prefilter.EVAL_SEED0 + 2000, prefilter.EVAL_SEED0 + 2006)
+    res = prefilter.evaluate(ctx, model, seeds, torch_dev, chunk=6, workers=1, log=lambda *a: None, workload="pileup")
+    assert res["extra"] == 0
+    assert res["road_reproduction"] >= 0.995, res
+

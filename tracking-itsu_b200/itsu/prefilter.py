@@ -17,7 +17,9 @@ become a cell. Everything below runs through the C ABI on one GPU:
    construction: a learned run's cells are a subset of the plain run's, and roads are the
    complete 5-cell chains of the cell graph).
 
-Run ``python -m itsu.prefilter --out <checkpoint>`` (from tracking-itsu_b200/) on a GPU machine.
+Run ``python -m itsu.prefilter [--workload pbpb|pileup]`` (from tracking-itsu_b200/) on a GPU
+machine; it writes ``weights/prefilter_<workload>.itsumlp`` and a JSON report beside it. The
+pile-up model learns from frames of 5 collisions (every vertex of a frame is one run).
 """
 from __future__ import annotations
 
@@ -34,7 +36,9 @@ from . import capi, gen
 
 TRAIN_SEED0 = 7_000_000  # training events: seeds TRAIN_SEED0 .. + n_train - 1
 EVAL_SEED0 = 8_000_000   # held-out events
-CHECKPOINT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights", "prefilter_pbpb.itsumlp")
+WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights")
+CHECKPOINT = os.path.join(WEIGHTS, "prefilter_pbpb.itsumlp")
+CHECKPOINTS = {"pbpb": CHECKPOINT, "pileup": os.path.join(WEIGHTS, "prefilter_pileup.itsumlp")}
 TWO_PI_F = np.float32(6.28318530717958647692)
 CELL_MAX_DCA = np.array([0.05, 0.04, 0.05, 0.2, 0.4], np.float32)
 
@@ -193,28 +197,42 @@ def compare_roads(plain_keys, plain_fake, learned_keys, learned_fake) -> dict:
 # pipeline (GPU)
 
 
-def make_events(seeds, workers: int | None = None) -> list:
-    """Central Pb-Pb-like events (6000 tracks, 5% noise) for the given seeds, generated in
-    parallel worker processes (spawned, so that no CUDA state is forked)."""
+def pileup_frame(seed: int) -> gen.Event:
+    """A pile-up frame as the pile-up stream makes them: 5 collisions of 1050-1950 tracks (drawn
+    from the seed), 10% noise."""
+    rng = np.random.default_rng(seed)
+    return gen.make_event(seed, int(rng.integers(1050, 1951)), pt_mean=0.6, noise=0.10, n_vertices=5)
+
+
+MAKERS = {"pbpb": gen.pbpb_event, "pileup": pileup_frame}
+
+
+def make_events(seeds, workers: int | None = None, workload: str = "pbpb") -> list:
+    """Central Pb-Pb-like events (6000 tracks, 5% noise), or pile-up frames, for the given seeds,
+    generated in parallel worker processes (spawned, so that no CUDA state is forked)."""
     seeds = list(seeds)
+    make = MAKERS[workload]
     workers = workers or min(32, os.cpu_count() or 1)
     if workers <= 1 or len(seeds) < 8:
-        return [gen.pbpb_event(s) for s in seeds]
+        return [make(s) for s in seeds]
     with multiprocessing.get_context("spawn").Pool(workers) as pool:
-        return pool.map(gen.pbpb_event, seeds, chunksize=max(1, len(seeds) // (4 * workers)))
+        return pool.map(make, seeds, chunksize=max(1, len(seeds) // (4 * workers)))
 
 
 class DeviceBatch:
-    """A batch of events resident on the device (torch owns the memory)."""
+    """A batch of runs resident on the device (torch owns the memory): every vertex of every
+    event is one run."""
 
     def __init__(self, ctx, events, device):
         import torch
 
-        clusters, offsets, vertices = gen.pack_batch(events)
+        runs = [(ev, iv) for ev in events for iv in range(len(ev.vertices))]
+        clusters, offsets, vertices = gen.pack_batch([ev for ev, _ in runs], [iv for _, iv in runs])
+        self.n_runs = len(runs)
         self.clusters = torch.from_numpy(clusters.view(np.uint8)).to(device)
         self.offsets = torch.from_numpy(offsets).to(device)
         self.vertices = torch.from_numpy(vertices).to(device)
-        self.batch = ctx.batch_device(self.clusters.data_ptr(), self.offsets.data_ptr(), self.vertices.data_ptr(), len(events),
+        self.batch = ctx.batch_device(self.clusters.data_ptr(), self.offsets.data_ptr(), self.vertices.data_ptr(), len(runs),
                                       len(clusters))
 
 
@@ -241,7 +259,7 @@ def export_roads(ctx, device):
     return keys[:n_roads].cpu().numpy(), fake[:n_roads].cpu().numpy()
 
 
-def collect(ctx, seeds, device, chunk: int = 100, workers: int | None = None, log=print) -> dict:
+def collect(ctx, seeds, device, chunk: int = 100, workers: int | None = None, log=print, workload: str = "pbpb") -> dict:
     """Plain runs over the events of `seeds`; all their samples, concatenated on the device."""
     import torch
 
@@ -249,7 +267,7 @@ def collect(ctx, seeds, device, chunk: int = 100, workers: int | None = None, lo
     base = 0
     seeds = list(seeds)
     for k in range(0, len(seeds), chunk):
-        events = make_events(seeds[k:k + chunk], workers)
+        events = make_events(seeds[k:k + chunk], workers, workload)
         b = DeviceBatch(ctx, events, device)
         ctx.prefilter_enable(False)
         ctx.batch_run(b.batch)
@@ -320,14 +338,14 @@ def train(ctx, data: dict, device, seed: int = 1, target: float = 0.997, log=pri
     return model, report
 
 
-def evaluate(ctx, model, seeds, device, chunk: int = 100, workers: int | None = None, log=print) -> dict:
+def evaluate(ctx, model, seeds, device, chunk: int = 100, workers: int | None = None, log=print, workload: str = "pbpb") -> dict:
     """Learned vs plain batched runs over the events of `seeds`."""
     ctx.prefilter_set_model(model)
     tot = dict(plain_roads=0, learned_roads=0, reproduced=0, extra=0, extra_fakes=0, plain_fakes=0, learned_fakes=0,
                plain_cells=0, learned_cells=0, events=0)
     seeds = list(seeds)
     for k in range(0, len(seeds), chunk):
-        events = make_events(seeds[k:k + chunk], workers)
+        events = make_events(seeds[k:k + chunk], workers, workload)
         b = DeviceBatch(ctx, events, device)
         ctx.prefilter_enable(False)
         ctx.batch_run(b.batch)
@@ -344,6 +362,7 @@ def evaluate(ctx, model, seeds, device, chunk: int = 100, workers: int | None = 
         tot["plain_cells"] += plain_cells
         tot["learned_cells"] += learned_cells
         tot["events"] += len(events)
+        tot["runs"] = tot.get("runs", 0) + b.n_runs
         log("evaluate: events %d..%d %s" % (k, k + len(events) - 1, json.dumps(c)))
     tot["road_reproduction"] = tot["reproduced"] / max(tot["plain_roads"], 1)
     tot["cells_kept"] = tot["learned_cells"] / max(tot["plain_cells"], 1)
@@ -352,7 +371,9 @@ def evaluate(ctx, model, seeds, device, chunk: int = 100, workers: int | None = 
 
 def main(argv=None):
     p = argparse.ArgumentParser(description="Train, calibrate and evaluate the learned prefilter on one GPU.")
-    p.add_argument("--out", default=CHECKPOINT, help="checkpoint to write")
+    p.add_argument("--workload", choices=("pbpb", "pileup"), default="pbpb",
+                   help="pbpb: central Pb-Pb-like events; pileup: frames of 5 collisions (every vertex is a run)")
+    p.add_argument("--out", default=None, help="checkpoint to write (default: weights/prefilter_<workload>.itsumlp)")
     p.add_argument("--report", default=None, help="JSON report (default: the checkpoint path with .json)")
     p.add_argument("--train-events", type=int, default=2000)
     p.add_argument("--eval-events", type=int, default=500)
@@ -363,20 +384,21 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--chunk", type=int, default=100)
     args = p.parse_args(argv)
+    args.out = args.out or CHECKPOINTS[args.workload]
     import torch
 
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
     ctx = capi.Context(device=0)
     t0 = time.perf_counter()
-    data = collect(ctx, range(TRAIN_SEED0, TRAIN_SEED0 + args.train_events), device, chunk=args.chunk)
+    data = collect(ctx, range(TRAIN_SEED0, TRAIN_SEED0 + args.train_events), device, chunk=args.chunk, workload=args.workload)
     collect_s = time.perf_counter() - t0
     model, report = train(ctx, data, device, seed=args.seed, target=args.target, steps=args.steps, batch=args.batch, lr=args.lr)
     del data
-    ev = evaluate(ctx, model, range(EVAL_SEED0, EVAL_SEED0 + args.eval_events), device, chunk=args.chunk)
+    ev = evaluate(ctx, model, range(EVAL_SEED0, EVAL_SEED0 + args.eval_events), device, chunk=args.chunk, workload=args.workload)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     capi.prefilter_save(model, args.out)
-    full = dict(train_events=args.train_events, train_seeds=[TRAIN_SEED0, TRAIN_SEED0 + args.train_events - 1],
+    full = dict(workload=args.workload, train_events=args.train_events, train_seeds=[TRAIN_SEED0, TRAIN_SEED0 + args.train_events - 1],
                 eval_events=args.eval_events, eval_seeds=[EVAL_SEED0, EVAL_SEED0 + args.eval_events - 1],
                 collect_seconds=collect_s, train=report, evaluation=ev)
     with open(args.report or os.path.splitext(args.out)[0] + ".json", "w") as fh:
