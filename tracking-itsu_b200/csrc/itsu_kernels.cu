@@ -40,6 +40,7 @@ constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr float kMaxAbsCoordinate = 1.0e6f;
 constexpr int kMaxPruneBin = 64;  // larger bins disable pruning for their layer
+static_assert(kMaxPruneBin <= 64, "a pruned column's passes are a 64-bit mask");
 
 __device__ __forceinline__ bool capacity_failed(const DevStatus *s) { return (*(volatile const int32_t *)&s->flags & kCapacityMask) != 0; }
 
@@ -514,7 +515,6 @@ __device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t 
   (void)layer;
 }
 
-constexpr int kColHits = 16;        // hits of one z-pruned column sorted back into index order
 constexpr int kTrackletSlots = kTrackletSlotsPerCluster;
 constexpr int kMaxMaskedOut = 64;  // out-degrees up to this are evaluated pair-parallel with a pass mask
 
@@ -579,38 +579,22 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
             hi = mid;
           }
         }
-        int hits[kColHits];
-        int h = 0;
-        bool overflow = false;
+        // a pruned column holds at most kMaxPruneBin (64) clusters: its passes as a mask over
+        // their positions in the column, emitted in index order
+        unsigned long long hit = 0ull;
         for (int k = lo; k < k1; ++k) {
           const float4 q = zs[k];  // z, r, phi and the sorted index of the k-th cluster by z
           if (!(q.x <= zhi)) {
             break;
           }
-          const int j = __float_as_int(q.w);
           if (probe.pass(q.x, q.y, q.z)) {
-            if (h == kColHits) {
-              overflow = true;
-              break;
-            }
-            int q = h++;
-            while (q > 0 && hits[q - 1] > j) {
-              hits[q] = hits[q - 1];
-              --q;
-            }
-            hits[q] = j;
+            hit |= 1ull << (__float_as_int(q.w) - k0);
           }
         }
-        if (!overflow) {
-          for (int q = 0; q < h; ++q) {
-            on_pass(hits[q]);
-          }
-        } else {
-          for (int j = k0; j < k1; ++j) {  // a crowded column: walk it in index order
-            if (probe.pass(j)) {
-              on_pass(j);
-            }
-          }
+        while (hit) {
+          const int b = __ffsll((long long)hit) - 1;
+          hit &= hit - 1ull;
+          on_pass(k0 + b);
         }
       }
       const int x = table[max_bin];  // the inclusive bound's candidate (P1: inside the layer)
