@@ -76,6 +76,7 @@ struct Arena {
   float *phi;
   itsu_cluster *tmp;
   int32_t *index_tables;
+  int32_t *clu_seg;  // per sorted cluster: its segment 7e + L (null: not wanted)
   // candidate-pruning index (null: not built): per bin, the bin's clusters sorted by (z, index),
   // each with its r and phi for the cut;
   // per (event, layer) the r range of its clusters and whether all its bins are regular

@@ -44,21 +44,6 @@ static_assert(kMaxPruneBin <= 64, "a pruned column's passes are a 64-bit mask");
 
 __device__ __forceinline__ bool capacity_failed(const DevStatus *s) { return (*(volatile const int32_t *)&s->flags & kCapacityMask) != 0; }
 
-// Largest s in [0, nseg) with off[s] <= i, for off[0] <= i < off[nseg]; never an empty segment.
-__device__ __forceinline__ int find_segment(const int32_t *__restrict__ off, int nseg, int64_t i)
-{
-  int lo = 0, hi = nseg;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(off + mid) <= i) {
-      lo = mid;
-    } else {
-      hi = mid;
-    }
-  }
-  return lo;
-}
-
 __device__ __forceinline__ int grid_threads() { return gridDim.x * blockDim.x; }
 __device__ __forceinline__ int64_t global_thread() { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
 
@@ -403,6 +388,9 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
     __syncwarp();
     if (valid) {
       store_sorted(a, begin + pos, c);
+      if (a.clu_seg) {
+        a.clu_seg[begin + pos] = seg;
+      }
     }
   }
 
@@ -631,7 +619,7 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
 {
   InnerCluster s;
   s.walk = false;
-  s.seg = find_segment(a.layer_off, a.n_events * ITSU_LAYERS, i);
+  s.seg = a.clu_seg[i];
   s.e = s.seg / ITSU_LAYERS;
   s.layer = s.seg % ITSU_LAYERS;
   const int32_t *lo = a.layer_off + s.e * ITSU_LAYERS;
@@ -709,7 +697,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_tail(Arena a)
     return;
   }
   const int32_t first = a.trk_off[i], count = a.trk_off[i + 1] - first;
-  const int seg = find_segment(a.layer_off, a.n_events * ITSU_LAYERS, i);
+  const int seg = a.clu_seg[i];
   const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
   a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && count > 0)
                         ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
