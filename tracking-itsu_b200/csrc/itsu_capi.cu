@@ -132,8 +132,11 @@ struct itsu_context {
   bool graph_prefilter = false;
 
   // streamed host runs (ITSU_FLAG_STREAM_HOST): upload stream, per-chunk events, batch-wide roads
-  cudaStream_t copy_stream = nullptr;
-  cudaEvent_t chunk_ready[16] = {};
+  cudaStream_t copy_stream = nullptr;   // uploads
+  cudaStream_t d2h_stream = nullptr;    // road downloads
+  cudaEvent_t chunk_ready[16] = {};     // a chunk's upload is done ([15]: the call's start)
+  cudaEvent_t chunk_done[16] = {};      // a chunk's roads, road end and status are on the host side
+  int32_t *h_road_end = nullptr;        // pinned: each chunk's end in the batch-wide roads
   int32_t *chunk_off = nullptr;   // each chunk's layer offsets, rebased to the chunk
   int64_t cap_chunk_off = 0;
   int32_t *h_chunk_off = nullptr;  // pinned staging of chunk_off
@@ -832,7 +835,12 @@ void itsu_context_destroy(itsu_context *ctx)
   for (cudaEvent_t &e : ctx->chunk_ready) {
     if (e) cudaEventDestroy(e);
   }
+  for (cudaEvent_t &e : ctx->chunk_done) {
+    if (e) cudaEventDestroy(e);
+  }
+  if (ctx->h_road_end) cudaFreeHost(ctx->h_road_end);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -1135,9 +1143,11 @@ itsu_status grow_buffer(itsu_context *ctx, T *&p, int64_t &cap, int64_t need)
 }
 
 // itsu_batch_run_host with ITSU_FLAG_STREAM_HOST: consecutive chunks of events, each one's
-// upload (copy stream) overlapping the work on the one before (context stream). Sets *done to
-// false, with nothing reported, when the batch is too small to split or a chunk outgrew the
-// arena: the caller then runs the batch in one pass (which grows the arena).
+// upload (copy stream) overlapping the work on the one before (context stream), and each one's
+// roads downloaded (download stream) while the next one works. The first chunk is smaller, so
+// that the device starts sooner. Sets *done to false, with nothing reported, when the batch is
+// too small to split or a chunk outgrew the arena: the caller then runs the batch in one pass
+// (which grows the arena).
 itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets, const float *vertices,
                               int32_t n_events, int64_t n_clusters, itsu_road *roads, int64_t roads_capacity,
                               int32_t *road_offsets, bool *done)
@@ -1146,11 +1156,12 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
   const int64_t per_chunk = ctx->chunk_clusters > 0 ? ctx->chunk_clusters : kChunkClusters;
   const int k_chunks = (int)std::min<int64_t>(std::min<int64_t>(kMaxChunks - 1, n_events), (n_clusters + per_chunk - 1) / per_chunk);
   if (k_chunks < 2) return ITSU_OK;
-  // chunk boundaries (events) with about equal cluster counts
+  // chunk boundaries (events): cluster shares 0.4 : 1 : 1 : ... (the first one small)
+  constexpr double kFirst = 0.4;
   std::vector<int32_t> ev(k_chunks + 1, 0);
   ev[k_chunks] = n_events;
   for (int c = 1, e = 0; c < k_chunks; ++c) {
-    const int64_t target = n_clusters * c / k_chunks;
+    const int64_t target = (int64_t)((double)n_clusters * (kFirst + (c - 1)) / (kFirst + (k_chunks - 1)));
     while (e < n_events && layer_offsets[(int64_t)e * ITSU_LAYERS] < target) ++e;
     ev[c] = std::max(e, ev[c - 1] + 1);
   }
@@ -1171,9 +1182,12 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
   if ((st = grow_buffer(ctx, ctx->road_off_all, ctx->cap_road_off_all, (int64_t)n_events + 1)) != ITSU_OK) return st;
   if (!ctx->chunk_status) ITSU_CUDA(ctx, cudaMalloc((void **)&ctx->chunk_status, sizeof(DevStatus) * kMaxChunks));
   if (!ctx->h_chunk_status) ITSU_CUDA(ctx, cudaMallocHost((void **)&ctx->h_chunk_status, sizeof(DevStatus) * kMaxChunks));
+  if (!ctx->h_road_end) ITSU_CUDA(ctx, cudaMallocHost((void **)&ctx->h_road_end, sizeof(int32_t) * kMaxChunks));
   if (!ctx->copy_stream) ITSU_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-  for (int c = 0; c < k_chunks; ++c) {
+  if (!ctx->d2h_stream) ITSU_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking));
+  for (int c = 0; c < kMaxChunks; ++c) {
     if (!ctx->chunk_ready[c]) ITSU_CUDA(ctx, cudaEventCreateWithFlags(&ctx->chunk_ready[c], cudaEventDisableTiming));
+    if (!ctx->chunk_done[c]) ITSU_CUDA(ctx, cudaEventCreateWithFlags(&ctx->chunk_done[c], cudaEventDisableTiming));
   }
   // each chunk's layer offsets, rebased (chunk c at 7 ev[c] + c), staged in pinned memory so that
   // their upload is asynchronous
@@ -1185,7 +1199,7 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
     ITSU_CUDA(ctx, cudaMallocHost((void **)&ctx->h_chunk_off, sizeof(int32_t) * grow_to(n_off)));
     ctx->cap_h_chunk_off = grow_to(n_off);
   }
-  // the previous call finished with a synchronisation: the staging buffer is free to refill
+  // the previous call finished with a synchronisation: the staging buffers are free to refill
   for (int c = 0; c < k_chunks; ++c) {
     const int32_t base = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS];
     for (int64_t k = (int64_t)ev[c] * ITSU_LAYERS; k <= (int64_t)ev[c + 1] * ITSU_LAYERS; ++k) {
@@ -1194,14 +1208,12 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
   }
   // All uploads go on the copy stream, the small ones first: host-to-device copies share the copy
   // engine in submission order, so a small copy queued behind the clusters would hold up the
-  // first chunk's work. The copy stream first waits for any earlier work of the context.
+  // first chunk's work. The copy and download streams first wait for any earlier work of the
+  // context.
   cudaEvent_t start = ctx->chunk_ready[kMaxChunks - 1];
-  if (!start) {
-    ITSU_CUDA(ctx, cudaEventCreateWithFlags(&ctx->chunk_ready[kMaxChunks - 1], cudaEventDisableTiming));
-    start = ctx->chunk_ready[kMaxChunks - 1];
-  }
   ITSU_CUDA(ctx, cudaEventRecord(start, ctx->stream));
   ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, start, 0));
+  ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->d2h_stream, start, 0));
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->chunk_off, ctx->h_chunk_off, sizeof(int32_t) * n_off, cudaMemcpyHostToDevice, ctx->copy_stream));
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, vertices, sizeof(float) * 3 * (int64_t)n_events, cudaMemcpyHostToDevice, ctx->copy_stream));
   for (int c = 0; c < k_chunks; ++c) {
@@ -1212,10 +1224,41 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
     }
     ITSU_CUDA(ctx, cudaEventRecord(ctx->chunk_ready[c], ctx->copy_stream));
   }
-  // the work: per chunk (after its upload, which follows the offsets and vertices), the whole
-  // sequence, then its roads appended to the batch-wide output
   ITSU_CUDA(ctx, cudaMemsetAsync(ctx->road_off_all, 0, sizeof(int32_t) * ((int64_t)n_events + 1), ctx->stream));
-  for (int c = 0; c < k_chunks; ++c) {
+
+  // The roads of a finished chunk go to the host on the download stream while later chunks work;
+  // the chunk's status is checked first, and decides whether the batch goes on streaming.
+  int64_t downloaded = 0;
+  bool fallback = false;
+  auto collect = [&](int c) -> itsu_status {
+    ITSU_CUDA(ctx, cudaEventSynchronize(ctx->chunk_done[c]));
+    const DevStatus &s = ctx->h_chunk_status[c];
+    if (s.flags & itsu::kFlagInvalid) {
+      if (s.invalid_event != INT32_MAX) {
+        return fail(ctx, ITSU_ERR_INVALID, "primary vertex of event %d is not finite or beyond 1e6 cm", ev[c] + s.invalid_event);
+      }
+      return fail(ctx, ITSU_ERR_INVALID, "cluster %lld is malformed: a coordinate is not finite or beyond 1e6 cm, or it sits on the beam line at the vertex z (r == 0 and z == vertex z)",
+                  (long long)layer_offsets[(int64_t)ev[c] * ITSU_LAYERS] + s.invalid_index);
+    }
+    if (s.flags & itsu::kCapacityMask) {
+      fallback = true;  // one pass instead, which grows the arena
+      return ITSU_OK;
+    }
+    const int64_t end = ctx->h_road_end[c];
+    if (roads && end > roads_capacity) {
+      return fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %lld given", (long long)end, (long long)roads_capacity);
+    }
+    if (roads && end > downloaded) {
+      ITSU_CUDA(ctx, cudaMemcpyAsync(roads + downloaded, ctx->roads_all + downloaded, sizeof(itsu_road) * (end - downloaded),
+                                     cudaMemcpyDeviceToHost, ctx->d2h_stream));
+    }
+    downloaded = end;
+    return ITSU_OK;
+  };
+
+  // the work: per chunk (after its upload, which follows the offsets and vertices), the whole
+  // sequence, its roads appended to the batch-wide output, its road end and status sent back
+  for (int c = 0; c < k_chunks && !fallback; ++c) {
     const int64_t a = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS], b = layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS];
     ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_ready[c], 0));
     ctx->n_events = ev[c + 1] - ev[c];
@@ -1228,39 +1271,31 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
     itsu::launch_append_roads(arena_of(ctx), launch_of(ctx), ctx->roads_all, ctx->road_off_all, ev[c], ctx->cap_roads_all,
                               ctx->chunk_status + c);
     ITSU_CUDA(ctx, cudaGetLastError());
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_chunk_status + c, ctx->chunk_status + c, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_road_end + c, ctx->road_off_all + ev[c + 1], sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    ITSU_CUDA(ctx, cudaEventRecord(ctx->chunk_done[c], ctx->stream));
+    ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->d2h_stream, ctx->chunk_done[c], 0));
+    if (c > 0 && (st = collect(c - 1)) != ITSU_OK) break;  // chunk c is queued: the device stays busy
   }
+  if (st == ITSU_OK && !fallback) st = collect(k_chunks - 1);
   ctx->stage = kNone;  // the arena holds only the last chunk's intermediate results
   ctx->n_events = 0;
   ctx->n_clusters = 0;
-  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_chunk_status, ctx->chunk_status, sizeof(DevStatus) * k_chunks, cudaMemcpyDeviceToHost,
-                                 ctx->stream));
-  int32_t total32 = 0;
-  ITSU_CUDA(ctx, cudaMemcpyAsync(&total32, ctx->road_off_all + n_events, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (int c = 0; c < k_chunks; ++c) {
-    const DevStatus &s = ctx->h_chunk_status[c];
-    if (s.flags & itsu::kFlagInvalid) {
-      if (s.invalid_event != INT32_MAX) {
-        return fail(ctx, ITSU_ERR_INVALID, "primary vertex of event %d is not finite or beyond 1e6 cm", ev[c] + s.invalid_event);
-      }
-      return fail(ctx, ITSU_ERR_INVALID, "cluster %lld is malformed: a coordinate is not finite or beyond 1e6 cm, or it sits on the beam line at the vertex z (r == 0 and z == vertex z)",
-                  (long long)layer_offsets[(int64_t)ev[c] * ITSU_LAYERS] + s.invalid_index);
-    }
-    if (s.flags & itsu::kCapacityMask) return ITSU_OK;  // *done stays false: one pass, which grows the arena
-  }
-  const int64_t total = total32;
-  if (road_offsets) {
+  if (st == ITSU_OK && !fallback && road_offsets) {
     ITSU_CUDA(ctx, cudaMemcpyAsync(road_offsets, ctx->road_off_all, sizeof(int32_t) * ((int64_t)n_events + 1), cudaMemcpyDeviceToHost,
-                                   ctx->stream));
+                                   ctx->d2h_stream));
   }
-  if (roads) {
-    if (total > roads_capacity) return fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %lld given", (long long)total, (long long)roads_capacity);
-    if (total > 0) {
-      ITSU_CUDA(ctx, cudaMemcpyAsync(roads, ctx->roads_all, sizeof(itsu_road) * total, cudaMemcpyDeviceToHost, ctx->stream));
-    }
-  }
-  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  *done = true;
+  // whatever happened, nothing of this call is left in flight
+  const cudaError_t e1 = cudaStreamSynchronize(ctx->stream);
+  const cudaError_t e2 = cudaStreamSynchronize(ctx->d2h_stream);
+  const cudaError_t e3 = cudaStreamSynchronize(ctx->copy_stream);
+  if (st != ITSU_OK) return st;
+  ITSU_CUDA(ctx, e1);
+  ITSU_CUDA(ctx, e2);
+  ITSU_CUDA(ctx, e3);
+  *done = !fallback;
   return ITSU_OK;
 }
 
