@@ -118,3 +118,20 @@ def test_streamed_roads_into_pinned_host_buffer():
     finally:
         one.close()
         ctx.close()
+
+
+def test_streamed_batch_outgrowing_the_arena_falls_back_and_grows():
+    """Tiny starting capacities: the first chunk overflows, the call runs the batch in one pass
+    (which grows the arena) and returns the same roads; the next call streams in the grown arena."""
+    events = [gen.pbpb_event(s, n_tracks=2000) for s in range(100, 106)]
+    clusters, offsets, vertices = gen.pack_batch(events)
+    one = capi.Context(device=0)
+    small = capi.Context(device=0, flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=30000, max_tracklets=1000,
+                         max_cells=1000, max_neighbours=1000, max_roads=100)
+    try:
+        want = one.batch_run_host(clusters, offsets, vertices)
+        _same(want, small.batch_run_host(clusters, offsets, vertices))
+        _same(want, small.batch_run_host(clusters, offsets, vertices))
+    finally:
+        one.close()
+        small.close()
