@@ -683,6 +683,36 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
   a.trk_count[i] = count;
 }
 
+__device__ __forceinline__ int warp_exclusive_sum(int v, int &total)
+{
+  const int lane = threadIdx.x & 31;
+  int inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) {
+      inc += t;
+    }
+  }
+  total = __shfl_sync(0xffffffffu, inc, 31);
+  return inc - v;
+}
+
+// Owner lane of flattened item t given the lanes' exclusive prefix sums: the last lane whose
+// prefix is <= t (for t < total this lane holds item t). All lanes must call it together.
+__device__ __forceinline__ int owner_of(int excl, int t)
+{
+  int owner = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    const int v = __shfl_sync(0xffffffffu, excl, owner + step);
+    if (v <= t) {
+      owner += step;
+    }
+  }
+  return owner;
+}
+
 // Per inner cluster, before the write pass: its entry of the tracklets lookup table
 // (Tracker.cxx:102-108) and, for each of its tracklet slots, the owner cluster and segment the
 // write pass reads. Clusters with more than kTrackletSlots tracklets (rare) walk their candidates
@@ -693,22 +723,37 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_tail(Arena a)
     return;
   }
   const int64_t i = global_thread();
-  if (i >= a.n_clusters) {
-    return;
+  const int lane = threadIdx.x & 31;
+  const bool valid = i < a.n_clusters;
+  int32_t first = 0, count = 0;
+  int seg = 0, sid = 0;
+  if (valid) {
+    first = a.trk_off[i];
+    count = a.trk_off[i + 1] - first;
+    seg = a.clu_seg[i];
+    const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
+    a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && count > 0)
+                          ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
+                          : ITSU_UNUSED_INDEX;
+    sid = e * ITSU_TRACKLET_LAYERS + layer;
   }
-  const int32_t first = a.trk_off[i], count = a.trk_off[i + 1] - first;
-  const int seg = a.clu_seg[i];
-  const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
-  a.trk_lookup[i] = (layer >= 1 && layer <= ITSU_CELL_LAYERS && count > 0)
-                        ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
-                        : ITSU_UNUSED_INDEX;
-  // every slot gets its owner (the write pass reads it for every tracklet)
-  const int sid = e * ITSU_TRACKLET_LAYERS + layer;
-  for (int r = 0; r < count; ++r) {
-    a.trk_owner[first + r] = (int32_t)i;
-    a.trk_seg_id[first + r] = sid;
+  // Every tracklet gets its owner and segment (the write pass reads them for every tracklet).
+  // The warp's 32 clusters own one contiguous range of tracklets: the warp fills it together,
+  // with coalesced stores.
+  int total = 0;
+  const int excl = warp_exclusive_sum(count, total);
+  const int32_t base = __shfl_sync(0xffffffffu, first, 0);
+  const int64_t i0 = i - lane;
+  for (int p0 = 0; p0 < total; p0 += 32) {
+    const int p = p0 + lane;
+    const int owner = owner_of(excl, p);
+    const int owner_sid = __shfl_sync(0xffffffffu, sid, owner);
+    if (p < total) {
+      a.trk_owner[base + p] = (int32_t)(i0 + owner);
+      a.trk_seg_id[base + p] = owner_sid;
+    }
   }
-  if (count > kTrackletSlots) {
+  if (valid && count > kTrackletSlots) {
     const InnerCluster s = inner_cluster(a, i);
     int out = first;
     walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, seg); });
@@ -862,36 +907,6 @@ __device__ __forceinline__ float4 shfl4(float4 v, int src)
 {
   return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
                      __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
-}
-
-// Owner lane of flattened item t given the lanes' exclusive prefix sums: the last lane whose
-// prefix is <= t (for t < total this lane holds item t). All lanes must call it together.
-__device__ __forceinline__ int owner_of(int excl, int t)
-{
-  int owner = 0;
-#pragma unroll
-  for (int step = 16; step > 0; step >>= 1) {
-    const int v = __shfl_sync(0xffffffffu, excl, owner + step);
-    if (v <= t) {
-      owner += step;
-    }
-  }
-  return owner;
-}
-
-__device__ __forceinline__ int warp_exclusive_sum(int v, int &total)
-{
-  const int lane = threadIdx.x & 31;
-  int inc = v;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, inc, d);
-    if (lane >= d) {
-      inc += t;
-    }
-  }
-  total = __shfl_sync(0xffffffffu, inc, 31);
-  return inc - v;
 }
 
 __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const CellLane &s, const itsu_tracklet &t2, int32_t j,
