@@ -165,7 +165,7 @@ KERNEL_STAGE = {
     "tracklets_tail": "tracklets",
     "cells_count": "cells",
     "cells_scatter": "cells",
-    "cells_lookup": "cells",
+    "cells_crowded": "cells",
     "neighbours_count": "neighbours",
     "neighbours_write": "neighbours",
     "roads_write": "roads",

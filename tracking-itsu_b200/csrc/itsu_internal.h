@@ -44,6 +44,7 @@ struct DevStatus {
   int32_t pad_;
   int64_t total[4];       // tracklets, cells, neighbours, roads
   int64_t cell_entries;   // cell entries reserved by the cell count pass (may exceed the scratch)
+  int64_t crowded;        // tracklets the cell count pass listed in cell_crowded
 };
 
 // A cell as the count pass finds it: its first and second tracklets (flat), the outgoing-tracklet
@@ -100,6 +101,7 @@ struct Arena {
   unsigned long long *cell_mask;  // per first tracklet: which outgoing tracklets make cells
   int32_t *cell_off;
   int32_t *cell_lookup;
+  int32_t *cell_crowded;  // tracklets whose outer cluster has more than 64 outgoing tracklets
   int32_t *cell_seg;
   itsu_cell *cells;
   int32_t *cell_seg_id;

@@ -59,6 +59,7 @@ __global__ void k_status_init(DevStatus *s)
     s->total[k] = 0;
   }
   s->cell_entries = 0;
+  s->crowded = 0;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1061,6 +1062,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
     if (s.k < n) {
       a.cell_count[s.k] = count;
       a.cell_mask[s.k] = big ? 0ull : masks[warp][lane];
+      a.cell_lookup[s.k] = ITSU_UNUSED_INDEX;  // the write pass fills it for tracklets with cells
+      if (big && count > 0) {
+        a.cell_crowded[atomicAdd(reinterpret_cast<unsigned long long *>(&a.status->crowded), 1ull)] = (int32_t)s.k;
+      }
     }
     __syncwarp();
   }
@@ -1168,9 +1173,13 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_scatter(Arena a)
       if (h[u].x < 0 || !((m[u] >> h[u].y) & 1ull)) {
         continue;  // an unused slot, or a pair removed by the learned prefilter
       }
-      const int32_t out = off[u] + __popcll(m[u] & ((1ull << h[u].y) - 1ull));
+      const int32_t rank = __popcll(m[u] & ((1ull << h[u].y) - 1ull));
+      const int32_t out = off[u] + rank;
       const int e = sid[u] / ITSU_TRACKLET_LAYERS, layer = sid[u] % ITSU_TRACKLET_LAYERS;
       const int32_t *ts = a.trk_seg + e * ITSU_TRACKLET_LAYERS;
+      if (rank == 0 && layer >= 1) {  // the tracklet's first cell: its cells lookup entry
+        a.cell_lookup[h[u].x] = out - a.cell_seg[e * ITSU_CELL_LAYERS + layer];
+      }
       int2 *dst = reinterpret_cast<int2 *>(a.cells + out);
       dst[0] = make_int2(t1[u].first_cluster, t1[u].second_cluster);
       dst[1] = make_int2(t2[u].second_cluster, h[u].x - ts[layer]);
@@ -1182,56 +1191,32 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_scatter(Arena a)
   }
 }
 
-// Write pass, part 2: the cells lookup of every tracklet, and the cells of the tracklets whose
-// outer cluster was too crowded for the pair-parallel count (their mask is empty), in order on
-// one lane.
-__global__ void __launch_bounds__(kMaxThreads) k_cells_lookup(Arena a)
+// Write pass, part 2: the tracklets whose outer cluster was too crowded for the pair-parallel
+// count (listed by the count pass; their mask is empty): their cells in order on one lane, and
+// their cells lookup entry.
+__global__ void __launch_bounds__(kMaxThreads) k_cells_crowded(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
   }
   const int64_t n = a.status->total[kTracklets];
-  const int64_t stride = grid_threads();
-  constexpr int kPer = 4;  // tracklets per thread per round, their loads in flight together
-  for (int64_t k0 = global_thread(); k0 < n; k0 += kPer * stride) {
-    int32_t first[kPer], last[kPer];
-    int sid[kPer];
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const int64_t k = k0 + u * stride;
-      first[u] = last[u] = 0;
-      sid[u] = 0;
-      if (k < n) {
-        first[u] = a.cell_off[k];
-        last[u] = a.cell_off[k + 1];
-        sid[u] = a.trk_seg_id[k];
-      }
+  const int64_t listed = a.status->crowded;
+  for (int64_t q = global_thread(); q < listed; q += grid_threads()) {
+    const int32_t k = a.cell_crowded[q];
+    const CellLane s = cell_lane(a, k, n);
+    const int32_t first = a.cell_off[k];
+    if (s.layer >= 1 && s.layer < ITSU_CELL_LAYERS) {
+      a.cell_lookup[k] = first - a.cell_seg[s.e * ITSU_CELL_LAYERS + s.layer];
     }
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const int64_t k = k0 + u * stride;
-      if (k >= n) {
-        continue;
-      }
-      const bool has = last[u] > first[u];
-      const int e = sid[u] / ITSU_TRACKLET_LAYERS, layer = sid[u] % ITSU_TRACKLET_LAYERS;
-      a.cell_lookup[k] = (layer >= 1 && layer < ITSU_CELL_LAYERS && has) ? first[u] - a.cell_seg[e * ITSU_CELL_LAYERS + layer]
-                                                                         : ITSU_UNUSED_INDEX;
-      if (has && a.cell_mask[k] == 0ull) {
-        // a tracklet whose outer cluster was too crowded for the pair-parallel count: its cells
-        // in order, on this lane
-        const CellLane s = cell_lane(a, k, n);
-        int64_t out = first[u];
-        for (int b = 0; b < s.n_out; ++b) {
-          const int32_t j = s.j0 + b;
-          const itsu_tracklet t2 = a.tracklets[j];
-          float3 normal;
-          float curvature;
-          if (cell_precut(s.layer, s.t1_tan_lambda, s.t1_phi, t2.tan_lambda, t2.phi, s.c1, s.vz) &&
-              cell_geometry(s.layer, s.c1, s.c2, a.xyzr[s.c3_base + t2.second_cluster], s.vx, s.vy, normal, curvature)) {
-            write_cell(a, out++, s, t2, j, normal, curvature);
-          }
-        }
+    int64_t out = first;
+    for (int b = 0; b < s.n_out; ++b) {
+      const int32_t j = s.j0 + b;
+      const itsu_tracklet t2 = a.tracklets[j];
+      float3 normal;
+      float curvature;
+      if (cell_precut(s.layer, s.t1_tan_lambda, s.t1_phi, t2.tan_lambda, t2.phi, s.c1, s.vz) &&
+          cell_geometry(s.layer, s.c1, s.c2, a.xyzr[s.c3_base + t2.second_cluster], s.vx, s.vy, normal, curvature)) {
+        write_cell(a, out++, s, t2, j, normal, curvature);
       }
     }
   }
@@ -1533,7 +1518,7 @@ void step_cells_prefilter(const Arena &a, const Launch &l)
 
 void step_cells_scatter(const Arena &a, const Launch &l) { k_cells_scatter<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
 
-void step_cells_lookup(const Arena &a, const Launch &l) { k_cells_lookup<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
+void step_cells_crowded(const Arena &a, const Launch &l) { k_cells_crowded<<<l.num_sms, 128, 0, l.stream>>>(a); }
 
 void step_cell_segments(const Arena &a, const Launch &l)
 {
@@ -1575,7 +1560,7 @@ const KernelStep kSteps[] = {
     {"scan_apply_cells", step_scan_apply<1>},            // 13
     {"cell_segments", step_cell_segments},               // 14
     {"cells_scatter", step_cells_scatter},               // 15
-    {"cells_lookup", step_cells_lookup},                 // 16
+    {"cells_crowded", step_cells_crowded},               // 16
     {"neighbour_reset", step_neighbour_reset},           // 17 (d)
     {"neighbours_count", step_neighbours<false>},        // 18
     {"scan_reduce_neighbours", step_scan_reduce<2>},     // 19
