@@ -107,20 +107,25 @@ __device__ __forceinline__ bool tracklet_cut(int layer, float tan_lambda, float 
 }
 
 // Tracker.cxx:161-173: the cheap cell cuts, which need only the two tracklets and the first
-// cluster (c = (x, y, z, r)); most pairs stop here.
-__device__ __forceinline__ bool cell_precut(int layer, float t1_tan_lambda, float t1_phi, float t2_tan_lambda, float t2_phi,
-                                            float4 c1, float vz)
+// cluster (c = (x, y, z, r)); most pairs stop here. Every term is evaluated (no early exit: the
+// terms are pure, so the result is the reference's short-circuit one) so that a loop over
+// outgoing tracklets runs without branches; max_dz is the layer's CellMaxDeltaZThreshold.
+__device__ __forceinline__ bool cell_precut_dz(float t1_tan_lambda, float t1_phi, float t2_tan_lambda, float t2_phi, float4 c1,
+                                               float vz, float max_dz)
 {
   const float delta_tan_lambda = fabsf(t1_tan_lambda - t2_tan_lambda);
   const float delta_phi = fabsf(t1_phi - t2_phi);
-  if (!(delta_tan_lambda < kCellMaxDeltaTanLambda &&
-        (delta_phi < kCellMaxDeltaPhi || fabsf(delta_phi - kTwoPi) < kCellMaxDeltaPhi))) {
-    return false;
-  }
   const float average_tan_lambda = 0.5f * (t1_tan_lambda + t2_tan_lambda);
   const float dir_z = -average_tan_lambda * c1.w + c1.z;
   const float delta_z = fabsf(dir_z - vz);
-  return delta_z < kC.cell_max_dz[layer];
+  return (delta_tan_lambda < kCellMaxDeltaTanLambda) &
+         ((delta_phi < kCellMaxDeltaPhi) | (fabsf(delta_phi - kTwoPi) < kCellMaxDeltaPhi)) & (delta_z < max_dz);
+}
+
+__device__ __forceinline__ bool cell_precut(int layer, float t1_tan_lambda, float t1_phi, float t2_tan_lambda, float t2_phi,
+                                            float4 c1, float vz)
+{
+  return cell_precut_dz(t1_tan_lambda, t1_phi, t2_tan_lambda, t2_phi, c1, vz, kC.cell_max_dz[layer]);
 }
 
 // Tracker.cxx:175-216: circle-plane normal, radius and DCA of the three clusters. Returns false

@@ -499,7 +499,7 @@ __device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t 
   t.tan_lambda = (c.z - d.z) / (c.w - d.w);
   t.phi = itsu_atan2f(c.y - d.y, c.x - d.x);
   a.tracklets[out] = t;
-  a.trk_tl[out] = t.tan_lambda;
+  a.trk_tlphi[out] = make_float2(t.tan_lambda, t.phi);
   (void)e;
   (void)layer;
 }
@@ -842,8 +842,6 @@ __device__ __forceinline__ bool cells_active(const int32_t *ts, int layer)
   return true;
 }
 
-constexpr int kCellQueue = 64;
-
 // Per-lane state of the warp-parallel cell stage: lane l owns first tracklet k = base + l.
 struct CellLane {
   int64_t k;
@@ -929,14 +927,14 @@ __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const Ce
 }
 
 // Count pass: for each first tracklet, a mask of which of its (<= 64) outgoing tracklets make a
-// cell, and their number. The warp flattens its 32 tracklets' pairs across lanes (Tracker.cxx:
-// 155-158 iterates them per tracklet); pairs that pass the cheap cuts queue up so the circle
-// geometry runs with all 32 lanes converged. Each pair that passes becomes a cell entry (its
-// tracklets, normal, curvature and DCA) in the warp's current chunk of the entry scratch, so the
-// write pass needs no geometry.
+// cell, and their number. Each lane runs the cheap cuts of its own tracklet's outgoing tracklets
+// (Tracker.cxx:155-173) on the compact (tanL, phi) pairs, one independent 8-byte load each; the
+// pairs that pass (about one in eighteen candidates) are then flattened across the warp's lanes so
+// that the circle geometry runs with the lanes converged. Each pair that passes the geometry
+// becomes a cell entry (its tracklets, normal, curvature and DCA) in the warp's current chunk of
+// the entry scratch, so the write pass needs no geometry.
 __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
 {
-  __shared__ int4 queue[kMaxThreads / 32][kCellQueue];             // (owner lane, pair bit, c3 flat, t2 flat)
   __shared__ unsigned long long masks[kMaxThreads / 32][32];
   if (capacity_failed(a.status)) {
     return;
@@ -948,35 +946,40 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
     const CellLane s = cell_lane(a, base + lane, n);
     const bool big = s.n_out > kMaxMaskedOut;
-    // Only outgoing tracklets with |dtanL| < 0.025 can pass (Tracker.cxx:161-166). The lane
-    // evaluates that first cut term exactly as cell_precut does, on the compact slopes (one
-    // independent 4-byte load per outgoing tracklet), and queues only the pairs it keeps.
-    unsigned long long window = 0;
+    unsigned long long window = 0;  // the outgoing tracklets that pass the cheap cuts
     if (!big && s.n_out > 0) {
-      const float *tl = a.trk_tl + s.j0;
+      const float max_dz = kC.cell_max_dz[s.layer];  // n_out > 0: an active cell layer
+      const float2 *tp = a.trk_tlphi + s.j0;
 #pragma unroll 4
       for (int q = 0; q < s.n_out; ++q) {
-        window |= (unsigned long long)(fabsf(s.t1_tan_lambda - tl[q]) < kCellMaxDeltaTanLambda) << q;
+        const float2 t2 = tp[q];
+        window |= (unsigned long long)cell_precut_dz(s.t1_tan_lambda, s.t1_phi, t2.x, t2.y, s.c1, s.vz, max_dz) << q;
       }
     }
     masks[warp][lane] = 0ull;
     int total = 0;
     const int excl = warp_exclusive_sum(__popcll(window), total);
     __syncwarp();
-    int queued = 0;
-    auto drain = [&](int count) {
-      const int4 q = queue[warp][lane < count ? lane : 0];
-      const int owner = q.x;
+    for (int p0 = 0; p0 < total; p0 += 32) {
+      const int p = p0 + lane;
+      const int owner = owner_of(excl, p);
+      const int r = p - __shfl_sync(0xffffffffu, excl, owner);
+      const unsigned long long wmask = __shfl_sync(0xffffffffu, window, owner);
+      const int32_t j0 = __shfl_sync(0xffffffffu, s.j0, owner);
+      const int64_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
       const float4 c1 = shfl4(s.c1, owner), c2 = shfl4(s.c2, owner);
       const float vx = __shfl_sync(0xffffffffu, s.vx, owner), vy = __shfl_sync(0xffffffffu, s.vy, owner);
       const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
       bool pass = false;
+      int b = 0;
       float3 normal = make_float3(0.0f, 0.0f, 0.0f);
       float curvature = 0.0f, dca = 0.0f;
-      if (lane < count) {
-        pass = cell_geometry(layer, c1, c2, a.xyzr[q.z], vx, vy, normal, curvature, dca);
+      if (p < total) {
+        b = nth_set_bit(wmask, r);
+        const int32_t c3 = a.tracklets[j0 + b].second_cluster;
+        pass = cell_geometry(layer, c1, c2, a.xyzr[c3_base + c3], vx, vy, normal, curvature, dca);
         if (pass) {
-          atomicOr(&masks[warp][owner], 1ull << q.y);
+          atomicOr(&masks[warp][owner], 1ull << b);
         }
       }
       // entries: the passing lanes' slots, contiguous in the warp's chunk
@@ -1002,50 +1005,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
       }
       if (pass && slot < a.cap_cell_entries) {
         int4 *dst = reinterpret_cast<int4 *>(a.cell_entries + slot);
-        dst[0] = make_int4((int)(base + owner), q.y, q.w, __float_as_int(dca));
+        dst[0] = make_int4((int)(base + owner), b, j0 + b, __float_as_int(dca));
         dst[1] = make_int4(__float_as_int(normal.x), __float_as_int(normal.y), __float_as_int(normal.z), __float_as_int(curvature));
       }
-    };
-    for (int p0 = 0; p0 < total; p0 += 32) {
-      const int p = p0 + lane;
-      const int owner = owner_of(excl, p);
-      const int r = p - __shfl_sync(0xffffffffu, excl, owner);
-      const unsigned long long wmask = __shfl_sync(0xffffffffu, window, owner);
-      const float tl = __shfl_sync(0xffffffffu, s.t1_tan_lambda, owner);
-      const float ph = __shfl_sync(0xffffffffu, s.t1_phi, owner);
-      const float4 c1 = shfl4(s.c1, owner);
-      const float vz = __shfl_sync(0xffffffffu, s.vz, owner);
-      const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
-      const int32_t j0 = __shfl_sync(0xffffffffu, s.j0, owner);
-      const int64_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
-      bool pre = false;
-      int64_t c3 = 0;
-      int b = 0;
-      if (p < total) {
-        b = nth_set_bit(wmask, r);
-        const itsu_tracklet t2 = a.tracklets[j0 + b];
-        pre = cell_precut(layer, tl, ph, t2.tan_lambda, t2.phi, c1, vz);
-        c3 = c3_base + t2.second_cluster;
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, pre);
-      if (pre) {
-        queue[warp][queued + __popc(m & ((1u << lane) - 1u))] = make_int4(owner, b, (int)c3, j0 + b);
-      }
-      queued += __popc(m);
-      if (queued >= 32) {
-        __syncwarp();
-        drain(32);
-        __syncwarp();
-        if (lane < queued - 32) {
-          queue[warp][lane] = queue[warp][lane + 32];
-        }
-        __syncwarp();
-        queued -= 32;
-      }
-    }
-    __syncwarp();
-    if (queued > 0) {
-      drain(queued);
     }
     __syncwarp();
     int count = __popcll(masks[warp][lane]);
