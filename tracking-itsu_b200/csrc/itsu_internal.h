@@ -95,7 +95,6 @@ struct Arena {
   int32_t *trk_seg;
   itsu_tracklet *tracklets;
   int32_t *trk_seg_id;
-  float2 *trk_tlphi;  // tan(lambda) and phi of each tracklet, compact (the cell stage's precut)
   // cells
   int32_t *cell_count;
   unsigned long long *cell_mask;  // per first tracklet: which outgoing tracklets make cells

@@ -41,6 +41,8 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr float kMaxAbsCoordinate = 1.0e6f;
 constexpr int kMaxPruneBin = 64;  // larger bins disable pruning for their layer
 static_assert(kMaxPruneBin <= 64, "a pruned column's passes are a 64-bit mask");
+static_assert(sizeof(itsu_tracklet) == 16 && offsetof(itsu_tracklet, tan_lambda) == 8 && offsetof(itsu_tracklet, phi) == 12,
+              "the cell count pass reads (tanL, phi) as the second 8 bytes of a tracklet");
 
 __device__ __forceinline__ bool capacity_failed(const DevStatus *s) { return (*(volatile const int32_t *)&s->flags & kCapacityMask) != 0; }
 
@@ -499,7 +501,6 @@ __device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t 
   t.tan_lambda = (c.z - d.z) / (c.w - d.w);
   t.phi = itsu_atan2f(c.y - d.y, c.x - d.x);
   a.tracklets[out] = t;
-  a.trk_tlphi[out] = make_float2(t.tan_lambda, t.phi);
   (void)e;
   (void)layer;
 }
@@ -928,7 +929,7 @@ __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const Ce
 
 // Count pass: for each first tracklet, a mask of which of its (<= 64) outgoing tracklets make a
 // cell, and their number. Each lane runs the cheap cuts of its own tracklet's outgoing tracklets
-// (Tracker.cxx:155-173) on the compact (tanL, phi) pairs, one independent 8-byte load each; the
+// (Tracker.cxx:155-173) on their (tanL, phi), one independent 8-byte load each; the
 // pairs that pass (about one in eighteen candidates) are then flattened across the warp's lanes so
 // that the circle geometry runs with the lanes converged. Each pair that passes the geometry
 // becomes a cell entry (its tracklets, normal, curvature and DCA) in the warp's current chunk of
@@ -949,10 +950,11 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
     unsigned long long window = 0;  // the outgoing tracklets that pass the cheap cuts
     if (!big && s.n_out > 0) {
       const float max_dz = kC.cell_max_dz[s.layer];  // n_out > 0: an active cell layer
-      const float2 *tp = a.trk_tlphi + s.j0;
+      // (tanL, phi), the second half of each 16-byte tracklet record
+      const float2 *tp = reinterpret_cast<const float2 *>(a.tracklets + s.j0) + 1;
 #pragma unroll 4
       for (int q = 0; q < s.n_out; ++q) {
-        const float2 t2 = tp[q];
+        const float2 t2 = tp[2 * q];
         window |= (unsigned long long)cell_precut_dz(s.t1_tan_lambda, s.t1_phi, t2.x, t2.y, s.c1, s.vz, max_dz) << q;
       }
     }
