@@ -79,6 +79,7 @@ struct itsu_context {
   int32_t *trk_count = nullptr, *trk_off = nullptr, *trk_lookup = nullptr;
   float4 *zs = nullptr;
   int32_t *clu_seg = nullptr;
+  int4 *clu_aux = nullptr;
   int32_t *trk_slots = nullptr;
   // event class
   float2 *seg_rrange = nullptr;
@@ -229,6 +230,7 @@ Arena arena_of(const itsu_context *ctx)
   a.index_tables = ctx->index_tables;
   a.zs = ctx->zs;
   a.clu_seg = ctx->clu_seg;
+  a.clu_aux = ctx->clu_aux;
   a.seg_rrange = ctx->seg_rrange;
   a.seg_regular = ctx->seg_regular;
   a.prune_tracklets = current_tune(ctx).prune;
@@ -309,6 +311,7 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ITSU_CUDA(ctx, alloc(ctx->trk_lookup, cap));
     ITSU_CUDA(ctx, alloc(ctx->zs, cap));
     ITSU_CUDA(ctx, alloc(ctx->clu_seg, cap));
+    ITSU_CUDA(ctx, alloc(ctx->clu_aux, cap));
     ITSU_CUDA(ctx, alloc(ctx->trk_slots, cap * itsu::kTrackletSlotsPerCluster));
     ctx->cap_clusters = cap;
     ctx->generation++;
@@ -819,7 +822,7 @@ void itsu_context_destroy(itsu_context *ctx)
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graph(ctx);
   release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
-  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->trk_slots);
+  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->clu_aux); release(ctx->trk_slots);
   release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);

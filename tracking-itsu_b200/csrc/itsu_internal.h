@@ -78,6 +78,7 @@ struct Arena {
   itsu_cluster *tmp;
   int32_t *index_tables;
   int32_t *clu_seg;  // per sorted cluster: its segment 7e + L (null: not wanted)
+  int4 *clu_aux;     // per sorted cluster: id, alpha bits, MC id, bin (the clustering scatters them here)
   // candidate-pruning index (null: not built): per bin, the bin's clusters sorted by (z, index),
   // each with its r and phi for the cut;
   // per (event, layer) the r range of its clusters and whether all its bins are regular

@@ -271,11 +271,66 @@ __device__ __forceinline__ void store_sorted(const Arena &a, int64_t at, const i
   a.phi[at] = c.phi;
 }
 
+// A warp's 32 consecutive 36-byte clusters move between global and shared memory as 288 words,
+// each load or store instruction covering 128 contiguous bytes; a lane then reads or writes its
+// own record in the stage (word stride 9, odd: no bank conflicts).
+constexpr int kClusterWords = sizeof(itsu_cluster) / 4;
+static_assert(sizeof(itsu_cluster) == 36 && alignof(itsu_cluster) == 4, "cluster layout");
+
+__device__ __forceinline__ void stage_in(int32_t *stage, const itsu_cluster *src, int count)
+{
+  const int32_t *w = reinterpret_cast<const int32_t *>(src);
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < kClusterWords; ++k) {
+    const int at = k * 32 + lane;
+    if (at < count * kClusterWords) {
+      stage[at] = w[at];
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void stage_out(itsu_cluster *dst, const int32_t *stage, int count)
+{
+  __syncwarp();
+  int32_t *w = reinterpret_cast<int32_t *>(dst);
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < kClusterWords; ++k) {
+    const int at = k * 32 + lane;
+    if (at < count * kClusterWords) {
+      w[at] = stage[at];
+    }
+  }
+}
+
+__device__ __forceinline__ itsu_cluster stage_get(const int32_t *stage, int lane)
+{
+  itsu_cluster c;
+  int32_t *w = reinterpret_cast<int32_t *>(&c);
+#pragma unroll
+  for (int k = 0; k < kClusterWords; ++k) {
+    w[k] = stage[lane * kClusterWords + k];
+  }
+  return c;
+}
+
+__device__ __forceinline__ void stage_put(int32_t *stage, int lane, const itsu_cluster &c)
+{
+  const int32_t *w = reinterpret_cast<const int32_t *>(&c);
+#pragma unroll
+  for (int k = 0; k < kClusterWords; ++k) {
+    stage[lane * kClusterWords + k] = w[k];
+  }
+}
+
 __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
 {
   __shared__ int hist[kSortWarps][kBuckets];
   __shared__ int bucket_total[kBuckets];
   __shared__ int bucket_base[kBuckets];
+  __shared__ int32_t stages[kSortWarps][32 * kClusterWords];
 
   const int seg = blockIdx.x;
   const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
@@ -298,23 +353,31 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   }
   __syncthreads();
 
-  // Pass 1: transform every cluster (input order), per-warp bucket histograms.
+  // Pass 1: transform every cluster (input order), per-warp bucket histograms. Each warp owns a
+  // consecutive input range and moves it through its stage 32 clusters at a time.
+  int32_t *stage = stages[warp];
   const int chunk = (n + kSortWarps - 1) / kSortWarps;
   const int wb = min(n, warp * chunk), we = min(n, wb + chunk);
-  for (int i = wb + lane; i < we; i += 32) {
-    itsu_cluster c = a.raw[raw_begin + i];
-    const Transformed t = transform_cluster(layer, c.x, c.y, c.z, vx, vy);
-    c.phi = t.phi;
-    c.r = t.r;
-    c.bin = t.bin;
-    const bool ok = isfinite(c.x) && isfinite(c.y) && isfinite(c.z) && fabsf(c.x) <= kMaxAbsCoordinate &&
-                    fabsf(c.y) <= kMaxAbsCoordinate && fabsf(c.z) <= kMaxAbsCoordinate && !(t.r == 0.0f && c.z == vz);
-    if (!ok) {
-      atomicOr(&a.status->flags, kFlagInvalid);
-      atomicMin(&a.status->invalid_index, (int)(begin + i));
+  for (int i0 = wb; i0 < we; i0 += 32) {
+    const int count = min(32, we - i0);
+    stage_in(stage, a.raw + raw_begin + i0, count);
+    if (lane < count) {
+      itsu_cluster c = stage_get(stage, lane);
+      const Transformed t = transform_cluster(layer, c.x, c.y, c.z, vx, vy);
+      c.phi = t.phi;
+      c.r = t.r;
+      c.bin = t.bin;
+      const bool ok = isfinite(c.x) && isfinite(c.y) && isfinite(c.z) && fabsf(c.x) <= kMaxAbsCoordinate &&
+                      fabsf(c.y) <= kMaxAbsCoordinate && fabsf(c.z) <= kMaxAbsCoordinate && !(t.r == 0.0f && c.z == vz);
+      if (!ok) {
+        atomicOr(&a.status->flags, kFlagInvalid);
+        atomicMin(&a.status->invalid_index, (int)(begin + i0 + lane));
+      }
+      stage_put(stage, lane, c);
+      atomicAdd(&hist[warp][bucket_of(t.bin)], 1);
     }
-    a.tmp[begin + i] = c;
-    atomicAdd(&hist[warp][bucket_of(t.bin)], 1);
+    stage_out(a.tmp + begin + i0, stage, count);
+    __syncwarp();  // the stage is refilled next
   }
   __syncthreads();
 
@@ -370,12 +433,13 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   // Pass 3: stable scatter. Warps own consecutive input ranges whose bucket offsets were
   // prefixed in warp order; inside a warp, lanes of equal bucket rank by lane order.
   for (int i0 = wb; i0 < we; i0 += 32) {
-    const int i = i0 + lane;
-    const bool valid = i < we;
+    const int count = min(32, we - i0);
+    stage_in(stage, a.tmp + begin + i0, count);
+    const bool valid = lane < count;
     itsu_cluster c;
     int bucket = -1 - lane;
     if (valid) {
-      c = a.tmp[begin + i];
+      c = stage_get(stage, lane);
       bucket = bucket_of(c.bin);
     }
     const unsigned peers = __match_any_sync(0xffffffffu, bucket);
@@ -390,11 +454,39 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
     }
     __syncwarp();
     if (valid) {
-      store_sorted(a, begin + pos, c);
+      const int64_t at = begin + pos;
+      a.xyzr[at] = make_float4(c.x, c.y, c.z, c.r);
+      a.phi[at] = c.phi;
+      a.clu_aux[at] = make_int4(c.cluster_id, __float_as_int(c.alpha), c.mc_id, c.bin);
+    }
+  }
+  __syncthreads();
+
+  // Pass 3b: the sorted records (reference layout) assembled from the scattered fields, in
+  // output order, through the stages: coalesced stores instead of nine scattered ones per cluster.
+  for (int i0 = warp * 32; i0 < n; i0 += kSortThreads) {
+    const int count = min(32, n - i0);
+    if (lane < count) {
+      const int64_t at = begin + i0 + lane;
+      const float4 p = a.xyzr[at];
+      const int4 x = a.clu_aux[at];
+      itsu_cluster c;
+      c.x = p.x;
+      c.y = p.y;
+      c.z = p.z;
+      c.phi = a.phi[at];
+      c.r = p.w;
+      c.cluster_id = x.x;
+      c.alpha = __int_as_float(x.y);
+      c.mc_id = x.z;
+      c.bin = x.w;
+      stage_put(stage, lane, c);
       if (a.clu_seg) {
-        a.clu_seg[begin + pos] = seg;
+        a.clu_seg[at] = seg;
       }
     }
+    stage_out(a.sorted + begin + i0, stage, count);
+    __syncwarp();  // the stage is refilled next
   }
 
   // Pass 4: negative bins share bucket 0 in input order; order them by bin, stably.
@@ -450,23 +542,36 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
       atomicOr(&s_irregular, 1);
     }
   }
-  // each cluster's rank in its bin by (z, sorted index)
-  for (int i = tid; i < n; i += kSortThreads) {
-    const int bin = a.sorted[begin + i].bin;
-    if (bin < 0 || bin >= kTableBins) {
-      continue;
-    }
+  // each cluster's rank in its bin by (z, sorted index): a warp per bin of at most kMaxPruneBin
+  // (64) clusters, two per lane, their z values passed round the warp
+  for (int bin = warp; bin < kTableBins; bin += kSortWarps) {
     const int st = bucket_base[bin + 1], cnt = bucket_total[bin + 1];
-    if (cnt > kMaxPruneBin) {
-      continue;
+    if (cnt == 0 || cnt > kMaxPruneBin) {
+      continue;  // warp-uniform
     }
-    const float4 c = a.xyzr[begin + i];
-    int rank = 0;
-    for (int k = 0; k < cnt; ++k) {
-      const float zk = a.xyzr[begin + st + k].z;
-      rank += zk < c.z || (zk == c.z && st + k < i);
+    const int k0 = lane, k1 = lane + 32;
+    float4 c0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), c1 = c0;
+    float phi0 = 0.0f, phi1 = 0.0f;
+    if (k0 < cnt) {
+      c0 = a.xyzr[begin + st + k0];
+      phi0 = a.phi[begin + st + k0];
     }
-    a.zs[begin + st + rank] = make_float4(c.z, c.w, a.phi[begin + i], __int_as_float(i));
+    if (k1 < cnt) {
+      c1 = a.xyzr[begin + st + k1];
+      phi1 = a.phi[begin + st + k1];
+    }
+    int rank0 = 0, rank1 = 0;
+    for (int j = 0; j < cnt; ++j) {
+      const float zj = __shfl_sync(0xffffffffu, j < 32 ? c0.z : c1.z, j & 31);
+      rank0 += zj < c0.z || (zj == c0.z && j < k0);
+      rank1 += zj < c1.z || (zj == c1.z && j < k1);
+    }
+    if (k0 < cnt) {
+      a.zs[begin + st + rank0] = make_float4(c0.z, c0.w, phi0, __int_as_float(st + k0));
+    }
+    if (k1 < cnt) {
+      a.zs[begin + st + rank1] = make_float4(c1.z, c1.w, phi1, __int_as_float(st + k1));
+    }
   }
   __syncthreads();
   if (tid == 0) {

@@ -31,12 +31,13 @@ namespace {
 constexpr int64_t kMaxClusters = ITSU_NOALLOC_MAX_CLUSTERS;
 constexpr size_t kAlign = 256;
 constexpr size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
-// layout: DevStatus | transformed clusters | xyzr | phi
+// layout: DevStatus | transformed clusters | xyzr | phi | per-cluster id, alpha, MC id, bin
 constexpr size_t kStatusOff = 0;
 constexpr size_t kTmpOff = align_up(sizeof(itsu::DevStatus));
 constexpr size_t kXyzrOff = kTmpOff + align_up(sizeof(itsu_cluster) * kMaxClusters);
 constexpr size_t kPhiOff = kXyzrOff + align_up(sizeof(float4) * kMaxClusters);
-constexpr size_t kScratchBytes = kPhiOff + align_up(sizeof(float) * kMaxClusters);
+constexpr size_t kAuxOff = kPhiOff + align_up(sizeof(float) * kMaxClusters);
+constexpr size_t kScratchBytes = kAuxOff + align_up(sizeof(int4) * kMaxClusters);
 
 static __device__ __align__(256) unsigned char itsu_noalloc_scratch[kScratchBytes];
 
@@ -114,6 +115,7 @@ extern "C" itsu_status itsu_pvc_initialize_noalloc(const itsu_cluster *clusters,
   a.tmp = reinterpret_cast<itsu_cluster *>(scratch + kTmpOff);
   a.xyzr = reinterpret_cast<float4 *>(scratch + kXyzrOff);
   a.phi = reinterpret_cast<float *>(scratch + kPhiOff);
+  a.clu_aux = reinterpret_cast<int4 *>(scratch + kAuxOff);
   const itsu::Launch l{stream, 0, 256, 8};
   itsu::launch_status_init(a, l);
   itsu::launch_cluster_sort(a, l);
