@@ -162,7 +162,6 @@ KERNEL_STAGE = {
     "cluster_sort": "cluster_sort",
     "tracklets_count": "tracklets",
     "tracklets_write": "tracklets",
-    "tracklets_tail": "tracklets",
     "cells_count": "cells",
     "cells_scatter": "cells",
     "cells_crowded": "cells",

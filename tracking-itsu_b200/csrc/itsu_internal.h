@@ -90,7 +90,6 @@ struct Arena {
   int32_t *trk_count;
   int32_t *trk_slots;  // slot n of inner cluster i at n * slot_stride + i: the outer clusters of its first tracklets
   int64_t slot_stride;
-  int32_t *trk_owner;  // per tracklet, its inner cluster (flat), filled before the write pass
   int32_t *trk_off;
   int32_t *trk_lookup;
   int32_t *trk_seg;

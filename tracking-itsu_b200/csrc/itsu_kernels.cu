@@ -594,20 +594,22 @@ __device__ __forceinline__ bool tracklets_active(const int32_t *lo, int layer)
   return true;
 }
 
-// Tracklet.cxx:32-40: the tracklet from inner cluster i_flat to outer cluster j_flat.
-__device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t i_flat, int64_t j_flat, int seg)
+// Tracklet.cxx:32-40: the tracklet from inner cluster c to outer cluster d (local indices given);
+// write_tracklet stores the one from flat cluster i_flat to j_flat.
+__device__ __forceinline__ itsu_tracklet make_tracklet(float4 c, float4 d, int32_t c_local, int32_t d_local)
 {
-  const int e = seg / ITSU_LAYERS, layer = seg % ITSU_LAYERS;
-  const float4 c = a.xyzr[i_flat];
-  const float4 d = a.xyzr[j_flat];
   itsu_tracklet t;
-  t.first_cluster = (int32_t)(i_flat - a.layer_off[seg]);
-  t.second_cluster = (int32_t)(j_flat - a.layer_off[seg + 1]);
+  t.first_cluster = c_local;
+  t.second_cluster = d_local;
   t.tan_lambda = (c.z - d.z) / (c.w - d.w);
   t.phi = itsu_atan2f(c.y - d.y, c.x - d.x);
-  a.tracklets[out] = t;
-  (void)e;
-  (void)layer;
+  return t;
+}
+
+__device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t i_flat, int64_t j_flat, int seg)
+{
+  a.tracklets[out] = make_tracklet(a.xyzr[i_flat], a.xyzr[j_flat], (int32_t)(i_flat - a.layer_off[seg]),
+                                   (int32_t)(j_flat - a.layer_off[seg + 1]));
 }
 
 constexpr int kTrackletSlots = kTrackletSlotsPerCluster;
@@ -790,6 +792,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
   a.trk_count[i] = count;
 }
 
+__device__ __forceinline__ float4 shfl4(float4 v, int src)
+{
+  return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                     __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+
 __device__ __forceinline__ int warp_exclusive_sum(int v, int &total)
 {
   const int lane = threadIdx.x & 31;
@@ -820,11 +828,14 @@ __device__ __forceinline__ int owner_of(int excl, int t)
   return owner;
 }
 
-// Per inner cluster, before the write pass: its entry of the tracklets lookup table
-// (Tracker.cxx:102-108) and, for each of its tracklet slots, the owner cluster and segment the
-// write pass reads. Clusters with more than kTrackletSlots tracklets (rare) walk their candidates
-// again here and write their tracklets in order.
-__global__ void __launch_bounds__(kMaxThreads) k_tracklets_tail(Arena a)
+// Write pass, a warp per 32 consecutive inner clusters: their tracklets form one contiguous range
+// (the scan of the counts), which the warp's lanes fill together: each lane takes the next
+// tracklet of the range, finds its inner cluster (owner) and rank there, reads the outer cluster
+// the count pass kept in that slot, and writes the tracklet (Tracklet.cxx:32-40) and its segment
+// id with coalesced stores; all lanes compute their binary64 azimuths together. Each cluster's
+// tracklets lookup entry is written here too. The tracklets of an inner cluster with more than
+// kTrackletSlots of them (not kept by the count pass) are found again by its own lane's walk.
+__global__ void __launch_bounds__(kMaxThreads) k_tracklets_write(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
@@ -832,8 +843,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_tail(Arena a)
   const int64_t i = global_thread();
   const int lane = threadIdx.x & 31;
   const bool valid = i < a.n_clusters;
-  int32_t first = 0, count = 0;
+  int32_t first = 0, count = 0, local = 0, next_begin = 0;
   int seg = 0, sid = 0;
+  float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   if (valid) {
     first = a.trk_off[i];
     count = a.trk_off[i + 1] - first;
@@ -843,10 +855,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_tail(Arena a)
                           ? first - a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer]
                           : ITSU_UNUSED_INDEX;
     sid = e * ITSU_TRACKLET_LAYERS + layer;
+    if (count > 0) {
+      c = a.xyzr[i];
+      local = (int32_t)(i - a.layer_off[seg]);
+      next_begin = a.layer_off[seg + 1];
+    }
   }
-  // Every tracklet gets its owner and segment (the write pass reads them for every tracklet).
-  // The warp's 32 clusters own one contiguous range of tracklets: the warp fills it together,
-  // with coalesced stores.
   int total = 0;
   const int excl = warp_exclusive_sum(count, total);
   const int32_t base = __shfl_sync(0xffffffffu, first, 0);
@@ -854,65 +868,25 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_tail(Arena a)
   for (int p0 = 0; p0 < total; p0 += 32) {
     const int p = p0 + lane;
     const int owner = owner_of(excl, p);
+    const int rank = p - __shfl_sync(0xffffffffu, excl, owner);
     const int owner_sid = __shfl_sync(0xffffffffu, sid, owner);
+    const int owner_count = __shfl_sync(0xffffffffu, count, owner);
+    const int32_t owner_local = __shfl_sync(0xffffffffu, local, owner);
+    const int32_t owner_next = __shfl_sync(0xffffffffu, next_begin, owner);
+    const float4 oc = shfl4(c, owner);
     if (p < total) {
-      a.trk_owner[base + p] = (int32_t)(i0 + owner);
       a.trk_seg_id[base + p] = owner_sid;
+      if (owner_count <= kTrackletSlots) {
+        const int32_t j = a.trk_slots[(int64_t)rank * a.slot_stride + i0 + owner];
+        const float4 d = a.xyzr[owner_next + j];
+        a.tracklets[base + p] = make_tracklet(oc, d, owner_local, j);
+      }
     }
   }
   if (valid && count > kTrackletSlots) {
     const InnerCluster s = inner_cluster(a, i);
     int out = first;
     walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, seg); });
-  }
-}
-
-// Write pass, one thread per tracklet (owner and segment filled in by k_tracklets_tail, outer
-// cluster kept by the count pass): all tracklets of a warp compute their binary64 azimuth
-// together. Tracklets of crowded clusters were written by k_tracklets_tail.
-__global__ void __launch_bounds__(kMaxThreads) k_tracklets_write(Arena a)
-{
-  if (capacity_failed(a.status)) {
-    return;
-  }
-  const int64_t n = a.status->total[kTracklets];
-  const int64_t stride = grid_threads();
-  constexpr int kPer = 2;  // tracklets per thread per round, their gathers in flight together
-  for (int64_t k0 = global_thread(); k0 < n; k0 += kPer * stride) {
-    int64_t owner[kPer];
-    int sid[kPer];
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const int64_t k = k0 + u * stride;
-      owner[u] = -1;
-      if (k < n) {
-        owner[u] = a.trk_owner[k];
-        sid[u] = a.trk_seg_id[k];
-      }
-    }
-    int32_t first[kPer], slot[kPer];
-    bool go[kPer];
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      go[u] = false;
-      if (owner[u] >= 0) {
-        first[u] = a.trk_off[owner[u]];
-        go[u] = a.trk_off[owner[u] + 1] - first[u] <= kTrackletSlots;  // else the tail wrote it
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      if (go[u]) {
-        slot[u] = a.trk_slots[(k0 + u * stride - first[u]) * a.slot_stride + owner[u]];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      if (go[u]) {
-        const int seg = sid[u] + sid[u] / ITSU_TRACKLET_LAYERS;  // (e, L) as a cluster segment: 7e + L
-        write_tracklet(a, (int)(k0 + u * stride), owner[u], a.layer_off[seg + 1] + slot[u], seg);
-      }
-    }
   }
 }
 
@@ -1006,12 +980,6 @@ __device__ __forceinline__ int nth_set_bit(unsigned long long m, int r)
     m &= m - 1ull;
   }
   return __ffsll((long long)m) - 1;
-}
-
-__device__ __forceinline__ float4 shfl4(float4 v, int src)
-{
-  return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
-                     __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
 }
 
 __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const CellLane &s, const itsu_tracklet &t2, int32_t j,
@@ -1560,13 +1528,11 @@ void step_tracklets_count(const Arena &a, const Launch &l)
   }
 }
 
-void step_tracklets_write(const Arena &a, const Launch &l) { k_tracklets_write<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
-
-void step_tracklets_tail(const Arena &a, const Launch &l)
+void step_tracklets_write(const Arena &a, const Launch &l)
 {
   const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
   if (blocks > 0) {
-    k_tracklets_tail<<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
+    k_tracklets_write<<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
   }
 }
 
@@ -1620,32 +1586,31 @@ const KernelStep kSteps[] = {
     {"scan_partials_tracklets", step_scan_partials<0>},  // 4
     {"scan_apply_tracklets", step_scan_apply<0>},        // 5
     {"tracklet_segments", step_tracklet_segments},       // 6
-    {"tracklets_tail", step_tracklets_tail},             // 7
-    {"tracklets_write", step_tracklets_write},           // 8
-    {"cells_count", step_cells_count},                   // 9  (c)
-    {"cells_prefilter", step_cells_prefilter, true},     // 10 (learned form only)
-    {"scan_reduce_cells", step_scan_reduce<1>},          // 11
-    {"scan_partials_cells", step_scan_partials<1>},      // 12
-    {"scan_apply_cells", step_scan_apply<1>},            // 13
-    {"cell_segments", step_cell_segments},               // 14
-    {"cells_scatter", step_cells_scatter},               // 15
-    {"cells_crowded", step_cells_crowded},               // 16
-    {"neighbour_reset", step_neighbour_reset},           // 17 (d)
-    {"neighbours_count", step_neighbours<false>},        // 18
-    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 19
-    {"scan_partials_neighbours", step_scan_partials<2>}, // 20
-    {"scan_apply_neighbours", step_scan_apply<2>},       // 21
-    {"neighbour_check", step_neighbour_check},           // 22
-    {"neighbours_write", step_neighbours<true>},         // 23
-    {"levels_1", step_levels<1>},                        // 24
-    {"levels_2", step_levels<2>},                        // 25
-    {"levels_3", step_levels<3>},                        // 26
-    {"levels_4", step_levels<4>},                        // 27
-    {"scan_reduce_roads", step_scan_reduce<3>},          // 28 (e)
-    {"scan_partials_roads", step_scan_partials<3>},      // 29
-    {"scan_apply_roads", step_scan_apply<3>},            // 30
-    {"road_segments", step_road_segments},               // 31
-    {"roads_write", step_roads},                         // 32
+    {"tracklets_write", step_tracklets_write},           // 7
+    {"cells_count", step_cells_count},                   // 8  (c)
+    {"cells_prefilter", step_cells_prefilter, true},     // 9 (learned form only)
+    {"scan_reduce_cells", step_scan_reduce<1>},          // 10
+    {"scan_partials_cells", step_scan_partials<1>},      // 11
+    {"scan_apply_cells", step_scan_apply<1>},            // 12
+    {"cell_segments", step_cell_segments},               // 13
+    {"cells_scatter", step_cells_scatter},               // 14
+    {"cells_crowded", step_cells_crowded},               // 15
+    {"neighbour_reset", step_neighbour_reset},           // 16 (d)
+    {"neighbours_count", step_neighbours<false>},        // 17
+    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 18
+    {"scan_partials_neighbours", step_scan_partials<2>}, // 19
+    {"scan_apply_neighbours", step_scan_apply<2>},       // 20
+    {"neighbour_check", step_neighbour_check},           // 21
+    {"neighbours_write", step_neighbours<true>},         // 22
+    {"levels_1", step_levels<1>},                        // 23
+    {"levels_2", step_levels<2>},                        // 24
+    {"levels_3", step_levels<3>},                        // 25
+    {"levels_4", step_levels<4>},                        // 26
+    {"scan_reduce_roads", step_scan_reduce<3>},          // 27 (e)
+    {"scan_partials_roads", step_scan_partials<3>},      // 28
+    {"scan_apply_roads", step_scan_apply<3>},            // 29
+    {"road_segments", step_road_segments},               // 30
+    {"roads_write", step_roads},                         // 31
 };
 constexpr int kNumSteps = sizeof(kSteps) / sizeof(kSteps[0]);
 
@@ -1705,13 +1670,13 @@ const KernelStep *pipeline_steps(int *count)
 void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l); }
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
-void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 14, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 16, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(17, 22, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(23, 27, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(28, 31, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(32, 32, a, l); }
+void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 7, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(8, 13, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 15, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
 
 int kernels_per_run()
 {
