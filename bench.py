@@ -162,6 +162,7 @@ KERNEL_STAGE = {
     "cluster_sort": "cluster_sort",
     "tracklets_count": "tracklets",
     "tracklets_write": "tracklets",
+    "tracklets_crowded": "tracklets",
     "cells_count": "cells",
     "cells_scatter": "cells",
     "cells_crowded": "cells",

@@ -64,6 +64,28 @@ def test_pbpb_event_matches_oracle(ctx, seed):
     assert len(want["roads"]) > 1000
 
 
+def test_jet_event_crowded_paths_match_oracle(ctx):
+    """A dense jet-like cone: inner clusters with more tracklets than the count pass keeps (48)
+    and middle clusters with more outgoing tracklets than the cell pass's pair mask holds (64)
+    take the crowded kernels. Stage by stage, whole path and batched beside a Pb-Pb event, the
+    results equal the oracle's."""
+    jet = gen.jet_event(5)
+    want = oracle.run_vertex(jet.layers, jet.vertices[0])
+    per_inner = [np.bincount(t["c1"]) for t in want["tracklets"]]
+    assert sum(int((p > 48).sum()) for p in per_inner) > 0
+    assert sum(int((p > 64).sum()) for p in per_inner[1:]) > 0
+    _assert_same(ctx.run_vertex(jet.layers, jet.vertices[0]), want, "jet stages")
+    roads = ctx.clusters_to_tracks(jet.layers, jet.vertices[0])
+    assert np.array_equal(roads.view(np.uint8), want["roads"].view(np.uint8))
+    bg = gen.pbpb_event(4)
+    want_bg = oracle.run_vertex(bg.layers, bg.vertices[0])
+    clusters, offsets, vertices = gen.pack_batch([bg, jet, bg])
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    for e, exp in enumerate([want_bg, want, want_bg]):
+        _assert_same(ctx.results(e), exp, "jet batch event %d" % e)
+        assert np.array_equal(roads[road_off[e]:road_off[e + 1]].view(np.uint8), exp["roads"].view(np.uint8))
+
+
 def test_pileup_frame_matches_oracle(ctx):
     ev = gen.pileup_frame(7)
     clusters, offsets, vertices = gen.pack_batch([ev] * 5, list(range(5)))

@@ -80,6 +80,7 @@ struct itsu_context {
   float4 *zs = nullptr;
   int32_t *clu_seg = nullptr;
   int4 *clu_aux = nullptr;
+  int32_t *clu_crowded = nullptr;
   int32_t *trk_slots = nullptr;
   // event class
   float2 *seg_rrange = nullptr;
@@ -230,6 +231,7 @@ Arena arena_of(const itsu_context *ctx)
   a.zs = ctx->zs;
   a.clu_seg = ctx->clu_seg;
   a.clu_aux = ctx->clu_aux;
+  a.clu_crowded = ctx->clu_crowded;
   a.seg_rrange = ctx->seg_rrange;
   a.seg_regular = ctx->seg_regular;
   a.prune_tracklets = current_tune(ctx).prune;
@@ -310,6 +312,7 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ITSU_CUDA(ctx, alloc(ctx->zs, cap));
     ITSU_CUDA(ctx, alloc(ctx->clu_seg, cap));
     ITSU_CUDA(ctx, alloc(ctx->clu_aux, cap));
+    ITSU_CUDA(ctx, alloc(ctx->clu_crowded, cap));
     ITSU_CUDA(ctx, alloc(ctx->trk_slots, cap * itsu::kTrackletSlotsPerCluster));
     ctx->cap_clusters = cap;
     ctx->generation++;
@@ -594,7 +597,8 @@ itsu_status stage_count_then_write(itsu_context *ctx, void (*count)(const Arena 
   itsu_status st;
   for (int attempt = 0;; ++attempt) {
     if ((st = clear_flags(ctx)) != ITSU_OK) return st;
-    ITSU_CUDA(ctx, cudaMemsetAsync(&ctx->d_status->cell_entries, 0, sizeof(int64_t), ctx->stream));
+    // the entry reservation and the crowded lists start empty for every count (also a retry)
+    ITSU_CUDA(ctx, cudaMemsetAsync(&ctx->d_status->cell_entries, 0, 3 * sizeof(int64_t), ctx->stream));
     count(arena_of(ctx), launch_of(ctx));
     if ((st = check_launch(ctx)) != ITSU_OK) return st;
     if ((st = sync_status(ctx)) != ITSU_OK) return st;
@@ -819,7 +823,7 @@ void itsu_context_destroy(itsu_context *ctx)
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graph(ctx);
   release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
-  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->clu_aux); release(ctx->trk_slots);
+  release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->clu_aux); release(ctx->clu_crowded); release(ctx->trk_slots);
   release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);

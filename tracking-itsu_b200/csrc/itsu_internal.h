@@ -45,7 +45,12 @@ struct DevStatus {
   int64_t total[4];       // tracklets, cells, neighbours, roads
   int64_t cell_entries;   // cell entries reserved by the cell count pass (may exceed the scratch)
   int64_t crowded;        // tracklets the cell count pass listed in cell_crowded
+  int64_t trk_crowded;    // inner clusters the tracklet count pass listed in clu_crowded
 };
+// The three list counters are reset together before each count pass (one 24-byte memset).
+static_assert(offsetof(DevStatus, crowded) == offsetof(DevStatus, cell_entries) + 8 &&
+                  offsetof(DevStatus, trk_crowded) == offsetof(DevStatus, cell_entries) + 16,
+              "status counters");
 
 // A cell as the count pass finds it: its first and second tracklets (flat), the outgoing-tracklet
 // bit it came from, and what its geometry gave. The write pass scatters each entry whose bit
@@ -79,6 +84,7 @@ struct Arena {
   int32_t *index_tables;
   int32_t *clu_seg;  // per sorted cluster: its segment 7e + L (null: not wanted)
   int4 *clu_aux;     // per sorted cluster: id, alpha bits, MC id, bin (the clustering scatters them here)
+  int32_t *clu_crowded;  // inner clusters with more than kTrackletSlotsPerCluster tracklets (count pass list)
   // candidate-pruning index (null: not built): per bin, the bin's clusters sorted by (z, index),
   // each with its r and phi for the cut;
   // per (event, layer) the r range of its clusters and whether all its bins are regular

@@ -62,6 +62,7 @@ __global__ void k_status_init(DevStatus *s)
   }
   s->cell_entries = 0;
   s->crowded = 0;
+  s->trk_crowded = 0;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -790,6 +791,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
     });
   }
   a.trk_count[i] = count;
+  if (count > kTrackletSlots) {  // rare: the write pass leaves this cluster to k_tracklets_crowded
+    const unsigned long long q = atomicAdd(reinterpret_cast<unsigned long long *>(&a.status->trk_crowded), 1ull);
+    if ((int64_t)q < a.n_clusters) {
+      a.clu_crowded[q] = (int32_t)i;
+    }
+  }
 }
 
 __device__ __forceinline__ float4 shfl4(float4 v, int src)
@@ -834,8 +841,9 @@ __device__ __forceinline__ int owner_of(int excl, int t)
 // the count pass kept in that slot, and writes the tracklet (Tracklet.cxx:32-40) and its segment
 // id with coalesced stores; all lanes compute their binary64 azimuths together. Each cluster's
 // tracklets lookup entry is written here too. The tracklets of an inner cluster with more than
-// kTrackletSlots of them (not kept by the count pass) are found again by its own lane's walk.
-__global__ void __launch_bounds__(kMaxThreads) k_tracklets_write(Arena a)
+// kTrackletSlots of them (not kept by the count pass) get their segment ids here and the rest
+// from k_tracklets_crowded.
+__global__ void __launch_bounds__(kMaxThreads, 2) k_tracklets_write(Arena a)  // 64 registers: 4 blocks of 256 per SM
 {
   if (capacity_failed(a.status)) {
     return;
@@ -883,10 +891,21 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_write(Arena a)
       }
     }
   }
-  if (valid && count > kTrackletSlots) {
+}
+
+// Write pass, part 2: the inner clusters with more than kTrackletSlots tracklets (listed by the
+// count pass, a handful per batch) walk their candidates again and write their tracklets in order.
+__global__ void __launch_bounds__(kMaxThreads) k_tracklets_crowded(Arena a)
+{
+  if (capacity_failed(a.status)) {
+    return;
+  }
+  const int64_t listed = min(a.status->trk_crowded, (int64_t)a.n_clusters);
+  for (int64_t q = global_thread(); q < listed; q += grid_threads()) {
+    const int64_t i = a.clu_crowded[q];
     const InnerCluster s = inner_cluster(a, i);
-    int out = first;
-    walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, seg); });
+    int out = a.trk_off[i];
+    walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, s.seg); });
   }
 }
 
@@ -1101,7 +1120,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
       a.cell_mask[s.k] = big ? 0ull : masks[warp][lane];
       a.cell_lookup[s.k] = ITSU_UNUSED_INDEX;  // the write pass fills it for tracklets with cells
       if (big && count > 0) {
-        a.cell_crowded[atomicAdd(reinterpret_cast<unsigned long long *>(&a.status->crowded), 1ull)] = (int32_t)s.k;
+        const unsigned long long q = atomicAdd(reinterpret_cast<unsigned long long *>(&a.status->crowded), 1ull);
+        if ((int64_t)q < n) {
+          a.cell_crowded[q] = (int32_t)s.k;
+        }
       }
     }
     __syncwarp();
@@ -1237,7 +1259,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_crowded(Arena a)
     return;
   }
   const int64_t n = a.status->total[kTracklets];
-  const int64_t listed = a.status->crowded;
+  const int64_t listed = min(a.status->crowded, n);
   for (int64_t q = global_thread(); q < listed; q += grid_threads()) {
     const int32_t k = a.cell_crowded[q];
     const CellLane s = cell_lane(a, k, n);
@@ -1536,6 +1558,8 @@ void step_tracklets_write(const Arena &a, const Launch &l)
   }
 }
 
+void step_tracklets_crowded(const Arena &a, const Launch &l) { k_tracklets_crowded<<<l.num_sms, 128, 0, l.stream>>>(a); }
+
 void step_tracklet_segments(const Arena &a, const Launch &l)
 {
   k_tracklet_segments<<<(a.n_events * ITSU_TRACKLET_LAYERS + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
@@ -1587,30 +1611,31 @@ const KernelStep kSteps[] = {
     {"scan_apply_tracklets", step_scan_apply<0>},        // 5
     {"tracklet_segments", step_tracklet_segments},       // 6
     {"tracklets_write", step_tracklets_write},           // 7
-    {"cells_count", step_cells_count},                   // 8  (c)
-    {"cells_prefilter", step_cells_prefilter, true},     // 9 (learned form only)
-    {"scan_reduce_cells", step_scan_reduce<1>},          // 10
-    {"scan_partials_cells", step_scan_partials<1>},      // 11
-    {"scan_apply_cells", step_scan_apply<1>},            // 12
-    {"cell_segments", step_cell_segments},               // 13
-    {"cells_scatter", step_cells_scatter},               // 14
-    {"cells_crowded", step_cells_crowded},               // 15
-    {"neighbour_reset", step_neighbour_reset},           // 16 (d)
-    {"neighbours_count", step_neighbours<false>},        // 17
-    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 18
-    {"scan_partials_neighbours", step_scan_partials<2>}, // 19
-    {"scan_apply_neighbours", step_scan_apply<2>},       // 20
-    {"neighbour_check", step_neighbour_check},           // 21
-    {"neighbours_write", step_neighbours<true>},         // 22
-    {"levels_1", step_levels<1>},                        // 23
-    {"levels_2", step_levels<2>},                        // 24
-    {"levels_3", step_levels<3>},                        // 25
-    {"levels_4", step_levels<4>},                        // 26
-    {"scan_reduce_roads", step_scan_reduce<3>},          // 27 (e)
-    {"scan_partials_roads", step_scan_partials<3>},      // 28
-    {"scan_apply_roads", step_scan_apply<3>},            // 29
-    {"road_segments", step_road_segments},               // 30
-    {"roads_write", step_roads},                         // 31
+    {"tracklets_crowded", step_tracklets_crowded},       // 8
+    {"cells_count", step_cells_count},                   // 9  (c)
+    {"cells_prefilter", step_cells_prefilter, true},     // 10 (learned form only)
+    {"scan_reduce_cells", step_scan_reduce<1>},          // 11
+    {"scan_partials_cells", step_scan_partials<1>},      // 12
+    {"scan_apply_cells", step_scan_apply<1>},            // 13
+    {"cell_segments", step_cell_segments},               // 14
+    {"cells_scatter", step_cells_scatter},               // 15
+    {"cells_crowded", step_cells_crowded},               // 16
+    {"neighbour_reset", step_neighbour_reset},           // 17 (d)
+    {"neighbours_count", step_neighbours<false>},        // 18
+    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 19
+    {"scan_partials_neighbours", step_scan_partials<2>}, // 20
+    {"scan_apply_neighbours", step_scan_apply<2>},       // 21
+    {"neighbour_check", step_neighbour_check},           // 22
+    {"neighbours_write", step_neighbours<true>},         // 23
+    {"levels_1", step_levels<1>},                        // 24
+    {"levels_2", step_levels<2>},                        // 25
+    {"levels_3", step_levels<3>},                        // 26
+    {"levels_4", step_levels<4>},                        // 27
+    {"scan_reduce_roads", step_scan_reduce<3>},          // 28 (e)
+    {"scan_partials_roads", step_scan_partials<3>},      // 29
+    {"scan_apply_roads", step_scan_apply<3>},            // 30
+    {"road_segments", step_road_segments},               // 31
+    {"roads_write", step_roads},                         // 32
 };
 constexpr int kNumSteps = sizeof(kSteps) / sizeof(kSteps[0]);
 
@@ -1670,13 +1695,13 @@ const KernelStep *pipeline_steps(int *count)
 void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l); }
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
-void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 7, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(8, 13, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 15, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
+void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 14, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 16, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(17, 22, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(23, 27, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(28, 31, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(32, 32, a, l); }
 
 int kernels_per_run()
 {

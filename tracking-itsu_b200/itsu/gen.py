@@ -65,12 +65,12 @@ LABEL_DTYPE = np.dtype(
 )
 
 
-def _collision(rng, n_tracks, pt_mean, vertex, mc_offset):
+def _collision(rng, n_tracks, pt_mean, vertex, mc_offset, eta_range=(-1.0, 1.0), phi_range=(0.0, 2.0 * math.pi)):
     """Hits of one collision: returns per-layer (x, y, z, mc) lists and the label table."""
     vx, vy, vz = (float(v) for v in vertex)
     pt = 0.1 + rng.exponential(pt_mean, n_tracks)
-    eta = rng.uniform(-1.0, 1.0, n_tracks)
-    phi0 = rng.uniform(0.0, 2.0 * math.pi, n_tracks)
+    eta = rng.uniform(eta_range[0], eta_range[1], n_tracks)
+    phi0 = rng.uniform(phi_range[0], phi_range[1], n_tracks)
     q = np.where(rng.random(n_tracks) < 0.5, -1.0, 1.0)
     radius = pt / (0.3 * FIELD_T) * 100.0  # cm
     # circle centre: left of the direction for q = +1 (counter-clockwise), right for q = -1
@@ -123,8 +123,11 @@ def make_event(
     pt_mean: float = 0.6,
     noise: float = 0.05,
     n_vertices: int = 1,
+    eta_range=(-1.0, 1.0),
+    phi_range=(0.0, 2.0 * math.pi),
 ) -> Event:
-    """One event with ``n_vertices`` overlapping collisions of ``n_tracks`` tracks each."""
+    """One event with ``n_vertices`` overlapping collisions of ``n_tracks`` tracks each, their
+    directions uniform in ``eta_range`` x ``phi_range``."""
     rng = np.random.default_rng(seed)
     vertices = np.zeros((n_vertices, 3), np.float32)
     per_layer = [[] for _ in range(LAYERS)]
@@ -132,7 +135,7 @@ def make_event(
     for iv in range(n_vertices):
         v = (rng.normal(0.0, 0.005), rng.normal(0.0, 0.005), rng.normal(0.0, 5.0))
         vertices[iv] = v
-        hits, lab = _collision(rng, n_tracks, pt_mean, v, PILEUP_MC_OFFSET * iv)
+        hits, lab = _collision(rng, n_tracks, pt_mean, v, PILEUP_MC_OFFSET * iv, eta_range, phi_range)
         labels.append(lab)
         for layer in range(LAYERS):
             per_layer[layer].append(hits[layer])
@@ -179,6 +182,13 @@ def batch_events(seed: int, n_events: int = 256, lo: int = 20, hi: int = 8000) -
     rng = np.random.default_rng(seed)
     mults = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n_events))).astype(int)
     return [make_event(seed * 100003 + i, int(m), pt_mean=0.6, noise=0.05) for i, m in enumerate(mults)]
+
+
+def jet_event(seed: int, n_tracks: int = 100) -> Event:
+    """A dense jet-like cone: ``n_tracks`` stiff tracks within 0.06 rad of azimuth and 0.06 of
+    pseudorapidity, no noise. Inner clusters there have more tracklets than the count pass keeps
+    per cluster, and tracklets more outgoing tracklets than the cell pass's pair mask holds."""
+    return make_event(seed, n_tracks, pt_mean=3.0, noise=0.0, eta_range=(0.0, 0.06), phi_range=(1.0, 1.06))
 
 
 def pileup_frame(seed: int, collisions: int = 5, n_tracks: int = 1500) -> Event:
