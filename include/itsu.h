@@ -195,8 +195,9 @@ itsu_status itsu_clusters_to_tracks(itsu_context *ctx, const itsu_cluster *const
 itsu_status itsu_batch_run(itsu_context *ctx, const itsu_batch *batch);
 /* Host in / host out: copies the batch to the device, runs it, and copies back the roads
  * (event-major) and road_offsets[n_events+1]. roads may be NULL to query the total. With
- * ITSU_FLAG_STREAM_HOST the copies of later events overlap the work on earlier ones (pinned
- * host buffers make the copies asynchronous). */
+ * ITSU_FLAG_STREAM_HOST the batch runs as chunks of events whose copies overlap the work on
+ * earlier chunks, two chunks in flight on two arenas (the context allocates its second arena
+ * and stream on first use; pinned host buffers make the copies asynchronous). */
 itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
                                 const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
                                 int32_t *road_offsets);

@@ -149,6 +149,10 @@ struct itsu_context {
   DevStatus *chunk_status = nullptr;  // 16 snapshots
   DevStatus *h_chunk_status = nullptr;
 
+  // streamed host runs: a second arena with its own stream, created on first use, so that two
+  // chunks are in flight (one's small tail kernels overlapping the next one's work)
+  itsu_context *twin = nullptr;
+
   // learned prefilter: FP32 master model and the device model the kernels read
   itsu_prefilter_model *d_master = nullptr;
   itsu::MlpDevice *d_mlp = nullptr;
@@ -484,10 +488,8 @@ itsu_status count_overflow(itsu_context *ctx)
 }
 
 // Enqueues every stage of the current inputs (no host synchronisation).
-void enqueue_all(itsu_context *ctx)
+void enqueue_run(const Arena &a, const Launch &l)
 {
-  const Arena a = arena_of(ctx);
-  const Launch l = launch_of(ctx);
   itsu::launch_status_init(a, l);
   itsu::launch_cluster_sort(a, l);
   itsu::launch_tracklets_count(a, l);
@@ -499,6 +501,8 @@ void enqueue_all(itsu_context *ctx)
   itsu::launch_roads_count(a, l);
   itsu::launch_roads_write(a, l);
 }
+
+void enqueue_all(itsu_context *ctx) { enqueue_run(arena_of(ctx), launch_of(ctx)); }
 
 void drop_graph(itsu_context *ctx)
 {
@@ -821,6 +825,7 @@ void itsu_context_destroy(itsu_context *ctx)
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->twin) itsu_context_destroy(ctx->twin);
   drop_graph(ctx);
   release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
   release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->clu_aux); release(ctx->clu_crowded); release(ctx->trk_slots);
@@ -1145,12 +1150,34 @@ itsu_status grow_buffer(itsu_context *ctx, T *&p, int64_t &cap, int64_t need)
   return ITSU_OK;
 }
 
+// The streamed path's second arena: a context on the same device with its own stream, the
+// parent's flags (less ITSU_FLAG_STREAM_HOST) and initial capacities. Created on first use.
+itsu_status ensure_twin(itsu_context *ctx)
+{
+  if (ctx->twin) return ITSU_OK;
+  itsu_config c;
+  itsu_config_default(&c);
+  c.device = ctx->device;
+  c.flags = ctx->flags & ~ITSU_FLAG_STREAM_HOST;
+  c.max_tracklets = ctx->init_tracklets;
+  c.max_cells = ctx->init_cells;
+  c.max_neighbours = ctx->init_neighbours;
+  c.max_roads = ctx->init_roads;
+  itsu_context *t = nullptr;
+  const itsu_status st = itsu_context_create(&c, &t);
+  if (st != ITSU_OK) return fail(ctx, st, "streamed run: second arena: %s", g_thread_error.c_str());
+  ctx->twin = t;
+  return ITSU_OK;
+}
+
 // itsu_batch_run_host with ITSU_FLAG_STREAM_HOST: consecutive chunks of events, each one's
-// upload (copy stream) overlapping the work on the one before (context stream), and each one's
-// roads downloaded (download stream) while the next one works. The first chunk is smaller, so
-// that the device starts sooner. Sets *done to false, with nothing reported, when the batch is
-// too small to split or a chunk outgrew the arena: the caller then runs the batch in one pass
-// (which grows the arena).
+// upload (copy stream) overlapping the work on the ones before, and each one's roads downloaded
+// (download stream) while later ones work. Chunks alternate between the context's arena and
+// stream and a second arena with its own stream, so two chunks are in flight and one's small
+// tail kernels overlap the next one's work; their roads are appended to the batch-wide output in
+// chunk order. The first chunk is smaller, so that the device starts sooner. Sets *done to false,
+// with nothing reported, when the batch is too small to split or a chunk outgrew its arena: the
+// caller then runs the batch in one pass (which grows the arena).
 itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets, const float *vertices,
                               int32_t n_events, int64_t n_clusters, itsu_road *roads, int64_t roads_capacity,
                               int32_t *road_offsets, bool *done)
@@ -1172,12 +1199,25 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
     if (ev[c] <= ev[c - 1]) return ITSU_OK;  // degenerate split: one pass instead
   }
   int64_t max_chunk = 0;
+  int32_t max_chunk_events = 0;
   for (int c = 0; c < k_chunks; ++c) {
     max_chunk = std::max<int64_t>(max_chunk, layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS] - layer_offsets[(int64_t)ev[c] * ITSU_LAYERS]);
+    max_chunk_events = std::max(max_chunk_events, ev[c + 1] - ev[c]);
   }
   itsu_status st;
   if ((st = ensure_clusters(ctx, n_clusters, n_events)) != ITSU_OK) return st;
   if ((st = ensure_outputs_for(ctx, max_chunk)) != ITSU_OK) return st;
+  // the second arena (not for a fixed-size arena: that one stays as the caller configured it)
+  itsu_context *twin = nullptr;
+  if (!(ctx->flags & ITSU_FLAG_NO_GROW)) {
+    if ((st = ensure_twin(ctx)) != ITSU_OK) return st;
+    twin = ctx->twin;
+    if ((st = ensure_clusters(twin, max_chunk, max_chunk_events)) != ITSU_OK) return fail(ctx, st, "%s", twin->error.c_str());
+    if ((st = ensure_outputs_for(twin, max_chunk)) != ITSU_OK) return fail(ctx, st, "%s", twin->error.c_str());
+    for (int b = 0; b < kBands; ++b) twin->tunes[b] = ctx->tunes[b];
+    twin->override_tune = ctx->override_tune;
+    twin->tuning = ctx->tuning;
+  }
   if ((st = grow_buffer(ctx, ctx->chunk_off, ctx->cap_chunk_off, (int64_t)n_events * ITSU_LAYERS + k_chunks)) != ITSU_OK) return st;
   if ((st = grow_buffer(ctx, ctx->roads_all, ctx->cap_roads_all, std::max<int64_t>(ctx->cap_roads, n_clusters / 2 + 4096))) != ITSU_OK) {
     return st;
@@ -1211,12 +1251,14 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
   }
   // All uploads go on the copy stream, the small ones first: host-to-device copies share the copy
   // engine in submission order, so a small copy queued behind the clusters would hold up the
-  // first chunk's work. The copy and download streams first wait for any earlier work of the
-  // context.
+  // first chunk's work. The copy, download and second-arena streams first wait for any earlier
+  // work of the context and for the zeroed road offsets.
+  ITSU_CUDA(ctx, cudaMemsetAsync(ctx->road_off_all, 0, sizeof(int32_t) * ((int64_t)n_events + 1), ctx->stream));
   cudaEvent_t start = ctx->chunk_ready[kMaxChunks - 1];
   ITSU_CUDA(ctx, cudaEventRecord(start, ctx->stream));
   ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, start, 0));
   ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->d2h_stream, start, 0));
+  if (twin) ITSU_CUDA(ctx, cudaStreamWaitEvent(twin->stream, start, 0));
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->chunk_off, ctx->h_chunk_off, sizeof(int32_t) * n_off, cudaMemcpyHostToDevice, ctx->copy_stream));
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, vertices, sizeof(float) * 3 * (int64_t)n_events, cudaMemcpyHostToDevice, ctx->copy_stream));
   for (int c = 0; c < k_chunks; ++c) {
@@ -1227,77 +1269,118 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
     }
     ITSU_CUDA(ctx, cudaEventRecord(ctx->chunk_ready[c], ctx->copy_stream));
   }
-  ITSU_CUDA(ctx, cudaMemsetAsync(ctx->road_off_all, 0, sizeof(int32_t) * ((int64_t)n_events + 1), ctx->stream));
 
-  // The roads of a finished chunk go to the host on the download stream while later chunks work;
-  // the chunk's status is checked first, and decides whether the batch goes on streaming.
+  // The work, all chunks enqueued at once: per chunk (on its arena's stream, after its upload),
+  // the whole sequence, then (after the previous chunk's append, which wrote this chunk's first
+  // road index) its roads appended to the batch-wide output and its road end and status sent
+  // back. The two arenas alternate; a stream runs its chunks in order, so an arena is reused only
+  // after its previous chunk's append.
+  for (int c = 0; c < k_chunks; ++c) {
+    itsu_context *x = (twin && (c & 1)) ? twin : ctx;
+    const int64_t a = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS], b = layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS];
+    ITSU_CUDA(ctx, cudaStreamWaitEvent(x->stream, ctx->chunk_ready[c], 0));
+    x->n_events = ev[c + 1] - ev[c];
+    x->n_clusters = b - a;
+    x->in_raw = ctx->raw + a;
+    x->in_raw_off = nullptr;
+    x->in_layer_off = ctx->chunk_off + (int64_t)ev[c] * ITSU_LAYERS + c;
+    x->in_vtx = ctx->vtx + 3 * (int64_t)ev[c];
+    Arena arena = arena_of(x);
+    arena.mlp = ctx->prefilter ? ctx->d_mlp : nullptr;  // the context's model serves both arenas
+    const Launch l = launch_of(x);
+    enqueue_run(arena, l);
+    if (c > 0 && twin) ITSU_CUDA(ctx, cudaStreamWaitEvent(x->stream, ctx->chunk_done[c - 1], 0));
+    itsu::launch_append_roads(arena, l, ctx->roads_all, ctx->road_off_all, ev[c], ctx->cap_roads_all, ctx->chunk_status + c);
+    ITSU_CUDA(ctx, cudaGetLastError());
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_chunk_status + c, ctx->chunk_status + c, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                   x->stream));
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_road_end + c, ctx->road_off_all + ev[c + 1], sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   x->stream));
+    ITSU_CUDA(ctx, cudaEventRecord(ctx->chunk_done[c], x->stream));
+  }
+
+  // Each finished chunk's status is checked, in chunk order, and its roads go to the host on the
+  // download stream while later chunks work. A chunk that outgrew its arena ends the streaming
+  // (the chunks after it ran, but their roads are not downloaded) and the batch runs in one pass.
   int64_t downloaded = 0;
   bool fallback = false;
-  auto collect = [&](int c) -> itsu_status {
-    ITSU_CUDA(ctx, cudaEventSynchronize(ctx->chunk_done[c]));
+  int fail_chunk = -1;
+  st = ITSU_OK;
+  for (int c = 0; c < k_chunks && st == ITSU_OK && !fallback; ++c) {
+    const cudaError_t err = cudaEventSynchronize(ctx->chunk_done[c]);
+    if (err != cudaSuccess) {
+      st = fail(ctx, ITSU_ERR_CUDA, "streamed run: chunk %d: %s", c, cudaGetErrorString(err));
+      break;
+    }
     const DevStatus &s = ctx->h_chunk_status[c];
     if (s.flags & itsu::kFlagInvalid) {
       if (s.invalid_event != INT32_MAX) {
-        return fail(ctx, ITSU_ERR_INVALID, "primary vertex of event %d is not finite or beyond 1e6 cm", ev[c] + s.invalid_event);
-      }
-      return fail(ctx, ITSU_ERR_INVALID, "cluster %lld is malformed: a coordinate is not finite or beyond 1e6 cm, or it sits on the beam line at the vertex z (r == 0 and z == vertex z)",
+        st = fail(ctx, ITSU_ERR_INVALID, "primary vertex of event %d is not finite or beyond 1e6 cm", ev[c] + s.invalid_event);
+      } else {
+        st = fail(ctx, ITSU_ERR_INVALID, "cluster %lld is malformed: a coordinate is not finite or beyond 1e6 cm, or it sits on the beam line at the vertex z (r == 0 and z == vertex z)",
                   (long long)layer_offsets[(int64_t)ev[c] * ITSU_LAYERS] + s.invalid_index);
+      }
+      break;
     }
     if (s.flags & itsu::kCapacityMask) {
       fallback = true;  // one pass instead, which grows the arena
-      return ITSU_OK;
+      fail_chunk = c;
+      break;
     }
     const int64_t end = ctx->h_road_end[c];
     if (roads && end > roads_capacity) {
-      return fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %lld given", (long long)end, (long long)roads_capacity);
+      st = fail(ctx, ITSU_ERR_CAPACITY, "%lld roads do not fit the %lld given", (long long)end, (long long)roads_capacity);
+      break;
     }
     if (roads && end > downloaded) {
-      ITSU_CUDA(ctx, cudaMemcpyAsync(roads + downloaded, ctx->roads_all + downloaded, sizeof(itsu_road) * (end - downloaded),
-                                     cudaMemcpyDeviceToHost, ctx->d2h_stream));
+      const cudaError_t e1 = cudaStreamWaitEvent(ctx->d2h_stream, ctx->chunk_done[c], 0);
+      const cudaError_t e2 = e1 != cudaSuccess ? e1
+                                               : cudaMemcpyAsync(roads + downloaded, ctx->roads_all + downloaded,
+                                                                 sizeof(itsu_road) * (end - downloaded), cudaMemcpyDeviceToHost,
+                                                                 ctx->d2h_stream);
+      if (e2 != cudaSuccess) {
+        st = fail(ctx, ITSU_ERR_CUDA, "streamed run: road download: %s", cudaGetErrorString(e2));
+        break;
+      }
     }
     downloaded = end;
-    return ITSU_OK;
-  };
-
-  // the work: per chunk (after its upload, which follows the offsets and vertices), the whole
-  // sequence, its roads appended to the batch-wide output, its road end and status sent back
-  for (int c = 0; c < k_chunks && !fallback; ++c) {
-    const int64_t a = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS], b = layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS];
-    ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_ready[c], 0));
-    ctx->n_events = ev[c + 1] - ev[c];
-    ctx->n_clusters = b - a;
-    ctx->in_raw = ctx->raw + a;
-    ctx->in_raw_off = nullptr;
-    ctx->in_layer_off = ctx->chunk_off + (int64_t)ev[c] * ITSU_LAYERS + c;
-    ctx->in_vtx = ctx->vtx + 3 * (int64_t)ev[c];
-    enqueue_all(ctx);
-    itsu::launch_append_roads(arena_of(ctx), launch_of(ctx), ctx->roads_all, ctx->road_off_all, ev[c], ctx->cap_roads_all,
-                              ctx->chunk_status + c);
-    ITSU_CUDA(ctx, cudaGetLastError());
-    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_chunk_status + c, ctx->chunk_status + c, sizeof(DevStatus), cudaMemcpyDeviceToHost,
-                                   ctx->stream));
-    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_road_end + c, ctx->road_off_all + ev[c + 1], sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                   ctx->stream));
-    ITSU_CUDA(ctx, cudaEventRecord(ctx->chunk_done[c], ctx->stream));
-    ITSU_CUDA(ctx, cudaStreamWaitEvent(ctx->d2h_stream, ctx->chunk_done[c], 0));
-    if (c > 0 && (st = collect(c - 1)) != ITSU_OK) break;  // chunk c is queued: the device stays busy
   }
-  if (st == ITSU_OK && !fallback) st = collect(k_chunks - 1);
-  ctx->stage = kNone;  // the arena holds only the last chunk's intermediate results
-  ctx->n_events = 0;
-  ctx->n_clusters = 0;
+  for (itsu_context *x : {ctx, twin}) {
+    if (!x) continue;
+    x->stage = kNone;  // the arenas hold only their last chunk's intermediate results
+    x->n_events = 0;
+    x->n_clusters = 0;
+  }
   if (st == ITSU_OK && !fallback && road_offsets) {
-    ITSU_CUDA(ctx, cudaMemcpyAsync(road_offsets, ctx->road_off_all, sizeof(int32_t) * ((int64_t)n_events + 1), cudaMemcpyDeviceToHost,
-                                   ctx->d2h_stream));
+    const cudaError_t e1 = cudaStreamWaitEvent(ctx->d2h_stream, ctx->chunk_done[k_chunks - 1], 0);
+    const cudaError_t e2 = e1 != cudaSuccess ? e1
+                                             : cudaMemcpyAsync(road_offsets, ctx->road_off_all, sizeof(int32_t) * ((int64_t)n_events + 1),
+                                                               cudaMemcpyDeviceToHost, ctx->d2h_stream);
+    if (e2 != cudaSuccess) st = fail(ctx, ITSU_ERR_CUDA, "streamed run: offsets download: %s", cudaGetErrorString(e2));
   }
   // whatever happened, nothing of this call is left in flight
   const cudaError_t e1 = cudaStreamSynchronize(ctx->stream);
   const cudaError_t e2 = cudaStreamSynchronize(ctx->d2h_stream);
   const cudaError_t e3 = cudaStreamSynchronize(ctx->copy_stream);
+  const cudaError_t e4 = twin ? cudaStreamSynchronize(twin->stream) : cudaSuccess;
   if (st != ITSU_OK) return st;
   ITSU_CUDA(ctx, e1);
   ITSU_CUDA(ctx, e2);
   ITSU_CUDA(ctx, e3);
+  ITSU_CUDA(ctx, e4);
+  if (fail_chunk >= 0 && !(ctx->flags & ITSU_FLAG_NO_GROW)) {
+    // the arena that overflowed grows to the counted totals of the stage that overflowed, so that
+    // later calls stream again (one stage per call when several are short)
+    itsu_context *x = (twin && (fail_chunk & 1)) ? twin : ctx;
+    const DevStatus &s = ctx->h_chunk_status[fail_chunk];
+    itsu_status g = ITSU_OK;
+    if (g == ITSU_OK && (s.flags & itsu::kFlagCapTracklets)) g = ensure_tracklets(x, s.total[itsu::kTracklets]);
+    if (g == ITSU_OK && (s.flags & itsu::kFlagCapScratch)) g = ensure_cell_entries(x, s.cell_entries + cell_entry_slack(x));
+    if (g == ITSU_OK && (s.flags & itsu::kFlagCapCells)) g = ensure_cells(x, s.total[itsu::kCells]);
+    if (g == ITSU_OK && (s.flags & itsu::kFlagCapNeighbours)) g = ensure_neighbours(x, s.total[itsu::kNeighbours]);
+    if (g == ITSU_OK && (s.flags & itsu::kFlagCapRoads)) g = ensure_roads(x, s.total[itsu::kRoads]);
+    if (g != ITSU_OK) return x == ctx ? g : fail(ctx, g, "%s", x->error.c_str());
+  }
   *done = !fallback;
   return ITSU_OK;
 }
