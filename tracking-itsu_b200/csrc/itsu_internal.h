@@ -52,18 +52,23 @@ static_assert(offsetof(DevStatus, crowded) == offsetof(DevStatus, cell_entries) 
                   offsetof(DevStatus, trk_crowded) == offsetof(DevStatus, cell_entries) + 16,
               "status counters");
 
-// A cell as the count pass finds it: its first and second tracklets (flat), the outgoing-tracklet
-// bit it came from, and what its geometry gave. The write pass scatters each entry whose bit
-// survived to cell_off[t1] + (its rank among the tracklet's set bits); t1 < 0 marks an unused
-// slot. The learned prefilter scores entries in place (the DCA is one of its features).
+// A cell as the count pass finds it: its first tracklet (flat) and the outgoing-tracklet bit it
+// came from, and everything the cell record needs: its segment (5 e + L), its three clusters
+// (local to layers L, L+1, L+2), its two tracklets (local to tracklet layers L and L+1), and what
+// its geometry gave. The write pass scatters each entry whose bit survived to cell_off[t1] + (the
+// rank of its bit among the tracklet's set bits) with no other gather; t1 < 0 marks an unused
+// slot. The learned prefilter scores entries in place (the DCA, one of its features, goes to a
+// separate array in that form only).
 struct __align__(16) CellEntry {
   int32_t t1;
   int32_t bit;
-  int32_t t2;
-  float dca;
+  int32_t seg;
+  int32_t c1;
+  int32_t c2, c3;
+  int32_t t1_local, t2_local;
   float nx, ny, nz, curvature;
 };
-static_assert(sizeof(CellEntry) == 32, "cell entry layout");
+static_assert(sizeof(CellEntry) == 48, "cell entry layout");
 
 enum TotalIndex { kTracklets = 0, kCells = 1, kNeighbours = 2, kRoads = 3 };
 
@@ -111,6 +116,7 @@ struct Arena {
   itsu_cell *cells;
   int32_t *cell_seg_id;
   CellEntry *cell_entries;  // scratch of the cell count pass
+  float *cell_dca;  // per entry, its DCA (written in the learned form only: a prefilter feature)
   int64_t cap_cell_entries;
   // neighbours, levels, roads
   int32_t *nb_count;

@@ -1066,11 +1066,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
       const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
       bool pass = false;
       int b = 0;
+      int32_t c3 = 0;
       float3 normal = make_float3(0.0f, 0.0f, 0.0f);
       float curvature = 0.0f, dca = 0.0f;
       if (p < total) {
         b = nth_set_bit(wmask, r);
-        const int32_t c3 = a.tracklets[j0 + b].second_cluster;
+        c3 = a.tracklets[j0 + b].second_cluster;
         pass = cell_geometry(layer, c1, c2, a.xyzr[c3_base + c3], vx, vy, normal, curvature, dca);
         if (pass) {
           atomicOr(&masks[warp][owner], 1ull << b);
@@ -1098,9 +1099,19 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
         chunk_pos += need;
       }
       if (pass && slot < a.cap_cell_entries) {
+        // the rest of the cell record, read again (cached since cell_lane) rather than kept in
+        // registers through the pair loops
+        const int64_t t1 = base + owner;
+        const int2 t1_clusters = *reinterpret_cast<const int2 *>(a.tracklets + t1);
+        const int e = a.trk_seg_id[t1] / ITSU_TRACKLET_LAYERS;
+        const int32_t *ts = a.trk_seg + e * ITSU_TRACKLET_LAYERS;
         int4 *dst = reinterpret_cast<int4 *>(a.cell_entries + slot);
-        dst[0] = make_int4((int)(base + owner), b, j0 + b, __float_as_int(dca));
-        dst[1] = make_int4(__float_as_int(normal.x), __float_as_int(normal.y), __float_as_int(normal.z), __float_as_int(curvature));
+        dst[0] = make_int4((int)t1, b, e * ITSU_CELL_LAYERS + layer, t1_clusters.x);
+        dst[1] = make_int4(t1_clusters.y, c3, (int)(t1 - ts[layer]), j0 + b - ts[layer + 1]);
+        dst[2] = make_int4(__float_as_int(normal.x), __float_as_int(normal.y), __float_as_int(normal.z), __float_as_int(curvature));
+        if (a.mlp) {
+          a.cell_dca[slot] = dca;
+        }
       }
     }
     __syncwarp();
@@ -1163,17 +1174,16 @@ __global__ void __launch_bounds__(kPrefilterThreads) k_cells_prefilter(Arena a)
     }
     float f[kMlpIn];
     if (h.x >= 0) {
-      const int t1k = h.x;
-      const int sid = a.trk_seg_id[t1k];
-      const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
+      const int4 g = reinterpret_cast<const int4 *>(a.cell_entries + i)[1];  // c2, c3, t1 local, t2 local
+      const int e = h.z / ITSU_CELL_LAYERS, layer = h.z % ITSU_CELL_LAYERS;
       const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
-      const itsu_tracklet t1 = a.tracklets[t1k];
-      const itsu_tracklet t2 = a.tracklets[h.z];
-      const float4 c1 = a.xyzr[lo[layer] + t1.first_cluster];
-      const float4 c2 = a.xyzr[lo[layer + 1] + t1.second_cluster];
-      const float4 c3 = a.xyzr[lo[layer + 2] + t2.second_cluster];
+      const itsu_tracklet t1 = a.tracklets[h.x];
+      const itsu_tracklet t2 = a.tracklets[a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer + 1] + g.w];
+      const float4 c1 = a.xyzr[lo[layer] + h.w];
+      const float4 c2 = a.xyzr[lo[layer + 1] + g.x];
+      const float4 c3 = a.xyzr[lo[layer + 2] + g.y];
       pair_features(layer, t1.tan_lambda, t1.phi, t2.tan_lambda, t2.phi, c1, c2, c3, a.vtx[3 * e], a.vtx[3 * e + 1],
-                    a.vtx[3 * e + 2], __int_as_float(h.w), f);
+                    a.vtx[3 * e + 2], a.cell_dca[i], f);
     } else {
       for (int k = 0; k < kMlpIn; ++k) {
         f[k] = mlp.mean[k];
@@ -1202,29 +1212,25 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_scatter(Arena a)
   const int64_t stride = grid_threads();
   constexpr int kPer = 4;  // entries per thread per round, their loads in flight together
   for (int64_t i0 = global_thread(); i0 < n; i0 += kPer * stride) {
-    int4 h[kPer], g[kPer];
+    int4 h[kPer], g[kPer], q[kPer];
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
       const int64_t i = i0 + u * stride;
       h[u] = make_int4(-1, 0, 0, 0);
       if (i < n) {
         const int4 *src = reinterpret_cast<const int4 *>(a.cell_entries + i);
-        h[u] = src[0];
-        g[u] = src[1];
+        h[u] = src[0];  // t1, bit, segment, c1
+        g[u] = src[1];  // c2, c3, t1 local, t2 local
+        q[u] = src[2];  // normal, curvature
       }
     }
     unsigned long long m[kPer];
     int32_t off[kPer];
-    int sid[kPer];
-    itsu_tracklet t1[kPer], t2[kPer];
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
       if (h[u].x >= 0) {
         m[u] = a.cell_mask[h[u].x];
         off[u] = a.cell_off[h[u].x];
-        sid[u] = a.trk_seg_id[h[u].x];
-        t1[u] = a.tracklets[h[u].x];
-        t2[u] = a.tracklets[h[u].z];
       }
     }
 #pragma unroll
@@ -1234,18 +1240,16 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_scatter(Arena a)
       }
       const int32_t rank = __popcll(m[u] & ((1ull << h[u].y) - 1ull));
       const int32_t out = off[u] + rank;
-      const int e = sid[u] / ITSU_TRACKLET_LAYERS, layer = sid[u] % ITSU_TRACKLET_LAYERS;
-      const int32_t *ts = a.trk_seg + e * ITSU_TRACKLET_LAYERS;
-      if (rank == 0 && layer >= 1) {  // the tracklet's first cell: its cells lookup entry
-        a.cell_lookup[h[u].x] = out - a.cell_seg[e * ITSU_CELL_LAYERS + layer];
+      if (rank == 0 && h[u].z % ITSU_CELL_LAYERS >= 1) {  // the tracklet's first cell: its cells lookup entry
+        a.cell_lookup[h[u].x] = out - a.cell_seg[h[u].z];
       }
       int2 *dst = reinterpret_cast<int2 *>(a.cells + out);
-      dst[0] = make_int2(t1[u].first_cluster, t1[u].second_cluster);
-      dst[1] = make_int2(t2[u].second_cluster, h[u].x - ts[layer]);
-      dst[2] = make_int2(h[u].z - ts[layer + 1], g[u].x);
-      dst[3] = make_int2(g[u].y, g[u].z);
-      dst[4] = make_int2(g[u].w, 1);
-      a.cell_seg_id[out] = e * ITSU_CELL_LAYERS + layer;
+      dst[0] = make_int2(h[u].w, g[u].x);
+      dst[1] = make_int2(g[u].y, g[u].z);
+      dst[2] = make_int2(g[u].w, q[u].x);
+      dst[3] = make_int2(q[u].y, q[u].z);
+      dst[4] = make_int2(q[u].w, 1);
+      a.cell_seg_id[out] = h[u].z;
     }
   }
 }
