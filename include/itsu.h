@@ -230,6 +230,42 @@ itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, i
  * memory, without waiting; itsu_batch_status waits and reports. */
 itsu_status itsu_relaunch(itsu_context *ctx);
 
+/* ---- road report: correct, duplicate and fake roads of each event ----
+ * IOUtils::writeRoadsReport (src/CA/IOUtils.cxx:125-170) over the roads of every vertex of an event
+ * and the event's labels map (IOUtils::loadLabels, IOUtils.cxx:80-123, keeps the particles with
+ * |pdg| == 211 and 7 clusters). A road whose label is not in the map is not reported; one whose
+ * label is in it is fake if the road is fake; otherwise it is correct when it is the first
+ * non-fake road of its label in the event (vertex order, then road order) and a duplicate after
+ * that. The classification runs on the device; the callers write the text streams
+ * (host/itsu_ioutils.hpp IOUtils::writeRoadsReport, itsu/io.py write_roads_report). */
+typedef struct itsu_label { /* Label (include/ITSReconstruction/CA/Label.h:27-40), same layout */
+  int32_t mc_id;
+  float pt, phi, eta;
+  int32_t pdg;
+  int32_t n_clusters;
+} itsu_label;
+#define ITSU_ROAD_UNREPORTED 0u
+#define ITSU_ROAD_CORRECT 1u
+#define ITSU_ROAD_DUPLICATE 2u
+#define ITSU_ROAD_FAKE 3u
+typedef struct itsu_report_counts {
+  int32_t labels;    /* distinct Monte Carlo ids in the event's labels map */
+  int32_t correct;   /* = labels found: the efficiency is correct / labels */
+  int32_t duplicate;
+  int32_t fake;
+} itsu_report_counts;
+/* roads, run_offsets: host, the roads of n_runs runs (vertices), run r's at
+ * [run_offsets[r], run_offsets[r+1]); both NULL: the device-resident roads of the context's last
+ * batch or frames run (n_runs must be its run count; not after a streamed host run, which keeps
+ * no per-run results). run_event: host, the event of each run, non-decreasing (NULL: run r is
+ * event r). labels, label_offsets: host, event e's labels map at [label_offsets[e],
+ * label_offsets[e+1]) (a repeated mc id keeps its first entry, as std::unordered_map::emplace;
+ * INT32_MIN is not a valid mc id). Outputs (host, each may be NULL): road_class[n_roads] (the
+ * ITSU_ROAD_* class of each road) and counts[n_events]. */
+itsu_status itsu_roads_report(itsu_context *ctx, const itsu_road *roads, const int32_t *run_offsets, const int32_t *run_event,
+                              int32_t n_runs, const itsu_label *labels, const int32_t *label_offsets, int32_t n_events,
+                              uint8_t *road_class, itsu_report_counts *counts);
+
 /* ---- launch-shape autotuner for batches (no counterpart in the reference) ----
  * Runs are grouped in multiplicity bands: band = floor(log2(mean clusters per event)). For the
  * band of the last run, itsu_autotune times every candidate launch shape (threads per block of

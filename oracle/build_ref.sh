@@ -11,7 +11,8 @@
 #   P5 Tracker.cxx:84      a phi row's upper bin index clamped to 400
 #   P4 (ref_cr only)       atan2f resolved to the correctly rounded itsu_atan2f
 # Binaries: ref_cr (P1-P5), ref_stock (P1-P3, P5: the C library's atan2f) and
-# ref_unstable (P1, P2, P4, P5: the reference's unstable std::sort).
+# ref_unstable (P1, P2, P4, P5: the reference's unstable std::sort); merge_pileup, the
+# reference's pile-up merger (benchmarks/scripts/root/generatePileUpData.cxx), unpatched.
 set -eu
 REF=${ITSU_REFERENCE:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -50,4 +51,6 @@ gcc -std=c99 -O2 -ffp-contract=off -c "$HERE/ref_atan2f.c" -o "$OUT/ref_atan2f.o
 $CXX $FLAGS -I"$HERE/../include" "$HARNESS" "$OUT"/src/*.cxx "$OUT/ref_atan2f.o" -o "$OUT/ref_cr" -DITSU_REF_CR=1
 $CXX $FLAGS -I"$HERE/../include" "$HARNESS" "$OUT"/src/*.cxx -o "$OUT/ref_stock"
 $CXX $FLAGS -I"$HERE/../include" "$HARNESS" "$OUT"/src_unstable/*.cxx "$OUT/ref_atan2f.o" -o "$OUT/ref_unstable" -DITSU_REF_CR=1
-echo "built $OUT/ref_cr $OUT/ref_stock $OUT/ref_unstable"
+# the reference's pile-up merger (a standalone program): merged_data.txt / merged_labels.txt
+$CXX -std=c++11 -O2 "$REF/benchmarks/scripts/root/generatePileUpData.cxx" -o "$OUT/merge_pileup"
+echo "built $OUT/ref_cr $OUT/ref_stock $OUT/ref_unstable $OUT/merge_pileup"

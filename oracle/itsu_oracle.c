@@ -719,3 +719,80 @@ int64_t oracle_run_batch(const itsu_cluster *clusters, const int32_t *layer_offs
   }
   return roads;
 }
+
+/* ---- road report: IOUtils::writeRoadsReport (IOUtils.cxx:125-170), classification part ----
+ * Per event, the labels map's ids (first entry per id, as unordered_map::emplace) are sorted for
+ * lookup; the roads of the event's vertices are walked in order: a road whose label is not in
+ * the map is skipped (:146-149); a fake one is reported fake (:153-155); otherwise the first road
+ * of its label is correct and later ones are duplicates (:159-166). */
+static int cmp_i32(const void *a, const void *b)
+{
+  const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+  return (x > y) - (x < y);
+}
+
+static int64_t find_sorted(const int32_t *ids, int64_t n, int32_t key)
+{
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (ids[mid] < key) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return (lo < n && ids[lo] == key) ? lo : -1;
+}
+
+int oracle_roads_report(const itsu_road *roads, const int32_t *run_offsets, const int32_t *run_event, int32_t n_runs,
+                        const itsu_label *labels, const int32_t *label_offsets, int32_t n_events, uint8_t *road_class,
+                        itsu_report_counts *counts)
+{
+  int32_t e, r = 0;
+  for (e = 0; e < n_events; ++e) {
+    const int64_t l0 = label_offsets[e], nl = label_offsets[e + 1] - label_offsets[e];
+    int32_t *ids = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nl > 0 ? nl : 1));
+    unsigned char *found = NULL;
+    int64_t n_ids = 0, k;
+    itsu_report_counts c = {0, 0, 0, 0};
+    if (!ids) return -1;
+    for (k = 0; k < nl; ++k) ids[k] = labels[l0 + k].mc_id;
+    qsort(ids, (size_t)nl, sizeof(int32_t), cmp_i32);
+    for (k = 0; k < nl; ++k) {
+      if (n_ids == 0 || ids[n_ids - 1] != ids[k]) ids[n_ids++] = ids[k];
+    }
+    found = (unsigned char *)calloc((size_t)(n_ids > 0 ? n_ids : 1), 1);
+    if (!found) {
+      free(ids);
+      return -1;
+    }
+    c.labels = (int32_t)n_ids;
+    /* the event's runs: consecutive, run_event non-decreasing (NULL: run r is event r) */
+    for (; r < n_runs && (run_event ? run_event[r] : r) == e; ++r) {
+      int64_t i;
+      for (i = run_offsets[r]; i < run_offsets[r + 1]; ++i) {
+        const int64_t slot = find_sorted(ids, n_ids, roads[i].label);
+        uint8_t cls = ITSU_ROAD_UNREPORTED;
+        if (slot >= 0) {
+          if (roads[i].is_fake) {
+            cls = ITSU_ROAD_FAKE;
+            ++c.fake;
+          } else if (found[slot]) {
+            cls = ITSU_ROAD_DUPLICATE;
+            ++c.duplicate;
+          } else {
+            cls = ITSU_ROAD_CORRECT;
+            ++c.correct;
+            found[slot] = 1;
+          }
+        }
+        if (road_class) road_class[i] = cls;
+      }
+    }
+    if (counts) counts[e] = c;
+    free(found);
+    free(ids);
+  }
+  return 0;
+}

@@ -56,6 +56,13 @@ void oracle_transform_cluster(int layer, const float vertex[3], const itsu_clust
 int64_t oracle_run_batch(const itsu_cluster *clusters, const int32_t *layer_offsets, const float *vertices,
                          int32_t n_events);
 
+/* IOUtils::writeRoadsReport (IOUtils.cxx:125-170), its classification: same arguments and
+ * outputs as itsu_roads_report with host roads (road_class and counts may be NULL). Returns 0, or
+ * -1 on allocation failure. */
+int oracle_roads_report(const itsu_road *roads, const int32_t *run_offsets, const int32_t *run_event, int32_t n_runs,
+                        const itsu_label *labels, const int32_t *label_offsets, int32_t n_events, uint8_t *road_class,
+                        itsu_report_counts *counts);
+
 #ifdef __cplusplus
 }
 #endif

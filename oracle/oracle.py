@@ -75,6 +75,8 @@ def lib():
         L.oracle_atan2f.argtypes = [ctypes.c_float, ctypes.c_float]
         L.oracle_run_batch.restype = ctypes.c_int64
         L.oracle_run_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]
+        L.oracle_roads_report.restype = ctypes.c_int
+        L.oracle_roads_report.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int32] + [ctypes.c_void_p] * 2 + [ctypes.c_int32] + [ctypes.c_void_p] * 2
         _lib = L
     return _lib
 
@@ -271,3 +273,38 @@ def canonical_sets(res: dict) -> dict:
             cl.append(int(ids[l + 2][cell["c3"]]))
         roads.append(tuple(cl))
     return dict(tracklets=sorted(trk), cells=sorted(cel), roads=sorted(roads))
+
+
+# ---- road report (IOUtils::writeRoadsReport) ----
+
+COUNTS_DTYPE = np.dtype([("labels", "<i4"), ("correct", "<i4"), ("duplicate", "<i4"), ("fake", "<i4")])
+
+
+def roads_report(roads, run_offsets, label_maps, run_event=None):
+    """The C restatement's road classes (ITSU_ROAD_*) and per-event counts for the roads of the
+    runs (vertices) in run_offsets and one labels map per event (itsu.io.read_reference_labels)."""
+    from itsu import io
+
+    roads = np.ascontiguousarray(roads, ROAD_DTYPE)
+    run_offsets = np.ascontiguousarray(run_offsets, np.int32)
+    labels, label_offsets = io.labels_for_report(label_maps)
+    n_runs, n_events = len(run_offsets) - 1, len(label_maps)
+    rev = None if run_event is None else np.ascontiguousarray(run_event, np.int32)
+    cls = np.zeros(max(len(roads), 1), np.uint8)
+    counts = np.zeros(max(n_events, 1), COUNTS_DTYPE)
+    ptr = lambda a: None if a is None or len(a) == 0 else a.ctypes.data  # noqa: E731
+    rc = lib().oracle_roads_report(ptr(roads), run_offsets.ctypes.data, ptr(rev), n_runs, ptr(labels), label_offsets.ctypes.data,
+                                   n_events, cls.ctypes.data, counts.ctypes.data)
+    if rc != 0:
+        raise MemoryError("oracle_roads_report failed")
+    return cls[:len(roads)], counts[:n_events]
+
+
+def run_reference_report(events_txt: str, labels_txt: str, outdir: str) -> dict:
+    """The reference's own road report (oracle/_ref/ref_cr report): loadEventData + loadLabels,
+    clustersToTracks per event and writeRoadsReport into outdir/{Correct,Duplicate,Fake}Roads.txt.
+    Returns the harness's JSON line (events, roads, seconds spent in writeRoadsReport)."""
+    import json
+
+    out = subprocess.run([ref_binary("cr"), "report", events_txt, labels_txt, outdir], check=True, capture_output=True, text=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])

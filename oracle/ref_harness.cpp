@@ -8,6 +8,13 @@
 //   ref_cr time <events.txt> <repeats>   time Tracker::clustersToTracks per event (steady_clock,
 //                                        one warm-up event first, as main.cpp:74-75) -> JSON line
 //   ref_cr timebin <events.bin> <repeats> [first count]   the same on binary events
+//   ref_cr report <events.txt> <labels.txt> <outdir>   main.cpp's benchmark data: every event
+//                                        through clustersToTracks, then IOUtils::writeRoadsReport
+//                                        into outdir/{Correct,Duplicate,Fake}Roads.txt; prints the
+//                                        time spent in writeRoadsReport (JSON line)
+//   ref_cr labels <labels.txt> <n_events> <out.txt>   IOUtils::loadLabels, each map's entries
+//                                        (ascending id) one per line, "-1" after each map
+//   ref_cr events <events.txt> <out.txt>   IOUtils::loadEventData, every vertex and cluster
 //
 // The dump needs the tracker's private per-vertex context and its protected stages, so the
 // reference headers are included with private/protected opened up (standard headers first, so
@@ -243,6 +250,71 @@ int run_time_events(std::vector<Event> &events, int repeats)
   return 0;
 }
 
+int run_report(const char *events_path, const char *labels_path, const std::string &outdir)
+{
+  std::vector<Event> events = IOUtils::loadEventData(events_path);
+  std::vector<std::unordered_map<int, Label>> labels = IOUtils::loadLabels(static_cast<int>(events.size()), labels_path);
+  std::ofstream correct(outdir + "/CorrectRoads.txt"), duplicate(outdir + "/DuplicateRoads.txt"),
+      fake(outdir + "/FakeRoads.txt");
+  Tracker<false> tracker{};
+  double seconds = 0;
+  long long n_roads = 0;
+  const std::unordered_map<int, Label> none{};
+  for (size_t e = 0; e < events.size(); ++e) {
+    std::vector<std::vector<Road>> roads = tracker.clustersToTracks(events[e]);
+    for (const auto &v : roads) n_roads += static_cast<long long>(v.size());
+    const auto t0 = std::chrono::steady_clock::now();
+    IOUtils::writeRoadsReport(correct, duplicate, fake, roads, e < labels.size() ? labels[e] : none);
+    const auto t1 = std::chrono::steady_clock::now();
+    seconds += std::chrono::duration<double>(t1 - t0).count();
+  }
+  std::printf("{\"events\": %lld, \"roads\": %lld, \"report_seconds\": %.9f}\n", static_cast<long long>(events.size()),
+              n_roads, seconds);
+  return 0;
+}
+
+int run_labels(const char *labels_path, int n_events, const char *out_path)
+{
+  std::vector<std::unordered_map<int, Label>> labels = IOUtils::loadLabels(n_events, labels_path);
+  std::FILE *f = std::fopen(out_path, "w");
+  if (!f) return 3;
+  for (const auto &m : labels) {
+    std::vector<int> ids;
+    for (const auto &kv : m) ids.push_back(kv.first);
+    std::sort(ids.begin(), ids.end());
+    for (int id : ids) {
+      const Label &l = m.at(id);
+      std::fprintf(f, "%d %.9g %.9g %.9g %d %d\n", l.monteCarloId, l.transverseMomentum, l.phiCoordinate, l.pseudorapidity,
+                   l.pdgCode, l.numberOfClusters);
+    }
+    std::fprintf(f, "-1\n");
+  }
+  std::fclose(f);
+  return 0;
+}
+
+int run_events(const char *events_path, const char *out_path)
+{
+  std::vector<Event> events = IOUtils::loadEventData(events_path);
+  std::FILE *f = std::fopen(out_path, "w");
+  if (!f) return 3;
+  for (const Event &ev : events) {
+    std::fprintf(f, "event %d vertices %d\n", ev.getEventId(), ev.getPrimaryVerticesNum());
+    for (int v = 0; v < ev.getPrimaryVerticesNum(); ++v) {
+      const float3 &p = ev.getPrimaryVertex(v);
+      std::fprintf(f, "v %.9g %.9g %.9g\n", p.x, p.y, p.z);
+    }
+    for (int l = 0; l < Constants::ITS::LayersNumber; ++l) {
+      for (const Cluster &c : ev.getLayer(l).getClusters()) {
+        std::fprintf(f, "c %d %d %.9g %.9g %.9g %.9g %d\n", l, c.clusterId, c.xCoordinate, c.yCoordinate, c.zCoordinate,
+                     c.alphaAngle, c.monteCarloId);
+      }
+    }
+  }
+  std::fclose(f);
+  return 0;
+}
+
 } // namespace
 
 int main(int argc, char **argv)
@@ -259,13 +331,17 @@ int main(int argc, char **argv)
   if (argc < 4) {
     std::fprintf(stderr,
                  "usage: %s dump <events.txt> <out.bin> | time <events.txt> <repeats> |"
-                 " timebin <events.bin> <repeats> [first count]\n",
+                 " timebin <events.bin> <repeats> [first count] | report <events.txt> <labels.txt> <outdir> |"
+                 " labels <labels.txt> <n_events> <out.txt> | events <events.txt> <out.txt>\n",
                  argv[0]);
     return 2;
   }
   const std::string mode = argv[1];
   if (mode == "dump") return run_dump(argv[2], argv[3]);
   if (mode == "time") return run_time(argv[2], std::atoi(argv[3]));
+  if (mode == "report" && argc > 4) return run_report(argv[2], argv[3], argv[4]);
+  if (mode == "labels" && argc > 4) return run_labels(argv[2], std::atoi(argv[3]), argv[4]);
+  if (mode == "events") return run_events(argv[2], argv[3]);
   if (mode == "timebin") {
     const int first = argc > 5 ? std::atoi(argv[4]) : 0;
     const int count = argc > 5 ? std::atoi(argv[5]) : -1;

@@ -25,7 +25,7 @@ def test_facade_driver_roads_match_reference(case):
         with gzip.open(os.path.join(GOLDEN, case + ".events.txt.gz"), "rb") as f, open(txt, "wb") as o:
             o.write(f.read())
         out = os.path.join(d, "roads.bin")
-        proc = subprocess.run([MAIN, txt, out], capture_output=True, text=True, timeout=300)
+        proc = subprocess.run([MAIN, txt, "--roads", out], capture_output=True, text=True, timeout=300)
         assert proc.returncode == 0, proc.stderr
         data = open(out, "rb").read()
     pos = 0

@@ -1135,6 +1135,138 @@ itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, 
   return ITSU_OK;
 }
 
+itsu_status itsu_roads_report(itsu_context *ctx, const itsu_road *roads, const int32_t *run_offsets, const int32_t *run_event,
+                              int32_t n_runs, const itsu_label *labels, const int32_t *label_offsets, int32_t n_events,
+                              uint8_t *road_class, itsu_report_counts *counts)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "itsu_roads_report: null context");
+  if (n_runs < 0 || n_events < 0) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: negative run or event count");
+  if ((roads == nullptr) != (run_offsets == nullptr)) {
+    return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: give both roads and run offsets, or neither");
+  }
+  if (n_events > 0 && !label_offsets) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: null label offsets");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  const bool resident = roads == nullptr;
+  if (resident) {
+    itsu_status st;
+    if ((st = require_stage(ctx, kRoads, "itsu_roads_report")) != ITSU_OK) return st;
+    if (n_runs != ctx->n_events) {
+      return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: %d runs given, the last run has %d", n_runs, ctx->n_events);
+    }
+  } else {
+    if (n_runs > 0 && run_offsets[0] != 0) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: run offsets must start at 0");
+    for (int32_t r = 0; r < n_runs; ++r) {
+      if (run_offsets[r + 1] < run_offsets[r]) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: run offsets decrease at %d", r);
+    }
+  }
+  for (int32_t r = 0; run_event && r < n_runs; ++r) {
+    if (run_event[r] < 0 || run_event[r] >= n_events || (r > 0 && run_event[r] < run_event[r - 1])) {
+      return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: run %d has event %d (events must be in [0, %d) and non-decreasing)", r,
+                  run_event[r], n_events);
+    }
+  }
+  if (!run_event && n_runs > n_events) {
+    return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: %d runs but %d events and no run-to-event map", n_runs, n_events);
+  }
+  if (n_events > 0 && label_offsets[0] != 0) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: label offsets must start at 0");
+  for (int32_t e = 0; e < n_events; ++e) {
+    if (label_offsets[e + 1] < label_offsets[e]) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: label offsets decrease at %d", e);
+  }
+  const int64_t n_labels = n_events > 0 ? label_offsets[n_events] : 0;
+  if (n_labels > 0 && !labels) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: null labels");
+  std::vector<int32_t> label_event((size_t)n_labels);
+  std::vector<int64_t> table_base((size_t)n_events + 1, 0);
+  for (int32_t e = 0; e < n_events; ++e) {
+    const int64_t n = label_offsets[e + 1] - label_offsets[e];
+    int64_t size = 2;
+    while (size < 2 * n) size <<= 1;  // power of two, at least twice the labels: probes end at an empty slot
+    table_base[e + 1] = table_base[e] + size;
+    for (int64_t i = label_offsets[e]; i < label_offsets[e + 1]; ++i) {
+      if (labels[i].mc_id == INT32_MIN) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: label %lld has mc id INT32_MIN", (long long)i);
+      label_event[(size_t)i] = e;
+    }
+  }
+  const int64_t table_size = table_base[(size_t)n_events];
+
+  // device inputs: the roads and their run offsets (the context's own when resident)
+  int64_t n_roads = 0;
+  if (resident) {
+    int32_t end = 0;
+    ITSU_CUDA(ctx, cudaMemcpyAsync(&end, ctx->road_seg + n_runs, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    n_roads = end;
+  } else {
+    n_roads = n_runs > 0 ? run_offsets[n_runs] : 0;
+    if (n_roads > 0 && !roads) return fail(ctx, ITSU_ERR_INVALID, "itsu_roads_report: null roads");
+  }
+  // one scratch allocation for everything, freed before returning
+  auto align = [](size_t n) { return (n + 255) / 256 * 256; };
+  const size_t o_roads = 0;
+  const size_t o_run = o_roads + (resident ? 0 : align(sizeof(itsu_road) * (size_t)n_roads));
+  const size_t o_rev = o_run + (resident ? 0 : align(sizeof(int32_t) * ((size_t)n_runs + 1)));
+  const size_t o_lab = o_rev + align(sizeof(int32_t) * (size_t)n_runs);
+  const size_t o_lev = o_lab + align(sizeof(itsu_label) * (size_t)n_labels);
+  const size_t o_tb = o_lev + align(sizeof(int32_t) * (size_t)n_labels);
+  const size_t o_keys = o_tb + align(sizeof(int64_t) * ((size_t)n_events + 1));
+  const size_t o_fl = o_keys + align(sizeof(int32_t) * (size_t)table_size);
+  const size_t o_fr = o_fl + align(sizeof(int32_t) * (size_t)table_size);
+  const size_t o_rs = o_fr + align(sizeof(int64_t) * (size_t)table_size);
+  const size_t o_re = o_rs + align(sizeof(int64_t) * (size_t)n_roads);
+  const size_t o_cls = o_re + align(sizeof(int32_t) * (size_t)n_roads);
+  const size_t o_cnt = o_cls + align((size_t)n_roads);
+  const size_t total = o_cnt + align(sizeof(itsu_report_counts) * (size_t)n_events);
+  unsigned char *buf = nullptr;
+  ITSU_CUDA(ctx, cudaMalloc((void **)&buf, std::max<size_t>(total, 256)));
+  struct Free {
+    unsigned char *p;
+    ~Free() { cudaFree(p); }
+  } free_buf{buf};
+  itsu::ReportArgs r{};
+  r.roads = resident ? ctx->roads : reinterpret_cast<itsu_road *>(buf + o_roads);
+  r.n_roads = n_roads;
+  r.run_offsets = resident ? ctx->road_seg : reinterpret_cast<int32_t *>(buf + o_run);
+  r.run_event = run_event ? reinterpret_cast<int32_t *>(buf + o_rev) : nullptr;
+  r.n_runs = n_runs;
+  r.n_events = n_events;
+  r.labels = reinterpret_cast<itsu_label *>(buf + o_lab);
+  r.label_event = reinterpret_cast<int32_t *>(buf + o_lev);
+  r.n_labels = n_labels;
+  r.table_base = reinterpret_cast<int64_t *>(buf + o_tb);
+  r.table_size = table_size;
+  r.keys = reinterpret_cast<int32_t *>(buf + o_keys);
+  r.first_label = reinterpret_cast<int32_t *>(buf + o_fl);
+  r.first_road = reinterpret_cast<int64_t *>(buf + o_fr);
+  r.road_slot = reinterpret_cast<int64_t *>(buf + o_rs);
+  r.road_event = reinterpret_cast<int32_t *>(buf + o_re);
+  r.road_class = buf + o_cls;
+  r.counts = reinterpret_cast<itsu_report_counts *>(buf + o_cnt);
+  cudaStream_t s = ctx->stream;
+  if (!resident && n_roads > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(buf + o_roads, roads, sizeof(itsu_road) * (size_t)n_roads, cudaMemcpyHostToDevice, s));
+  }
+  if (!resident) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(buf + o_run, run_offsets, sizeof(int32_t) * ((size_t)n_runs + 1), cudaMemcpyHostToDevice, s));
+  }
+  if (run_event && n_runs > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(buf + o_rev, run_event, sizeof(int32_t) * (size_t)n_runs, cudaMemcpyHostToDevice, s));
+  }
+  if (n_labels > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(buf + o_lab, labels, sizeof(itsu_label) * (size_t)n_labels, cudaMemcpyHostToDevice, s));
+    ITSU_CUDA(ctx, cudaMemcpyAsync(buf + o_lev, label_event.data(), sizeof(int32_t) * (size_t)n_labels, cudaMemcpyHostToDevice, s));
+  }
+  ITSU_CUDA(ctx, cudaMemcpyAsync(buf + o_tb, table_base.data(), sizeof(int64_t) * ((size_t)n_events + 1), cudaMemcpyHostToDevice, s));
+  itsu::launch_report(r, s, ctx->num_sms);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  if (road_class && n_roads > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(road_class, r.road_class, (size_t)n_roads, cudaMemcpyDeviceToHost, s));
+  }
+  if (counts && n_events > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(counts, r.counts, sizeof(itsu_report_counts) * (size_t)n_events, cudaMemcpyDeviceToHost, s));
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(s));
+  return ITSU_OK;
+}
+
 }  // extern "C"
 
 namespace {

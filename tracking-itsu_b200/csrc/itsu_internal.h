@@ -162,6 +162,29 @@ void launch_roads_write(const Arena &a, const Launch &l);
 void launch_append_roads(const Arena &a, const Launch &l, itsu_road *dst, int32_t *dst_off, int32_t e0, int64_t cap,
                          DevStatus *snap);
 
+// The road report (itsu_report.cu): device buffers of one itsu_roads_report call.
+struct ReportArgs {
+  const itsu_road *roads;      // n_roads, run-major
+  int64_t n_roads;
+  const int32_t *run_offsets;  // n_runs + 1
+  const int32_t *run_event;    // n_runs (null: run r is event r)
+  int32_t n_runs;
+  int32_t n_events;
+  const itsu_label *labels;    // n_labels, event-major
+  const int32_t *label_event;  // the event of each label
+  int64_t n_labels;
+  const int64_t *table_base;   // n_events + 1: event e's table at [table_base[e], table_base[e+1]), a power of two
+  int64_t table_size;
+  int32_t *keys;               // per slot: the Monte Carlo id (INT32_MIN: empty)
+  int32_t *first_label;        // per slot: its first label entry
+  int64_t *first_road;         // per slot: its first non-fake road
+  int64_t *road_slot;          // per road: its label's slot, -1 if the label is not in the map
+  int32_t *road_event;         // per road: its event
+  uint8_t *road_class;         // per road: ITSU_ROAD_*
+  itsu_report_counts *counts;  // per event
+};
+void launch_report(const ReportArgs &r, cudaStream_t stream, int num_sms);
+
 // Every kernel of a run, in launch order, with its name (the instrumentation API times them
 // one by one). The stage launchers above enqueue consecutive ranges of this table.
 struct KernelStep {

@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -105,6 +106,23 @@ class Road final {
   itsu_road r_{};
 };
 static_assert(sizeof(Road) == sizeof(itsu_road) && sizeof(Road) == 32, "Road layout");
+
+// Label.h:27-41 and its stream format (Label.cxx:32-37)
+constexpr int PionCode = 211;  // Constants::PDGCodes::PionCode
+struct Label final {
+  int monteCarloId;
+  float transverseMomentum;
+  float phiCoordinate;
+  float pseudorapidity;
+  int pdgCode;
+  int numberOfClusters;
+};
+static_assert(sizeof(Label) == sizeof(itsu_label) && sizeof(Label) == 24, "Label layout");
+inline std::ostream &operator<<(std::ostream &out, const Label &l)
+{
+  return out << l.monteCarloId << "\t" << l.transverseMomentum << "\t" << l.phiCoordinate << "\t" << l.pseudorapidity << "\t"
+             << l.pdgCode << "\t" << l.numberOfClusters;
+}
 
 // Layer.h:30-46
 class Layer final {

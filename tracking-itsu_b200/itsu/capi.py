@@ -22,6 +22,7 @@ CELL_DTYPE = np.dtype(
      ("nz", "<f4"), ("curvature", "<f4"), ("level", "<i4")]
 )
 ROAD_DTYPE = np.dtype([("cells", "<i4", (5,)), ("size", "<i4"), ("label", "<i4"), ("fake", "u1"), ("pad", "u1", (3,))])
+REPORT_COUNTS_DTYPE = np.dtype([("labels", "<i4"), ("correct", "<i4"), ("duplicate", "<i4"), ("fake", "<i4")])
 
 OK, ERR_INVALID, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NOMEM, ERR_STATE = range(7)
 FLAG_NO_GROW = 1
@@ -143,6 +144,9 @@ SIGNATURES = [
     ("itsu_frames_run_host", ctypes.c_int,
      [ctypes.c_void_p, ctypes.POINTER(Frames), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     ("itsu_relaunch", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_roads_report", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     ("itsu_kernels_per_run", ctypes.c_int32, []),
     ("itsu_multiplicity_band", ctypes.c_int32, [ctypes.c_int64, ctypes.c_int32]),
     ("itsu_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Tune)]),
@@ -330,6 +334,37 @@ class Context:
         return roads
 
     # ---- batches ----
+    def roads_report(self, label_maps, roads=None, run_offsets=None, run_event=None, n_runs=None):
+        """itsu_roads_report: the road classes (ITSU_ROAD_*: 0 unreported, 1 correct, 2 duplicate,
+        3 fake) and per-event counts (labels, correct, duplicate, fake) of IOUtils::writeRoadsReport.
+        label_maps: one LABEL_DTYPE array per event (itsu.io.read_reference_labels). roads and
+        run_offsets on the host, or neither for the device-resident roads of the last batch or frames
+        run (n_runs: its run count). run_event maps runs (vertices) to events (default: run r is
+        event r)."""
+        from .io import labels_for_report
+
+        labels, label_offsets = labels_for_report(label_maps)
+        n_events = len(label_maps)
+        if roads is not None:
+            roads = np.ascontiguousarray(roads, ROAD_DTYPE)
+            if len(roads) == 0:
+                roads = np.zeros(1, ROAD_DTYPE)  # a valid pointer: the offsets say there are none
+            run_offsets = np.ascontiguousarray(run_offsets, np.int32)
+            n_runs = len(run_offsets) - 1
+            n_roads = int(run_offsets[-1])
+        else:
+            if n_runs is None:
+                raise ValueError("n_runs is required for the device-resident roads")
+            n_roads = sum(self.counts(r).roads for r in range(n_runs))
+        rev = None if run_event is None else np.ascontiguousarray(run_event, np.int32)
+        cls = np.zeros(max(n_roads, 1), np.uint8)
+        counts = np.zeros(max(n_events, 1), REPORT_COUNTS_DTYPE)
+        self._check(self.lib.itsu_roads_report(
+            self.h, _ptr(roads) if roads is not None else None, _ptr(run_offsets) if roads is not None else None,
+            _ptr(rev) if rev is not None else None, n_runs, _ptr(labels) if len(labels) else None, _ptr(label_offsets),
+            n_events, cls.ctypes.data, counts.ctypes.data))
+        return cls[:n_roads], counts[:n_events]
+
     def batch_run_host(self, clusters, layer_offsets, vertices, roads_capacity=None):
         """Host in / host out over a batch; returns (roads, road_offsets)."""
         clusters = np.ascontiguousarray(clusters, CLUSTER_DTYPE)
