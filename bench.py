@@ -477,6 +477,14 @@ def run_ours(args):
         launch()  # back to the plain graph (the profile below times the plain kernels)
         ctx.batch_status()
 
+    # ---- road report (IOUtils::writeRoadsReport) on the device, over the roads left resident ----
+    report = road_report_mode(ctx, events, frames, args, rank, world)
+    usage = ctx.memory_usage()
+    arena = dict(usage, occupancy={k: (usage["used"][k] / usage["capacity"][k]) if usage["capacity"][k] else None
+                                   for k in usage["capacity"]},
+                 note="itsu_memory_usage_get after the step: the arena sized by the count passes (exact totals, grown "
+                      "once), against the reference's per-vertex coefficient reservations (itsu.io.MemoryModel)")
+
     # ---- live per-kernel timing for the roofline ----
     prof = ctx.profile(repeats=3)
     step_bytes = {}
@@ -576,7 +584,9 @@ def run_ours(args):
                     "kernel_ms": {name: round(t, 4) for name, t in learned["prof"]},
                     "note": "same resident batch and timing as the plain value; fused BF16 MLP (mma.sync) in the cell stage",
                 },
+                "road_report": report,
             },
+            "arena": arena,
             "kernel_ms": {name: round(t, 4) for name, t in prof},
             "algorithmic_bytes_per_step": step_bytes.get("event"),
             "achieved_gbs_whole_step": step_bytes.get("event") / (ms / args.steps * 1e-3) / 1e9,
@@ -589,6 +599,57 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+def road_report_mode(ctx, events, frames, args, rank, world):
+    """itsu_roads_report over the step's roads, left on the device by the last graph replay: the
+    correct / duplicate / fake classification of IOUtils::writeRoadsReport against each event's
+    labels map (the particles with |pdg| == 211 and 7 clusters). Timed per call (labels up, road
+    classes and counts down, wall clock around the synchronous call), next to the reference's own
+    writeRoadsReport on a sample of the same events (oracle/_ref/ref_cr report)."""
+    import tempfile
+
+    from itsu import io
+
+    owners = frames if frames is not None else events
+    maps = [np.ascontiguousarray(ev.labels[(np.abs(ev.labels["pdg"]) == io.PION_CODE) & (ev.labels["ncl"] == 7)], io.LABEL_DTYPE)
+            for ev in owners]
+    run_event = None
+    if frames is not None:
+        run_event = np.concatenate([np.full(len(f.vertices), k, np.int32) for k, f in enumerate(frames)])
+    n_runs = len(events)
+    for _ in range(2):
+        ctx.roads_report(maps, run_event=run_event, n_runs=n_runs)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        cls, counts = ctx.roads_report(maps, run_event=run_event, n_runs=n_runs)
+    call_ms = (time.perf_counter() - t0) / reps * 1e3
+    labels = int(counts["labels"].sum())
+    out = {"ms_per_step": call_ms, "events_per_s": len(owners) / (call_ms * 1e-3), "events": len(owners),
+           "roads": int(len(cls)), "labels": labels, "correct": int(counts["correct"].sum()),
+           "duplicate": int(counts["duplicate"].sum()), "fake": int(counts["fake"].sum()),
+           "efficiency": (int(counts["correct"].sum()) / labels) if labels else None,
+           "api": "itsu_roads_report on the device-resident roads (labels uploaded, classes and counts downloaded per call)",
+           "reference": None}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import oracle
+
+            if oracle.ref_available("cr"):
+                sample = owners[: min(8, len(owners))]
+                with tempfile.TemporaryDirectory() as tmp:
+                    gen.write_reference_events(sample, os.path.join(tmp, "data.txt"))
+                    gen.write_reference_labels(sample, os.path.join(tmp, "labels.txt"))
+                    r = oracle.run_reference_report(os.path.join(tmp, "data.txt"), os.path.join(tmp, "labels.txt"), tmp)
+                out["reference"] = {"events_per_s": r["events"] / r["report_seconds"] if r["report_seconds"] > 0 else None,
+                                    "sample_events": r["events"], "report_seconds": r["report_seconds"], "cores": 1,
+                                    "kind": "reference",
+                                    "note": "IOUtils::writeRoadsReport of the reference build (ref_cr report), one core, "
+                                            "steady_clock around each call, roads from its own Tracker"}
+        except Exception as exc:  # the baseline is reported, not required
+            out["reference"] = {"error": str(exc)}
+    return out
 
 
 def learned_mode(ctx, launch, args, stream, dist, device):

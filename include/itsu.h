@@ -207,6 +207,8 @@ itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch);
 itsu_status itsu_batch_status(itsu_context *ctx);
 /* Device pointer to the roads of the last batch (event-major) and to road_offsets[n_events+1]. */
 itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, const int32_t **road_offsets);
+/* Number of roads of the last batch or frames run (all its runs), read from the device. */
+itsu_status itsu_batch_road_count(itsu_context *ctx, int64_t *n_roads);
 
 /* ---- pile-up frames: several primary vertices over the same clusters ----
  * The reference tracks every vertex of an event over all of the event's clusters, running the
@@ -385,6 +387,24 @@ itsu_status itsu_prefilter_train(itsu_context *ctx, const float *features, const
  * grad[ITSU_MLP_PARAMS] in itsu_prefilter_model order). */
 itsu_status itsu_prefilter_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
                                     float pos_weight, float *grad, float *loss);
+
+/* ---- arena occupancy ----
+ * The reference preallocates each vertex's tracklet and cell vectors from coefficients of the
+ * cluster counts (Constants::Memory, Constants.h:87-92; PrimaryVertexContext.cxx:59-73, 125-131)
+ * and its memory benchmark prints capacity against use per vertex
+ * (Tracker::clustersToTracksMemoryBenchmark, Tracker.cxx:304-363; itsu/io.py MemoryModel writes
+ * that file from per-run counts). Here the count passes size the arena exactly (it grows to the
+ * counted totals, across multiplicity bands); this reports what the arena holds against what the
+ * last run used. */
+typedef struct itsu_memory_usage {
+  int64_t device_bytes;          /* arena buffers of the context and of its streamed second arena */
+  int64_t clusters_capacity;     /* clusters and events the arena holds */
+  int64_t events_capacity;
+  int64_t capacity[4];           /* tracklets, cells, neighbours, roads the arena holds */
+  int64_t used[4];               /* the last synchronised run's totals (0 before any) */
+  int64_t cell_entries_capacity; /* the cell count pass's entry scratch */
+} itsu_memory_usage;
+itsu_status itsu_memory_usage_get(itsu_context *ctx, itsu_memory_usage *out);
 
 /* ---- clustering without any allocation ----
  * No counterpart in the reference: its GPU backend allocates per call (gpu/Vector.h:97-122).

@@ -15,6 +15,8 @@
 //   ref_cr labels <labels.txt> <n_events> <out.txt>   IOUtils::loadLabels, each map's entries
 //                                        (ascending id) one per line, "-1" after each map
 //   ref_cr events <events.txt> <out.txt>   IOUtils::loadEventData, every vertex and cluster
+//   ref_cr memory <events.txt> <out.txt>   main.cpp's MEMORY_BENCHMARK run: one warm-up event,
+//                                        then Tracker::clustersToTracksMemoryBenchmark per event
 //
 // The dump needs the tracker's private per-vertex context and its protected stages, so the
 // reference headers are included with private/protected opened up (standard headers first, so
@@ -315,6 +317,18 @@ int run_events(const char *events_path, const char *out_path)
   return 0;
 }
 
+int run_memory(const char *events_path, const char *out_path)
+{
+  std::vector<Event> events = IOUtils::loadEventData(events_path);
+  std::ofstream out(out_path);
+  Tracker<false> tracker{};
+  if (!events.empty()) tracker.clustersToTracks(events[0]);  // main.cpp:74-75
+  for (size_t e = 0; e < events.size(); ++e) {
+    tracker.clustersToTracksMemoryBenchmark(events[e], out);
+  }
+  return 0;
+}
+
 } // namespace
 
 int main(int argc, char **argv)
@@ -332,7 +346,7 @@ int main(int argc, char **argv)
     std::fprintf(stderr,
                  "usage: %s dump <events.txt> <out.bin> | time <events.txt> <repeats> |"
                  " timebin <events.bin> <repeats> [first count] | report <events.txt> <labels.txt> <outdir> |"
-                 " labels <labels.txt> <n_events> <out.txt> | events <events.txt> <out.txt>\n",
+                 " labels <labels.txt> <n_events> <out.txt> | events <events.txt> <out.txt> | memory <events.txt> <out.txt>\n",
                  argv[0]);
     return 2;
   }
@@ -342,6 +356,7 @@ int main(int argc, char **argv)
   if (mode == "report" && argc > 4) return run_report(argv[2], argv[3], argv[4]);
   if (mode == "labels" && argc > 4) return run_labels(argv[2], std::atoi(argv[3]), argv[4]);
   if (mode == "events") return run_events(argv[2], argv[3]);
+  if (mode == "memory") return run_memory(argv[2], argv[3]);
   if (mode == "timebin") {
     const int first = argc > 5 ? std::atoi(argv[4]) : 0;
     const int count = argc > 5 ? std::atoi(argv[5]) : -1;

@@ -6,8 +6,9 @@ oracle/_ref/merge_pileup (it needs the reference sources):  python tests/golden/
 Cases (seeded synthetic events, written in the reference's text formats):
   mixed   a 120-track event, a dense 60-track jet (duplicate and fake roads) and a 3-vertex
           pile-up event of 120-track collisions: data.txt / labels.txt, the reference's road report
-          ({Correct,Duplicate,Fake}Roads.txt: ref_cr report = main.cpp's benchmark data), and
-          the reference loaders' parse of both files (events.dump, labels.dump)
+          ({Correct,Duplicate,Fake}Roads.txt: ref_cr report = main.cpp's benchmark data), the
+          reference loaders' parse of both files (events.dump, labels.dump) and the MEMORY_BENCHMARK
+          build's MemoryOccupancy.txt (ref_cr memory)
   merge   six 40-track events merged into frames of 3 by the reference's merger
           (merged_data.txt, merged_labels.txt)
 Everything is stored gzip-compressed.
@@ -60,7 +61,8 @@ def main() -> None:
         oracle.run_reference_report(data, labels, tmp)
         subprocess.check_call([ref, "events", data, os.path.join(tmp, "events.dump")])
         subprocess.check_call([ref, "labels", labels, str(len(events)), os.path.join(tmp, "labels.dump")])
-        for name in ("data.txt", "labels.txt", "events.dump", "labels.dump") + REPORT_FILES:
+        subprocess.check_call([ref, "memory", data, os.path.join(tmp, "MemoryOccupancy.txt")])
+        for name in ("data.txt", "labels.txt", "events.dump", "labels.dump", "MemoryOccupancy.txt") + REPORT_FILES:
             _gz(os.path.join(tmp, name), "mixed." + name)
     with tempfile.TemporaryDirectory() as tmp:
         events = merge_events()

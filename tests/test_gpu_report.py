@@ -111,3 +111,33 @@ def test_facade_driver_writes_the_reference_report(tmp_path):
     assert proc.returncode == 0, proc.stderr
     for n in REPORT_FILES:
         assert (tmp_path / n).read_text() == _golden("mixed." + n), n
+
+
+def test_memory_occupancy_and_arena_usage(tmp_path):
+    """The reference's MemoryOccupancy.txt from the device's per-run counts, and the arena's own
+    occupancy (itsu_memory_usage_get): capacities hold the counted totals, bytes follow growth."""
+    _unpack(tmp_path, "mixed", ("data.txt",))
+    events = io.read_reference_events(str(tmp_path / "data.txt"))
+    clusters, offsets, vertices, _ = _runs_batch(events)
+    c = capi.Context(device=0)
+    try:
+        c.batch_run_host(clusters, offsets, vertices)
+        runs = []
+        for r in range(len(vertices) // 3):
+            n = c.counts(r)
+            runs.append((list(n.clusters), list(n.tracklets), list(n.cells), n.roads))
+        assert io.memory_occupancy(runs[: len(events[0].vertices)], runs) == _golden("mixed.MemoryOccupancy.txt")
+        small = c.memory_usage()
+        totals = dict(tracklets=sum(sum(r[1]) for r in runs), cells=sum(sum(r[2]) for r in runs),
+                      roads=sum(r[3] for r in runs))
+        for k, v in totals.items():
+            assert small["used"][k] == v and small["capacity"][k] >= v, k
+        assert small["device_bytes"] > 0 and small["clusters_capacity"] >= len(clusters)
+        big = [gen.pbpb_event(s, n_tracks=3000) for s in (71, 72, 73, 74)]
+        c.batch_run_host(*gen.pack_batch(big))
+        grown = c.memory_usage()
+        assert grown["device_bytes"] > small["device_bytes"]
+        for k in ("tracklets", "cells", "neighbours", "roads"):
+            assert grown["capacity"][k] >= grown["used"][k] > 0, k
+    finally:
+        c.close()

@@ -166,3 +166,35 @@ def test_fresh_case_through_the_reference(tmp_path):
         io.merge_pileup(2, str(tmp_path), str(tmp_path))
         for n in ("merged_data.txt", "merged_labels.txt"):
             assert (tmp_path / n).read_text() == (out / n).read_text(), n
+
+
+def test_binary_events_round_trip(tmp_path):
+    """The binary loader gives the text loader's events (ids, coordinates, alpha, MC ids bit for bit)."""
+    _unpack(tmp_path, "mixed", ("data.txt",))
+    text_events = io.read_reference_events(str(tmp_path / "data.txt"))
+    gen.write_binary_events(text_events, str(tmp_path / "events.bin"))
+    bin_events = io.read_binary_events(str(tmp_path / "events.bin"))
+    assert events_dump(bin_events) == events_dump(text_events) == _golden("mixed.events.dump")
+    for a, b in zip(text_events, bin_events):
+        assert np.array_equal(a.vertices.view(np.uint32), b.vertices.view(np.uint32))
+        for la, lb in zip(a.layers, b.layers):
+            assert np.array_equal(la.view(np.uint8), lb.view(np.uint8))
+
+
+def run_counts(events):
+    """Per run (every vertex of every event): cluster, tracklet and cell counts per layer and roads."""
+    out = []
+    for ev, iv, _ in runs_of(events):
+        r = oracle.run_vertex(ev.layers, ev.vertices[iv])
+        out.append(([len(x) for x in r["clusters"]], [len(x) for x in r["tracklets"]], [len(x) for x in r["cells"]], len(r["roads"])))
+    return out
+
+
+def test_memory_occupancy_matches_the_reference_benchmark(tmp_path):
+    """MemoryOccupancy.txt of the reference's MEMORY_BENCHMARK build, from the oracle's counts: the
+    coefficient reservations, push_back growth and capacities kept across vertices restated."""
+    _unpack(tmp_path, "mixed", ("data.txt",))
+    events = io.read_reference_events(str(tmp_path / "data.txt"))
+    counts = run_counts(events)
+    warmup = counts[: len(events[0].vertices)]
+    assert io.memory_occupancy(warmup, counts) == _golden("mixed.MemoryOccupancy.txt")

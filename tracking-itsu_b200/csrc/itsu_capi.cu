@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "itsu.h"
@@ -160,6 +161,14 @@ struct itsu_context {
   bool has_model = false;
   bool prefilter = false;
 
+  // road report scratch (itsu_roads_report)
+  unsigned char *report_scratch = nullptr;
+  int64_t cap_report_scratch = 0;
+
+  // device bytes of the arena's buffers (alloc), for itsu_memory_usage
+  std::unordered_map<const void *, size_t> arena_sizes;
+  int64_t arena_bytes = 0;
+
   std::string error;
 };
 
@@ -197,11 +206,25 @@ void release(T *&p)
   }
 }
 
+// Arena allocation: replaces p by a buffer of count elements and keeps the context's byte count.
 template <typename T>
-cudaError_t alloc(T *&p, int64_t count)
+cudaError_t alloc(itsu_context *ctx, T *&p, int64_t count)
 {
+  if (p) {
+    auto it = ctx->arena_sizes.find((const void *)p);
+    if (it != ctx->arena_sizes.end()) {
+      ctx->arena_bytes -= (int64_t)it->second;
+      ctx->arena_sizes.erase(it);
+    }
+  }
   release(p);
-  return cudaMalloc((void **)&p, (size_t)std::max<int64_t>(count, 1) * sizeof(T));
+  const size_t bytes = (size_t)std::max<int64_t>(count, 1) * sizeof(T);
+  const cudaError_t err = cudaMalloc((void **)&p, bytes);
+  if (err == cudaSuccess) {
+    ctx->arena_sizes[(const void *)p] = bytes;
+    ctx->arena_bytes += (int64_t)bytes;
+  }
+  return err;
 }
 
 Tune current_tune(const itsu_context *ctx)
@@ -294,7 +317,7 @@ itsu_status ensure_partials(itsu_context *ctx)
 {
   const int64_t need = std::max({ctx->cap_clusters, ctx->cap_tracklets, ctx->cap_cells}) / 2048 + 2;
   if (need > ctx->cap_partials) {
-    ITSU_CUDA(ctx, alloc(ctx->scan_partials, need));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->scan_partials, need));
     ctx->cap_partials = need;
     ctx->generation++;
   }
@@ -307,19 +330,19 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     itsu_status st = growth_allowed(ctx, "clusters", n_clusters, ctx->cap_clusters);
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(n_clusters);
-    ITSU_CUDA(ctx, alloc(ctx->raw, cap));
-    ITSU_CUDA(ctx, alloc(ctx->sorted, cap));
-    ITSU_CUDA(ctx, alloc(ctx->tmp, cap));
-    ITSU_CUDA(ctx, alloc(ctx->xyzr, cap));
-    ITSU_CUDA(ctx, alloc(ctx->phi, cap));
-    ITSU_CUDA(ctx, alloc(ctx->trk_count, cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->trk_off, cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->trk_lookup, cap));
-    ITSU_CUDA(ctx, alloc(ctx->zs, cap));
-    ITSU_CUDA(ctx, alloc(ctx->clu_seg, cap));
-    ITSU_CUDA(ctx, alloc(ctx->clu_aux, cap));
-    ITSU_CUDA(ctx, alloc(ctx->clu_crowded, cap));
-    ITSU_CUDA(ctx, alloc(ctx->trk_slots, cap * itsu::kTrackletSlotsPerCluster));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->raw, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->sorted, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->tmp, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->xyzr, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->phi, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->trk_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->trk_off, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->trk_lookup, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->zs, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->clu_seg, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->clu_aux, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->clu_crowded, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->trk_slots, cap * itsu::kTrackletSlotsPerCluster));
     ctx->cap_clusters = cap;
     ctx->generation++;
   }
@@ -327,15 +350,15 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     itsu_status st = growth_allowed(ctx, "events", n_events, ctx->cap_events);
     if (st != ITSU_OK) return st;
     const int32_t cap = n_events + n_events / 4 + 4;
-    ITSU_CUDA(ctx, alloc(ctx->layer_off, (int64_t)cap * ITSU_LAYERS + 1));
-    ITSU_CUDA(ctx, alloc(ctx->vtx, (int64_t)cap * 3));
-    ITSU_CUDA(ctx, alloc(ctx->index_tables, (int64_t)cap * ITSU_TRACKLET_LAYERS * ITSU_INDEX_TABLE_SIZE));
-    ITSU_CUDA(ctx, alloc(ctx->trk_seg, (int64_t)cap * ITSU_TRACKLET_LAYERS + 1));
-    ITSU_CUDA(ctx, alloc(ctx->cell_seg, (int64_t)cap * ITSU_CELL_LAYERS + 1));
-    ITSU_CUDA(ctx, alloc(ctx->road_seg, (int64_t)cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->seg_rrange, (int64_t)cap * ITSU_LAYERS));
-    ITSU_CUDA(ctx, alloc(ctx->seg_regular, (int64_t)cap * ITSU_LAYERS));
-    ITSU_CUDA(ctx, alloc(ctx->raw_off, (int64_t)cap * ITSU_LAYERS));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->layer_off, (int64_t)cap * ITSU_LAYERS + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->vtx, (int64_t)cap * 3));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->index_tables, (int64_t)cap * ITSU_TRACKLET_LAYERS * ITSU_INDEX_TABLE_SIZE));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->trk_seg, (int64_t)cap * ITSU_TRACKLET_LAYERS + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_seg, (int64_t)cap * ITSU_CELL_LAYERS + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->road_seg, (int64_t)cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->seg_rrange, (int64_t)cap * ITSU_LAYERS));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->seg_regular, (int64_t)cap * ITSU_LAYERS));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->raw_off, (int64_t)cap * ITSU_LAYERS));
     ctx->cap_events = cap;
     ctx->generation++;
   }
@@ -348,13 +371,13 @@ itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
     itsu_status st = growth_allowed(ctx, "tracklets", need, ctx->cap_tracklets);
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
-    ITSU_CUDA(ctx, alloc(ctx->tracklets, cap));
-    ITSU_CUDA(ctx, alloc(ctx->trk_seg_id, cap));
-    ITSU_CUDA(ctx, alloc(ctx->cell_count, cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->cell_mask, cap));
-    ITSU_CUDA(ctx, alloc(ctx->cell_off, cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->cell_lookup, cap));
-    ITSU_CUDA(ctx, alloc(ctx->cell_crowded, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->tracklets, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->trk_seg_id, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_mask, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_off, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_lookup, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_crowded, cap));
     ctx->cap_tracklets = cap;
     ctx->generation++;
   }
@@ -377,8 +400,8 @@ itsu_status ensure_cell_entries(itsu_context *ctx, int64_t need)
     itsu_status st = growth_allowed(ctx, "cell entries", need, ctx->cap_cell_entries);
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
-    ITSU_CUDA(ctx, alloc(ctx->cell_entries, cap));
-    ITSU_CUDA(ctx, alloc(ctx->cell_dca, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_entries, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_dca, cap));
     ctx->cap_cell_entries = cap;
     ctx->generation++;
   }
@@ -391,14 +414,14 @@ itsu_status ensure_cells(itsu_context *ctx, int64_t need)
     itsu_status st = growth_allowed(ctx, "cells", need, ctx->cap_cells);
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
-    ITSU_CUDA(ctx, alloc(ctx->cells, cap));
-    ITSU_CUDA(ctx, alloc(ctx->cell_seg_id, cap));
-    ITSU_CUDA(ctx, alloc(ctx->nb_count, cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->nb_off, cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->nb_fill, cap));
-    ITSU_CUDA(ctx, alloc(ctx->paths, cap));
-    ITSU_CUDA(ctx, alloc(ctx->road_count, cap + 1));
-    ITSU_CUDA(ctx, alloc(ctx->road_off, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cells, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_seg_id, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->nb_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->nb_off, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->nb_fill, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->paths, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->road_count, cap + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->road_off, cap + 1));
     ctx->cap_cells = cap;
     ctx->generation++;
   }
@@ -413,7 +436,7 @@ itsu_status ensure_neighbours(itsu_context *ctx, int64_t need)
     itsu_status st = growth_allowed(ctx, "neighbours", need, ctx->cap_neighbours);
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
-    ITSU_CUDA(ctx, alloc(ctx->nb, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->nb, cap));
     ctx->cap_neighbours = cap;
     ctx->generation++;
   }
@@ -426,7 +449,7 @@ itsu_status ensure_roads(itsu_context *ctx, int64_t need)
     itsu_status st = growth_allowed(ctx, "roads", need, ctx->cap_roads);
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
-    ITSU_CUDA(ctx, alloc(ctx->roads, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->roads, cap));
     ctx->cap_roads = cap;
     ctx->generation++;
   }
@@ -840,7 +863,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
   release(ctx->d_master); release(ctx->d_mlp);
-  release(ctx->chunk_off); release(ctx->roads_all); release(ctx->road_off_all); release(ctx->chunk_status);
+  release(ctx->report_scratch); release(ctx->chunk_off); release(ctx->roads_all); release(ctx->road_off_all); release(ctx->chunk_status);
   if (ctx->h_chunk_status) cudaFreeHost(ctx->h_chunk_status);
   if (ctx->h_chunk_off) cudaFreeHost(ctx->h_chunk_off);
   for (cudaEvent_t &e : ctx->chunk_ready) {
@@ -1135,6 +1158,35 @@ itsu_status itsu_batch_roads_device(itsu_context *ctx, const itsu_road **roads, 
   return ITSU_OK;
 }
 
+itsu_status itsu_memory_usage_get(itsu_context *ctx, itsu_memory_usage *out)
+{
+  if (!ctx || !out) return fail(ctx, ITSU_ERR_INVALID, "itsu_memory_usage_get: null argument");
+  std::memset(out, 0, sizeof *out);
+  out->device_bytes = ctx->arena_bytes + (ctx->twin ? ctx->twin->arena_bytes : 0);
+  out->clusters_capacity = ctx->cap_clusters;
+  out->events_capacity = ctx->cap_events;
+  out->capacity[0] = ctx->cap_tracklets;
+  out->capacity[1] = ctx->cap_cells;
+  out->capacity[2] = ctx->cap_neighbours;
+  out->capacity[3] = ctx->cap_roads;
+  for (int k = 0; k < 4; ++k) out->used[k] = ctx->h_status ? ctx->h_status->total[k] : 0;
+  out->cell_entries_capacity = ctx->cap_cell_entries;
+  return ITSU_OK;
+}
+
+itsu_status itsu_batch_road_count(itsu_context *ctx, int64_t *n_roads)
+{
+  itsu_status st;
+  if (!n_roads) return fail(ctx, ITSU_ERR_INVALID, "itsu_batch_road_count: null output");
+  if ((st = require_stage(ctx, kRoads, "itsu_batch_road_count")) != ITSU_OK) return st;
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  int32_t end = 0;
+  ITSU_CUDA(ctx, cudaMemcpyAsync(&end, ctx->road_seg + ctx->n_events, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *n_roads = end;
+  return ITSU_OK;
+}
+
 itsu_status itsu_roads_report(itsu_context *ctx, const itsu_road *roads, const int32_t *run_offsets, const int32_t *run_event,
                               int32_t n_runs, const itsu_label *labels, const int32_t *label_offsets, int32_t n_events,
                               uint8_t *road_class, itsu_report_counts *counts)
@@ -1215,12 +1267,12 @@ itsu_status itsu_roads_report(itsu_context *ctx, const itsu_road *roads, const i
   const size_t o_cls = o_re + align(sizeof(int32_t) * (size_t)n_roads);
   const size_t o_cnt = o_cls + align((size_t)n_roads);
   const size_t total = o_cnt + align(sizeof(itsu_report_counts) * (size_t)n_events);
-  unsigned char *buf = nullptr;
-  ITSU_CUDA(ctx, cudaMalloc((void **)&buf, std::max<size_t>(total, 256)));
-  struct Free {
-    unsigned char *p;
-    ~Free() { cudaFree(p); }
-  } free_buf{buf};
+  // the scratch stays with the context (grown when a call needs more)
+  if ((int64_t)total > ctx->cap_report_scratch) {
+    ITSU_CUDA(ctx, alloc(ctx, ctx->report_scratch, grow_to((int64_t)total)));
+    ctx->cap_report_scratch = grow_to((int64_t)total);
+  }
+  unsigned char *buf = ctx->report_scratch;
   itsu::ReportArgs r{};
   r.roads = resident ? ctx->roads : reinterpret_cast<itsu_road *>(buf + o_roads);
   r.n_roads = n_roads;
@@ -1279,7 +1331,7 @@ itsu_status grow_buffer(itsu_context *ctx, T *&p, int64_t &cap, int64_t need)
 {
   if (need > cap) {
     const int64_t c = grow_to(need);
-    ITSU_CUDA(ctx, alloc(p, c));
+    ITSU_CUDA(ctx, alloc(ctx, p, c));
     cap = c;
   }
   return ITSU_OK;

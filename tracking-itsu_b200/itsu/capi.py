@@ -71,6 +71,11 @@ class Tune(ctypes.Structure):
                 ("prune", ctypes.c_int32), ("ms", ctypes.c_float), ("reserved_", ctypes.c_int32)]
 
 
+class MemoryUsage(ctypes.Structure):
+    _fields_ = [("device_bytes", ctypes.c_int64), ("clusters_capacity", ctypes.c_int64), ("events_capacity", ctypes.c_int64),
+                ("capacity", ctypes.c_int64 * 4), ("used", ctypes.c_int64 * 4), ("cell_entries_capacity", ctypes.c_int64)]
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("clusters", ctypes.c_void_p), ("layer_offsets", ctypes.c_void_p), ("vertices", ctypes.c_void_p),
                 ("n_events", ctypes.c_int32), ("reserved_", ctypes.c_int32), ("n_clusters", ctypes.c_int64)]
@@ -144,6 +149,8 @@ SIGNATURES = [
     ("itsu_frames_run_host", ctypes.c_int,
      [ctypes.c_void_p, ctypes.POINTER(Frames), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     ("itsu_relaunch", ctypes.c_int, [ctypes.c_void_p]),
+    ("itsu_memory_usage_get", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MemoryUsage)]),
+    ("itsu_batch_road_count", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     ("itsu_roads_report", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
@@ -334,6 +341,15 @@ class Context:
         return roads
 
     # ---- batches ----
+    def memory_usage(self) -> dict:
+        """itsu_memory_usage_get: arena bytes, capacities and the last run's totals."""
+        m = MemoryUsage()
+        self._check(self.lib.itsu_memory_usage_get(self.h, ctypes.byref(m)))
+        names = ("tracklets", "cells", "neighbours", "roads")
+        return dict(device_bytes=m.device_bytes, clusters_capacity=m.clusters_capacity, events_capacity=m.events_capacity,
+                    capacity=dict(zip(names, list(m.capacity))), used=dict(zip(names, list(m.used))),
+                    cell_entries_capacity=m.cell_entries_capacity)
+
     def roads_report(self, label_maps, roads=None, run_offsets=None, run_event=None, n_runs=None):
         """itsu_roads_report: the road classes (ITSU_ROAD_*: 0 unreported, 1 correct, 2 duplicate,
         3 fake) and per-event counts (labels, correct, duplicate, fake) of IOUtils::writeRoadsReport.
@@ -355,7 +371,9 @@ class Context:
         else:
             if n_runs is None:
                 raise ValueError("n_runs is required for the device-resident roads")
-            n_roads = sum(self.counts(r).roads for r in range(n_runs))
+            n = ctypes.c_int64()
+            self._check(self.lib.itsu_batch_road_count(self.h, ctypes.byref(n)))
+            n_roads = n.value
         rev = None if run_event is None else np.ascontiguousarray(run_event, np.int32)
         cls = np.zeros(max(n_roads, 1), np.uint8)
         counts = np.zeros(max(n_events, 1), REPORT_COUNTS_DTYPE)

@@ -6,7 +6,8 @@ Same formats and semantics as the reference's tools:
   write_roads_report     IOUtils::writeRoadsReport (src/CA/IOUtils.cxx:125-170), from the road
                          classes the library computes on the device (itsu_roads_report)
   merge_pileup           mergeEvents / mergeLabels of benchmarks/scripts/root/generatePileUpData.cxx
-The writers of the two input formats are itsu.gen.write_reference_events / _labels.
+  read_binary_events     the binary event format of itsu.gen.write_binary_events (no parsing)
+The writers of the input formats are itsu.gen.write_reference_events / _labels / write_binary_events.
 """
 from __future__ import annotations
 
@@ -108,6 +109,45 @@ def read_reference_events(path: str) -> list:
             a["mc"] = cols[5]
             arrays.append(a)
         events.append(gen.Event(vertices=v, layers=arrays, labels=np.zeros(0, gen.LABEL_DTYPE)))
+    return events
+
+
+BINARY_MAGIC = b"ITSUEVT1"
+_BINARY_RECORD = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("alpha", "<f4"), ("mc", "<i4")])
+
+
+def read_binary_events(path: str) -> list:
+    """The binary event file written by itsu.gen.write_binary_events (and read by the reference
+    harness): the events of the text format without parsing, cluster ids implied by order as in
+    loadEventData. A fast loader for large samples; read_reference_events(f) and
+    read_binary_events(g) give the same events when g was written from f's events."""
+    buf = np.fromfile(path, np.uint8)
+    if buf[:8].tobytes() != BINARY_MAGIC:
+        raise ValueError("%s: not an ITSUEVT1 file" % path)
+    pos = 8
+
+    def take(dtype, count):
+        nonlocal pos
+        a = np.frombuffer(buf, dtype, count, pos)
+        pos += a.nbytes
+        return a
+
+    n_events = int(take(np.int32, 1)[0])
+    events = []
+    for _ in range(n_events):
+        nv = int(take(np.int32, 1)[0])
+        vertices = take(np.float32, 3 * nv).reshape(nv, 3).copy()
+        counts = take(np.int32, gen.LAYERS)
+        layers, next_id = [], 0
+        for n in counts:
+            r = take(_BINARY_RECORD, int(n))
+            a = np.zeros(int(n), gen.CLUSTER_DTYPE)
+            for k in ("x", "y", "z", "alpha", "mc"):
+                a[k] = r[k]
+            a["id"] = np.arange(next_id, next_id + int(n), dtype=np.int32)
+            next_id += int(n)
+            layers.append(a)
+        events.append(gen.Event(vertices=vertices, layers=layers, labels=np.zeros(0, gen.LABEL_DTYPE)))
     return events
 
 
@@ -239,3 +279,64 @@ def merge_pileup(pile_up: int, input_folder: str, output_folder: str = None) -> 
     output_folder = input_folder if output_folder is None else output_folder
     _merge(pile_up, os.path.join(input_folder, "data.txt"), os.path.join(output_folder, "merged_data.txt"), 10, 8, False)
     _merge(pile_up, os.path.join(input_folder, "labels.txt"), os.path.join(output_folder, "merged_labels.txt"), 6, 0, True)
+
+
+# ---- memory occupancy (Tracker::clustersToTracksMemoryBenchmark, src/CA/Tracker.cxx:304-363) ----
+
+# Constants::Memory (include/ITSReconstruction/CA/Constants.h:87-92): the reference's preallocation
+# coefficients, reserve = ceil(coefficient * N_L * N_L+1 (* N_L+2 for cells)) in binary32
+TRACKLETS_MEMORY_COEFFICIENTS = np.array([0.0016353, 0.0013627, 0.000984, 0.00078135, 0.00057934, 0.00052217], np.float32)
+CELLS_MEMORY_COEFFICIENTS = np.array([2.3208e-08, 2.104e-08, 1.6432e-08, 1.2412e-08, 1.3543e-08], np.float32)
+
+
+def _reserve(capacity: int, size_f: np.float32) -> int:
+    """`if (size > v.capacity()) v.reserve(size)` with a float size (PrimaryVertexContext.cxx:60-64,
+    125-130): the comparison in binary32, reserve() of the truncated value."""
+    return int(size_f) if size_f > np.float32(capacity) else capacity
+
+
+def _grow(capacity: int, size: int) -> int:
+    """The capacity after `size` emplace_backs into a cleared vector (libstdc++: a full vector of n
+    elements reallocates to n + max(n, 1))."""
+    while capacity < size:
+        capacity = capacity + max(capacity, 1)
+    return capacity
+
+
+class MemoryModel:
+    """The reference tracker's per-layer vectors (tracklets, cells) across the vertices it runs:
+    cleared and reserved from the coefficients at each initialize, grown by push_back, never
+    shrunk. run() takes one vertex's counts and returns its MemoryOccupancy.txt lines (the CPU
+    build's six lines)."""
+
+    def __init__(self):
+        self.trk_cap = [0] * (gen.LAYERS - 1)
+        self.cell_cap = [0] * 5
+
+    def run(self, n, t, c, roads: int) -> str:
+        n = [int(x) for x in n]
+        nf = [np.float32(x) for x in n]
+        for l in range(5):
+            size = np.float32(np.ceil(np.float32(np.float32(CELLS_MEMORY_COEFFICIENTS[l] * nf[l]) * nf[l + 1]) * nf[l + 2]))
+            self.cell_cap[l] = _reserve(self.cell_cap[l], size)
+        for l in range(gen.LAYERS - 1):
+            size = np.float32(np.ceil(np.float32(TRACKLETS_MEMORY_COEFFICIENTS[l] * nf[l]) * nf[l + 1]))
+            self.trk_cap[l] = _reserve(self.trk_cap[l], size)
+        lines = ["".join("%d\t" % x for x in n), "".join("%d\t" % x for x in self.trk_cap)]
+        for l in range(gen.LAYERS - 1):
+            self.trk_cap[l] = _grow(self.trk_cap[l], int(t[l]))
+        lines += ["".join("%d\t" % int(x) for x in t), "".join("%d\t" % x for x in self.cell_cap)]
+        for l in range(5):
+            self.cell_cap[l] = _grow(self.cell_cap[l], int(c[l]))
+        lines += ["".join("%d\t" % int(x) for x in c), "%d" % int(roads)]
+        return "\n".join(lines) + "\n"
+
+
+def memory_occupancy(warmup_runs, runs) -> str:
+    """MemoryOccupancy.txt as the reference's MEMORY_BENCHMARK build writes it (main.cpp:67-70,
+    85-86): the warm-up event's vertices first (not written), then one six-line block per vertex.
+    Each run is (clusters[7], tracklets[6], cells[5], roads), e.g. from itsu_get_counts."""
+    model = MemoryModel()
+    for n, t, c, r in warmup_runs:
+        model.run(n, t, c, r)
+    return "".join(model.run(n, t, c, r) for n, t, c, r in runs)
