@@ -86,6 +86,22 @@ def test_jet_event_crowded_paths_match_oracle(ctx):
         assert np.array_equal(roads[road_off[e]:road_off[e + 1]].view(np.uint8), exp["roads"].view(np.uint8))
 
 
+def test_bins_above_128_clusters_match_oracle(ctx):
+    """A 150-track jet puts about 150 clusters into one index-table bin on every layer: the
+    tracklet walk's pruned columns then need the four-word pass mask (layers of smaller bins use
+    one or two words). Stage by stage and batched beside a Pb-Pb event."""
+    jet = gen.jet_event(3, 150)
+    want = oracle.run_vertex(jet.layers, jet.vertices[0])
+    largest = [int(np.bincount(c["bin"][(c["bin"] >= 0) & (c["bin"] < 400)], minlength=400).max()) for c in want["clusters"][1:]]
+    assert min(largest) > 128
+    _assert_same(ctx.run_vertex(jet.layers, jet.vertices[0]), want, "dense jet stages")
+    bg = gen.pbpb_event(5)
+    clusters, offsets, vertices = gen.pack_batch([jet, bg])
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    _assert_same(ctx.results(0), want, "dense jet batched")
+    _assert_same(ctx.results(1), oracle.run_vertex(bg.layers, bg.vertices[0]), "Pb-Pb beside the jet")
+
+
 def test_pileup_frame_matches_oracle(ctx):
     ev = gen.pileup_frame(7)
     clusters, offsets, vertices = gen.pack_batch([ev] * 5, list(range(5)))

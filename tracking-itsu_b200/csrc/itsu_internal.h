@@ -95,7 +95,7 @@ struct Arena {
   // per (event, layer) the r range of its clusters and whether all its bins are regular
   float4 *zs;  // (z, r, phi, sorted index as int bits)
   float2 *seg_rrange;
-  int32_t *seg_regular;
+  int32_t *seg_regular;  // per segment: 0 if not regular, else the pass-mask words its largest bin needs
   int32_t prune_tracklets;  // use the index (tuning knob; results are identical either way)
   // tracklets
   int32_t *trk_count;

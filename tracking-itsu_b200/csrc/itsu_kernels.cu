@@ -39,8 +39,9 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr float kMaxAbsCoordinate = 1.0e6f;
-constexpr int kMaxPruneBin = 64;  // larger bins disable pruning for their layer
-static_assert(kMaxPruneBin <= 64, "a pruned column's passes are a 64-bit mask");
+constexpr int kMaxPruneBin = 256;  // larger bins disable pruning for their layer
+constexpr int kPruneWords = kMaxPruneBin / 64;  // a pruned column's passes: a mask of this many 64-bit words
+static_assert(kMaxPruneBin % 64 == 0, "a pruned column's passes are whole 64-bit words");
 static_assert(sizeof(itsu_tracklet) == 16 && offsetof(itsu_tracklet, tan_lambda) == 8 && offsetof(itsu_tracklet, phi) == 12,
               "the cell count pass reads (tanL, phi) as the second 8 bytes of a tracklet");
 
@@ -518,10 +519,12 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   }
   __shared__ int s_irregular;
   __shared__ int s_rmin, s_rmax;  // float bits; r >= 0 orders like its bits
+  __shared__ int s_largest;       // the largest bin
   if (tid == 0) {
     s_irregular = m > 0 || bucket_total[kBuckets - 1] > 0;  // negative bins or bin 400
     s_rmin = 0x7f800000;
     s_rmax = 0;
+    s_largest = 0;
   }
   __syncthreads();
   int irregular = 0, rmin = 0x7f800000, rmax = 0;
@@ -538,45 +541,42 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   }
   atomicMin(&s_rmin, rmin);
   atomicMax(&s_rmax, rmax);
+  int largest = 0;
   for (int b = tid; b < kTableBins; b += kSortThreads) {
-    if (bucket_total[b + 1] > kMaxPruneBin) {
-      atomicOr(&s_irregular, 1);
-    }
+    largest = max(largest, bucket_total[b + 1]);
   }
+  if (largest > kMaxPruneBin) {
+    atomicOr(&s_irregular, 1);
+  }
+  atomicMax(&s_largest, largest);
   // each cluster's rank in its bin by (z, sorted index): a warp per bin of at most kMaxPruneBin
-  // (64) clusters, two per lane, their z values passed round the warp
+  // (256) clusters, the bin's z values staged in the warp's record stage (free in this pass)
+  static_assert(kMaxPruneBin <= 32 * kClusterWords, "a bin's z values fit a warp's stage");
+  float *zstage = reinterpret_cast<float *>(stage);
   for (int bin = warp; bin < kTableBins; bin += kSortWarps) {
     const int st = bucket_base[bin + 1], cnt = bucket_total[bin + 1];
     if (cnt == 0 || cnt > kMaxPruneBin) {
       continue;  // warp-uniform
     }
-    const int k0 = lane, k1 = lane + 32;
-    float4 c0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), c1 = c0;
-    float phi0 = 0.0f, phi1 = 0.0f;
-    if (k0 < cnt) {
-      c0 = a.xyzr[begin + st + k0];
-      phi0 = a.phi[begin + st + k0];
+    for (int k = lane; k < cnt; k += 32) {
+      zstage[k] = a.xyzr[begin + st + k].z;
     }
-    if (k1 < cnt) {
-      c1 = a.xyzr[begin + st + k1];
-      phi1 = a.phi[begin + st + k1];
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+      const float4 c = a.xyzr[begin + st + k];
+      int rank = 0;
+      for (int j = 0; j < cnt; ++j) {
+        const float zj = zstage[j];
+        rank += zj < c.z || (zj == c.z && j < k);
+      }
+      a.zs[begin + st + rank] = make_float4(c.z, c.w, a.phi[begin + st + k], __int_as_float(st + k));
     }
-    int rank0 = 0, rank1 = 0;
-    for (int j = 0; j < cnt; ++j) {
-      const float zj = __shfl_sync(0xffffffffu, j < 32 ? c0.z : c1.z, j & 31);
-      rank0 += zj < c0.z || (zj == c0.z && j < k0);
-      rank1 += zj < c1.z || (zj == c1.z && j < k1);
-    }
-    if (k0 < cnt) {
-      a.zs[begin + st + rank0] = make_float4(c0.z, c0.w, phi0, __int_as_float(st + k0));
-    }
-    if (k1 < cnt) {
-      a.zs[begin + st + rank1] = make_float4(c1.z, c1.w, phi1, __int_as_float(st + k1));
-    }
+    __syncwarp();  // the stage is refilled for the warp's next bin
   }
   __syncthreads();
   if (tid == 0) {
-    a.seg_regular[seg] = !s_irregular;
+    // 0: not regular; else the 64-bit words of a pass mask over its largest bin (1, 2 or 4)
+    a.seg_regular[seg] = s_irregular ? 0 : (s_largest <= 64 ? 1 : (s_largest <= 128 ? 2 : kPruneWords));
     a.seg_rrange[seg] = make_float2(__int_as_float(s_rmin), __int_as_float(s_rmax));
   }
 }
@@ -650,10 +650,11 @@ struct TrackletProbe {
   }
 };
 
-template <typename OnPass>
+template <int kWords, typename OnPass>
 __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next, int4 rect, int layer, const TrackletProbe &probe,
                                                 bool prune, float zlo, float zhi, const float4 *zs, OnPass &&on_pass)
 {
+  static_assert(kWords >= 1 && kWords <= kPruneWords, "mask words");
   int phi_bins = rect.w - rect.y + 1;
   if (phi_bins < 0) {
     phi_bins += kPhiBins;
@@ -677,22 +678,35 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
             hi = mid;
           }
         }
-        // a pruned column holds at most kMaxPruneBin (64) clusters: its passes as a mask over
-        // their positions in the column, emitted in index order
-        unsigned long long hit = 0ull;
+        // a pruned column holds at most 64 * kWords clusters (the layer's largest bin chose
+        // kWords): its passes as a mask over their positions in the column, in registers,
+        // emitted in index order
+        unsigned long long hit[kWords];
+#pragma unroll
+        for (int w = 0; w < kWords; ++w) {
+          hit[w] = 0ull;
+        }
         for (int k = lo; k < k1; ++k) {
           const float4 q = zs[k];  // z, r, phi and the sorted index of the k-th cluster by z
           if (!(q.x <= zhi)) {
             break;
           }
           if (probe.pass(q.x, q.y, q.z)) {
-            hit |= 1ull << (__float_as_int(q.w) - k0);
+            const int pos = __float_as_int(q.w) - k0;
+            const unsigned long long bit = 1ull << (pos & 63);
+#pragma unroll
+            for (int w = 0; w < kWords; ++w) {
+              hit[w] |= (pos >> 6) == w ? bit : 0ull;
+            }
           }
         }
-        while (hit) {
-          const int b = __ffsll((long long)hit) - 1;
-          hit &= hit - 1ull;
-          on_pass(k0 + b);
+#pragma unroll
+        for (int w = 0; w < kWords; ++w) {
+          while (hit[w]) {
+            const int b = __ffsll((long long)hit[w]) - 1;
+            hit[w] &= hit[w] - 1ull;
+            on_pass(k0 + 64 * w + b);
+          }
         }
       }
       const int x = table[max_bin];  // the inclusive bound's candidate (P1: inside the layer)
@@ -719,6 +733,7 @@ struct InnerCluster {
   int4 rect;
   TrackletProbe probe;
   bool prune;
+  int words;
   float zlo, zhi;
   const int32_t *table;
   int n_next;
@@ -751,7 +766,8 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
   s.probe.phi = a.phi + s.next_begin;
   s.probe.max_dz = kC.trk_max_dz[s.layer];
   const int next_seg = s.seg + 1;
-  s.prune = a.prune_tracklets && a.seg_regular[next_seg] != 0;
+  s.words = a.seg_regular[next_seg];  // 0: not regular, else the mask words its largest bin needs
+  s.prune = a.prune_tracklets && s.words != 0;
   s.zlo = s.zhi = 0;
   if (s.prune) {
     const float2 rr = a.seg_rrange[next_seg];
@@ -769,7 +785,14 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
 template <typename OnPass>
 __device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s, OnPass &&on_pass)
 {
-  walk_candidates(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, a.zs + s.next_begin, on_pass);
+  const float4 *zs = a.zs + s.next_begin;
+  if (s.words <= 1) {  // unpruned, or bins of at most 64 clusters
+    walk_candidates<1>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, on_pass);
+  } else if (s.words == 2) {
+    walk_candidates<2>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, on_pass);
+  } else {
+    walk_candidates<kPruneWords>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, on_pass);
+  }
 }
 
 // Count pass, one thread per inner cluster: the number of tracklets, and the outer clusters of
