@@ -660,7 +660,8 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
     phi_bins += kPhiBins;
   }
   const int zb_lo = prune ? max(rect.x, z_bin_index(layer + 1, zlo)) : 0;
-  const int zb_hi = prune ? min(rect.z, z_bin_index(layer + 1, zhi)) : -1;
+  const int zb_top = prune ? z_bin_index(layer + 1, zhi) : 0;  // clusters of higher z bins have z > zhi
+  const int zb_hi = prune ? min(rect.z, zb_top) : -1;
   for (int phi_bin = rect.y, phi_count = 0; phi_count < phi_bins;
        phi_bin = (phi_bin + 1 == kPhiBins) ? 0 : phi_bin + 1, ++phi_count) {
     const int first_bin = bin_index(rect.x, phi_bin);
@@ -709,8 +710,13 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
           }
         }
       }
-      const int x = table[max_bin];  // the inclusive bound's candidate (P1: inside the layer)
-      if (x < n_next && probe.pass(x)) {
+      // The inclusive bound's candidate (P1: inside the layer): the first cluster of bin
+      // max_bin, the row's next z column. When that bin is not empty and its z column lies
+      // beyond zhi's (z bins are monotone in z; a regular layer's clusters sit in exactly their
+      // bins), the candidate's z exceeds zhi and it fails the Δz cut: it is not read.
+      const int x = table[max_bin];
+      const bool beyond = rect.z + 1 < kZBins && rect.z + 1 > zb_top && table[max_bin + 1] > x;
+      if (!beyond && x < n_next && probe.pass(x)) {
         on_pass(x);
       }
     } else {
