@@ -627,8 +627,10 @@ itsu_status stage_count_then_write(itsu_context *ctx, void (*count)(const Arena 
   itsu_status st;
   for (int attempt = 0;; ++attempt) {
     if ((st = clear_flags(ctx)) != ITSU_OK) return st;
-    // the entry reservation and the crowded lists start empty for every count (also a retry)
+    // the entry reservation, the crowded lists and the cells scan's tile sums (added to by the
+    // cell count pass) start empty for every count, also a retry
     ITSU_CUDA(ctx, cudaMemsetAsync(&ctx->d_status->cell_entries, 0, 3 * sizeof(int64_t), ctx->stream));
+    ITSU_CUDA(ctx, cudaMemsetAsync(ctx->scan_partials, 0, sizeof(int64_t) * ctx->cap_partials, ctx->stream));
     count(arena_of(ctx), launch_of(ctx));
     if ((st = check_launch(ctx)) != ITSU_OK) return st;
     if ((st = sync_status(ctx)) != ITSU_OK) return st;

@@ -941,6 +941,13 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_crowded(Arena a)
 // trk_seg[6e+L] = first tracklet of (e, L); capacity check of the tracklet total.
 __global__ void k_tracklet_segments(Arena a)
 {
+  // the cells scan's tile sums start at zero: the cell count pass adds each warp's cells there
+  const int64_t n_trk = a.status->total[kTracklets];
+  if (n_trk <= a.cap_tracklets) {
+    for (int64_t t = global_thread(); t < (n_trk + kScanTile - 1) / kScanTile; t += grid_threads()) {
+      a.scan_partials[t] = 0;
+    }
+  }
   const int nseg = a.n_events * ITSU_TRACKLET_LAYERS;
   for (int s = (int)global_thread(); s <= nseg; s += grid_threads()) {
     if (s == nseg) {
@@ -1155,6 +1162,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
                  cell_geometry(s.layer, s.c1, s.c2, a.xyzr[s.c3_base + t2.second_cluster], s.vx, s.vy, normal, curvature);
       }
     }
+    // the warp's 32 tracklets lie in one scan tile: their cells go to its sum (the cells scan
+    // has no reduce pass)
+    const int batch_cells = (int)__reduce_add_sync(0xffffffffu, (unsigned)count);
+    if (lane == 0 && batch_cells != 0) {
+      atomicAdd(reinterpret_cast<unsigned long long *>(&a.scan_partials[base / kScanTile]), (unsigned long long)batch_cells);
+    }
     if (s.k < n) {
       a.cell_count[s.k] = count;
       a.cell_mask[s.k] = big ? 0ull : masks[warp][lane];
@@ -1224,6 +1237,7 @@ __global__ void __launch_bounds__(kPrefilterThreads) k_cells_prefilter(Arena a)
     if (h.x >= 0 && logit < mlp.threshold) {
       atomicAnd(&a.cell_mask[h.x], ~(1ull << h.y));
       atomicSub(&a.cell_count[h.x], 1);
+      atomicAdd(reinterpret_cast<unsigned long long *>(&a.scan_partials[h.x / kScanTile]), ~0ull);  // its tile sum - 1
     }
     __syncwarp();
   }
@@ -1647,28 +1661,27 @@ const KernelStep kSteps[] = {
     {"tracklets_crowded", step_tracklets_crowded},       // 8
     {"cells_count", step_cells_count},                   // 9  (c)
     {"cells_prefilter", step_cells_prefilter, true},     // 10 (learned form only)
-    {"scan_reduce_cells", step_scan_reduce<1>},          // 11
-    {"scan_partials_cells", step_scan_partials<1>},      // 12
-    {"scan_apply_cells", step_scan_apply<1>},            // 13
-    {"cell_segments", step_cell_segments},               // 14
-    {"cells_scatter", step_cells_scatter},               // 15
-    {"cells_crowded", step_cells_crowded},               // 16
-    {"neighbour_reset", step_neighbour_reset},           // 17 (d)
-    {"neighbours_count", step_neighbours<false>},        // 18
-    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 19
-    {"scan_partials_neighbours", step_scan_partials<2>}, // 20
-    {"scan_apply_neighbours", step_scan_apply<2>},       // 21
-    {"neighbour_check", step_neighbour_check},           // 22
-    {"neighbours_write", step_neighbours<true>},         // 23
-    {"levels_1", step_levels<1>},                        // 24
-    {"levels_2", step_levels<2>},                        // 25
-    {"levels_3", step_levels<3>},                        // 26
-    {"levels_4", step_levels<4>},                        // 27
-    {"scan_reduce_roads", step_scan_reduce<3>},          // 28 (e)
-    {"scan_partials_roads", step_scan_partials<3>},      // 29
-    {"scan_apply_roads", step_scan_apply<3>},            // 30
-    {"road_segments", step_road_segments},               // 31
-    {"roads_write", step_roads},                         // 32
+    {"scan_partials_cells", step_scan_partials<1>},      // 11
+    {"scan_apply_cells", step_scan_apply<1>},            // 12
+    {"cell_segments", step_cell_segments},               // 13
+    {"cells_scatter", step_cells_scatter},               // 14
+    {"cells_crowded", step_cells_crowded},               // 15
+    {"neighbour_reset", step_neighbour_reset},           // 16 (d)
+    {"neighbours_count", step_neighbours<false>},        // 17
+    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 18
+    {"scan_partials_neighbours", step_scan_partials<2>}, // 19
+    {"scan_apply_neighbours", step_scan_apply<2>},       // 20
+    {"neighbour_check", step_neighbour_check},           // 21
+    {"neighbours_write", step_neighbours<true>},         // 22
+    {"levels_1", step_levels<1>},                        // 23
+    {"levels_2", step_levels<2>},                        // 24
+    {"levels_3", step_levels<3>},                        // 25
+    {"levels_4", step_levels<4>},                        // 26
+    {"scan_reduce_roads", step_scan_reduce<3>},          // 27 (e)
+    {"scan_partials_roads", step_scan_partials<3>},      // 28
+    {"scan_apply_roads", step_scan_apply<3>},            // 29
+    {"road_segments", step_road_segments},               // 30
+    {"roads_write", step_roads},                         // 31
 };
 constexpr int kNumSteps = sizeof(kSteps) / sizeof(kSteps[0]);
 
@@ -1729,12 +1742,12 @@ void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l)
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
 void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 14, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 16, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(17, 22, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(23, 27, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(28, 31, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(32, 32, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 13, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 15, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
 
 int kernels_per_run()
 {
