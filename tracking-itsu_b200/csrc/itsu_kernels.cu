@@ -53,8 +53,19 @@ __device__ __forceinline__ int64_t global_thread() { return (int64_t)blockIdx.x 
 // ------------------------------------------------------------------------------------------
 // status
 
-__global__ void k_status_init(DevStatus *s)
+// Status reset of a run; the tracklet scan's tile sums start at zero too (the tracklet count
+// pass adds each warp's tracklets to them).
+__global__ void k_status_init(Arena a)
 {
+  if (a.scan_partials) {
+    for (int64_t t = global_thread(); t < (a.n_clusters + kScanTile - 1) / kScanTile; t += grid_threads()) {
+      a.scan_partials[t] = 0;
+    }
+  }
+  if (global_thread() != 0) {
+    return;
+  }
+  DevStatus *s = a.status;
   s->flags = 0;
   s->invalid_index = INT_MAX;
   s->invalid_event = INT_MAX;
@@ -806,18 +817,27 @@ __device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s
 __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
 {
   const int64_t i = global_thread();
-  if (i >= a.n_clusters) {
-    return;
-  }
-  const InnerCluster s = inner_cluster(a, i);
+  const bool valid = i < a.n_clusters;
   int count = 0;
-  if (s.walk) {
-    walk_inner(a, s, [&](int j) {
-      if (count < kTrackletSlots) {
-        a.trk_slots[count * a.slot_stride + i] = j;
-      }
-      ++count;
-    });
+  if (valid) {
+    const InnerCluster s = inner_cluster(a, i);
+    if (s.walk) {
+      walk_inner(a, s, [&](int j) {
+        if (count < kTrackletSlots) {
+          a.trk_slots[count * a.slot_stride + i] = j;
+        }
+        ++count;
+      });
+    }
+  }
+  // the warp's 32 clusters lie in one scan tile: their tracklets go to its sum (the tracklet
+  // scan has no reduce pass)
+  const int warp_count = (int)__reduce_add_sync(0xffffffffu, (unsigned)count);
+  if ((threadIdx.x & 31) == 0 && warp_count != 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&a.scan_partials[i / kScanTile]), (unsigned long long)warp_count);
+  }
+  if (!valid) {
+    return;
   }
   a.trk_count[i] = count;
   if (count > kTrackletSlots) {  // rare: the write pass leaves this cluster to k_tracklets_crowded
@@ -1580,7 +1600,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_roads(Arena a)
 // block size so that the number of resident threads stays comparable.
 int fixed_grid(const Launch &l) { return l.num_sms * l.blocks_per_sm; }
 
-void step_status_init(const Arena &a, const Launch &l) { k_status_init<<<1, 1, 0, l.stream>>>(a.status); }
+void step_status_init(const Arena &a, const Launch &l)
+{
+  const int64_t tiles = (a.n_clusters + kScanTile - 1) / kScanTile;
+  const int64_t blocks = a.scan_partials ? std::min<int64_t>((tiles + kThreads - 1) / kThreads, l.num_sms) : 0;
+  k_status_init<<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, 0, l.stream>>>(a);
+}
 
 void step_cluster_sort(const Arena &a, const Launch &l)
 {
@@ -1653,35 +1678,34 @@ const KernelStep kSteps[] = {
     {"status_init", step_status_init},                   // 0
     {"cluster_sort", step_cluster_sort},                 // 1  (a)
     {"tracklets_count", step_tracklets_count},           // 2  (b)
-    {"scan_reduce_tracklets", step_scan_reduce<0>},      // 3
-    {"scan_partials_tracklets", step_scan_partials<0>},  // 4
-    {"scan_apply_tracklets", step_scan_apply<0>},        // 5
-    {"tracklet_segments", step_tracklet_segments},       // 6
-    {"tracklets_write", step_tracklets_write},           // 7
-    {"tracklets_crowded", step_tracklets_crowded},       // 8
-    {"cells_count", step_cells_count},                   // 9  (c)
-    {"cells_prefilter", step_cells_prefilter, true},     // 10 (learned form only)
-    {"scan_partials_cells", step_scan_partials<1>},      // 11
-    {"scan_apply_cells", step_scan_apply<1>},            // 12
-    {"cell_segments", step_cell_segments},               // 13
-    {"cells_scatter", step_cells_scatter},               // 14
-    {"cells_crowded", step_cells_crowded},               // 15
-    {"neighbour_reset", step_neighbour_reset},           // 16 (d)
-    {"neighbours_count", step_neighbours<false>},        // 17
-    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 18
-    {"scan_partials_neighbours", step_scan_partials<2>}, // 19
-    {"scan_apply_neighbours", step_scan_apply<2>},       // 20
-    {"neighbour_check", step_neighbour_check},           // 21
-    {"neighbours_write", step_neighbours<true>},         // 22
-    {"levels_1", step_levels<1>},                        // 23
-    {"levels_2", step_levels<2>},                        // 24
-    {"levels_3", step_levels<3>},                        // 25
-    {"levels_4", step_levels<4>},                        // 26
-    {"scan_reduce_roads", step_scan_reduce<3>},          // 27 (e)
-    {"scan_partials_roads", step_scan_partials<3>},      // 28
-    {"scan_apply_roads", step_scan_apply<3>},            // 29
-    {"road_segments", step_road_segments},               // 30
-    {"roads_write", step_roads},                         // 31
+    {"scan_partials_tracklets", step_scan_partials<0>},  // 3
+    {"scan_apply_tracklets", step_scan_apply<0>},        // 4
+    {"tracklet_segments", step_tracklet_segments},       // 5
+    {"tracklets_write", step_tracklets_write},           // 6
+    {"tracklets_crowded", step_tracklets_crowded},       // 7
+    {"cells_count", step_cells_count},                   // 8  (c)
+    {"cells_prefilter", step_cells_prefilter, true},     // 9 (learned form only)
+    {"scan_partials_cells", step_scan_partials<1>},      // 10
+    {"scan_apply_cells", step_scan_apply<1>},            // 11
+    {"cell_segments", step_cell_segments},               // 12
+    {"cells_scatter", step_cells_scatter},               // 13
+    {"cells_crowded", step_cells_crowded},               // 14
+    {"neighbour_reset", step_neighbour_reset},           // 15 (d)
+    {"neighbours_count", step_neighbours<false>},        // 16
+    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 17
+    {"scan_partials_neighbours", step_scan_partials<2>}, // 18
+    {"scan_apply_neighbours", step_scan_apply<2>},       // 19
+    {"neighbour_check", step_neighbour_check},           // 20
+    {"neighbours_write", step_neighbours<true>},         // 21
+    {"levels_1", step_levels<1>},                        // 22
+    {"levels_2", step_levels<2>},                        // 23
+    {"levels_3", step_levels<3>},                        // 24
+    {"levels_4", step_levels<4>},                        // 25
+    {"scan_reduce_roads", step_scan_reduce<3>},          // 26 (e)
+    {"scan_partials_roads", step_scan_partials<3>},      // 27
+    {"scan_apply_roads", step_scan_apply<3>},            // 28
+    {"road_segments", step_road_segments},               // 29
+    {"roads_write", step_roads},                         // 30
 };
 constexpr int kNumSteps = sizeof(kSteps) / sizeof(kSteps[0]);
 
@@ -1740,14 +1764,14 @@ const KernelStep *pipeline_steps(int *count)
 
 void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l); }
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
-void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
-void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 13, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 15, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
+void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 5, a, l); }
+void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(6, 7, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(8, 12, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(13, 14, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(15, 20, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(21, 25, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(26, 29, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(30, 30, a, l); }
 
 int kernels_per_run()
 {
