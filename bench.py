@@ -157,19 +157,23 @@ def algorithmic_bytes(counts) -> dict:
     return b
 
 
-# kernel -> stage whose compulsory bytes it moves
-KERNEL_STAGE = {
-    "cluster_sort": "cluster_sort",
-    "tracklets_count": "tracklets",
-    "tracklets_write": "tracklets",
-    "tracklets_crowded": "tracklets",
-    "cells_count": "cells",
-    "cells_scatter": "cells",
-    "cells_crowded": "cells",
-    "neighbours_count": "neighbours",
-    "neighbours_write": "neighbours",
-    "roads_write": "roads",
-}
+def kernel_bytes(counts) -> dict:
+    """Each main kernel's own share of the compulsory bytes (the stage sums above split by which
+    kernel reads or writes each object): the tracklet count pass reads both layers' clusters, the
+    tracklet write pass writes the tracklets and their lookup table, the cell count pass reads the
+    tracklets of both layers and the three layers' clusters, the cell scatter writes the cells and
+    their lookup table."""
+    N, T, C = counts["N"], counts["T"], counts["C"]
+    b = algorithmic_bytes(counts)
+    return {
+        "cluster_sort": b["cluster_sort"],
+        "tracklets_count": sum(36 * (N[l] + N[l + 1]) for l in range(6)),
+        "tracklets_write": sum(16 * T[l] for l in range(6)) + sum(4 * N[l] for l in range(1, 6)),
+        "cells_count": sum(16 * (T[l] + T[l + 1]) + 36 * (N[l] + N[l + 1] + N[l + 2]) for l in range(5)),
+        "cells_scatter": sum(40 * C[l] for l in range(5)) + sum(4 * T[l] for l in range(1, 5)),
+        "neighbours_write": b["neighbours"],
+        "roads_write": b["roads"],
+    }
 
 
 # ------------------------------------------------------------------------------------------
@@ -491,21 +495,30 @@ def run_ours(args):
     for c in counts:
         for k, v in algorithmic_bytes(c).items():
             step_bytes[k] = step_bytes.get(k, 0) + v
+    own_bytes = {}
+    for c in counts:
+        for k, v in kernel_bytes(c).items():
+            own_bytes[k] = own_bytes.get(k, 0) + v
     top_name, top_ms = max(prof, key=lambda x: x[1])
-    stage = KERNEL_STAGE.get(top_name)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         peak, peak_src = 6650.0, "fallback"
-    achieved = (step_bytes[stage] / (top_ms * 1e-3) / 1e9) if stage else None
+    achieved = (own_bytes[top_name] / (top_ms * 1e-3) / 1e9) if top_name in own_bytes else None
+    per_kernel = {name: {"ms": round(t, 4), "own_bytes": own_bytes[name],
+                         "gbs": own_bytes[name] / (t * 1e-3) / 1e9, "frac": own_bytes[name] / (t * 1e-3) / 1e9 / peak}
+                  for name, t in prof if name in own_bytes and t > 0}
+    # DRAM bytes of the kernel from an ncu capture of this same workload (profiles/traffic.json,
+    # per event, scaled to this launch's events); none for a workload that was not captured
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        per_event = tr.get("kernels", {}).get(top_name, {}).get("dram_bytes_per_event")
-        if per_event is not None:
-            traffic = per_event * n_events
+        if tr.get("workload") == args.workload:
+            per_event = tr.get("kernels", {}).get(top_name, {}).get("dram_bytes_per_event")
+            if per_event is not None:
+                traffic = per_event * n_events
     except (OSError, ValueError):
         pass
 
@@ -563,7 +576,10 @@ def run_ours(args):
             "gpu_launches": kernels * args.steps,
             "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": step_bytes.get(stage), "launch_ms": top_ms,
+                         "algorithmic_bytes_per_launch": own_bytes.get(top_name), "launch_ms": top_ms,
+                         "bytes_note": "the kernel's own compulsory bytes: the objects it must read or write once, "
+                                       "in the reference layouts (bench.py kernel_bytes)",
+                         "kernels": per_kernel,
                          "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_src if peak_src == "measured" else "fallback 6.65 TB/s"},
             "modes": {
                 "batched_plain_events_per_s": value,

@@ -2,7 +2,7 @@
 # Builds the reference CPU Tracker from its own sources into oracle/_ref/ (git-ignored).
 #
 # TEST INFRASTRUCTURE ONLY. The reference sources are read where they lie (ITSU_REFERENCE,
-# default /root/reference); a patched working copy is written to oracle/_ref/src/ and compiled
+# default: a checkout named "reference" beside this repository); a patched working copy is written to oracle/_ref/src/ and compiled
 # with the reference's own flags (-std=c++11 -O3, no -march, so no FMA contraction on x86-64).
 # Patches (each a memory-safety or determinism fix; each sed is checked to apply exactly once):
 #   P1 Tracker.cxx:88      candidate loop also stops at the end of the next layer
@@ -14,8 +14,8 @@
 # ref_unstable (P1, P2, P4, P5: the reference's unstable std::sort); merge_pileup, the
 # reference's pile-up merger (benchmarks/scripts/root/generatePileUpData.cxx), unpatched.
 set -eu
-REF=${ITSU_REFERENCE:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${ITSU_REFERENCE:-$HERE/../../reference}
 OUT="$HERE/_ref"
 CXX=${CXX:-g++}
 

@@ -61,3 +61,37 @@ def load_case(name: str):
 def vertex_runs(events):
     """(event, vertex index) pairs in the reference's loop order (Tracker.cxx:251)."""
     return [(ev, iv) for ev in events for iv in range(len(ev.vertices))]
+
+
+def beyond_z_event(seed: int, n_beyond: int = 700):
+    """A 2000-track event plus ``n_beyond`` clusters in each of layers 1, 2 and 5 whose z lies
+    beyond the tracker's half-length of that layer, most of them in phi bin 0, where that gives a
+    negative bin (sorted apart from the index table, PrimaryVertexContext.cxx:52-54), many of them
+    sharing a bin so that the stable order of ties matters, and a few beyond +z (bin 400)."""
+    rng = np.random.default_rng(seed)
+    ev = gen.make_event(seed, 2000)
+    half = {1: 16.333, 2: 16.333, 5: 73.745}
+    radius = {1: 3.1, 2: 3.9, 5: 34.4}
+    layers = list(ev.layers)
+    for layer in (1, 2, 5):
+        extra = np.zeros(n_beyond, gen.CLUSTER_DTYPE)
+        # a bin is phi bin * 20 + z bin: negative only in phi bin 0 (phi < 2 pi / 20)
+        phi = rng.uniform(0.0, 0.3, n_beyond)
+        phi[: n_beyond // 2] = rng.choice([0.05, 0.2], n_beyond // 2)  # shared phi values
+        phi[-n_beyond // 10:] = rng.uniform(0.0, 2.0 * np.pi, n_beyond // 10)  # the rest elsewhere
+        z = -half[layer] - rng.uniform(0.0, 400.0, n_beyond)
+        z[: n_beyond // 3] = -half[layer] - 5.0  # shared z bin as well: exact ties
+        z[-10:] = half[layer] + rng.uniform(1.0, 5.0, 10)  # beyond +z: bin 400
+        extra["x"] = (radius[layer] * np.cos(phi)).astype(np.float32)
+        extra["y"] = (radius[layer] * np.sin(phi)).astype(np.float32)
+        extra["z"] = z.astype(np.float32)
+        extra["mc"] = -1
+        # interleave with the layer's own clusters so that input order is not bin order
+        merged = np.concatenate([layers[layer], extra])
+        layers[layer] = merged[rng.permutation(len(merged))]
+    # cluster ids run in file order, as the reference's loader numbers them (IOUtils.cxx:38-78)
+    first = 0
+    for l in layers:
+        l["id"] = np.arange(first, first + len(l))
+        first += len(l)
+    return gen.Event(vertices=ev.vertices, layers=layers, labels=ev.labels)

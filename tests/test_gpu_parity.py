@@ -7,7 +7,7 @@ roads with their labels.
 import numpy as np
 import pytest
 
-from helpers import CASES, load_case, vertex_runs
+from helpers import CASES, beyond_z_event, load_case, vertex_runs
 from itsu import capi, gen
 from oracle import oracle
 
@@ -259,3 +259,59 @@ def test_launch_shapes_and_autotuner_keep_results(ctx):
         assert np.array_equal(roads.view(np.uint8), base_roads.view(np.uint8))
     finally:
         ctx.set_tune(band, 256, 8, 1)
+
+
+def test_uneven_batch_of_256_events(ctx):
+    """The batched form at its stated size: 256 events of log-uniform 20-8000 tracks in one pass.
+    Every event's roads equal its own single-vertex run (itsu_clusters_to_tracks) byte for byte
+    and its counts equal that run's; a stratified sample (the 8 largest and 8 random events) equals
+    the oracle in every output."""
+    events = gen.batch_events(31, n_events=256)
+    clusters, offsets, vertices = gen.pack_batch(events)
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    sizes = np.array([sum(len(l) for l in ev.layers) for ev in events])
+    rng = np.random.default_rng(31)
+    largest = list(np.argsort(sizes)[-8:])
+    sample = sorted(set(largest) | set(rng.choice(np.setdiff1d(np.arange(256), largest), 8, replace=False)))
+    batch_results = {int(e): ctx.results(int(e)) for e in sample}
+    batch_counts = [ctx.counts(e) for e in range(len(events))]
+    for e in sample:
+        ev = events[e]
+        _assert_same(batch_results[e], oracle.run_vertex(ev.layers, ev.vertices[0]), "256-event batch, event %d" % e)
+    for e, ev in enumerate(events):
+        single = ctx.clusters_to_tracks(ev.layers, ev.vertices[0])
+        assert np.array_equal(single.view(np.uint8), roads[road_off[e]:road_off[e + 1]].view(np.uint8)), e
+        c = ctx.counts(0)
+        b = batch_counts[e]
+        assert list(c.tracklets) == list(b.tracklets) and list(c.cells) == list(b.cells), e
+        assert list(c.neighbours) == list(b.neighbours) and c.roads == b.roads, e
+    assert sizes.max() > 50000 and sizes.min() < 1000  # the log-uniform span
+
+
+def test_pileup_frames_at_stated_size(ctx):
+    """Pile-up frames of 5 collisions of 1500 tracks with 10% noise through the frames API (each
+    frame's clusters uploaded once, every vertex run over them): each run equals the oracle."""
+    frames = [gen.pileup_frame(7), gen.pileup_frame(8)]
+    clusters, offsets, vertices, vertex_frame = gen.pack_frames(frames)
+    roads, road_off = ctx.frames_run_host(clusters, offsets, vertices, vertex_frame)
+    runs = [(ev, iv) for ev in frames for iv in range(len(ev.vertices))]
+    assert len(runs) == 10 and len(road_off) == 11
+    for v, (ev, iv) in enumerate(runs):
+        want = oracle.run_vertex(ev.layers, ev.vertices[iv])
+        _assert_same(ctx.results(v), want, "frame run %d" % v)
+        assert np.array_equal(roads[road_off[v]:road_off[v + 1]].view(np.uint8), want["roads"].view(np.uint8))
+
+
+def test_clusters_beyond_z_range_match_oracle(ctx):
+    """Hundreds of clusters per layer beyond the z range, most with negative bins (sorted apart
+    from the index table, stably, by the clustering's merge sort), many tied: stage by stage and
+    batched beside a Pb-Pb event, equal to the oracle."""
+    ev = beyond_z_event(4244)
+    want = oracle.run_vertex(ev.layers, ev.vertices[0])
+    assert sum(int((c["bin"] < 0).sum()) for c in want["clusters"]) > 1500
+    _assert_same(ctx.run_vertex(ev.layers, ev.vertices[0]), want, "beyond-z stages")
+    bg = gen.pbpb_event(6)
+    clusters, offsets, vertices = gen.pack_batch([bg, ev])
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    _assert_same(ctx.results(1), want, "beyond-z batched")
+    assert np.array_equal(roads[road_off[1]:road_off[2]].view(np.uint8), want["roads"].view(np.uint8))

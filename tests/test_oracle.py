@@ -7,7 +7,7 @@ import tempfile
 
 import pytest
 
-from helpers import CASES, load_case, vertex_runs
+from helpers import CASES, beyond_z_event, load_case, vertex_runs
 from itsu import gen
 from oracle import oracle
 
@@ -47,3 +47,21 @@ def test_oracle_matches_reference_fresh_events(seed):
         expected = oracle.run_reference(events, d, "cr")
     for (ev, iv), exp in zip(vertex_runs(events), expected):
         assert oracle.diff(oracle.run_vertex(ev.layers, ev.vertices[iv]), exp) == []
+
+
+@needs_ref
+def test_oracle_matches_reference_at_full_size():
+    """The sizes the GPU tests lean on the oracle for, against the reference binary directly: a
+    central Pb-Pb-like event (6000 tracks, 5% noise), a pile-up frame of 5 collisions of 1500
+    tracks with 10% noise (every vertex), and a layer with hundreds of clusters beyond its z
+    range (negative z bins sorted apart from the index table)."""
+    # the Pb-Pb events and the frame the GPU parity tests compare with the oracle
+    events = [gen.pbpb_event(1), gen.pbpb_event(2), gen.pbpb_event(3), gen.pileup_frame(7), beyond_z_event(4244)]
+    with tempfile.TemporaryDirectory() as d:
+        expected = oracle.run_reference(events, d, "cr")
+    runs = vertex_runs(events)
+    assert len(runs) == len(expected) == 9
+    for k, ((ev, iv), exp) in enumerate(zip(runs, expected)):
+        assert oracle.diff(oracle.run_vertex(ev.layers, ev.vertices[iv]), exp) == [], k
+    assert min(sum(len(t) for t in expected[k]["tracklets"]) for k in range(3)) > 200000  # central events indeed
+    assert sum(int((c["bin"] < 0).sum()) for c in expected[-1]["clusters"]) > 1500

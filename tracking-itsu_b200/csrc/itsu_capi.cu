@@ -484,6 +484,9 @@ itsu_status sync_status(itsu_context *ctx)
 {
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, ctx->stream));
   ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_status->flags & itsu::kFlagLaunchShape) {
+    return fail(ctx, ITSU_ERR_INVALID, "launch shape: the per-item passes need a block size that is a multiple of 32");
+  }
   return ITSU_OK;
 }
 
@@ -627,8 +630,8 @@ itsu_status stage_count_then_write(itsu_context *ctx, void (*count)(const Arena 
   itsu_status st;
   for (int attempt = 0;; ++attempt) {
     if ((st = clear_flags(ctx)) != ITSU_OK) return st;
-    // the entry reservation, the crowded lists and the cells scan's tile sums (added to by the
-    // cell count pass) start empty for every count, also a retry
+    // the entry reservation, the crowded lists and the tile sums of the tracklet and cell scans
+    // (the count passes add to them) start empty for every count, also a retry
     ITSU_CUDA(ctx, cudaMemsetAsync(&ctx->d_status->cell_entries, 0, 3 * sizeof(int64_t), ctx->stream));
     ITSU_CUDA(ctx, cudaMemsetAsync(ctx->scan_partials, 0, sizeof(int64_t) * ctx->cap_partials, ctx->stream));
     count(arena_of(ctx), launch_of(ctx));

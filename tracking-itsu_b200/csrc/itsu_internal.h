@@ -30,10 +30,12 @@ enum : int32_t {
   kFlagCapRoads = 16,
   kFlagCountOverflow = 32,
   kFlagCapScratch = 64,  // the cell entries of the count pass exceed their scratch
+  kFlagLaunchShape = 128,  // a per-item pass was given a block size that is not whole warps (nothing ran)
 };
 constexpr int kTrackletSlotsPerCluster = 48;  // outer clusters the tracklet count pass keeps per inner cluster
-constexpr int32_t kCapacityMask =
-    kFlagCapTracklets | kFlagCapCells | kFlagCapNeighbours | kFlagCapRoads | kFlagCountOverflow | kFlagCapScratch;
+// Any of these stops every later kernel of the run (they check the mask first).
+constexpr int32_t kCapacityMask = kFlagCapTracklets | kFlagCapCells | kFlagCapNeighbours | kFlagCapRoads |
+                                  kFlagCountOverflow | kFlagCapScratch | kFlagLaunchShape;
 constexpr int kCellChunk = 64;  // cell entries a warp of the cell count pass reserves at a time
 
 // Totals and requirements of a run, written by the device.

@@ -38,6 +38,10 @@ constexpr int kBuckets = kTableSize + 1;  // bucket 0: negative bins; bucket b+1
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+// The tracklet and cell count passes add each warp's total to the tile sum of the warp's first
+// item, which is only right if no warp straddles two tiles: whole warps (block sizes are
+// multiples of 32, checked at launch) over tiles of a whole number of warps.
+static_assert(kScanTile % 32 == 0, "a warp's 32 items lie in one scan tile");
 constexpr float kMaxAbsCoordinate = 1.0e6f;
 constexpr int kMaxPruneBin = 256;  // larger bins disable pruning for their layer
 constexpr int kPruneWords = kMaxPruneBin / 64;  // a pruned column's passes: a mask of this many 64-bit words
@@ -77,8 +81,12 @@ __global__ void k_status_init(Arena a)
   s->trk_crowded = 0;
 }
 
+// A launch shape the per-item passes cannot run: the run stops and reports it.
+__global__ void k_flag_bad_launch(DevStatus *s) { atomicOr(&s->flags, kFlagLaunchShape); }
+
 // ------------------------------------------------------------------------------------------
-// exclusive scan of int32 counts (three kernels: tile sums, scan of tile sums, tile scans)
+// exclusive scan of int32 counts (tile sums, scan of tile sums, tile scans; the tracklet and
+// cell count passes fill their scans' tile sums themselves)
 
 __device__ __forceinline__ int64_t scan_length(const int64_t *n_dev, int64_t n_host) { return n_dev ? *n_dev : n_host; }
 
@@ -231,7 +239,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int32_t *__re
 int scan_grid(const Launch &l) { return l.num_sms * 4; }
 
 // The four scans of a run: tracklets per cluster, cells per tracklet, neighbours per cell, roads
-// per cell. Each is three kernels (tile sums, scan of tile sums, tile scans).
+// per cell. The neighbour and road scans are three kernels (tile sums, scan of tile sums, tile
+// scans); the tracklet and cell scans are two, their tile sums added up by the count passes.
 struct ScanArgs {
   const int32_t *in;
   int32_t *out;
@@ -276,13 +285,6 @@ void step_scan_apply(const Arena &a, const Launch &l)
 // (a) clustering: PrimaryVertexContext::initialize (PrimaryVertexContext.cxx:31-142)
 
 __device__ __forceinline__ int bucket_of(int bin) { return bin < 0 ? 0 : bin + 1; }
-
-__device__ __forceinline__ void store_sorted(const Arena &a, int64_t at, const itsu_cluster &c)
-{
-  a.sorted[at] = c;
-  a.xyzr[at] = make_float4(c.x, c.y, c.z, c.r);
-  a.phi[at] = c.phi;
-}
 
 // A warp's 32 consecutive 36-byte clusters move between global and shared memory as 288 words,
 // each load or store instruction covering 128 contiguous bytes; a lane then reads or writes its
@@ -502,22 +504,47 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
     __syncwarp();  // the stage is refilled next
   }
 
-  // Pass 4: negative bins share bucket 0 in input order; order them by bin, stably.
+  // Pass 4: negative bins share bucket 0 in input order; order them by bin, stably. A bottom-up
+  // merge sort between the sorted segment and tmp: in each round, runs of `width` are merged in
+  // pairs, every cluster moving to (its place in its run) + (the clusters of the partner run that
+  // go before it: smaller bins, and for the right run equal bins too), so ties keep input order.
+  // O(m log^2 m) work over the block, for layers with many clusters beyond the z range.
   const int m = bucket_total[0];
   if (m > 1) {
-    __syncthreads();
-    for (int i = tid; i < m; i += kSortThreads) {
-      const itsu_cluster c = a.sorted[begin + i];
-      int rank = 0;
-      for (int j = 0; j < m; ++j) {
-        const int kj = a.sorted[begin + j].bin;
-        rank += (kj < c.bin) || (kj == c.bin && j < i);
+    itsu_cluster *src = a.sorted + begin, *dst = a.tmp + begin;
+    for (int width = 1; width < m; width *= 2) {
+      __syncthreads();
+      for (int i = tid; i < m; i += kSortThreads) {
+        const int run = i / width;
+        const bool left = (run & 1) == 0;
+        const int own_start = run * width;
+        const int other_start = left ? own_start + width : own_start - width;
+        const int other_end = min(other_start + width, m);
+        const itsu_cluster c = src[i];
+        int lo = other_start, hi = max(other_start, other_end);  // an empty partner run: no move
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          const int k = src[mid].bin;
+          if (k < c.bin || (!left && k == c.bin)) {
+            lo = mid + 1;
+          } else {
+            hi = mid;
+          }
+        }
+        dst[min(own_start, other_start) + (i - own_start) + (lo - other_start)] = c;
       }
-      a.tmp[begin + rank] = c;
+      itsu_cluster *t = src;
+      src = dst;
+      dst = t;
     }
     __syncthreads();
     for (int i = tid; i < m; i += kSortThreads) {
-      store_sorted(a, begin + i, a.tmp[begin + i]);
+      const itsu_cluster c = src[i];
+      if (src != a.sorted + begin) {
+        a.sorted[begin + i] = c;
+      }
+      a.xyzr[begin + i] = make_float4(c.x, c.y, c.z, c.r);
+      a.phi[begin + i] = c.phi;
     }
   }
 
@@ -1614,8 +1641,21 @@ void step_cluster_sort(const Arena &a, const Launch &l)
   }
 }
 
+// The per-item count passes need whole warps: each warp adds its items' total to one scan tile.
+bool whole_warps(const Arena &a, const Launch &l)
+{
+  if (l.block % 32 == 0) {
+    return true;
+  }
+  k_flag_bad_launch<<<1, 1, 0, l.stream>>>(a.status);
+  return false;
+}
+
 void step_tracklets_count(const Arena &a, const Launch &l)
 {
+  if (!whole_warps(a, l)) {
+    return;
+  }
   const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
   if (blocks > 0) {
     k_tracklets_count<<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
@@ -1637,7 +1677,12 @@ void step_tracklet_segments(const Arena &a, const Launch &l)
   k_tracklet_segments<<<(a.n_events * ITSU_TRACKLET_LAYERS + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
 }
 
-void step_cells_count(const Arena &a, const Launch &l) { k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
+void step_cells_count(const Arena &a, const Launch &l)
+{
+  if (whole_warps(a, l)) {
+    k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a);
+  }
+}
 
 // Launches only in the learned form (a.mlp set).
 void step_cells_prefilter(const Arena &a, const Launch &l)
