@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from itsu import capi, gen
 
@@ -54,3 +55,19 @@ def test_context_creation_fails_loudly_without_a_b200():
         assert e.status == capi.ERR_CUDA
     else:
         raise AssertionError("a context was created without a GPU")
+
+
+def test_reference_backend_is_built_against_the_library():
+    """Where the reference was built (oracle/_ref), its tracker with the B200 backend behind its
+    seam (ref_b200, tracking-itsu_b200/host/reference_backend/TrackerB200.cxx) is built too and
+    resolves libitsu_b200.so from the tree (its GPU runs are in test_gpu_reference_backend.py)."""
+    import subprocess
+
+    from oracle import oracle
+
+    if not oracle.ref_available("cr"):
+        pytest.skip("reference build (oracle/_ref) not present")
+    assert oracle.ref_available("b200")
+    ldd = subprocess.run(["ldd", oracle.ref_binary("b200")], capture_output=True, text=True, check=True).stdout
+    line = [l for l in ldd.splitlines() if "libitsu_b200.so" in l]
+    assert line and "not found" not in line[0] and "tracking-itsu_b200/lib" in line[0]
