@@ -388,6 +388,60 @@ itsu_status itsu_prefilter_train(itsu_context *ctx, const float *features, const
 itsu_status itsu_prefilter_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
                                     float pos_weight, float *grad, float *loss);
 
+/* ---- learned tracklet gate (no counterpart in the reference) ----
+ * The learned form's upstream stage: a smaller MLP (8 -> 16 -> 16 -> 1, ReLU, sigmoid output;
+ * BF16 weights and activations, FP32 accumulation) scores every tracklet the tracklet stage finds
+ * (the seam of TrackerTraits::computeLayerTracklets, src/CA/Tracker.cxx:45-117) before the
+ * tracklets are written, and a tracklet whose logit is below the gate's threshold is not kept: the
+ * cell stage then enumerates only pairs of kept tracklets (Tracker.cxx:133-158), where the plain
+ * path spends most of its time. Its features, per tracklet: |dphi| and dphi of its clusters'
+ * azimuths about the vertex, the tracklet cut's dz (Tracker.cxx:93-95) and |dz|, the signed
+ * curvature of the circle through the vertex and its two clusters, the inner layer, the inner
+ * cluster's radius and its slope from the vertex. Training labels come from plain runs (1 = the
+ * tracklet is part of a found road). A learned run's tracklets, and so its cells and roads, are
+ * subsets of the plain run's. Inner clusters with more than 48 tracklets keep all of theirs.
+ * The gate and the pair prefilter are enabled separately; the learned form is either or both. */
+#define ITSU_GATE_HIDDEN 16
+#define ITSU_GATE_PARAMS (ITSU_GATE_HIDDEN * ITSU_MLP_INPUTS + ITSU_GATE_HIDDEN + ITSU_GATE_HIDDEN * ITSU_GATE_HIDDEN + \
+                          ITSU_GATE_HIDDEN + ITSU_GATE_HIDDEN + 1)
+/* Same field order as itsu_prefilter_model, at the gate's width. */
+typedef struct itsu_gate_model {
+  float w1[ITSU_GATE_HIDDEN][ITSU_MLP_INPUTS]; /* [out][in] */
+  float b1[ITSU_GATE_HIDDEN];
+  float w2[ITSU_GATE_HIDDEN][ITSU_GATE_HIDDEN]; /* [out][in] */
+  float b2[ITSU_GATE_HIDDEN];
+  float w3[ITSU_GATE_HIDDEN];
+  float b3;
+  float mean[ITSU_MLP_INPUTS];
+  float inv_std[ITSU_MLP_INPUTS];
+  float logit_threshold;          /* a tracklet is kept unless its logit is below this */
+} itsu_gate_model;
+
+/* Device buffers that itsu_gate_export fills; every array may be NULL (then not written). */
+typedef struct itsu_gate_samples {
+  float *features;   /* [capacity][8]: the gate features of each tracklet of the last run */
+  uint8_t *labels;   /* [capacity]: 1 if a found road uses the tracklet */
+  int64_t capacity;  /* rows available; the export fails with ITSU_ERR_CAPACITY below n_tracklets */
+  int32_t *road_tracklets; /* [road_capacity][6]: each road's tracklets as sample rows, layers 0..5 */
+  int64_t road_capacity;
+  int64_t n_tracklets; /* out: tracklets of the last run (rows in event, layer, tracklet order) */
+  int64_t n_roads;     /* out: roads of the last run */
+} itsu_gate_samples;
+
+/* The gate's counterparts of the itsu_prefilter_* calls above, with the same semantics. */
+void itsu_gate_init(itsu_gate_model *model, uint64_t seed);
+itsu_status itsu_gate_save(const itsu_gate_model *model, const char *path);
+itsu_status itsu_gate_load(const char *path, itsu_gate_model *model);
+itsu_status itsu_gate_set_model(itsu_context *ctx, const itsu_gate_model *model);
+itsu_status itsu_gate_get_model(itsu_context *ctx, itsu_gate_model *model);
+itsu_status itsu_gate_enable(itsu_context *ctx, int32_t enable);
+itsu_status itsu_gate_export(itsu_context *ctx, itsu_gate_samples *samples);
+itsu_status itsu_gate_score(itsu_context *ctx, const float *features, int64_t n, float *logits);
+itsu_status itsu_gate_train(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
+                            const itsu_train_config *cfg, float *losses);
+itsu_status itsu_gate_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
+                               float pos_weight, float *grad, float *loss);
+
 /* ---- arena occupancy ----
  * The reference preallocates each vertex's tracklet and cell vectors from coefficients of the
  * cluster counts (Constants::Memory, Constants.h:87-92; PrimaryVertexContext.cxx:59-73, 125-131)

@@ -1,0 +1,261 @@
+"""The learned tracklet gate on the GPU: sample export, the gate pass of the tracklet stage, the
+scorer, training gradients and the committed checkpoint.
+
+The plain path is the judge: a gated run must keep exactly the plain tracklets the gate scores at
+or above its threshold (inner clusters with more than 48 tracklets keep all of theirs), in the
+plain run's order; it must equal the plain run when the threshold keeps everything; and its roads
+must be exactly the plain roads whose 6 tracklets all survive.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from itsu import capi, gen, prefilter
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_dev():
+    import torch
+
+    torch.cuda.init()
+    return torch.device("cuda", 0)
+
+
+@pytest.fixture(scope="module")
+def ctx(torch_dev):
+    c = capi.Context(device=0)
+    yield c
+    c.close()
+
+
+def _gate(features, seed=3, threshold=0.0):
+    m = capi.gate_init(seed)
+    f = features[np.isfinite(features).all(axis=1)]
+    mean, std = f.mean(axis=0), f.std(axis=0)
+    std[std == 0] = 1.0
+    for k in range(8):
+        m.mean[k], m.inv_std[k] = float(mean[k]), float(1.0 / std[k])
+    m.logit_threshold = threshold
+    return m
+
+
+def _score(ctx, features, torch_dev):
+    import torch
+
+    f = features if hasattr(features, "data_ptr") else torch.from_numpy(np.ascontiguousarray(features)).to(torch_dev)
+    out = torch.empty(max(len(f), 1), dtype=torch.float32, device=torch_dev)
+    ctx.gate_score(f.data_ptr(), len(f), out.data_ptr())
+    return out[:len(f)].cpu().numpy()
+
+
+def _plain(ctx, torch_dev, events):
+    b = prefilter.DeviceBatch(ctx, events, torch_dev)
+    prefilter.set_learned(ctx, False, False)
+    ctx.batch_run(b.batch)
+    f, l, r = prefilter.export_gate_samples(ctx, torch_dev)
+    return b, f, l, r
+
+
+def test_gate_export_matches_oracle_tracklets(ctx, torch_dev):
+    """Features bit-exact to the float32 restatement on the oracle's tracklets; labels and road
+    rows from the oracle's roads."""
+    ev = gen.pbpb_event(61, n_tracks=1500)
+    want = oracle.run_vertex(ev.layers, ev.vertices[0])
+    ctx.run_vertex(ev.layers, ev.vertices[0])
+    f, l, r = prefilter.export_gate_samples(ctx, torch_dev)
+    feats = prefilter.tracklet_features(want)
+    assert f.shape[0] == len(feats) > 0
+    assert np.array_equal(f.cpu().numpy().view(np.uint32), feats.view(np.uint32))
+    rows = prefilter.road_tracklets(want)
+    assert np.array_equal(r.cpu().numpy(), rows)
+    labels = np.zeros(len(feats), np.uint8)
+    labels[rows.ravel()] = 1
+    assert np.array_equal(l.cpu().numpy(), labels)
+
+
+def test_gate_scorer_matches_numpy_reference(ctx, torch_dev):
+    """Tensor-core logits vs a float64 restatement with the same BF16 roundings (ReLU is exact; a
+    different FP32 summation order can move a BF16 activation by one unit): 0.02 absolute + 1%
+    relative on the logit."""
+    ev = gen.pbpb_event(62, n_tracks=1500)
+    feats = prefilter.tracklet_features(oracle.run_vertex(ev.layers, ev.vertices[0]))
+    m = _gate(feats)
+    rng = np.random.default_rng(5)
+    m.b3 = 0.3
+    for k in range(16):
+        m.b1[k], m.b2[k] = float(rng.normal(0, 0.2)), float(rng.normal(0, 0.2))
+    ctx.gate_set_model(m)
+    got = _score(ctx, feats, torch_dev)
+    ref = prefilter.mlp_forward(m.arrays(), feats, act="relu")["z"]
+    err = np.abs(got - ref)
+    assert np.all(err <= 0.02 + 0.01 * np.abs(ref)), (err.max(), np.argmax(err))
+    assert np.corrcoef(got, ref)[0, 1] > 0.9999
+    assert np.std(ref) > 0.05
+
+
+def test_gate_threshold_minus_infinity_gives_the_plain_run(ctx, torch_dev):
+    events = [gen.pbpb_event(s, n_tracks=2000) for s in (63, 64)] + [gen.pp_event(65), gen.jet_event(5)]
+    b, f, _, _ = _plain(ctx, torch_dev, events)
+    plain = [ctx.results(e) for e in range(len(events))]
+    ctx.gate_set_model(_gate(f.cpu().numpy(), threshold=float("-inf")))
+    prefilter.set_learned(ctx, False, True)
+    try:
+        ctx.batch_run(b.batch)
+        for e in range(len(events)):
+            assert oracle.diff(ctx.results(e), plain[e]) == [], e
+    finally:
+        prefilter.set_learned(ctx, False, False)
+
+
+def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev):
+    """Threshold at the median logit, on central events and a dense jet (inner clusters with more
+    than 48 tracklets): the gated run's tracklets are the plain tracklets scored at or above it
+    (all of a crowded cluster's), in order; its roads are exactly the plain roads whose 6
+    tracklets all survive, with the same labels."""
+    events = [gen.pbpb_event(s, n_tracks=2500) for s in (66, 67)] + [gen.jet_event(5)]
+    b, f, l, r = _plain(ctx, torch_dev, events)
+    pkeys, pfake = prefilter.export_roads(ctx, torch_dev)
+    plain = [ctx.results(e) for e in range(len(events))]
+    m = _gate(f.cpu().numpy(), seed=11)
+    ctx.gate_set_model(m)
+    logits = _score(ctx, f, torch_dev)
+    thr = float(np.median(logits))
+    m.logit_threshold = thr
+    ctx.gate_set_model(m)
+    keep = ~(logits < thr)
+    # inner clusters with more than 48 tracklets keep all of them
+    row = 0
+    crowded = 0
+    for e in range(len(events)):
+        for layer in range(6):
+            t = plain[e]["tracklets"][layer]
+            per = np.bincount(t["c1"], minlength=len(plain[e]["clusters"][layer]))
+            big = per[t["c1"]] > 48
+            keep[row:row + len(t)] |= big
+            crowded += int(big.sum())
+            row += len(t)
+    assert row == len(keep) and crowded > 0
+    assert 0.3 < keep.mean() < 0.8
+    prefilter.set_learned(ctx, False, True)
+    try:
+        ctx.batch_run(b.batch)
+        lkeys, lfake = prefilter.export_roads(ctx, torch_dev)
+        row = 0
+        for e in range(len(events)):
+            got = ctx.results(e)
+            for layer in range(6):
+                pt = plain[e]["tracklets"][layer]
+                kept = pt[keep[row:row + len(pt)]]
+                row += len(pt)
+                assert np.array_equal(got["tracklets"][layer].view(np.uint8), kept.view(np.uint8)), (e, layer)
+    finally:
+        prefilter.set_learned(ctx, False, False)
+    rows = r.cpu().numpy().astype(np.int64)
+    survives = keep[rows].all(axis=1)
+    cmp = prefilter.compare_roads(pkeys, pfake, lkeys, lfake)
+    assert cmp["extra"] == 0 and cmp["extra_fakes"] == 0
+    assert cmp["reproduced"] == int(survives.sum()) == cmp["learned_roads"]
+    assert 0 < cmp["reproduced"] < cmp["plain_roads"]
+    # the surviving roads keep their Monte Carlo labels and fake flags (same 7 clusters)
+    lab = {bytes(k): fk for k, fk in zip(np.ascontiguousarray(pkeys), pfake)}
+    assert all(lab[bytes(k)] == fk for k, fk in zip(np.ascontiguousarray(lkeys), lfake))
+
+
+def test_gate_and_pair_prefilter_together(ctx, torch_dev):
+    """Both learned networks on: the result is the gated run's cells filtered by the pair scores,
+    and every road is a plain road."""
+    events = [gen.pbpb_event(s, n_tracks=2000) for s in (68, 69)]
+    b, f, _, _ = _plain(ctx, torch_dev, events)
+    pkeys, pfake = prefilter.export_roads(ctx, torch_dev)
+    gm = _gate(f.cpu().numpy(), seed=12)
+    ctx.gate_set_model(gm)
+    logits = _score(ctx, f, torch_dev)
+    gm.logit_threshold = float(np.quantile(logits, 0.3))
+    ctx.gate_set_model(gm)
+    prefilter.set_learned(ctx, False, True)
+    ctx.batch_run(b.batch)
+    pf, _, _ = prefilter.export_samples(ctx, torch_dev)
+    pm = capi.prefilter_init(13)
+    ff = pf.cpu().numpy()
+    mean, std = ff.mean(axis=0), ff.std(axis=0)
+    std[std == 0] = 1.0
+    for k in range(8):
+        pm.mean[k], pm.inv_std[k] = float(mean[k]), float(1.0 / std[k])
+    ctx.prefilter_set_model(pm)
+    pl = prefilter.score(ctx, pf, torch_dev).cpu().numpy()
+    pm.logit_threshold = float(np.quantile(pl, 0.3))
+    ctx.prefilter_set_model(pm)
+    gated = [ctx.results(e) for e in range(len(events))]
+    prefilter.set_learned(ctx, True, True)
+    try:
+        ctx.batch_run(b.batch)
+        both = [ctx.results(e) for e in range(len(events))]
+        lkeys, lfake = prefilter.export_roads(ctx, torch_dev)
+    finally:
+        prefilter.set_learned(ctx, False, False)
+    keep = ~(pl < pm.logit_threshold)
+    row = 0
+    for e in range(len(events)):
+        assert all(np.array_equal(both[e]["tracklets"][l].view(np.uint8), gated[e]["tracklets"][l].view(np.uint8))
+                   for l in range(6)), e
+        for layer in range(5):
+            gc = gated[e]["cells"][layer]
+            kept = gc[keep[row:row + len(gc)]]
+            row += len(gc)
+            assert np.array_equal(both[e]["cells"][layer]["c3"], kept["c3"]), (e, layer)
+    cmp = prefilter.compare_roads(pkeys, pfake, lkeys, lfake)
+    assert cmp["extra"] == 0 and 0 < cmp["learned_roads"] < cmp["plain_roads"]
+
+
+def test_gate_gradient_matches_numpy_reference(ctx, torch_dev):
+    """Device minibatch gradient of the gate vs the float64 restatement: relative error of each
+    parameter block below 3%, loss within 1e-3."""
+    import torch
+
+    ev = gen.pbpb_event(70, n_tracks=1500)
+    feats = prefilter.tracklet_features(oracle.run_vertex(ev.layers, ev.vertices[0]))[:1000]
+    labels = np.zeros(len(feats), np.uint8)
+    labels[::4] = 1
+    m = _gate(feats, seed=13)
+    rng = np.random.default_rng(6)
+    for k in range(16):
+        m.b1[k], m.b2[k] = float(rng.normal(0, 0.2)), float(rng.normal(0, 0.2))
+    ctx.gate_set_model(m)
+    df = torch.from_numpy(feats).to(torch_dev)
+    dl = torch.from_numpy(labels).to(torch_dev)
+    g, loss = ctx.gate_gradient(df.data_ptr(), dl.data_ptr(), len(feats), 2.0)
+    gr, lr = prefilter.mlp_gradient(m.arrays(), feats, labels, 2.0, act="relu")
+    assert abs(loss - lr) <= 1e-3 * max(1.0, abs(lr))
+    bounds = [0, 128, 144, 400, 416, 432, 433]
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        rel = np.linalg.norm(g[a:b] - gr[a:b]) / max(np.linalg.norm(gr[a:b]), 1e-12)
+        assert rel < 0.03, (a, b, rel)
+
+
+def test_gate_training_lowers_the_loss(ctx, torch_dev):
+    events = [gen.pbpb_event(s, n_tracks=3000) for s in (71, 72)]
+    _, f, l, _ = _plain(ctx, torch_dev, events)
+    ctx.gate_set_model(_gate(f.cpu().numpy(), seed=17))
+    before = ctx.gate_get_model().params()
+    cfg = capi.train_config(steps=400, batch=4096, lr=3e-3, lr_final=3e-4, seed=5)
+    losses = ctx.gate_train(f.data_ptr(), l.data_ptr(), len(f), cfg)
+    after = ctx.gate_get_model()
+    assert np.isfinite(losses).all()
+    assert losses[-50:].mean() < 0.85 * losses[:50].mean()
+    assert not np.array_equal(before, after.params())
+
+
+@pytest.mark.skipif(not os.path.exists(prefilter.GATE_CHECKPOINTS["pbpb"]), reason="no trained gate checkpoint")
+def test_committed_gate_reproduces_plain_roads(ctx, torch_dev):
+    """Held-out central Pb-Pb-like events (seeds after the evaluation set): the gate alone keeps at
+    least 99.5% of the plain roads and no road the plain path lacks, with fewer tracklets."""
+    gate = capi.gate_load(prefilter.GATE_CHECKPOINTS["pbpb"])
+    seeds = range(prefilter.EVAL_SEED0 + 1000, prefilter.EVAL_SEED0 + 1008)
+    res = prefilter.evaluate(ctx, None, seeds, torch_dev, chunk=8, workers=1, log=lambda *a: None, gate=gate)
+    assert res["extra"] == 0
+    assert res["road_reproduction"] >= 0.995, res
+    assert res["tracklets_kept"] < 0.5, res

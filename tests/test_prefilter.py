@@ -132,3 +132,87 @@ def test_compare_roads():
     l = np.array([[1, 1, 2, 3, 4, 5, 6, 7], [2, 0, 0, 0, 0, 0, 0, 0]], np.int32)
     c = prefilter.compare_roads(p, np.array([0, 1, 0]), l, np.array([1, 1]))
     assert c == dict(plain_roads=3, learned_roads=2, reproduced=1, extra=1, extra_fakes=1, plain_fakes=1, learned_fakes=2)
+
+
+# ---- the tracklet gate (8 -> 16 -> 16 -> 1, ReLU) ----
+
+
+def test_gate_model_layout_and_init():
+    assert ctypes.sizeof(capi.GateModel) == 4 * (capi.GATE_PARAMS + 2 * 8 + 1)
+    assert capi.GATE_PARAMS == 433
+    assert ctypes.sizeof(capi.GateSamples) == 56
+    a, b, c = capi.gate_init(1), capi.gate_init(1), capi.gate_init(2)
+    assert bytes(a) == bytes(b) and bytes(a) != bytes(c)
+    p = a.params()
+    assert np.all(np.abs(p[:128]) <= np.sqrt(6 / 24) + 1e-7)
+    assert np.all(p[128:144] == 0) and a.logit_threshold == 0.0
+
+
+def test_gate_checkpoint_round_trip_and_kinds(tmp_path):
+    """The gate's checkpoint has its own magic: neither kind loads as the other."""
+    g = capi.gate_init(4)
+    g.logit_threshold = -2.5
+    path = str(tmp_path / "g.itsugate")
+    capi.gate_save(g, path)
+    assert bytes(capi.gate_load(path)) == bytes(g)
+    with pytest.raises(capi.ItsuError):
+        capi.prefilter_load(path)
+    pair = str(tmp_path / "p.itsumlp")
+    capi.prefilter_save(capi.prefilter_init(4), pair)
+    with pytest.raises(capi.ItsuError):
+        capi.gate_load(pair)
+    raw = bytearray(open(path, "rb").read())
+    raw[60] ^= 1
+    open(path, "wb").write(bytes(raw))
+    with pytest.raises(capi.ItsuError) as e:
+        capi.gate_load(path)
+    assert "checksum" in str(e.value)
+
+
+def test_gate_numpy_gradient_matches_finite_differences():
+    rng = np.random.default_rng(2)
+    m = capi.gate_init(3).arrays()
+    m["b1"], m["b2"], m["b3"] = rng.normal(0, 0.1, 16), rng.normal(0, 0.1, 16), 0.1
+    f = rng.normal(0, 1, (64, 8)).astype(np.float32)
+    y = (rng.random(64) < 0.3).astype(np.float64)
+    g, _ = prefilter.mlp_gradient(m, f, y, 2.0, rounding=False, act="relu")
+    flat = np.concatenate([m["w1"].ravel(), m["b1"], m["w2"].ravel(), m["b2"], m["w3"], [m["b3"]]]).astype(np.float64)
+    assert len(flat) == capi.GATE_PARAMS
+    shapes = (("w1", (16, 8)), ("b1", (16,)), ("w2", (16, 16)), ("b2", (16,)), ("w3", (16,)), ("b3", ()))
+
+    def loss_at(v):
+        mm, o = dict(m), 0
+        for k, shp in shapes:
+            n = int(np.prod(shp)) if shp else 1
+            mm[k] = v[o:o + n].reshape(shp) if shp else v[o]
+            o += n
+        return prefilter.mlp_gradient(mm, f, y, 2.0, rounding=False, act="relu")[1]
+
+    for i in list(rng.choice(len(flat), 30, replace=False)) + [0, 128, 150, 400, 420, 432]:
+        up, dn = flat.copy(), flat.copy()
+        up[i] += 1e-6
+        dn[i] -= 1e-6
+        assert abs((loss_at(up) - loss_at(dn)) / 2e-6 - g[i]) < 1e-7 + 1e-5 * abs(g[i])
+
+
+def test_tracklet_features_of_oracle_tracklets():
+    """The gate's features of the plain path's tracklets respect the tracklet cuts that made them
+    (Tracker.cxx:93-100), and each road's 6 tracklet rows run through layers 0..5."""
+    ev = gen.pbpb_event(6, n_tracks=800)
+    res = oracle.run_vertex(ev.layers, ev.vertices[0])
+    f = prefilter.tracklet_features(res)
+    assert len(f) == sum(len(t) for t in res["tracklets"]) > 0 and np.isfinite(f).all()
+    layer = f[:, 4].astype(int)
+    assert np.all(f[:, 2] < np.array([0.1, 0.1, 0.3, 0.3, 0.3, 0.3], np.float32)[layer])
+    assert np.all(f[:, 0] < 0.3) and np.all(f[:, 0] == np.abs(f[:, 7])) and np.all(f[:, 2] == np.abs(f[:, 1]))
+    rows = prefilter.road_tracklets(res)
+    assert len(rows) == len(res["roads"]) > 0
+    assert np.all(f[rows, 4] == np.arange(6)[None, :])
+
+
+def test_committed_gate_checkpoint_loads():
+    path = prefilter.GATE_CHECKPOINTS["pbpb"]
+    if not os.path.exists(path):
+        pytest.skip("no trained gate checkpoint")
+    m = capi.gate_load(path)
+    assert np.isfinite(m.params()).all() and np.isfinite(m.logit_threshold)

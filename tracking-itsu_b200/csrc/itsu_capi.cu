@@ -132,6 +132,7 @@ struct itsu_context {
   bool tuning = false;
   int graph_tune[3] = {0, 0, -1};
   bool graph_prefilter = false;
+  bool graph_gate = false;
 
   // streamed host runs (ITSU_FLAG_STREAM_HOST): upload stream, per-chunk events, batch-wide roads
   cudaStream_t copy_stream = nullptr;   // uploads
@@ -159,6 +160,11 @@ struct itsu_context {
   itsu_prefilter_model *d_master = nullptr;
   itsu::MlpDevice *d_mlp = nullptr;
   bool has_model = false;
+  // learned tracklet gate: its FP32 master and device model, and whether the learned form uses it
+  itsu_gate_model *d_gate_master = nullptr;
+  itsu::GateDevice *d_gate = nullptr;
+  bool has_gate = false;
+  bool gate = false;
   bool prefilter = false;
 
   // road report scratch (itsu_roads_report)
@@ -292,6 +298,7 @@ Arena arena_of(const itsu_context *ctx)
   a.road_seg = ctx->road_seg;
   a.roads = ctx->roads;
   a.mlp = ctx->prefilter ? ctx->d_mlp : nullptr;
+  a.gate = ctx->gate ? ctx->d_gate : nullptr;
   a.scan_partials = ctx->scan_partials;
   a.status = ctx->d_status;
   a.cap_tracklets = ctx->cap_tracklets;
@@ -549,6 +556,7 @@ itsu_status launch_all(itsu_context *ctx)
   const bool same = ctx->graph && ctx->graph_generation == ctx->generation && ctx->graph_key[0] == ctx->in_raw &&
                     ctx->graph_tune[0] == tune.block && ctx->graph_tune[1] == tune.blocks_per_sm &&
                     ctx->graph_tune[2] == tune.prune && ctx->graph_prefilter == ctx->prefilter &&
+                    ctx->graph_gate == ctx->gate &&
                     ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
                     ctx->graph_key[3] == ctx->in_raw_off &&
                     ctx->graph_events == ctx->n_events && ctx->graph_clusters == ctx->n_clusters;
@@ -579,6 +587,7 @@ itsu_status launch_all(itsu_context *ctx)
     ctx->graph_tune[1] = tune.blocks_per_sm;
     ctx->graph_tune[2] = tune.prune;
     ctx->graph_prefilter = ctx->prefilter;
+    ctx->graph_gate = ctx->gate;
     ctx->graph_events = ctx->n_events;
     ctx->graph_clusters = ctx->n_clusters;
   }
@@ -868,6 +877,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
   release(ctx->d_master); release(ctx->d_mlp);
+  release(ctx->d_gate_master); release(ctx->d_gate);
   release(ctx->report_scratch); release(ctx->chunk_off); release(ctx->roads_all); release(ctx->road_off_all); release(ctx->chunk_status);
   if (ctx->h_chunk_status) cudaFreeHost(ctx->h_chunk_status);
   if (ctx->h_chunk_off) cudaFreeHost(ctx->h_chunk_off);
@@ -1478,7 +1488,8 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
     x->in_layer_off = ctx->chunk_off + (int64_t)ev[c] * ITSU_LAYERS + c;
     x->in_vtx = ctx->vtx + 3 * (int64_t)ev[c];
     Arena arena = arena_of(x);
-    arena.mlp = ctx->prefilter ? ctx->d_mlp : nullptr;  // the context's model serves both arenas
+    arena.mlp = ctx->prefilter ? ctx->d_mlp : nullptr;  // the context's models serve both arenas
+    arena.gate = ctx->gate ? ctx->d_gate : nullptr;
     const Launch l = launch_of(x);
     enqueue_run(arena, l);
     if (c > 0 && twin) ITSU_CUDA(ctx, cudaStreamWaitEvent(x->stream, ctx->chunk_done[c - 1], 0));
@@ -1814,7 +1825,10 @@ itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_t
   const itsu::KernelStep *all = itsu::pipeline_steps(&n_all);
   std::vector<itsu::KernelStep> steps;  // the steps that launch a kernel in this context's form
   for (int k = 0; k < n_all; ++k) {
-    if (!all[k].learned_only || ctx->prefilter) steps.push_back(all[k]);
+    const int only = all[k].learned_only;
+    if (only == 0 || (only == itsu::kPairPrefilterStep && ctx->prefilter) || (only == itsu::kGateStep && ctx->gate)) {
+      steps.push_back(all[k]);
+    }
   }
   const int n = (int)steps.size();
   std::vector<cudaEvent_t> ev(n + 1, nullptr);
@@ -1886,9 +1900,50 @@ uint64_t fnv1a64(const unsigned char *p, size_t n, uint64_t h = 0xcbf29ce4842223
   return h;
 }
 
-constexpr char kCheckpointMagic[8] = {'I', 'T', 'S', 'U', 'M', 'L', 'P', '1'};
+// The two learned networks: the pair prefilter (itsu_prefilter_model) and the tracklet gate
+// (itsu_gate_model) share their checkpoint format, training loop and host calls; NetOf<Model>
+// names what differs.
+template <class Model>
+struct NetOf;
+
+template <>
+struct NetOf<itsu_prefilter_model> {
+  using Model = itsu_prefilter_model;
+  using Device = itsu::MlpDevice;
+  static constexpr int kHidden = ITSU_MLP_HIDDEN;
+  static constexpr int kParams = ITSU_MLP_PARAMS;
+  static constexpr char kMagic[8] = {'I', 'T', 'S', 'U', 'M', 'L', 'P', '1'};
+  static constexpr const char *kName = "prefilter";
+  static Model *&master(itsu_context *c) { return c->d_master; }
+  static Device *&device(itsu_context *c) { return c->d_mlp; }
+  static bool &has(itsu_context *c) { return c->has_model; }
+  static bool &enabled(itsu_context *c) { return c->prefilter; }
+  static size_t device_bytes() { return itsu::mlp_device_bytes(); }
+};
+
+template <>
+struct NetOf<itsu_gate_model> {
+  using Model = itsu_gate_model;
+  using Device = itsu::GateDevice;
+  static constexpr int kHidden = ITSU_GATE_HIDDEN;
+  static constexpr int kParams = ITSU_GATE_PARAMS;
+  static constexpr char kMagic[8] = {'I', 'T', 'S', 'U', 'G', 'A', 'T', '1'};
+  static constexpr const char *kName = "gate";
+  static Model *&master(itsu_context *c) { return c->d_gate_master; }
+  static Device *&device(itsu_context *c) { return c->d_gate; }
+  static bool &has(itsu_context *c) { return c->has_gate; }
+  static bool &enabled(itsu_context *c) { return c->gate; }
+  static size_t device_bytes() { return itsu::gate_device_bytes(); }
+};
+
 constexpr uint32_t kCheckpointVersion = 1;
-constexpr uint32_t kBf16Weights = ITSU_MLP_HIDDEN * ITSU_MLP_INPUTS + ITSU_MLP_HIDDEN * ITSU_MLP_HIDDEN + ITSU_MLP_HIDDEN;
+
+template <class Model>
+constexpr uint32_t bf16_count()
+{
+  constexpr int H = NetOf<Model>::kHidden;
+  return H * ITSU_MLP_INPUTS + H * H + H;
+}
 
 struct CheckpointHeader {
   char magic[8];
@@ -1896,15 +1951,17 @@ struct CheckpointHeader {
 };
 
 // The BF16 copies of w1, w2, w3 in that order.
-std::vector<uint16_t> bf16_weights(const itsu_prefilter_model &m)
+template <class Model>
+std::vector<uint16_t> bf16_weights(const Model &m)
 {
+  constexpr int H = NetOf<Model>::kHidden;
   std::vector<uint16_t> out;
-  out.reserve(kBf16Weights);
-  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
+  out.reserve(bf16_count<Model>());
+  for (int o = 0; o < H; ++o)
     for (int i = 0; i < ITSU_MLP_INPUTS; ++i) out.push_back(host_bf16(m.w1[o][i]));
-  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
-    for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) out.push_back(host_bf16(m.w2[o][i]));
-  for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) out.push_back(host_bf16(m.w3[i]));
+  for (int o = 0; o < H; ++o)
+    for (int i = 0; i < H; ++i) out.push_back(host_bf16(m.w2[o][i]));
+  for (int i = 0; i < H; ++i) out.push_back(host_bf16(m.w3[i]));
   return out;
 }
 
@@ -1914,24 +1971,20 @@ struct DeviceScratch {  // a temporary device allocation freed on scope exit
   ~DeviceScratch() { if (p) cudaFree(p); }
 };
 
-itsu_status require_model(itsu_context *ctx, const char *what)
+template <class Model>
+itsu_status require_net(itsu_context *ctx, const char *what)
 {
   if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "%s: null context", what);
-  if (!ctx->has_model) return fail(ctx, ITSU_ERR_STATE, "%s: no prefilter model set", what);
+  if (!NetOf<Model>::has(ctx)) return fail(ctx, ITSU_ERR_STATE, "%s: no %s model set", what, NetOf<Model>::kName);
   return ITSU_OK;
 }
 
 bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
-}  // namespace
-
-extern "C" {
-
-static_assert(sizeof(itsu_prefilter_model) == sizeof(float) * (ITSU_MLP_PARAMS + 2 * ITSU_MLP_INPUTS + 1), "model layout");
-static_assert(ITSU_MLP_PARAMS == itsu::kMlpParams, "parameter count");
-
-void itsu_prefilter_init(itsu_prefilter_model *model, uint64_t seed)
+template <class Model>
+void net_init(Model *model, uint64_t seed)
 {
+  constexpr int H = NetOf<Model>::kHidden;
   if (!model) return;
   std::memset(model, 0, sizeof *model);
   uint64_t state = seed;
@@ -1940,17 +1993,211 @@ void itsu_prefilter_init(itsu_prefilter_model *model, uint64_t seed)
     return (float)((2.0 * u - 1.0) * limit);
   };
   // Glorot-uniform limits sqrt(6 / (fan_in + fan_out))
-  const float l1 = (float)std::sqrt(6.0 / (ITSU_MLP_INPUTS + ITSU_MLP_HIDDEN));
-  const float l2 = (float)std::sqrt(6.0 / (2 * ITSU_MLP_HIDDEN));
-  const float l3 = (float)std::sqrt(6.0 / (ITSU_MLP_HIDDEN + 1));
-  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
+  const float l1 = (float)std::sqrt(6.0 / (ITSU_MLP_INPUTS + H));
+  const float l2 = (float)std::sqrt(6.0 / (2 * H));
+  const float l3 = (float)std::sqrt(6.0 / (H + 1));
+  for (int o = 0; o < H; ++o)
     for (int i = 0; i < ITSU_MLP_INPUTS; ++i) model->w1[o][i] = uniform(l1);
-  for (int o = 0; o < ITSU_MLP_HIDDEN; ++o)
-    for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) model->w2[o][i] = uniform(l2);
-  for (int i = 0; i < ITSU_MLP_HIDDEN; ++i) model->w3[i] = uniform(l3);
+  for (int o = 0; o < H; ++o)
+    for (int i = 0; i < H; ++i) model->w2[o][i] = uniform(l2);
+  for (int i = 0; i < H; ++i) model->w3[i] = uniform(l3);
   for (int i = 0; i < ITSU_MLP_INPUTS; ++i) model->inv_std[i] = 1.0f;
   model->logit_threshold = 0.0f;
 }
+
+template <class Model>
+itsu_status net_save(const Model *model, const char *path, const char *what)
+{
+  if (!model || !path) return fail(nullptr, ITSU_ERR_INVALID, "%s: null argument", what);
+  CheckpointHeader h;
+  std::memcpy(h.magic, NetOf<Model>::kMagic, sizeof h.magic);
+  h.version = kCheckpointVersion;
+  h.n_params = NetOf<Model>::kParams;
+  h.model_bytes = sizeof(Model);
+  h.n_bf16 = bf16_count<Model>();
+  const std::vector<uint16_t> bf = bf16_weights(*model);
+  std::vector<unsigned char> buf(sizeof h + sizeof *model + sizeof(uint16_t) * bf.size());
+  std::memcpy(buf.data(), &h, sizeof h);
+  std::memcpy(buf.data() + sizeof h, model, sizeof *model);
+  std::memcpy(buf.data() + sizeof h + sizeof *model, bf.data(), sizeof(uint16_t) * bf.size());
+  const uint64_t sum = fnv1a64(buf.data(), buf.size());
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(nullptr, ITSU_ERR_INVALID, "%s: cannot open %s", what, path);
+  const bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size() && std::fwrite(&sum, sizeof sum, 1, f) == 1;
+  if (std::fclose(f) != 0 || !ok) return fail(nullptr, ITSU_ERR_INVALID, "%s: write to %s failed", what, path);
+  return ITSU_OK;
+}
+
+template <class Model>
+itsu_status net_load(const char *path, Model *model, const char *what)
+{
+  if (!model || !path) return fail(nullptr, ITSU_ERR_INVALID, "%s: null argument", what);
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(nullptr, ITSU_ERR_INVALID, "%s: cannot open %s", what, path);
+  const size_t body = sizeof(CheckpointHeader) + sizeof(Model) + sizeof(uint16_t) * bf16_count<Model>();
+  std::vector<unsigned char> buf(body + sizeof(uint64_t) + 1);
+  const size_t got = std::fread(buf.data(), 1, buf.size(), f);
+  std::fclose(f);
+  if (got != body + sizeof(uint64_t)) {
+    return fail(nullptr, ITSU_ERR_INVALID, "%s: %s has %zu bytes, a checkpoint has %zu", what, path, got, body + sizeof(uint64_t));
+  }
+  CheckpointHeader h;
+  std::memcpy(&h, buf.data(), sizeof h);
+  if (std::memcmp(h.magic, NetOf<Model>::kMagic, sizeof h.magic) != 0 || h.version != kCheckpointVersion ||
+      h.n_params != (uint32_t)NetOf<Model>::kParams || h.model_bytes != sizeof(Model) || h.n_bf16 != bf16_count<Model>()) {
+    return fail(nullptr, ITSU_ERR_INVALID, "%s: %s is not a version-%u %s checkpoint", what, path, kCheckpointVersion,
+                NetOf<Model>::kName);
+  }
+  uint64_t sum;
+  std::memcpy(&sum, buf.data() + body, sizeof sum);
+  if (fnv1a64(buf.data(), body) != sum) return fail(nullptr, ITSU_ERR_INVALID, "%s: %s: checksum mismatch", what, path);
+  Model m;
+  std::memcpy(&m, buf.data() + sizeof h, sizeof m);
+  const std::vector<uint16_t> bf = bf16_weights(m);
+  if (std::memcmp(bf.data(), buf.data() + sizeof h + sizeof m, sizeof(uint16_t) * bf.size()) != 0) {
+    return fail(nullptr, ITSU_ERR_INVALID, "%s: %s: BF16 weights do not match the FP32 master", what, path);
+  }
+  *model = m;
+  return ITSU_OK;
+}
+
+template <class Model>
+itsu_status net_set_model(itsu_context *ctx, const Model *model, const char *what)
+{
+  using N = NetOf<Model>;
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "%s: null context", what);
+  if (!model) return fail(ctx, ITSU_ERR_INVALID, "%s: null model", what);
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!N::master(ctx)) ITSU_CUDA(ctx, cudaMalloc((void **)&N::master(ctx), sizeof(Model)));
+  if (!N::device(ctx)) ITSU_CUDA(ctx, cudaMalloc((void **)&N::device(ctx), N::device_bytes()));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(N::master(ctx), model, sizeof *model, cudaMemcpyHostToDevice, ctx->stream));
+  itsu::launch_mlp_publish(N::master(ctx), N::device(ctx), ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  N::has(ctx) = true;
+  return ITSU_OK;
+}
+
+template <class Model>
+itsu_status net_get_model(itsu_context *ctx, Model *model, const char *what)
+{
+  itsu_status st;
+  if ((st = require_net<Model>(ctx, what)) != ITSU_OK) return st;
+  if (!model) return fail(ctx, ITSU_ERR_INVALID, "%s: null model", what);
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(model, NetOf<Model>::master(ctx), sizeof *model, cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+template <class Model>
+itsu_status net_enable(itsu_context *ctx, int32_t enable, const char *what)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "%s: null context", what);
+  if (enable && !NetOf<Model>::has(ctx)) return fail(ctx, ITSU_ERR_STATE, "%s: no %s model set", what, NetOf<Model>::kName);
+  NetOf<Model>::enabled(ctx) = enable != 0;
+  return ITSU_OK;
+}
+
+template <class Model>
+itsu_status net_score(itsu_context *ctx, const float *features, int64_t n, float *logits, const char *what)
+{
+  itsu_status st;
+  if ((st = require_net<Model>(ctx, what)) != ITSU_OK) return st;
+  if (n < 0 || (n > 0 && (!features || !logits))) return fail(ctx, ITSU_ERR_INVALID, "%s: bad arguments", what);
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu::launch_mlp_score(NetOf<Model>::device(ctx), features, n, logits, ctx->num_sms, ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+template <class Model>
+itsu_status net_train(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n, const itsu_train_config *cfg,
+                      float *losses, const char *what)
+{
+  using N = NetOf<Model>;
+  itsu_status st;
+  if ((st = require_net<Model>(ctx, what)) != ITSU_OK) return st;
+  if (!cfg || !features || !labels || n <= 0) return fail(ctx, ITSU_ERR_INVALID, "%s: bad arguments", what);
+  if (cfg->steps < 0 || cfg->batch <= 0 || cfg->batch % 32 != 0 || !(cfg->lr >= 0.0f) || !(cfg->lr_final >= 0.0f) ||
+      !(cfg->beta1 >= 0.0f && cfg->beta1 < 1.0f) || !(cfg->beta2 >= 0.0f && cfg->beta2 < 1.0f) || !(cfg->eps > 0.0f)) {
+    return fail(ctx, ITSU_ERR_INVALID, "%s: bad configuration", what);
+  }
+  if (!aligned16(features)) return fail(ctx, ITSU_ERR_INVALID, "%s: features must be 16-byte aligned", what);
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int blocks = itsu::mlp_gradient_blocks(cfg->batch);
+  DeviceScratch<float> partials, m, v, loss;
+  ITSU_CUDA(ctx, cudaMalloc((void **)&partials.p, sizeof(float) * blocks * N::kParams));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&m.p, sizeof(float) * N::kParams));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&v.p, sizeof(float) * N::kParams));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&loss.p, sizeof(float) * std::max<int64_t>(cfg->steps, 1)));
+  ITSU_CUDA(ctx, cudaMemsetAsync(m.p, 0, sizeof(float) * N::kParams, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemsetAsync(v.p, 0, sizeof(float) * N::kParams, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemsetAsync(loss.p, 0, sizeof(float) * std::max<int64_t>(cfg->steps, 1), ctx->stream));
+  double b1t = 1.0, b2t = 1.0;
+  for (int64_t step = 0; step < cfg->steps; ++step) {
+    // cosine decay from lr to lr_final
+    const double frac = cfg->steps > 1 ? (double)step / (double)(cfg->steps - 1) : 0.0;
+    const float lr = (float)(cfg->lr_final + 0.5 * (cfg->lr - cfg->lr_final) * (1.0 + std::cos(3.14159265358979323846 * frac)));
+    b1t *= cfg->beta1;
+    b2t *= cfg->beta2;
+    itsu::launch_mlp_gradient(N::device(ctx), features, labels, n, cfg->batch, false, cfg->seed, step, cfg->pos_weight, partials.p,
+                              loss.p + step, ctx->stream);
+    itsu::launch_mlp_adam(N::master(ctx), partials.p, blocks, m.p, v.p, lr, cfg->beta1, cfg->beta2, cfg->eps, cfg->weight_decay,
+                          (float)(1.0 - b1t), (float)(1.0 - b2t), N::device(ctx), ctx->stream);
+    if ((step & 1023) == 0) ITSU_CUDA(ctx, cudaGetLastError());
+  }
+  ITSU_CUDA(ctx, cudaGetLastError());
+  if (losses && cfg->steps > 0) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(losses, loss.p, sizeof(float) * cfg->steps, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
+template <class Model>
+itsu_status net_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n, float pos_weight, float *grad,
+                         float *loss_out, const char *what)
+{
+  using N = NetOf<Model>;
+  itsu_status st;
+  if ((st = require_net<Model>(ctx, what)) != ITSU_OK) return st;
+  if (!features || !labels || !grad || n <= 0 || n > INT32_MAX - 31) return fail(ctx, ITSU_ERR_INVALID, "%s: bad arguments", what);
+  if (!aligned16(features)) return fail(ctx, ITSU_ERR_INVALID, "%s: features must be 16-byte aligned", what);
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int32_t batch = (int32_t)n;
+  const int blocks = itsu::mlp_gradient_blocks(batch);
+  DeviceScratch<float> partials, loss;
+  ITSU_CUDA(ctx, cudaMalloc((void **)&partials.p, sizeof(float) * blocks * N::kParams));
+  ITSU_CUDA(ctx, cudaMalloc((void **)&loss.p, sizeof(float)));
+  ITSU_CUDA(ctx, cudaMemsetAsync(loss.p, 0, sizeof(float), ctx->stream));
+  itsu::launch_mlp_gradient(N::device(ctx), features, labels, n, batch, true, 0, 0, pos_weight, partials.p, loss.p, ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  std::vector<float> h((size_t)blocks * N::kParams);
+  float l = 0.0f;
+  ITSU_CUDA(ctx, cudaMemcpyAsync(h.data(), partials.p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaMemcpyAsync(&l, loss.p, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < N::kParams; ++i) {
+    double sum = 0.0;
+    for (int b = 0; b < blocks; ++b) sum += h[(size_t)b * N::kParams + i];
+    grad[i] = (float)sum;
+  }
+  if (loss_out) *loss_out = l;
+  return ITSU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+static_assert(sizeof(itsu_prefilter_model) == sizeof(float) * (ITSU_MLP_PARAMS + 2 * ITSU_MLP_INPUTS + 1), "model layout");
+static_assert(ITSU_MLP_PARAMS == itsu::kMlpParams, "parameter count");
+static_assert(ITSU_GATE_PARAMS == itsu::kGateParams && ITSU_GATE_HIDDEN == itsu::kGateHidden, "gate parameter count");
+
+void itsu_prefilter_init(itsu_prefilter_model *model, uint64_t seed) { net_init(model, seed); }
+void itsu_gate_init(itsu_gate_model *model, uint64_t seed) { net_init(model, seed); }
 
 void itsu_train_config_default(itsu_train_config *cfg)
 {
@@ -1968,94 +2215,26 @@ void itsu_train_config_default(itsu_train_config *cfg)
   cfg->seed = 1;
 }
 
-itsu_status itsu_prefilter_save(const itsu_prefilter_model *model, const char *path)
-{
-  if (!model || !path) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_save: null argument");
-  CheckpointHeader h;
-  std::memcpy(h.magic, kCheckpointMagic, sizeof h.magic);
-  h.version = kCheckpointVersion;
-  h.n_params = ITSU_MLP_PARAMS;
-  h.model_bytes = sizeof(itsu_prefilter_model);
-  h.n_bf16 = kBf16Weights;
-  const std::vector<uint16_t> bf = bf16_weights(*model);
-  std::vector<unsigned char> buf(sizeof h + sizeof *model + sizeof(uint16_t) * bf.size());
-  std::memcpy(buf.data(), &h, sizeof h);
-  std::memcpy(buf.data() + sizeof h, model, sizeof *model);
-  std::memcpy(buf.data() + sizeof h + sizeof *model, bf.data(), sizeof(uint16_t) * bf.size());
-  const uint64_t sum = fnv1a64(buf.data(), buf.size());
-  FILE *f = std::fopen(path, "wb");
-  if (!f) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_save: cannot open %s", path);
-  const bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size() && std::fwrite(&sum, sizeof sum, 1, f) == 1;
-  if (std::fclose(f) != 0 || !ok) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_save: write to %s failed", path);
-  return ITSU_OK;
-}
-
-itsu_status itsu_prefilter_load(const char *path, itsu_prefilter_model *model)
-{
-  if (!model || !path) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: null argument");
-  FILE *f = std::fopen(path, "rb");
-  if (!f) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: cannot open %s", path);
-  const size_t body = sizeof(CheckpointHeader) + sizeof(itsu_prefilter_model) + sizeof(uint16_t) * kBf16Weights;
-  std::vector<unsigned char> buf(body + sizeof(uint64_t) + 1);
-  const size_t got = std::fread(buf.data(), 1, buf.size(), f);
-  std::fclose(f);
-  if (got != body + sizeof(uint64_t)) {
-    return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s has %zu bytes, a checkpoint has %zu", path, got,
-                body + sizeof(uint64_t));
-  }
-  CheckpointHeader h;
-  std::memcpy(&h, buf.data(), sizeof h);
-  if (std::memcmp(h.magic, kCheckpointMagic, sizeof h.magic) != 0 || h.version != kCheckpointVersion ||
-      h.n_params != ITSU_MLP_PARAMS || h.model_bytes != sizeof(itsu_prefilter_model) || h.n_bf16 != kBf16Weights) {
-    return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s is not a version-%u prefilter checkpoint", path,
-                kCheckpointVersion);
-  }
-  uint64_t sum;
-  std::memcpy(&sum, buf.data() + body, sizeof sum);
-  if (fnv1a64(buf.data(), body) != sum) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s: checksum mismatch", path);
-  itsu_prefilter_model m;
-  std::memcpy(&m, buf.data() + sizeof h, sizeof m);
-  const std::vector<uint16_t> bf = bf16_weights(m);
-  if (std::memcmp(bf.data(), buf.data() + sizeof h + sizeof m, sizeof(uint16_t) * bf.size()) != 0) {
-    return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_load: %s: BF16 weights do not match the FP32 master", path);
-  }
-  *model = m;
-  return ITSU_OK;
-}
+itsu_status itsu_prefilter_save(const itsu_prefilter_model *model, const char *path) { return net_save(model, path, "itsu_prefilter_save"); }
+itsu_status itsu_gate_save(const itsu_gate_model *model, const char *path) { return net_save(model, path, "itsu_gate_save"); }
+itsu_status itsu_prefilter_load(const char *path, itsu_prefilter_model *model) { return net_load(path, model, "itsu_prefilter_load"); }
+itsu_status itsu_gate_load(const char *path, itsu_gate_model *model) { return net_load(path, model, "itsu_gate_load"); }
 
 itsu_status itsu_prefilter_set_model(itsu_context *ctx, const itsu_prefilter_model *model)
 {
-  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_set_model: null context");
-  if (!model) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_set_model: null model");
-  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
-  if (!ctx->d_master) ITSU_CUDA(ctx, cudaMalloc((void **)&ctx->d_master, sizeof(itsu_prefilter_model)));
-  if (!ctx->d_mlp) ITSU_CUDA(ctx, cudaMalloc((void **)&ctx->d_mlp, itsu::mlp_device_bytes()));
-  ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->d_master, model, sizeof *model, cudaMemcpyHostToDevice, ctx->stream));
-  itsu::launch_mlp_publish(ctx->d_master, ctx->d_mlp, ctx->stream);
-  ITSU_CUDA(ctx, cudaGetLastError());
-  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->has_model = true;
-  return ITSU_OK;
+  return net_set_model(ctx, model, "itsu_prefilter_set_model");
 }
-
+itsu_status itsu_gate_set_model(itsu_context *ctx, const itsu_gate_model *model) { return net_set_model(ctx, model, "itsu_gate_set_model"); }
 itsu_status itsu_prefilter_get_model(itsu_context *ctx, itsu_prefilter_model *model)
 {
-  itsu_status st;
-  if ((st = require_model(ctx, "itsu_prefilter_get_model")) != ITSU_OK) return st;
-  if (!model) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_get_model: null model");
-  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
-  ITSU_CUDA(ctx, cudaMemcpyAsync(model, ctx->d_master, sizeof *model, cudaMemcpyDeviceToHost, ctx->stream));
-  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return ITSU_OK;
+  return net_get_model(ctx, model, "itsu_prefilter_get_model");
 }
-
+itsu_status itsu_gate_get_model(itsu_context *ctx, itsu_gate_model *model) { return net_get_model(ctx, model, "itsu_gate_get_model"); }
 itsu_status itsu_prefilter_enable(itsu_context *ctx, int32_t enable)
 {
-  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "itsu_prefilter_enable: null context");
-  if (enable && !ctx->has_model) return fail(ctx, ITSU_ERR_STATE, "itsu_prefilter_enable: no prefilter model set");
-  ctx->prefilter = enable != 0;
-  return ITSU_OK;
+  return net_enable<itsu_prefilter_model>(ctx, enable, "itsu_prefilter_enable");
 }
+itsu_status itsu_gate_enable(itsu_context *ctx, int32_t enable) { return net_enable<itsu_gate_model>(ctx, enable, "itsu_gate_enable"); }
 
 itsu_status itsu_prefilter_export(itsu_context *ctx, itsu_prefilter_samples *samples)
 {
@@ -2084,90 +2263,61 @@ itsu_status itsu_prefilter_export(itsu_context *ctx, itsu_prefilter_samples *sam
   return ITSU_OK;
 }
 
-itsu_status itsu_prefilter_score(itsu_context *ctx, const float *features, int64_t n, float *logits)
+itsu_status itsu_gate_export(itsu_context *ctx, itsu_gate_samples *samples)
 {
   itsu_status st;
-  if ((st = require_model(ctx, "itsu_prefilter_score")) != ITSU_OK) return st;
-  if (n < 0 || (n > 0 && (!features || !logits))) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_score: bad arguments");
+  if ((st = require_stage(ctx, kRoads, "itsu_gate_export")) != ITSU_OK) return st;
+  if (!samples) return fail(ctx, ITSU_ERR_INVALID, "itsu_gate_export: null samples");
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
-  itsu::launch_mlp_score(ctx->d_mlp, features, n, logits, ctx->num_sms, ctx->stream);
+  if ((st = sync_status(ctx)) != ITSU_OK) return st;
+  const int64_t n = ctx->h_status->total[itsu::kTracklets], n_roads = ctx->h_status->total[itsu::kRoads];
+  samples->n_tracklets = n;
+  samples->n_roads = n_roads;
+  if ((samples->features || samples->labels) && samples->capacity < n) {
+    return fail(ctx, ITSU_ERR_CAPACITY, "itsu_gate_export: %lld tracklets, room for %lld", (long long)n, (long long)samples->capacity);
+  }
+  if (samples->road_tracklets && samples->road_capacity < n_roads) {
+    return fail(ctx, ITSU_ERR_CAPACITY, "itsu_gate_export: %lld roads, room for %lld", (long long)n_roads,
+                (long long)samples->road_capacity);
+  }
+  if (samples->features && !aligned16(samples->features)) {
+    return fail(ctx, ITSU_ERR_INVALID, "itsu_gate_export: features must be 16-byte aligned");
+  }
+  itsu::launch_gate_export(arena_of(ctx), *samples, ctx->num_sms, ctx->stream);
   ITSU_CUDA(ctx, cudaGetLastError());
   ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ITSU_OK;
+}
+
+itsu_status itsu_prefilter_score(itsu_context *ctx, const float *features, int64_t n, float *logits)
+{
+  return net_score<itsu_prefilter_model>(ctx, features, n, logits, "itsu_prefilter_score");
+}
+itsu_status itsu_gate_score(itsu_context *ctx, const float *features, int64_t n, float *logits)
+{
+  return net_score<itsu_gate_model>(ctx, features, n, logits, "itsu_gate_score");
 }
 
 itsu_status itsu_prefilter_train(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
                                  const itsu_train_config *cfg, float *losses)
 {
-  itsu_status st;
-  if ((st = require_model(ctx, "itsu_prefilter_train")) != ITSU_OK) return st;
-  if (!cfg || !features || !labels || n <= 0) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_train: bad arguments");
-  if (cfg->steps < 0 || cfg->batch <= 0 || cfg->batch % 32 != 0 || !(cfg->lr >= 0.0f) || !(cfg->lr_final >= 0.0f) ||
-      !(cfg->beta1 >= 0.0f && cfg->beta1 < 1.0f) || !(cfg->beta2 >= 0.0f && cfg->beta2 < 1.0f) || !(cfg->eps > 0.0f)) {
-    return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_train: bad configuration");
-  }
-  if (!aligned16(features)) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_train: features must be 16-byte aligned");
-  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
-  const int blocks = itsu::mlp_gradient_blocks(cfg->batch);
-  DeviceScratch<float> partials, m, v, loss;
-  ITSU_CUDA(ctx, cudaMalloc((void **)&partials.p, sizeof(float) * blocks * ITSU_MLP_PARAMS));
-  ITSU_CUDA(ctx, cudaMalloc((void **)&m.p, sizeof(float) * ITSU_MLP_PARAMS));
-  ITSU_CUDA(ctx, cudaMalloc((void **)&v.p, sizeof(float) * ITSU_MLP_PARAMS));
-  ITSU_CUDA(ctx, cudaMalloc((void **)&loss.p, sizeof(float) * std::max<int64_t>(cfg->steps, 1)));
-  ITSU_CUDA(ctx, cudaMemsetAsync(m.p, 0, sizeof(float) * ITSU_MLP_PARAMS, ctx->stream));
-  ITSU_CUDA(ctx, cudaMemsetAsync(v.p, 0, sizeof(float) * ITSU_MLP_PARAMS, ctx->stream));
-  ITSU_CUDA(ctx, cudaMemsetAsync(loss.p, 0, sizeof(float) * std::max<int64_t>(cfg->steps, 1), ctx->stream));
-  double b1t = 1.0, b2t = 1.0;
-  for (int64_t step = 0; step < cfg->steps; ++step) {
-    // cosine decay from lr to lr_final
-    const double frac = cfg->steps > 1 ? (double)step / (double)(cfg->steps - 1) : 0.0;
-    const float lr = (float)(cfg->lr_final + 0.5 * (cfg->lr - cfg->lr_final) * (1.0 + std::cos(3.14159265358979323846 * frac)));
-    b1t *= cfg->beta1;
-    b2t *= cfg->beta2;
-    itsu::launch_mlp_gradient(ctx->d_mlp, features, labels, n, cfg->batch, false, cfg->seed, step, cfg->pos_weight, partials.p,
-                              loss.p + step, ctx->stream);
-    itsu::launch_mlp_adam(ctx->d_master, partials.p, blocks, m.p, v.p, lr, cfg->beta1, cfg->beta2, cfg->eps, cfg->weight_decay,
-                          (float)(1.0 - b1t), (float)(1.0 - b2t), ctx->d_mlp, ctx->stream);
-    if ((step & 1023) == 0) ITSU_CUDA(ctx, cudaGetLastError());
-  }
-  ITSU_CUDA(ctx, cudaGetLastError());
-  if (losses && cfg->steps > 0) {
-    ITSU_CUDA(ctx, cudaMemcpyAsync(losses, loss.p, sizeof(float) * cfg->steps, cudaMemcpyDeviceToHost, ctx->stream));
-  }
-  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return ITSU_OK;
+  return net_train<itsu_prefilter_model>(ctx, features, labels, n, cfg, losses, "itsu_prefilter_train");
+}
+itsu_status itsu_gate_train(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n, const itsu_train_config *cfg,
+                            float *losses)
+{
+  return net_train<itsu_gate_model>(ctx, features, labels, n, cfg, losses, "itsu_gate_train");
 }
 
 itsu_status itsu_prefilter_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n,
                                     float pos_weight, float *grad, float *loss_out)
 {
-  itsu_status st;
-  if ((st = require_model(ctx, "itsu_prefilter_gradient")) != ITSU_OK) return st;
-  if (!features || !labels || !grad || n <= 0 || n > INT32_MAX - 31) {
-    return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_gradient: bad arguments");
-  }
-  if (!aligned16(features)) return fail(ctx, ITSU_ERR_INVALID, "itsu_prefilter_gradient: features must be 16-byte aligned");
-  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
-  const int32_t batch = (int32_t)n;
-  const int blocks = itsu::mlp_gradient_blocks(batch);
-  DeviceScratch<float> partials, loss;
-  ITSU_CUDA(ctx, cudaMalloc((void **)&partials.p, sizeof(float) * blocks * ITSU_MLP_PARAMS));
-  ITSU_CUDA(ctx, cudaMalloc((void **)&loss.p, sizeof(float)));
-  ITSU_CUDA(ctx, cudaMemsetAsync(loss.p, 0, sizeof(float), ctx->stream));
-  itsu::launch_mlp_gradient(ctx->d_mlp, features, labels, n, batch, true, 0, 0, pos_weight, partials.p, loss.p, ctx->stream);
-  ITSU_CUDA(ctx, cudaGetLastError());
-  std::vector<float> h((size_t)blocks * ITSU_MLP_PARAMS);
-  float l = 0.0f;
-  ITSU_CUDA(ctx, cudaMemcpyAsync(h.data(), partials.p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
-  ITSU_CUDA(ctx, cudaMemcpyAsync(&l, loss.p, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (int i = 0; i < ITSU_MLP_PARAMS; ++i) {
-    double sum = 0.0;
-    for (int b = 0; b < blocks; ++b) sum += h[(size_t)b * ITSU_MLP_PARAMS + i];
-    grad[i] = (float)sum;
-  }
-  if (loss_out) *loss_out = l;
-  return ITSU_OK;
+  return net_gradient<itsu_prefilter_model>(ctx, features, labels, n, pos_weight, grad, loss_out, "itsu_prefilter_gradient");
+}
+itsu_status itsu_gate_gradient(itsu_context *ctx, const float *features, const uint8_t *labels, int64_t n, float pos_weight,
+                               float *grad, float *loss_out)
+{
+  return net_gradient<itsu_gate_model>(ctx, features, labels, n, pos_weight, grad, loss_out, "itsu_gate_gradient");
 }
 
 }  // extern "C"

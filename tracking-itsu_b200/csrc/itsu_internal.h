@@ -20,7 +20,10 @@
 
 namespace itsu {
 
-struct MlpDevice;  // the prefilter model (itsu_mlp.cuh)
+template <int H>
+struct MlpDeviceT;                   // a learned network as the device keeps it (itsu_mlp.cuh)
+using MlpDevice = MlpDeviceT<64>;    // the tracklet-pair prefilter (8 -> 64 -> 64 -> 1, GELU)
+using GateDevice = MlpDeviceT<16>;   // the tracklet gate (8 -> 16 -> 16 -> 1, ReLU)
 
 enum : int32_t {
   kFlagInvalid = 1,
@@ -132,6 +135,8 @@ struct Arena {
   itsu_road *roads;
   // learned prefilter of the cell stage (null: the plain path)
   const MlpDevice *mlp;
+  // learned gate of the tracklet stage (null: the plain path)
+  const GateDevice *gate;
   // scan scratch and status
   int64_t *scan_partials;
   DevStatus *status;
@@ -189,26 +194,37 @@ void launch_report(const ReportArgs &r, cudaStream_t stream, int num_sms);
 
 // Every kernel of a run, in launch order, with its name (the instrumentation API times them
 // one by one). The stage launchers above enqueue consecutive ranges of this table.
+enum : int { kPairPrefilterStep = 1, kGateStep = 2 };
 struct KernelStep {
   const char *name;
   void (*launch)(const Arena &, const Launch &);
-  bool learned_only;  // launches a kernel only in the learned-prefilter form
+  int learned_only;  // 0; or the learned network whose form alone launches it (kPairPrefilterStep, kGateStep)
 };
 const KernelStep *pipeline_steps(int *count);
 int kernels_per_run();  // kernels one plain run launches (the learned form adds the learned_only steps)
 
-// Learned prefilter (itsu_prefilter.cu), all asynchronous on `stream`.
-// The FP32 master parameters (itsu_prefilter_model) -> the device model (BF16 weights).
+// Learned networks (itsu_prefilter.cu), all asynchronous on `stream`; each call has an
+// overload for the pair prefilter (itsu_prefilter_model, MlpDevice) and one for the tracklet gate
+// (itsu_gate_model, GateDevice).
+// The FP32 master parameters -> the device model (BF16 weights).
 void launch_mlp_publish(const itsu_prefilter_model *master, MlpDevice *model, cudaStream_t stream);
+void launch_mlp_publish(const itsu_gate_model *master, GateDevice *model, cudaStream_t stream);
 // One training sample per cell of the last run: its pair features and whether a found road uses
 // it; per road, its 5 cells as sample rows and its key (event, 7 layer-local cluster indices).
 void launch_prefilter_export(const Arena &a, const itsu_prefilter_samples &out, int num_sms, cudaStream_t stream);
+// One training sample per tracklet of the last run: its gate features and whether a found road
+// uses it.
+void launch_gate_export(const Arena &a, const itsu_gate_samples &out, int num_sms, cudaStream_t stream);
 void launch_mlp_score(const MlpDevice *model, const float *features, int64_t n, float *logits, int num_sms, cudaStream_t stream);
+void launch_mlp_score(const GateDevice *model, const float *features, int64_t n, float *logits, int num_sms, cudaStream_t stream);
 // Mean-loss gradient of one minibatch: each block writes its partial sum of the gradient to
-// grad_partials[block][kMlpParams] (mlp_gradient_blocks(batch) blocks) and adds the batch loss
+// grad_partials[block][params] (mlp_gradient_blocks(batch) blocks) and adds the batch loss
 // to *loss. With sequential set the batch is samples 0..batch-1; otherwise `batch` samples drawn
 // with replacement from n by (seed, step). features: 16-byte aligned rows of 8 floats.
 void launch_mlp_gradient(const MlpDevice *model, const float *features, const uint8_t *labels, int64_t n, int32_t batch,
+                         bool sequential, uint64_t seed, int64_t step, float pos_weight, float *grad_partials, float *loss,
+                         cudaStream_t stream);
+void launch_mlp_gradient(const GateDevice *model, const float *features, const uint8_t *labels, int64_t n, int32_t batch,
                          bool sequential, uint64_t seed, int64_t step, float pos_weight, float *grad_partials, float *loss,
                          cudaStream_t stream);
 int mlp_gradient_blocks(int32_t batch);
@@ -217,7 +233,10 @@ int mlp_max_gradient_blocks();
 void launch_mlp_adam(itsu_prefilter_model *master, const float *grad_partials, int blocks, float *m, float *v, float lr,
                      float beta1, float beta2, float eps, float weight_decay, float bias1, float bias2, MlpDevice *model,
                      cudaStream_t stream);
+void launch_mlp_adam(itsu_gate_model *master, const float *grad_partials, int blocks, float *m, float *v, float lr, float beta1,
+                     float beta2, float eps, float weight_decay, float bias1, float bias2, GateDevice *model, cudaStream_t stream);
 size_t mlp_device_bytes();
+size_t gate_device_bytes();
 
 // Sets the calling thread's last error message (returned by itsu_last_error(NULL)).
 void set_thread_error(const char *message);

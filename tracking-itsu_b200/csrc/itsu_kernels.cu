@@ -911,6 +911,105 @@ __device__ __forceinline__ int owner_of(int excl, int t)
   return owner;
 }
 
+// Learned form: the tracklet gate. After the count pass and before the tracklet scan, a warp per
+// 32 consecutive inner clusters scores their tracklets (the outer clusters the count pass kept in
+// their slots), 32 at a time on the tensor cores (8 -> 16 -> 16 -> 1, ReLU, BF16 / FP32), keeps
+// those whose logit is not below the gate's threshold (a NaN logit keeps its tracklet), moves the
+// kept slots to the front in their order and lowers the cluster's count and its scan tile's sum by
+// the dropped ones. The write pass then writes the kept tracklets in emission order, as in the plain
+// form. Inner clusters with more than kTrackletSlots tracklets keep all of them, unscored (the
+// crowded pass writes them).
+constexpr int kGateThreads = 256;
+
+__global__ void __launch_bounds__(kGateThreads) k_tracklets_gate(Arena a)
+{
+  __shared__ GateSmem net;
+  __shared__ __align__(16) __nv_bfloat16 rows[kGateThreads / 32][32][kRowPitch];
+  __shared__ unsigned long long keep[kGateThreads / 32][32];
+  load_mlp(net, *a.gate);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t n = a.n_clusters;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
+    const int64_t i = base + lane;
+    int count = 0, layer = 0;
+    int64_t next_begin = 0;
+    float4 c1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float phi1 = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    if (i < n) {
+      count = a.trk_count[i];
+      if (count > 0 && count <= kTrackletSlots) {
+        const int seg = a.clu_seg[i], e = seg / ITSU_LAYERS;
+        layer = seg % ITSU_LAYERS;
+        c1 = a.xyzr[i];
+        phi1 = a.phi[i];
+        next_begin = a.layer_off[seg + 1];
+        vx = a.vtx[3 * e];
+        vy = a.vtx[3 * e + 1];
+        vz = a.vtx[3 * e + 2];
+      }
+    }
+    const bool scored = count <= kTrackletSlots;
+    keep[warp][lane] = 0ull;
+    int total = 0;
+    const int excl = warp_exclusive_sum(scored ? count : 0, total);
+    __syncwarp();
+    for (int p0 = 0; p0 < total; p0 += 32) {
+      const int p = p0 + lane;
+      const int owner = owner_of(excl, p);
+      const int rank = p - __shfl_sync(0xffffffffu, excl, owner);
+      const float4 oc = shfl4(c1, owner);
+      const float ophi = __shfl_sync(0xffffffffu, phi1, owner);
+      const int olayer = __shfl_sync(0xffffffffu, layer, owner);
+      const int64_t onext = __shfl_sync(0xffffffffu, next_begin, owner);
+      const float ovx = __shfl_sync(0xffffffffu, vx, owner), ovy = __shfl_sync(0xffffffffu, vy, owner);
+      const float ovz = __shfl_sync(0xffffffffu, vz, owner);
+      float f[kMlpIn];
+      if (p < total) {
+        const int64_t j = onext + a.trk_slots[(int64_t)rank * a.slot_stride + base + owner];
+        tracklet_features(olayer, oc, ophi, a.xyzr[j], a.phi[j], ovx, ovy, ovz, f);
+      } else {
+#pragma unroll
+        for (int k = 0; k < kMlpIn; ++k) {
+          f[k] = net.mean[k];
+        }
+      }
+      feature_row(net.mean, net.inv_std, f, rows[warp][lane]);
+      __syncwarp();
+      const float logit = mlp_logits_warp<false, kGateHidden, true>(net, rows[warp], nullptr);
+      if (p < total && !(logit < net.threshold)) {
+        atomicOr(&keep[warp][owner], 1ull << rank);
+      }
+      __syncwarp();
+    }
+    // kept slots to the front, in order (coalesced across the warp's clusters, slot by slot)
+    const unsigned long long m = keep[warp][lane];
+    const int scan_to = __reduce_max_sync(0xffffffffu, (unsigned)(scored ? count : 0));
+    int kept = 0;
+    for (int q = 0; q < scan_to; ++q) {
+      if (q < count && ((m >> q) & 1ull)) {
+        if (kept != q) {
+          a.trk_slots[(int64_t)kept * a.slot_stride + i] = a.trk_slots[(int64_t)q * a.slot_stride + i];
+        }
+        ++kept;
+      }
+    }
+    int dropped = 0;
+    if (i < n && scored && count > 0) {
+      a.trk_count[i] = kept;
+      dropped = count - kept;
+    }
+    // the warp's 32 clusters lie in one scan tile (the count pass added their tracklets to its sum)
+    const int warp_dropped = (int)__reduce_add_sync(0xffffffffu, (unsigned)dropped);
+    if (lane == 0 && warp_dropped != 0) {
+      atomicAdd(reinterpret_cast<unsigned long long *>(&a.scan_partials[base / kScanTile]),
+                (unsigned long long)(-(int64_t)warp_dropped));
+    }
+    __syncwarp();
+  }
+}
+
 // Write pass, a warp per 32 consecutive inner clusters: their tracklets form one contiguous range
 // (the scan of the counts), which the warp's lanes fill together: each lane takes the next
 // tracklet of the range, finds its inner cluster (owner) and rank there, reads the outer cluster
@@ -1662,6 +1761,16 @@ void step_tracklets_count(const Arena &a, const Launch &l)
   }
 }
 
+// Launches only in the learned form with the tracklet gate (a.gate set).
+void step_tracklets_gate(const Arena &a, const Launch &l)
+{
+  if (a.gate && a.n_clusters > 0) {
+    const int64_t tiles = (a.n_clusters + 31) / 32;
+    const int64_t blocks = std::min<int64_t>((tiles + kGateThreads / 32 - 1) / (kGateThreads / 32), (int64_t)l.num_sms * 8);
+    k_tracklets_gate<<<(unsigned)blocks, kGateThreads, 0, l.stream>>>(a);
+  }
+}
+
 void step_tracklets_write(const Arena &a, const Launch &l)
 {
   const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
@@ -1720,37 +1829,38 @@ void step_roads(const Arena &a, const Launch &l) { k_roads<<<fixed_grid(l), l.bl
 
 // The whole run, kernel by kernel, in launch order.
 const KernelStep kSteps[] = {
-    {"status_init", step_status_init},                   // 0
-    {"cluster_sort", step_cluster_sort},                 // 1  (a)
-    {"tracklets_count", step_tracklets_count},           // 2  (b)
-    {"scan_partials_tracklets", step_scan_partials<0>},  // 3
-    {"scan_apply_tracklets", step_scan_apply<0>},        // 4
-    {"tracklet_segments", step_tracklet_segments},       // 5
-    {"tracklets_write", step_tracklets_write},           // 6
-    {"tracklets_crowded", step_tracklets_crowded},       // 7
-    {"cells_count", step_cells_count},                   // 8  (c)
-    {"cells_prefilter", step_cells_prefilter, true},     // 9 (learned form only)
-    {"scan_partials_cells", step_scan_partials<1>},      // 10
-    {"scan_apply_cells", step_scan_apply<1>},            // 11
-    {"cell_segments", step_cell_segments},               // 12
-    {"cells_scatter", step_cells_scatter},               // 13
-    {"cells_crowded", step_cells_crowded},               // 14
-    {"neighbour_reset", step_neighbour_reset},           // 15 (d)
-    {"neighbours_count", step_neighbours<false>},        // 16
-    {"scan_reduce_neighbours", step_scan_reduce<2>},     // 17
-    {"scan_partials_neighbours", step_scan_partials<2>}, // 18
-    {"scan_apply_neighbours", step_scan_apply<2>},       // 19
-    {"neighbour_check", step_neighbour_check},           // 20
-    {"neighbours_write", step_neighbours<true>},         // 21
-    {"levels_1", step_levels<1>},                        // 22
-    {"levels_2", step_levels<2>},                        // 23
-    {"levels_3", step_levels<3>},                        // 24
-    {"levels_4", step_levels<4>},                        // 25
-    {"scan_reduce_roads", step_scan_reduce<3>},          // 26 (e)
-    {"scan_partials_roads", step_scan_partials<3>},      // 27
-    {"scan_apply_roads", step_scan_apply<3>},            // 28
-    {"road_segments", step_road_segments},               // 29
-    {"roads_write", step_roads},                         // 30
+    {"status_init", step_status_init, 0},                    // 0
+    {"cluster_sort", step_cluster_sort, 0},                  // 1  (a)
+    {"tracklets_count", step_tracklets_count, 0},            // 2  (b)
+    {"tracklets_gate", step_tracklets_gate, kGateStep},      // 3  (learned form with the gate)
+    {"scan_partials_tracklets", step_scan_partials<0>, 0},   // 4
+    {"scan_apply_tracklets", step_scan_apply<0>, 0},         // 5
+    {"tracklet_segments", step_tracklet_segments, 0},        // 6
+    {"tracklets_write", step_tracklets_write, 0},            // 7
+    {"tracklets_crowded", step_tracklets_crowded, 0},        // 8
+    {"cells_count", step_cells_count, 0},                    // 9  (c)
+    {"cells_prefilter", step_cells_prefilter, kPairPrefilterStep},  // 10 (learned form with the pair prefilter)
+    {"scan_partials_cells", step_scan_partials<1>, 0},       // 11
+    {"scan_apply_cells", step_scan_apply<1>, 0},             // 12
+    {"cell_segments", step_cell_segments, 0},                // 13
+    {"cells_scatter", step_cells_scatter, 0},                // 14
+    {"cells_crowded", step_cells_crowded, 0},                // 15
+    {"neighbour_reset", step_neighbour_reset, 0},            // 16 (d)
+    {"neighbours_count", step_neighbours<false>, 0},         // 17
+    {"scan_reduce_neighbours", step_scan_reduce<2>, 0},      // 18
+    {"scan_partials_neighbours", step_scan_partials<2>, 0},  // 19
+    {"scan_apply_neighbours", step_scan_apply<2>, 0},        // 20
+    {"neighbour_check", step_neighbour_check, 0},            // 21
+    {"neighbours_write", step_neighbours<true>, 0},          // 22
+    {"levels_1", step_levels<1>, 0},                         // 23
+    {"levels_2", step_levels<2>, 0},                         // 24
+    {"levels_3", step_levels<3>, 0},                         // 25
+    {"levels_4", step_levels<4>, 0},                         // 26
+    {"scan_reduce_roads", step_scan_reduce<3>, 0},           // 27 (e)
+    {"scan_partials_roads", step_scan_partials<3>, 0},       // 28
+    {"scan_apply_roads", step_scan_apply<3>, 0},             // 29
+    {"road_segments", step_road_segments, 0},                // 30
+    {"roads_write", step_roads, 0},                          // 31
 };
 constexpr int kNumSteps = sizeof(kSteps) / sizeof(kSteps[0]);
 
@@ -1809,14 +1919,14 @@ const KernelStep *pipeline_steps(int *count)
 
 void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l); }
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
-void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 5, a, l); }
-void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(6, 7, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(8, 12, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(13, 14, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(15, 20, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(21, 25, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(26, 29, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(30, 30, a, l); }
+void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
+void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 13, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 15, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
 
 int kernels_per_run()
 {

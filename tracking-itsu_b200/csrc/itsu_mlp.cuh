@@ -20,66 +20,96 @@
 namespace itsu {
 
 constexpr int kMlpIn = 8;
+
+// Parameter count and offsets of the trainable parameters of an 8 -> H -> H -> 1 network in its
+// flat FP32 master array (w1 [H][8], b1, w2 [H][H], b2, w3 [H], b3: the C ABI model order).
+template <int H>
+struct MlpShape {
+  static_assert(H % 16 == 0 && H >= 16 && H <= 64, "hidden width: whole 16-wide MMA tiles");
+  static constexpr int kHidden = H;
+  static constexpr int kParams = H * kMlpIn + H + H * H + H + H + 1;
+  static constexpr int kOffW1 = 0;
+  static constexpr int kOffB1 = kOffW1 + H * kMlpIn;
+  static constexpr int kOffW2 = kOffB1 + H;
+  static constexpr int kOffB2 = kOffW2 + H * H;
+  static constexpr int kOffW3 = kOffB2 + H;
+  static constexpr int kOffB3 = kOffW3 + H;
+  // row pitch (BF16 elements) of the [out][in] W2 / W3 operands and of hidden-activation rows:
+  // H + 8, so that the 8 rows one fragment load touches fall in distinct banks
+  static constexpr int kHidPitch = H + 8;
+};
+
+// The pair prefilter's network (8 -> 64 -> 64 -> 1, GELU).
 constexpr int kMlpHidden = 64;
-constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1;
-// Offsets of the trainable parameters in the flat FP32 master array (itsu_prefilter_model order).
-constexpr int kOffW1 = 0;
-constexpr int kOffB1 = kOffW1 + kMlpHidden * kMlpIn;
-constexpr int kOffW2 = kOffB1 + kMlpHidden;
-constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;
-constexpr int kOffW3 = kOffB2 + kMlpHidden;
-constexpr int kOffB3 = kOffW3 + kMlpHidden;
+constexpr int kMlpParams = MlpShape<kMlpHidden>::kParams;
+constexpr int kOffW1 = MlpShape<kMlpHidden>::kOffW1;
+constexpr int kOffB1 = MlpShape<kMlpHidden>::kOffB1;
+constexpr int kOffW2 = MlpShape<kMlpHidden>::kOffW2;
+constexpr int kOffB2 = MlpShape<kMlpHidden>::kOffB2;
+constexpr int kOffW3 = MlpShape<kMlpHidden>::kOffW3;
+constexpr int kOffB3 = MlpShape<kMlpHidden>::kOffB3;
 static_assert(kOffB3 + 1 == kMlpParams, "parameter layout");
+// The tracklet gate's network (8 -> 16 -> 16 -> 1, ReLU).
+constexpr int kGateHidden = 16;
+constexpr int kGateParams = MlpShape<kGateHidden>::kParams;
 
 // Row pitches (in BF16 elements) of the shared-memory operands, padded so that the 8 rows one
 // MMA fragment load touches fall in distinct banks.
 constexpr int kRowPitch = 24;  // feature rows and W1 rows (16 used)
-constexpr int kHidPitch = 72;  // W2 / W3 rows and hidden-activation rows (64 used)
+constexpr int kHidPitch = MlpShape<kMlpHidden>::kHidPitch;  // the pair network's W2 / W3 / hidden rows
 constexpr int kSmpPitch = 40;  // transposed [unit][sample] operands (32 used)
 
-// The model as the device keeps it in global memory.
-struct MlpDevice {
-  __nv_bfloat16 w1[kMlpHidden][kMlpIn];       // [out][in]
-  __nv_bfloat16 w2[kMlpHidden][kMlpHidden];   // [out][in]
-  __nv_bfloat16 w3[kMlpHidden];
-  float b1[kMlpHidden];
-  float b2[kMlpHidden];
+// A network as the device keeps it in global memory.
+template <int H>
+struct MlpDeviceT {
+  __nv_bfloat16 w1[H][kMlpIn];  // [out][in]
+  __nv_bfloat16 w2[H][H];       // [out][in]
+  __nv_bfloat16 w3[H];
+  float b1[H];
+  float b2[H];
   float b3;
   float threshold;
   float mean[kMlpIn];
   float inv_std[kMlpIn];
 };
 
-// The model staged in shared memory in MMA-friendly, zero-padded form.
-struct __align__(16) MlpSmem {
-  __nv_bfloat16 w1[kMlpHidden][kRowPitch];  // columns 8.. are zero (the first MMA has K = 16)
-  __nv_bfloat16 w2[kMlpHidden][kHidPitch];
-  __nv_bfloat16 w3[8][kHidPitch];           // row 0 holds the output weights, rows 1..7 are zero (N = 8)
-  float b1[kMlpHidden];
-  float b2[kMlpHidden];
+// A network staged in shared memory in MMA-friendly, zero-padded form.
+template <int H>
+struct __align__(16) MlpSmemT {
+  static constexpr int kPitch = MlpShape<H>::kHidPitch;
+  __nv_bfloat16 w1[H][kRowPitch];  // columns 8.. are zero (the first MMA has K = 16)
+  __nv_bfloat16 w2[H][kPitch];
+  __nv_bfloat16 w3[8][kPitch];     // row 0 holds the output weights, rows 1..7 are zero (N = 8)
+  float b1[H];
+  float b2[H];
   float b3;
   float threshold;
   float mean[kMlpIn];
   float inv_std[kMlpIn];
 };
 
-// Block-cooperative copy of the model into shared memory (the caller synchronises the block).
-__device__ __forceinline__ void load_mlp(MlpSmem &s, const MlpDevice &g)
+using MlpSmem = MlpSmemT<kMlpHidden>;
+using GateSmem = MlpSmemT<kGateHidden>;
+
+// Block-cooperative copy of a network into shared memory (the caller synchronises the block).
+template <int H>
+__device__ __forceinline__ void load_mlp(MlpSmemT<H> &s, const MlpDeviceT<H> &g)
 {
+  constexpr int P = MlpSmemT<H>::kPitch;
   const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
-  for (int i = threadIdx.x; i < kMlpHidden * kRowPitch; i += blockDim.x) {
+  for (int i = threadIdx.x; i < H * kRowPitch; i += blockDim.x) {
     const int r = i / kRowPitch, c = i % kRowPitch;
     s.w1[r][c] = c < kMlpIn ? g.w1[r][c] : zero;
   }
-  for (int i = threadIdx.x; i < kMlpHidden * kHidPitch; i += blockDim.x) {
-    const int r = i / kHidPitch, c = i % kHidPitch;
-    s.w2[r][c] = c < kMlpHidden ? g.w2[r][c] : zero;
+  for (int i = threadIdx.x; i < H * P; i += blockDim.x) {
+    const int r = i / P, c = i % P;
+    s.w2[r][c] = c < H ? g.w2[r][c] : zero;
   }
-  for (int i = threadIdx.x; i < 8 * kHidPitch; i += blockDim.x) {
-    const int r = i / kHidPitch, c = i % kHidPitch;
-    s.w3[r][c] = (r == 0 && c < kMlpHidden) ? g.w3[c] : zero;
+  for (int i = threadIdx.x; i < 8 * P; i += blockDim.x) {
+    const int r = i / P, c = i % P;
+    s.w3[r][c] = (r == 0 && c < H) ? g.w3[c] : zero;
   }
-  for (int i = threadIdx.x; i < kMlpHidden; i += blockDim.x) {
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
     s.b1[i] = g.b1[i];
     s.b2[i] = g.b2[i];
   }
@@ -177,19 +207,44 @@ __device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], uint32
 // and (k 2t+8.., col g); D holds (row g, col 2t), (row g, col 2t+1), (row g+8, col 2t), (row g+8,
 // col 2t+1).
 
+// Hidden-layer activation: GELU (the pair prefilter) or ReLU (the tracklet gate, which scores
+// every tracklet: its activation must be cheap).
+template <bool kRelu>
+__device__ __forceinline__ float act(float x)
+{
+  if constexpr (kRelu) {
+    return fmaxf(x, 0.0f);
+  } else {
+    return gelu(x);
+  }
+}
+
+template <bool kRelu>
+__device__ __forceinline__ float act_grad(float x)
+{
+  if constexpr (kRelu) {
+    return x > 0.0f ? 1.0f : 0.0f;
+  } else {
+    return gelu_grad(x);
+  }
+}
+
 // Where the training pass keeps a 32-sample tile's intermediate values.
-struct MlpTrace {
-  float (*a1)[kMlpHidden + 1];  // [sample][unit] layer-1 pre-activations
-  float (*a2)[kMlpHidden + 1];  // [sample][unit] layer-2 pre-activations
+template <int H>
+struct MlpTraceT {
+  float (*a1)[H + 1];               // [sample][unit] layer-1 pre-activations
+  float (*a2)[H + 1];               // [sample][unit] layer-2 pre-activations
   __nv_bfloat16 (*h1t)[kSmpPitch];  // [unit][sample] layer-1 activations (BF16, as the next MMA sees them)
 };
+using MlpTrace = MlpTraceT<kMlpHidden>;
 
 // Forward pass of rows 16 mt .. 16 mt + 15 of a 32-row tile; returns the logits of rows g and
 // g + 8 of the tile in lo / hi (valid in lanes with t == 0). All lanes of the warp take part.
-template <bool kTrace>
-__device__ __forceinline__ void mlp_forward_m16(const MlpSmem &m, const __nv_bfloat16 (*rows)[kRowPitch], int mt, float &lo,
-                                                float &hi, const MlpTrace *trace)
+template <bool kTrace, int H, bool kRelu>
+__device__ __forceinline__ void mlp_forward_m16(const MlpSmemT<H> &m, const __nv_bfloat16 (*rows)[kRowPitch], int mt, float &lo,
+                                                float &hi, const MlpTraceT<H> *trace)
 {
+  constexpr int NT = H / 8, KT = H / 16;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int r0 = mt * 16 + g, r1 = r0 + 8;
   uint32_t a[4];
@@ -197,10 +252,10 @@ __device__ __forceinline__ void mlp_forward_m16(const MlpSmem &m, const __nv_bfl
   a[1] = ld32(&rows[r1][2 * t]);
   a[2] = ld32(&rows[r0][2 * t + 8]);
   a[3] = ld32(&rows[r1][2 * t + 8]);
-  // layer 1: [16 x 16] x [16 x 64] -> GELU -> BF16 A fragments of layer 2 (hk[kk] covers k 16kk..)
-  uint32_t hk[4][4];
+  // layer 1: [16 x 16] x [16 x H] -> activation -> BF16 A fragments of layer 2 (hk[kk] covers k 16kk..)
+  uint32_t hk[KT][4];
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
+  for (int nt = 0; nt < NT; ++nt) {
     float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     mma_bf16(c, a, ld32(&m.w1[nt * 8 + g][2 * t]), ld32(&m.w1[nt * 8 + g][2 * t + 8]));
     const int col = nt * 8 + 2 * t;
@@ -208,7 +263,8 @@ __device__ __forceinline__ void mlp_forward_m16(const MlpSmem &m, const __nv_bfl
     c[1] += m.b1[col + 1];
     c[2] += m.b1[col];
     c[3] += m.b1[col + 1];
-    const uint32_t top = pack_bf16(gelu(c[0]), gelu(c[1])), bottom = pack_bf16(gelu(c[2]), gelu(c[3]));
+    const uint32_t top = pack_bf16(act<kRelu>(c[0]), act<kRelu>(c[1]));
+    const uint32_t bottom = pack_bf16(act<kRelu>(c[2]), act<kRelu>(c[3]));
     hk[nt >> 1][(nt & 1) * 2 + 0] = top;
     hk[nt >> 1][(nt & 1) * 2 + 1] = bottom;
     if constexpr (kTrace) {
@@ -224,23 +280,23 @@ __device__ __forceinline__ void mlp_forward_m16(const MlpSmem &m, const __nv_bfl
       trace->h1t[col + 1][r1] = bv.y;
     }
   }
-  // layer 2: [16 x 64] x [64 x 64]
-  float h2[8][4];
+  // layer 2: [16 x H] x [H x H]
+  float h2[NT][4];
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
+  for (int nt = 0; nt < NT; ++nt) {
     h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.0f;
   }
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < KT; ++kk) {
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
+    for (int nt = 0; nt < NT; ++nt) {
       mma_bf16(h2[nt], hk[kk], ld32(&m.w2[nt * 8 + g][16 * kk + 2 * t]), ld32(&m.w2[nt * 8 + g][16 * kk + 2 * t + 8]));
     }
   }
-  // layer 3: [16 x 64] x [64 x 8], column 0 real
+  // layer 3: [16 x H] x [H x 8], column 0 real
   float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < KT; ++kk) {
     uint32_t ak[4];
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
@@ -254,8 +310,8 @@ __device__ __forceinline__ void mlp_forward_m16(const MlpSmem &m, const __nv_bfl
         trace->a2[r1][col] = v2;
         trace->a2[r1][col + 1] = v3;
       }
-      ak[half * 2 + 0] = pack_bf16(gelu(v0), gelu(v1));
-      ak[half * 2 + 1] = pack_bf16(gelu(v2), gelu(v3));
+      ak[half * 2 + 0] = pack_bf16(act<kRelu>(v0), act<kRelu>(v1));
+      ak[half * 2 + 1] = pack_bf16(act<kRelu>(v2), act<kRelu>(v3));
     }
     mma_bf16(o, ak, ld32(&m.w3[g][16 * kk + 2 * t]), ld32(&m.w3[g][16 * kk + 2 * t + 8]));
   }
@@ -263,16 +319,22 @@ __device__ __forceinline__ void mlp_forward_m16(const MlpSmem &m, const __nv_bfl
   hi = o[2] + m.b3;
 }
 
+template <class T>
+struct NoDeduce {
+  using type = T;
+};
+
 // Logits of the 32 rows of a tile; lane l gets row l's. All lanes of the warp take part.
-template <bool kTrace>
-__device__ __forceinline__ float mlp_logits_warp(const MlpSmem &m, const __nv_bfloat16 (*rows)[kRowPitch], const MlpTrace *trace)
+template <bool kTrace, int H = kMlpHidden, bool kRelu = false>
+__device__ __forceinline__ float mlp_logits_warp(const MlpSmemT<H> &m, const __nv_bfloat16 (*rows)[kRowPitch],
+                                                 const typename NoDeduce<MlpTraceT<H>>::type *trace)
 {
   const int lane = threadIdx.x & 31;
   float mine = 0.0f;
 #pragma unroll 1
   for (int mt = 0; mt < 2; ++mt) {
     float lo, hi;
-    mlp_forward_m16<kTrace>(m, rows, mt, lo, hi, trace);
+    mlp_forward_m16<kTrace, H, kRelu>(m, rows, mt, lo, hi, trace);
     // row r of this m-tile sits in lane 4 (r mod 8), in lo for r < 8 and hi otherwise
     const int src = (lane & 7) << 2;
     lo = __shfl_sync(0xffffffffu, lo, src);
@@ -282,6 +344,29 @@ __device__ __forceinline__ float mlp_logits_warp(const MlpSmem &m, const __nv_bf
     }
   }
   return mine;
+}
+
+// The tracklet gate's 8 raw features of the tracklet from inner cluster c1 to outer cluster c2
+// (c = (x, y, z, r), phi the clusters' azimuths about the vertex, as the clustering computed
+// them): |dphi| and dphi (wrapped to [-pi, pi]), the tracklet cut's dz (Tracker.cxx:93-95) and its
+// absolute value, the signed curvature of the circle through the vertex and both clusters, the
+// inner layer, the inner cluster's radius and its slope from the vertex.
+__device__ __forceinline__ void tracklet_features(int layer, float4 c1, float phi1, float4 c2, float phi2, float vx, float vy,
+                                                  float vz, float f[kMlpIn])
+{
+  constexpr float kPiF = 3.14159265358979323846f, kTwoPiF = 6.28318530717958647692f;
+  float dphi = phi1 - phi2;
+  dphi = dphi > kPiF ? dphi - kTwoPiF : (dphi < -kPiF ? dphi + kTwoPiF : dphi);
+  const float tan_lambda = (c1.z - vz) / c1.w;
+  const float dz = tan_lambda * (c2.w - c1.w) + c1.z - c2.z;
+  f[0] = fabsf(dphi);
+  f[1] = dz;
+  f[2] = fabsf(dz);
+  f[3] = circle_curvature(vx, vy, c1.x, c1.y, c2.x, c2.y);
+  f[4] = (float)layer;
+  f[5] = c1.w;
+  f[6] = tan_lambda;
+  f[7] = dphi;
 }
 
 }  // namespace itsu

@@ -37,31 +37,40 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x)
 
 // ---- publish: FP32 master -> device model ----
 
-__global__ void k_mlp_publish(const itsu_prefilter_model *master, MlpDevice *model)
+// The FP32 master of an 8 -> H -> H -> 1 network (itsu_prefilter_model / itsu_gate_model): the
+// trainable parameters in MlpShape<H> order, then mean[8], inv_std[8] and the logit threshold.
+template <int H>
+__device__ __forceinline__ void publish_param(MlpDeviceT<H> *model, int i, float w)
 {
-  const float *p = &master->w1[0][0];
-  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
-    const float w = p[i];
-    if (i < kOffB1) {
-      model->w1[i / kMlpIn][i % kMlpIn] = __float2bfloat16_rn(w);
-    } else if (i < kOffW2) {
-      model->b1[i - kOffB1] = w;
-    } else if (i < kOffB2) {
-      model->w2[(i - kOffW2) / kMlpHidden][(i - kOffW2) % kMlpHidden] = __float2bfloat16_rn(w);
-    } else if (i < kOffW3) {
-      model->b2[i - kOffB2] = w;
-    } else if (i < kOffB3) {
-      model->w3[i - kOffW3] = __float2bfloat16_rn(w);
-    } else {
-      model->b3 = w;
-    }
+  using S = MlpShape<H>;
+  if (i < S::kOffB1) {
+    model->w1[i / kMlpIn][i % kMlpIn] = __float2bfloat16_rn(w);
+  } else if (i < S::kOffW2) {
+    model->b1[i - S::kOffB1] = w;
+  } else if (i < S::kOffB2) {
+    model->w2[(i - S::kOffW2) / H][(i - S::kOffW2) % H] = __float2bfloat16_rn(w);
+  } else if (i < S::kOffW3) {
+    model->b2[i - S::kOffB2] = w;
+  } else if (i < S::kOffB3) {
+    model->w3[i - S::kOffW3] = __float2bfloat16_rn(w);
+  } else {
+    model->b3 = w;
+  }
+}
+
+template <int H>
+__global__ void k_mlp_publish(const float *master, MlpDeviceT<H> *model)
+{
+  constexpr int P = MlpShape<H>::kParams;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    publish_param<H>(model, i, master[i]);
   }
   for (int i = threadIdx.x; i < kMlpIn; i += blockDim.x) {
-    model->mean[i] = master->mean[i];
-    model->inv_std[i] = master->inv_std[i];
+    model->mean[i] = master[P + i];
+    model->inv_std[i] = master[P + kMlpIn + i];
   }
   if (threadIdx.x == 0) {
-    model->threshold = master->logit_threshold;
+    model->threshold = master[P + 2 * kMlpIn];
   }
 }
 
@@ -145,13 +154,81 @@ __global__ void k_export_roads(Arena a, itsu_prefilter_samples out)
   }
 }
 
+// ---- gate export: one sample per tracklet, on-road labels ----
+
+__global__ void k_export_tracklets(Arena a, itsu_gate_samples out)
+{
+  const int64_t n = a.status->total[kTracklets];
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    if (out.labels) {
+      out.labels[k] = 0;
+    }
+    if (!out.features) {
+      continue;
+    }
+    const int sid = a.trk_seg_id[k];
+    const int e = sid / ITSU_TRACKLET_LAYERS, layer = sid % ITSU_TRACKLET_LAYERS;
+    const itsu_tracklet t = a.tracklets[k];
+    const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
+    const int64_t i1 = lo[layer] + t.first_cluster, i2 = lo[layer + 1] + t.second_cluster;
+    float f[kMlpIn];
+    tracklet_features(layer, a.xyzr[i1], a.phi[i1], a.xyzr[i2], a.phi[i2], a.vtx[3 * e], a.vtx[3 * e + 1], a.vtx[3 * e + 2], f);
+    float4 *dst = reinterpret_cast<float4 *>(out.features + k * kMlpIn);
+    dst[0] = make_float4(f[0], f[1], f[2], f[3]);
+    dst[1] = make_float4(f[4], f[5], f[6], f[7]);
+  }
+}
+
+// Marks the two tracklets of every cell of every road (after k_export_tracklets cleared them) and
+// lists each road's tracklets, layers 0..5 (-1 where the road has no cell).
+__global__ void k_export_tracklet_labels(Arena a, itsu_gate_samples out)
+{
+  const int64_t n = a.status->total[kRoads];
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    int lo_e = 0, hi_e = a.n_events - 1;  // the road's event: last e with road_seg[e] <= r
+    while (lo_e < hi_e) {
+      const int mid = (lo_e + hi_e + 1) >> 1;
+      if (a.road_seg[mid] <= r) {
+        lo_e = mid;
+      } else {
+        hi_e = mid - 1;
+      }
+    }
+    const itsu_road road = a.roads[r];
+    const int32_t *cs = a.cell_seg + lo_e * ITSU_CELL_LAYERS;
+    const int32_t *ts = a.trk_seg + lo_e * ITSU_TRACKLET_LAYERS;
+    int32_t rows[ITSU_TRACKLET_LAYERS];
+    for (int l = 0; l < ITSU_TRACKLET_LAYERS; ++l) {
+      rows[l] = -1;
+    }
+    for (int l = 0; l < ITSU_CELL_LAYERS; ++l) {
+      if (road.cell_ids[l] < 0) {
+        continue;
+      }
+      const itsu_cell cell = a.cells[cs[l] + road.cell_ids[l]];
+      rows[l] = ts[l] + cell.first_tracklet;
+      rows[l + 1] = ts[l + 1] + cell.second_tracklet;
+    }
+    for (int l = 0; l < ITSU_TRACKLET_LAYERS; ++l) {
+      if (out.labels && rows[l] >= 0) {
+        out.labels[rows[l]] = 1;
+      }
+      if (out.road_tracklets) {
+        out.road_tracklets[r * ITSU_TRACKLET_LAYERS + l] = rows[l];
+      }
+    }
+  }
+}
+
 // ---- scoring ----
 
 constexpr int kScoreThreads = 256;
 
-__global__ void __launch_bounds__(kScoreThreads) k_mlp_score(const MlpDevice *model, const float *features, int64_t n, float *logits)
+template <int H, bool kRelu>
+__global__ void __launch_bounds__(kScoreThreads) k_mlp_score(const MlpDeviceT<H> *model, const float *features, int64_t n,
+                                                            float *logits)
 {
-  __shared__ MlpSmem mlp;
+  __shared__ MlpSmemT<H> mlp;
   __shared__ __align__(16) __nv_bfloat16 rows[kScoreThreads / 32][32][kRowPitch];
   load_mlp(mlp, *model);
   __syncthreads();
@@ -165,7 +242,7 @@ __global__ void __launch_bounds__(kScoreThreads) k_mlp_score(const MlpDevice *mo
     }
     feature_row(mlp.mean, mlp.inv_std, f, rows[warp][lane]);
     __syncwarp();
-    const float logit = mlp_logits_warp<false>(mlp, rows[warp], nullptr);
+    const float logit = mlp_logits_warp<false, H, kRelu>(mlp, rows[warp], nullptr);
     if (row < n) {
       logits[row] = logit;
     }
@@ -175,45 +252,51 @@ __global__ void __launch_bounds__(kScoreThreads) k_mlp_score(const MlpDevice *mo
 
 // ---- training: minibatch gradient ----
 
-// One warp's 32-sample tile of the training pass.
+// One warp's 32-sample tile of the training pass of an 8 -> H -> H -> 1 network.
+template <int H>
 struct TrainWarp {
-  __nv_bfloat16 x[32][kRowPitch];             // standardised inputs [sample][feature] (A of layer 1)
-  __nv_bfloat16 xt[8][kSmpPitch];             // the same, [feature][sample] (B of dW1)
-  float a1[32][kMlpHidden + 1];               // layer-1 pre-activations, then dL/da1
-  float a2[32][kMlpHidden + 1];               // layer-2 pre-activations, then dL/da2
-  __nv_bfloat16 h1t[kMlpHidden][kSmpPitch];   // layer-1 activations [unit][sample] (B of dW2)
-  __nv_bfloat16 d2[32][kHidPitch];            // dL/da2 [sample][unit] (A of dh1)
-  __nv_bfloat16 d2t[kMlpHidden][kSmpPitch];   // dL/da2 [unit][sample] (A of dW2)
-  __nv_bfloat16 d1t[kMlpHidden][kSmpPitch];   // dL/da1 [unit][sample] (A of dW1)
-  float dz[32];                               // dL/dlogit
+  static constexpr int kPitch = MlpShape<H>::kHidPitch;
+  __nv_bfloat16 x[32][kRowPitch];     // standardised inputs [sample][feature] (A of layer 1)
+  __nv_bfloat16 xt[8][kSmpPitch];     // the same, [feature][sample] (B of dW1)
+  float a1[32][H + 1];                // layer-1 pre-activations, then dL/da1
+  float a2[32][H + 1];                // layer-2 pre-activations, then dL/da2
+  __nv_bfloat16 h1t[H][kSmpPitch];    // layer-1 activations [unit][sample] (B of dW2)
+  __nv_bfloat16 d2[32][kPitch];       // dL/da2 [sample][unit] (A of dh1)
+  __nv_bfloat16 d2t[H][kSmpPitch];    // dL/da2 [unit][sample] (A of dW2)
+  __nv_bfloat16 d1t[H][kSmpPitch];    // dL/da1 [unit][sample] (A of dW1)
+  float dz[32];                       // dL/dlogit
 };
 
+template <int H>
 struct __align__(16) TrainBlock {
-  MlpSmem mlp;
-  __nv_bfloat16 w2t[kMlpHidden][kHidPitch];   // W2 transposed [in][out] (B of dh1)
-  float grad[kMlpParams];
-  TrainWarp warps[kTrainWarps];
+  MlpSmemT<H> mlp;
+  __nv_bfloat16 w2t[H][MlpShape<H>::kHidPitch];  // W2 transposed [in][out] (B of dh1)
+  float grad[MlpShape<H>::kParams];
+  TrainWarp<H> warps[kTrainWarps];
 };
 
-__global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDevice *model, const float *features,
+template <int H, bool kRelu>
+__global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDeviceT<H> *model, const float *features,
                                                                    const uint8_t *labels, int64_t n, int32_t batch,
                                                                    int32_t sequential, uint64_t seed, int64_t step,
                                                                    float pos_weight, float *grad_partials, float *loss)
 {
+  using S = MlpShape<H>;
+  constexpr int NT = H / 8, KT = H / 16, P = S::kHidPitch;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TrainBlock &B = *reinterpret_cast<TrainBlock *>(smem_raw);
+  TrainBlock<H> &B = *reinterpret_cast<TrainBlock<H> *>(smem_raw);
   load_mlp(B.mlp, *model);
-  for (int i = threadIdx.x; i < kMlpHidden * kHidPitch; i += blockDim.x) {
-    const int r = i / kHidPitch, c = i % kHidPitch;
-    B.w2t[r][c] = c < kMlpHidden ? model->w2[c][r] : __float2bfloat16_rn(0.0f);
+  for (int i = threadIdx.x; i < H * P; i += blockDim.x) {
+    const int r = i / P, c = i % P;
+    B.w2t[r][c] = c < H ? model->w2[c][r] : __float2bfloat16_rn(0.0f);
   }
-  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+  for (int i = threadIdx.x; i < S::kParams; i += blockDim.x) {
     B.grad[i] = 0.0f;
   }
   __syncthreads();
-  const MlpSmem &P = B.mlp;
+  const MlpSmemT<H> &M = B.mlp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-  TrainWarp &W = B.warps[warp];
+  TrainWarp<H> &W = B.warps[warp];
   const float inv_batch = 1.0f / (float)batch;
   const int64_t tiles = (batch + 31) / 32;
   for (int64_t tile = (int64_t)blockIdx.x * kTrainWarps + warp; tile < tiles; tile += (int64_t)gridDim.x * kTrainWarps) {
@@ -230,17 +313,17 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDevi
       y = labels[idx] ? 1.0f : 0.0f;
     } else {
       for (int q = 0; q < kMlpIn; ++q) {
-        f[q] = P.mean[q];
+        f[q] = M.mean[q];
       }
     }
-    feature_row(P.mean, P.inv_std, f, W.x[lane]);
+    feature_row(M.mean, M.inv_std, f, W.x[lane]);
     for (int q = 0; q < kMlpIn; ++q) {
       W.xt[q][lane] = W.x[lane][q];
     }
     __syncwarp();
     // 2. forward, keeping the pre-activations and the layer-1 activations
-    const MlpTrace trace{W.a1, W.a2, W.h1t};
-    const float z = mlp_logits_warp<true>(P, W.x, &trace);
+    const MlpTraceT<H> trace{W.a1, W.a2, W.h1t};
+    const float z = mlp_logits_warp<true, H, kRelu>(M, W.x, &trace);
     // 3. loss and dL/dz: weighted binary cross-entropy of sigmoid(z), averaged over the batch
     const float wgt = valid ? (y > 0.0f ? pos_weight : 1.0f) : 0.0f;
     const float prob = 1.0f / (1.0f + expf(-z));
@@ -253,23 +336,23 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDevi
     }
     if (lane == 0) {
       atomicAdd(loss, l);
-      atomicAdd(&B.grad[kOffB3], dzsum);
+      atomicAdd(&B.grad[S::kOffB3], dzsum);
     }
     __syncwarp();
     // 4. dW3 (lane owns units lane and lane + 32)
-    for (int jj = lane; jj < kMlpHidden; jj += 32) {
+    for (int jj = lane; jj < H; jj += 32) {
       float acc = 0.0f;
-      for (int s = 0; s < 32; ++s) {
-        acc += W.dz[s] * bf16r(gelu(W.a2[s][jj]));
+      for (int s2 = 0; s2 < 32; ++s2) {
+        acc += W.dz[s2] * bf16r(act<kRelu>(W.a2[s2][jj]));
       }
-      atomicAdd(&B.grad[kOffW3 + jj], acc);
+      atomicAdd(&B.grad[S::kOffW3 + jj], acc);
     }
     __syncwarp();
     // 5. dL/da2 (lane owns sample lane)
     {
       const float dz = W.dz[lane];
-      for (int j = 0; j < kMlpHidden; ++j) {
-        const float d = dz * __bfloat162float(P.w3[0][j]) * gelu_grad(W.a2[lane][j]);
+      for (int j = 0; j < H; ++j) {
+        const float d = dz * __bfloat162float(M.w3[0][j]) * act_grad<kRelu>(W.a2[lane][j]);
         W.a2[lane][j] = d;
         const __nv_bfloat16 db = __float2bfloat16_rn(d);
         W.d2[lane][j] = db;
@@ -277,18 +360,18 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDevi
       }
     }
     __syncwarp();
-    for (int jj = lane; jj < kMlpHidden; jj += 32) {
+    for (int jj = lane; jj < H; jj += 32) {
       float acc = 0.0f;
-      for (int s = 0; s < 32; ++s) {
-        acc += W.a2[s][jj];
+      for (int s2 = 0; s2 < 32; ++s2) {
+        acc += W.a2[s2][jj];
       }
-      atomicAdd(&B.grad[kOffB2 + jj], acc);
+      atomicAdd(&B.grad[S::kOffB2 + jj], acc);
     }
-    // 6. dW2 = dL/da2^T h1: [64 j x 32 s] x [32 s x 64 i]
-    for (int mt = 0; mt < 4; ++mt) {
-      float acc[8][4];
+    // 6. dW2 = dL/da2^T h1: [H j x 32 s] x [32 s x H i]
+    for (int mt = 0; mt < KT; ++mt) {
+      float acc[NT][4];
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
+      for (int nt = 0; nt < NT; ++nt) {
         acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
       }
 #pragma unroll
@@ -299,60 +382,60 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDevi
         a[2] = ld32(&W.d2t[16 * mt + g][16 * kk + 2 * t + 8]);
         a[3] = ld32(&W.d2t[16 * mt + g + 8][16 * kk + 2 * t + 8]);
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
+        for (int nt = 0; nt < NT; ++nt) {
           mma_bf16(acc[nt], a, ld32(&W.h1t[nt * 8 + g][16 * kk + 2 * t]), ld32(&W.h1t[nt * 8 + g][16 * kk + 2 * t + 8]));
         }
       }
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        float *row0 = &B.grad[kOffW2 + (16 * mt + g) * kMlpHidden + nt * 8 + 2 * t];
-        float *row1 = row0 + 8 * kMlpHidden;
+      for (int nt = 0; nt < NT; ++nt) {
+        float *row0 = &B.grad[S::kOffW2 + (16 * mt + g) * H + nt * 8 + 2 * t];
+        float *row1 = row0 + 8 * H;
         atomicAdd(row0, acc[nt][0]);
         atomicAdd(row0 + 1, acc[nt][1]);
         atomicAdd(row1, acc[nt][2]);
         atomicAdd(row1 + 1, acc[nt][3]);
       }
     }
-    // 7. dL/da1 = (dL/da2 W2) * gelu'(a1): [32 s x 64 j] x [64 j x 64 i]
+    // 7. dL/da1 = (dL/da2 W2) * act'(a1): [32 s x H j] x [H j x H i]
     for (int mt = 0; mt < 2; ++mt) {
-      float acc[8][4];
+      float acc[NT][4];
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
+      for (int nt = 0; nt < NT; ++nt) {
         acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
       }
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
+      for (int kk = 0; kk < KT; ++kk) {
         uint32_t a[4];
         a[0] = ld32(&W.d2[16 * mt + g][16 * kk + 2 * t]);
         a[1] = ld32(&W.d2[16 * mt + g + 8][16 * kk + 2 * t]);
         a[2] = ld32(&W.d2[16 * mt + g][16 * kk + 2 * t + 8]);
         a[3] = ld32(&W.d2[16 * mt + g + 8][16 * kk + 2 * t + 8]);
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
+        for (int nt = 0; nt < NT; ++nt) {
           mma_bf16(acc[nt], a, ld32(&B.w2t[nt * 8 + g][16 * kk + 2 * t]), ld32(&B.w2t[nt * 8 + g][16 * kk + 2 * t + 8]));
         }
       }
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
+      for (int nt = 0; nt < NT; ++nt) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const int s = 16 * mt + g + (q >> 1) * 8, i = nt * 8 + 2 * t + (q & 1);
-          const float d = acc[nt][q] * gelu_grad(W.a1[s][i]);
-          W.a1[s][i] = d;
-          W.d1t[i][s] = __float2bfloat16_rn(d);
+          const int s2 = 16 * mt + g + (q >> 1) * 8, i = nt * 8 + 2 * t + (q & 1);
+          const float d = acc[nt][q] * act_grad<kRelu>(W.a1[s2][i]);
+          W.a1[s2][i] = d;
+          W.d1t[i][s2] = __float2bfloat16_rn(d);
         }
       }
     }
     __syncwarp();
-    for (int jj = lane; jj < kMlpHidden; jj += 32) {
+    for (int jj = lane; jj < H; jj += 32) {
       float acc = 0.0f;
-      for (int s = 0; s < 32; ++s) {
-        acc += W.a1[s][jj];
+      for (int s2 = 0; s2 < 32; ++s2) {
+        acc += W.a1[s2][jj];
       }
-      atomicAdd(&B.grad[kOffB1 + jj], acc);
+      atomicAdd(&B.grad[S::kOffB1 + jj], acc);
     }
-    // 8. dW1 = dL/da1^T x: [64 i x 32 s] x [32 s x 8 f]
-    for (int mt = 0; mt < 4; ++mt) {
+    // 8. dW1 = dL/da1^T x: [H i x 32 s] x [32 s x 8 f]
+    for (int mt = 0; mt < KT; ++mt) {
       float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk) {
@@ -363,7 +446,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDevi
         a[3] = ld32(&W.d1t[16 * mt + g + 8][16 * kk + 2 * t + 8]);
         mma_bf16(acc, a, ld32(&W.xt[g][16 * kk + 2 * t]), ld32(&W.xt[g][16 * kk + 2 * t + 8]));
       }
-      float *row0 = &B.grad[kOffW1 + (16 * mt + g) * kMlpIn + 2 * t];
+      float *row0 = &B.grad[S::kOffW1 + (16 * mt + g) * kMlpIn + 2 * t];
       float *row1 = row0 + 8 * kMlpIn;
       atomicAdd(row0, acc[0]);
       atomicAdd(row0 + 1, acc[1]);
@@ -373,50 +456,39 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_gradient(const MlpDevi
     __syncwarp();
   }
   __syncthreads();
-  float *out = grad_partials + (int64_t)blockIdx.x * kMlpParams;
-  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+  float *out = grad_partials + (int64_t)blockIdx.x * S::kParams;
+  for (int i = threadIdx.x; i < S::kParams; i += blockDim.x) {
     out[i] = B.grad[i];
   }
 }
 
 // ---- Adam ----
 
-__global__ void k_mlp_adam(itsu_prefilter_model *master, const float *grad_partials, int blocks, float *m, float *v, float lr,
-                           float beta1, float beta2, float eps, float weight_decay, float bias1, float bias2, MlpDevice *model)
+template <int H>
+__global__ void k_mlp_adam(float *master, const float *grad_partials, int blocks, float *m, float *v, float lr, float beta1,
+                           float beta2, float eps, float weight_decay, float bias1, float bias2, MlpDeviceT<H> *model)
 {
+  using S = MlpShape<H>;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= kMlpParams) {
+  if (i >= S::kParams) {
     return;
   }
   float gsum = 0.0f;
   for (int b = 0; b < blocks; ++b) {
-    gsum += grad_partials[(int64_t)b * kMlpParams + i];
+    gsum += grad_partials[(int64_t)b * S::kParams + i];
   }
   const float mm = beta1 * m[i] + (1.0f - beta1) * gsum;
   const float vv = beta2 * v[i] + (1.0f - beta2) * gsum * gsum;
   m[i] = mm;
   v[i] = vv;
-  float *p = &master->w1[0][0];
-  float w = p[i];
-  const bool is_weight = i < kOffB1 || (i >= kOffW2 && i < kOffB2) || (i >= kOffW3 && i < kOffB3);
+  float w = master[i];
+  const bool is_weight = i < S::kOffB1 || (i >= S::kOffW2 && i < S::kOffB2) || (i >= S::kOffW3 && i < S::kOffB3);
   if (is_weight) {
     w -= lr * weight_decay * w;
   }
   w -= lr * (mm / bias1) / (sqrtf(vv / bias2) + eps);
-  p[i] = w;
-  if (i < kOffB1) {
-    model->w1[i / kMlpIn][i % kMlpIn] = __float2bfloat16_rn(w);
-  } else if (i < kOffW2) {
-    model->b1[i - kOffB1] = w;
-  } else if (i < kOffB2) {
-    model->w2[(i - kOffW2) / kMlpHidden][(i - kOffW2) % kMlpHidden] = __float2bfloat16_rn(w);
-  } else if (i < kOffW3) {
-    model->b2[i - kOffB2] = w;
-  } else if (i < kOffB3) {
-    model->w3[i - kOffW3] = __float2bfloat16_rn(w);
-  } else {
-    model->b3 = w;
-  }
+  master[i] = w;
+  publish_param<H>(model, i, w);
 }
 
 int gradient_blocks(int32_t batch)
@@ -428,13 +500,49 @@ int gradient_blocks(int32_t batch)
 
 }  // namespace
 
+namespace {
+
+template <int H, bool kRelu>
+void score_net(const MlpDeviceT<H> *model, const float *features, int64_t n, float *logits, int num_sms, cudaStream_t stream)
+{
+  const int64_t tiles = (n + 31) / 32;
+  int64_t blocks = (tiles + kScoreThreads / 32 - 1) / (kScoreThreads / 32);
+  if (blocks > (int64_t)num_sms * 8) {
+    blocks = (int64_t)num_sms * 8;
+  }
+  if (blocks > 0) {
+    k_mlp_score<H, kRelu><<<(unsigned)blocks, kScoreThreads, 0, stream>>>(model, features, n, logits);
+  }
+}
+
+template <int H, bool kRelu>
+void gradient_net(const MlpDeviceT<H> *model, const float *features, const uint8_t *labels, int64_t n, int32_t batch, bool sequential,
+                  uint64_t seed, int64_t step, float pos_weight, float *grad_partials, float *loss, cudaStream_t stream)
+{
+  // per device and cheap: set before every launch (training runs outside graph capture)
+  cudaFuncSetAttribute(k_mlp_gradient<H, kRelu>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainBlock<H>));
+  k_mlp_gradient<H, kRelu><<<gradient_blocks(batch), kTrainWarps * 32, sizeof(TrainBlock<H>), stream>>>(
+      model, features, labels, n, batch, sequential ? 1 : 0, seed, step, pos_weight, grad_partials, loss);
+}
+
+}  // namespace
+
+static_assert(sizeof(itsu_prefilter_model) == sizeof(float) * (kMlpParams + 2 * kMlpIn + 1), "pair model layout");
+static_assert(sizeof(itsu_gate_model) == sizeof(float) * (kGateParams + 2 * kMlpIn + 1), "gate model layout");
+
 size_t mlp_device_bytes() { return sizeof(MlpDevice); }
+size_t gate_device_bytes() { return sizeof(GateDevice); }
 int mlp_gradient_blocks(int32_t batch) { return gradient_blocks(batch); }
 int mlp_max_gradient_blocks() { return kMaxGradBlocks; }
 
 void launch_mlp_publish(const itsu_prefilter_model *master, MlpDevice *model, cudaStream_t stream)
 {
-  k_mlp_publish<<<1, 512, 0, stream>>>(master, model);
+  k_mlp_publish<kMlpHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], model);
+}
+
+void launch_mlp_publish(const itsu_gate_model *master, GateDevice *model, cudaStream_t stream)
+{
+  k_mlp_publish<kGateHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], model);
 }
 
 void launch_prefilter_export(const Arena &a, const itsu_prefilter_samples &out, int num_sms, cudaStream_t stream)
@@ -443,34 +551,51 @@ void launch_prefilter_export(const Arena &a, const itsu_prefilter_samples &out, 
   k_export_roads<<<num_sms * 4, 256, 0, stream>>>(a, out);
 }
 
+void launch_gate_export(const Arena &a, const itsu_gate_samples &out, int num_sms, cudaStream_t stream)
+{
+  k_export_tracklets<<<num_sms * 8, 256, 0, stream>>>(a, out);
+  if (out.labels || out.road_tracklets) {
+    k_export_tracklet_labels<<<num_sms * 4, 256, 0, stream>>>(a, out);
+  }
+}
+
 void launch_mlp_score(const MlpDevice *model, const float *features, int64_t n, float *logits, int num_sms, cudaStream_t stream)
 {
-  const int64_t tiles = (n + 31) / 32;
-  int64_t blocks = (tiles + kScoreThreads / 32 - 1) / (kScoreThreads / 32);
-  if (blocks > (int64_t)num_sms * 8) {
-    blocks = (int64_t)num_sms * 8;
-  }
-  if (blocks > 0) {
-    k_mlp_score<<<(unsigned)blocks, kScoreThreads, 0, stream>>>(model, features, n, logits);
-  }
+  score_net<kMlpHidden, false>(model, features, n, logits, num_sms, stream);
+}
+
+void launch_mlp_score(const GateDevice *model, const float *features, int64_t n, float *logits, int num_sms, cudaStream_t stream)
+{
+  score_net<kGateHidden, true>(model, features, n, logits, num_sms, stream);
 }
 
 void launch_mlp_gradient(const MlpDevice *model, const float *features, const uint8_t *labels, int64_t n, int32_t batch,
                          bool sequential, uint64_t seed, int64_t step, float pos_weight, float *grad_partials, float *loss,
                          cudaStream_t stream)
 {
-  // per device and cheap: set before every launch (training runs outside graph capture)
-  cudaFuncSetAttribute(k_mlp_gradient, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainBlock));
-  k_mlp_gradient<<<gradient_blocks(batch), kTrainWarps * 32, sizeof(TrainBlock), stream>>>(
-      model, features, labels, n, batch, sequential ? 1 : 0, seed, step, pos_weight, grad_partials, loss);
+  gradient_net<kMlpHidden, false>(model, features, labels, n, batch, sequential, seed, step, pos_weight, grad_partials, loss, stream);
+}
+
+void launch_mlp_gradient(const GateDevice *model, const float *features, const uint8_t *labels, int64_t n, int32_t batch,
+                         bool sequential, uint64_t seed, int64_t step, float pos_weight, float *grad_partials, float *loss,
+                         cudaStream_t stream)
+{
+  gradient_net<kGateHidden, true>(model, features, labels, n, batch, sequential, seed, step, pos_weight, grad_partials, loss, stream);
 }
 
 void launch_mlp_adam(itsu_prefilter_model *master, const float *grad_partials, int blocks, float *m, float *v, float lr,
                      float beta1, float beta2, float eps, float weight_decay, float bias1, float bias2, MlpDevice *model,
                      cudaStream_t stream)
 {
-  k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, stream>>>(master, grad_partials, blocks, m, v, lr, beta1, beta2, eps,
-                                                           weight_decay, bias1, bias2, model);
+  k_mlp_adam<kMlpHidden><<<(kMlpParams + 255) / 256, 256, 0, stream>>>(&master->w1[0][0], grad_partials, blocks, m, v, lr,
+                                                                       beta1, beta2, eps, weight_decay, bias1, bias2, model);
+}
+
+void launch_mlp_adam(itsu_gate_model *master, const float *grad_partials, int blocks, float *m, float *v, float lr, float beta1,
+                     float beta2, float eps, float weight_decay, float bias1, float bias2, GateDevice *model, cudaStream_t stream)
+{
+  k_mlp_adam<kGateHidden><<<(kGateParams + 255) / 256, 256, 0, stream>>>(&master->w1[0][0], grad_partials, blocks, m, v, lr,
+                                                                         beta1, beta2, eps, weight_decay, bias1, bias2, model);
 }
 
 }  // namespace itsu

@@ -85,15 +85,25 @@ MLP_INPUTS, MLP_HIDDEN = 8, 64
 MLP_PARAMS = MLP_HIDDEN * MLP_INPUTS + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
 
 
+GATE_HIDDEN = 16
+GATE_PARAMS = GATE_HIDDEN * MLP_INPUTS + GATE_HIDDEN + GATE_HIDDEN * GATE_HIDDEN + GATE_HIDDEN + GATE_HIDDEN + 1
+
+
+def _model_fields(hidden):
+    return [("w1", (ctypes.c_float * MLP_INPUTS) * hidden), ("b1", ctypes.c_float * hidden),
+            ("w2", (ctypes.c_float * hidden) * hidden), ("b2", ctypes.c_float * hidden),
+            ("w3", ctypes.c_float * hidden), ("b3", ctypes.c_float), ("mean", ctypes.c_float * MLP_INPUTS),
+            ("inv_std", ctypes.c_float * MLP_INPUTS), ("logit_threshold", ctypes.c_float)]
+
+
 class PrefilterModel(ctypes.Structure):
-    _fields_ = [("w1", (ctypes.c_float * MLP_INPUTS) * MLP_HIDDEN), ("b1", ctypes.c_float * MLP_HIDDEN),
-                ("w2", (ctypes.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b2", ctypes.c_float * MLP_HIDDEN),
-                ("w3", ctypes.c_float * MLP_HIDDEN), ("b3", ctypes.c_float), ("mean", ctypes.c_float * MLP_INPUTS),
-                ("inv_std", ctypes.c_float * MLP_INPUTS), ("logit_threshold", ctypes.c_float)]
+    """itsu_prefilter_model: the pair prefilter (8 -> 64 -> 64 -> 1, GELU)."""
+    _fields_ = _model_fields(MLP_HIDDEN)
+    N_PARAMS = MLP_PARAMS
 
     def params(self) -> np.ndarray:
         """The trainable parameters as one float32 array (w1, b1, w2, b2, w3, b3)."""
-        return np.frombuffer(bytes(self), np.float32, MLP_PARAMS).copy()
+        return np.frombuffer(bytes(self), np.float32, self.N_PARAMS).copy()
 
     def arrays(self) -> dict:
         return dict(w1=np.ctypeslib.as_array(self.w1).copy(), b1=np.ctypeslib.as_array(self.b1).copy(),
@@ -101,6 +111,20 @@ class PrefilterModel(ctypes.Structure):
                     w3=np.ctypeslib.as_array(self.w3).copy(), b3=float(self.b3),
                     mean=np.ctypeslib.as_array(self.mean).copy(), inv_std=np.ctypeslib.as_array(self.inv_std).copy(),
                     logit_threshold=float(self.logit_threshold))
+
+
+class GateModel(ctypes.Structure):
+    """itsu_gate_model: the tracklet gate (8 -> 16 -> 16 -> 1, ReLU); same field order."""
+    _fields_ = _model_fields(GATE_HIDDEN)
+    N_PARAMS = GATE_PARAMS
+    params = PrefilterModel.params
+    arrays = PrefilterModel.arrays
+
+
+class GateSamples(ctypes.Structure):
+    _fields_ = [("features", ctypes.c_void_p), ("labels", ctypes.c_void_p), ("capacity", ctypes.c_int64),
+                ("road_tracklets", ctypes.c_void_p), ("road_capacity", ctypes.c_int64), ("n_tracklets", ctypes.c_int64),
+                ("n_roads", ctypes.c_int64)]
 
 
 class PrefilterSamples(ctypes.Structure):
@@ -177,6 +201,19 @@ SIGNATURES = [
     ("itsu_prefilter_gradient", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p,
       ctypes.POINTER(ctypes.c_float)]),
+    ("itsu_gate_init", None, [ctypes.POINTER(GateModel), ctypes.c_uint64]),
+    ("itsu_gate_save", ctypes.c_int, [ctypes.POINTER(GateModel), ctypes.c_char_p]),
+    ("itsu_gate_load", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(GateModel)]),
+    ("itsu_gate_set_model", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GateModel)]),
+    ("itsu_gate_get_model", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GateModel)]),
+    ("itsu_gate_enable", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("itsu_gate_export", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GateSamples)]),
+    ("itsu_gate_score", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
+    ("itsu_gate_train", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(TrainConfig), ctypes.c_void_p]),
+    ("itsu_gate_gradient", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p,
+      ctypes.POINTER(ctypes.c_float)]),
 ]
 
 
@@ -206,6 +243,29 @@ def prefilter_load(path: str) -> PrefilterModel:
     L = load()
     m = PrefilterModel()
     st = L.itsu_prefilter_load(path.encode(), ctypes.byref(m))
+    if st != OK:
+        raise ItsuError(st, L.itsu_last_error(None).decode())
+    return m
+
+
+def gate_init(seed: int) -> GateModel:
+    """A fresh seeded tracklet gate (host only)."""
+    m = GateModel()
+    load().itsu_gate_init(ctypes.byref(m), seed)
+    return m
+
+
+def gate_save(model: GateModel, path: str):
+    L = load()
+    st = L.itsu_gate_save(ctypes.byref(model), path.encode())
+    if st != OK:
+        raise ItsuError(st, L.itsu_last_error(None).decode())
+
+
+def gate_load(path: str) -> GateModel:
+    L = load()
+    m = GateModel()
+    st = L.itsu_gate_load(path.encode(), ctypes.byref(m))
     if st != OK:
         raise ItsuError(st, L.itsu_last_error(None).decode())
     return m
@@ -497,4 +557,41 @@ class Context:
         loss = ctypes.c_float()
         self._check(self.lib.itsu_prefilter_gradient(self.h, ctypes.c_void_p(features_ptr), ctypes.c_void_p(labels_ptr), n,
                                                      pos_weight, _ptr(grad), ctypes.byref(loss)))
+        return grad, loss.value
+
+    # ---- learned tracklet gate ----
+
+    def gate_set_model(self, model: GateModel):
+        self._check(self.lib.itsu_gate_set_model(self.h, ctypes.byref(model)))
+
+    def gate_get_model(self) -> GateModel:
+        m = GateModel()
+        self._check(self.lib.itsu_gate_get_model(self.h, ctypes.byref(m)))
+        return m
+
+    def gate_enable(self, enable: bool = True):
+        self._check(self.lib.itsu_gate_enable(self.h, 1 if enable else 0))
+
+    def gate_export(self, features=0, labels=0, capacity=0, road_tracklets=0, road_capacity=0):
+        """Device pointers (ints) of the buffers to fill; returns (n_tracklets, n_roads)."""
+        s = GateSamples()
+        s.features, s.labels, s.capacity = features or None, labels or None, capacity
+        s.road_tracklets, s.road_capacity = road_tracklets or None, road_capacity
+        self._check(self.lib.itsu_gate_export(self.h, ctypes.byref(s)))
+        return s.n_tracklets, s.n_roads
+
+    def gate_score(self, features_ptr: int, n: int, logits_ptr: int):
+        self._check(self.lib.itsu_gate_score(self.h, ctypes.c_void_p(features_ptr), n, ctypes.c_void_p(logits_ptr)))
+
+    def gate_train(self, features_ptr: int, labels_ptr: int, n: int, cfg: TrainConfig) -> np.ndarray:
+        losses = np.zeros(max(int(cfg.steps), 1), np.float32)
+        self._check(self.lib.itsu_gate_train(self.h, ctypes.c_void_p(features_ptr), ctypes.c_void_p(labels_ptr), n,
+                                             ctypes.byref(cfg), _ptr(losses)))
+        return losses[:int(cfg.steps)]
+
+    def gate_gradient(self, features_ptr: int, labels_ptr: int, n: int, pos_weight: float = 1.0):
+        grad = np.zeros(GATE_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        self._check(self.lib.itsu_gate_gradient(self.h, ctypes.c_void_p(features_ptr), ctypes.c_void_p(labels_ptr), n,
+                                                pos_weight, _ptr(grad), ctypes.byref(loss)))
         return grad, loss.value

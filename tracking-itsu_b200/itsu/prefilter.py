@@ -39,6 +39,7 @@ EVAL_SEED0 = 8_000_000   # held-out events
 WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights")
 CHECKPOINT = os.path.join(WEIGHTS, "prefilter_pbpb.itsumlp")
 CHECKPOINTS = {"pbpb": CHECKPOINT, "pileup": os.path.join(WEIGHTS, "prefilter_pileup.itsumlp")}
+GATE_CHECKPOINTS = {"pbpb": os.path.join(WEIGHTS, "gate_pbpb.itsugate"), "pileup": os.path.join(WEIGHTS, "gate_pileup.itsugate")}
 TWO_PI_F = np.float32(6.28318530717958647692)
 CELL_MAX_DCA = np.array([0.05, 0.04, 0.05, 0.2, 0.4], np.float32)
 
@@ -64,25 +65,39 @@ def gelu_grad(x):
     return 0.5 * (1.0 + th) + 0.5 * x * (1.0 - th * th) * 0.7978845608028654 * (1.0 + 3.0 * 0.044715 * x * x)
 
 
-def mlp_forward(m: dict, features, rounding: bool = True):
+def relu(x):
+    return np.maximum(np.asarray(x, np.float64), 0.0)
+
+
+def relu_grad(x):
+    return (np.asarray(x, np.float64) > 0).astype(np.float64)
+
+
+ACTIVATIONS = {"gelu": (gelu, gelu_grad), "relu": (relu, relu_grad)}
+
+
+def mlp_forward(m: dict, features, rounding: bool = True, act: str = "gelu"):
     """Logits as the device computes them (BF16 inputs, weights and activations; wide
-    accumulation). rounding=False gives the same network in plain float64."""
+    accumulation). rounding=False gives the same network in plain float64. act: "gelu" (the pair
+    prefilter) or "relu" (the tracklet gate)."""
+    fn = ACTIVATIONS[act][0]
     rnd = (lambda a: bf16_round(np.asarray(a, np.float32)).astype(np.float64)) if rounding else (lambda a: np.asarray(a, np.float64))
     f = np.asarray(features, np.float32)
     x = rnd((f - m["mean"].astype(np.float32)) * m["inv_std"].astype(np.float32))
     w1, w2, w3 = (rnd(m[k]) for k in ("w1", "w2", "w3"))
     a1 = x @ w1.T + m["b1"]
-    h1 = rnd(gelu(a1))
+    h1 = rnd(fn(a1))
     a2 = h1 @ w2.T + m["b2"]
-    h2 = rnd(gelu(a2))
+    h2 = rnd(fn(a2))
     z = h2 @ w3 + m["b3"]
     return dict(x=x, a1=a1, h1=h1, a2=a2, h2=h2, z=z, w2=w2, w3=w3)
 
 
-def mlp_gradient(m: dict, features, labels, pos_weight: float = 1.0, rounding: bool = True):
+def mlp_gradient(m: dict, features, labels, pos_weight: float = 1.0, rounding: bool = True, act: str = "gelu"):
     """Mean weighted binary cross-entropy and its gradient (itsu_prefilter_model parameter order),
     in float64 through the forward values (straight-through for the BF16 rounding)."""
-    fw = mlp_forward(m, features, rounding)
+    dact = ACTIVATIONS[act][1]
+    fw = mlp_forward(m, features, rounding, act)
     y = np.asarray(labels, np.float64)
     n = len(y)
     w = np.where(y > 0, pos_weight, 1.0)
@@ -91,10 +106,10 @@ def mlp_gradient(m: dict, features, labels, pos_weight: float = 1.0, rounding: b
     dz = w * (1.0 / (1.0 + np.exp(-z)) - y) / n
     g_w3 = fw["h2"].T @ dz
     g_b3 = dz.sum()
-    d2 = dz[:, None] * fw["w3"][None, :] * gelu_grad(fw["a2"])
+    d2 = dz[:, None] * fw["w3"][None, :] * dact(fw["a2"])
     g_w2 = d2.T @ fw["h1"]
     g_b2 = d2.sum(0)
-    d1 = (d2 @ fw["w2"]) * gelu_grad(fw["a1"])
+    d1 = (d2 @ fw["w2"]) * dact(fw["a1"])
     g_w1 = d1.T @ fw["x"]
     g_b1 = d1.sum(0)
     grad = np.concatenate([g_w1.ravel(), g_b1, g_w2.ravel(), g_b2, g_w3, [g_b3]])
@@ -158,6 +173,47 @@ def pair_features(res: dict) -> np.ndarray:
     return np.concatenate(out) if out else np.zeros((0, 8), np.float32)
 
 
+def tracklet_features(res: dict) -> np.ndarray:
+    """The tracklet gate's 8 features of every tracklet of one vertex's results (oracle canonical
+    form), float32 in the device's order, in the export's row order (layer by layer)."""
+    out = []
+    vx, vy, vz = (np.float32(v) for v in res["vertex"])
+    pi_f, two_pi_f = np.float32(3.14159265358979323846), TWO_PI_F
+    for layer in range(6):
+        t = res["tracklets"][layer]
+        if len(t) == 0:
+            continue
+        c1 = res["clusters"][layer][t["c1"]]
+        c2 = res["clusters"][layer + 1][t["c2"]]
+        dphi = c1["phi"] - c2["phi"]
+        dphi = np.where(dphi > pi_f, dphi - two_pi_f, np.where(dphi < -pi_f, dphi + two_pi_f, dphi)).astype(np.float32)
+        tan_lambda = (c1["z"] - vz) / c1["r"]
+        dz = tan_lambda * (c2["r"] - c1["r"]) + c1["z"] - c2["z"]
+        f = np.zeros((len(t), 8), np.float32)
+        f[:, 0] = np.abs(dphi)
+        f[:, 1] = dz
+        f[:, 2] = np.abs(dz)
+        f[:, 3] = _curvature(vx, vy, c1["x"], c1["y"], c2["x"], c2["y"])
+        f[:, 4] = np.float32(layer)
+        f[:, 5] = c1["r"]
+        f[:, 6] = tan_lambda
+        f[:, 7] = dphi
+        out.append(f)
+    return np.concatenate(out) if out else np.zeros((0, 8), np.float32)
+
+
+def road_tracklets(res: dict) -> np.ndarray:
+    """Each road's 6 tracklets as rows of tracklet_features(res)."""
+    base = np.concatenate([[0], np.cumsum([len(t) for t in res["tracklets"]])])[:6]
+    rows = np.zeros((len(res["roads"]), 6), np.int64)
+    for k, road in enumerate(res["roads"]):
+        for l in range(5):
+            cell = res["cells"][l][road["cells"][l]]
+            rows[k, l] = base[l] + cell["t1"]
+            rows[k, l + 1] = base[l + 1] + cell["t2"]
+    return rows
+
+
 def road_cells(res: dict) -> np.ndarray:
     """Each road's 5 cells as rows of pair_features(res)."""
     base = np.concatenate([[0], np.cumsum([len(c) for c in res["cells"]])])[:5]
@@ -168,6 +224,7 @@ def calibrate(logits: np.ndarray, road_rows: np.ndarray, target: float) -> float
     """Largest threshold t such that at least `target` of the roads keep all their cells
     (logit >= t; NaN logits keep their cell)."""
     lg = np.where(np.isnan(logits), np.inf, logits.astype(np.float64))
+    lg = np.append(lg, np.inf)  # row -1 (no object in that layer) never drops its road
     road_min = lg[road_rows].min(axis=1) if len(road_rows) else np.zeros(0)
     if len(road_min) == 0:
         return float("-inf")
@@ -269,7 +326,7 @@ def collect(ctx, seeds, device, chunk: int = 100, workers: int | None = None, lo
     for k in range(0, len(seeds), chunk):
         events = make_events(seeds[k:k + chunk], workers, workload)
         b = DeviceBatch(ctx, events, device)
-        ctx.prefilter_enable(False)
+        set_learned(ctx, False, False)
         ctx.batch_run(b.batch)
         f, l, r = export_samples(ctx, device)
         feats.append(f.clone())
@@ -338,69 +395,205 @@ def train(ctx, data: dict, device, seed: int = 1, target: float = 0.997, log=pri
     return model, report
 
 
-def evaluate(ctx, model, seeds, device, chunk: int = 100, workers: int | None = None, log=print, workload: str = "pbpb") -> dict:
-    """Learned vs plain batched runs over the events of `seeds`."""
-    ctx.prefilter_set_model(model)
+def export_gate_samples(ctx, device):
+    """Tracklet samples and road rows of the context's last run, as device tensors."""
+    import torch
+
+    n, n_roads = ctx.gate_export()
+    feats = torch.empty((max(n, 1), 8), dtype=torch.float32, device=device)
+    labels = torch.empty(max(n, 1), dtype=torch.uint8, device=device)
+    rows = torch.empty((max(n_roads, 1), 6), dtype=torch.int32, device=device)
+    ctx.gate_export(features=feats.data_ptr(), labels=labels.data_ptr(), capacity=n, road_tracklets=rows.data_ptr(),
+                    road_capacity=n_roads)
+    return feats[:n], labels[:n], rows[:n_roads]
+
+
+def collect_gate(ctx, seeds, device, chunk: int = 50, workers: int | None = None, log=print, workload: str = "pbpb") -> dict:
+    """Plain runs over the events of `seeds`; one sample per tracklet (label 1: a found road uses
+    it) and each road's 6 tracklets as sample rows, concatenated on the device."""
+    import torch
+
+    feats, labels, rows = [], [], []
+    base = 0
+    seeds = list(seeds)
+    for k in range(0, len(seeds), chunk):
+        events = make_events(seeds[k:k + chunk], workers, workload)
+        b = DeviceBatch(ctx, events, device)
+        set_learned(ctx, False, False)
+        ctx.batch_run(b.batch)
+        f, l, r = export_gate_samples(ctx, device)
+        feats.append(f.clone())
+        labels.append(l.clone())
+        r = r.to(torch.int64)
+        rows.append(torch.where(r >= 0, r + base, r))
+        base += len(f)
+        log("collect gate: events %d..%d, %d tracklets (%d on roads), %d roads" % (k, k + len(events) - 1, len(f),
+                                                                                   int(l.sum().item()), len(r)))
+    return dict(features=torch.cat(feats), labels=torch.cat(labels), road_rows=torch.cat(rows))
+
+
+def ctx_has_gate(ctx) -> bool:
+    try:
+        ctx.gate_get_model()
+        return True
+    except capi.ItsuError:
+        return False
+
+
+def train_gate(ctx, data: dict, device, seed: int = 1, target: float = 0.999, log=print, **train_kw) -> tuple:
+    """Trains a tracklet gate on `data` (from collect_gate) and calibrates its threshold on road
+    reproduction (a road survives the gate iff all its 6 tracklets are kept); returns (model, report)."""
+    import torch
+
+    model = capi.gate_init(seed)
+    mean, inv_std = standardisation(data["features"])
+    for k in range(8):
+        model.mean[k], model.inv_std[k] = float(mean[k]), float(inv_std[k])
+    ctx.gate_set_model(model)
+    ok = torch.isfinite(data["features"]).all(dim=1)
+    f = data["features"][ok].contiguous()
+    y = data["labels"][ok].contiguous()
+    cfg = capi.train_config(**train_kw)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = ctx.gate_train(f.data_ptr(), y.data_ptr(), len(f), cfg)
+    train_s = time.perf_counter() - t0
+    model = ctx.gate_get_model()
+    n = len(data["features"])
+    logits_t = torch.empty(max(n, 1), dtype=torch.float32, device=device)
+    ctx.gate_score(data["features"].data_ptr(), n, logits_t.data_ptr())
+    logits = logits_t[:n].cpu().numpy()
+    rows = data["road_rows"].cpu().numpy()
+    thr = calibrate(logits, rows, target)
+    model.logit_threshold = thr
+    ctx.gate_set_model(model)
+    labels = data["labels"].cpu().numpy()
+    kept = ~(logits < thr)
+    report = dict(
+        samples=int(len(f)), positives=int(y.sum().item()), steps=int(cfg.steps), batch=int(cfg.batch), lr=float(cfg.lr),
+        lr_final=float(cfg.lr_final), train_seconds=train_s, loss_first=float(np.mean(losses[:100])) if len(losses) else None,
+        loss_last=float(np.mean(losses[-100:])) if len(losses) else None, threshold=thr, calibration_target=target,
+        train_tracklets_kept=float(kept.mean()), train_positive_tracklets_kept=float(kept[labels == 1].mean()),
+        train_negative_tracklets_kept=float(kept[labels == 0].mean()),
+    )
+    log("train gate: %s" % json.dumps(report))
+    return model, report
+
+
+def evaluate(ctx, model, seeds, device, chunk: int = 100, workers: int | None = None, log=print, workload: str = "pbpb",
+             gate=None) -> dict:
+    """Learned vs plain batched runs over the events of `seeds`: the learned form runs the pair
+    prefilter `model` (None: not used) and the tracklet gate `gate` (None: not used)."""
+    if model is not None:
+        ctx.prefilter_set_model(model)
+    if gate is not None:
+        ctx.gate_set_model(gate)
     tot = dict(plain_roads=0, learned_roads=0, reproduced=0, extra=0, extra_fakes=0, plain_fakes=0, learned_fakes=0,
                plain_cells=0, learned_cells=0, events=0)
     seeds = list(seeds)
     for k in range(0, len(seeds), chunk):
         events = make_events(seeds[k:k + chunk], workers, workload)
         b = DeviceBatch(ctx, events, device)
-        ctx.prefilter_enable(False)
+        set_learned(ctx, False, False)
         ctx.batch_run(b.batch)
         plain_cells, _ = ctx.prefilter_export()
+        plain_tracklets = ctx.gate_export()[0]
         pk, pf = export_roads(ctx, device)
-        ctx.prefilter_enable(True)
+        set_learned(ctx, model is not None, gate is not None)
         ctx.batch_run(b.batch)
         learned_cells, _ = ctx.prefilter_export()
+        learned_tracklets = ctx.gate_export()[0]
         lk, lf = export_roads(ctx, device)
-        ctx.prefilter_enable(False)
+        set_learned(ctx, False, False)
         c = compare_roads(pk, pf, lk, lf)
         for key in c:
             tot[key] += c[key]
         tot["plain_cells"] += plain_cells
         tot["learned_cells"] += learned_cells
+        tot["plain_tracklets"] = tot.get("plain_tracklets", 0) + plain_tracklets
+        tot["learned_tracklets"] = tot.get("learned_tracklets", 0) + learned_tracklets
         tot["events"] += len(events)
         tot["runs"] = tot.get("runs", 0) + b.n_runs
         log("evaluate: events %d..%d %s" % (k, k + len(events) - 1, json.dumps(c)))
     tot["road_reproduction"] = tot["reproduced"] / max(tot["plain_roads"], 1)
     tot["cells_kept"] = tot["learned_cells"] / max(tot["plain_cells"], 1)
+    tot["tracklets_kept"] = tot.get("learned_tracklets", 0) / max(tot.get("plain_tracklets", 0), 1)
+    tot["learned_form"] = "+".join(k for k, v in (("tracklet gate", gate), ("pair prefilter", model)) if v is not None)
     return tot
 
 
+def set_learned(ctx, pair: bool, gate: bool):
+    """The learned form's networks on or off (a network must have a model to be turned on)."""
+    if pair or ctx_has_pair(ctx):
+        ctx.prefilter_enable(pair)
+    if gate or ctx_has_gate(ctx):
+        ctx.gate_enable(gate)
+
+
+def ctx_has_pair(ctx) -> bool:
+    try:
+        ctx.prefilter_get_model()
+        return True
+    except capi.ItsuError:
+        return False
+
+
 def main(argv=None):
-    p = argparse.ArgumentParser(description="Train, calibrate and evaluate the learned prefilter on one GPU.")
+    p = argparse.ArgumentParser(description="Train, calibrate and evaluate a learned network of the learned form on one GPU.")
+    p.add_argument("--model", choices=("pair", "gate"), default="pair",
+                   help="pair: the tracklet-pair prefilter of the cell stage; gate: the tracklet gate of the tracklet stage")
     p.add_argument("--workload", choices=("pbpb", "pileup"), default="pbpb",
                    help="pbpb: central Pb-Pb-like events; pileup: frames of 5 collisions (every vertex is a run)")
-    p.add_argument("--out", default=None, help="checkpoint to write (default: weights/prefilter_<workload>.itsumlp)")
+    p.add_argument("--out", default=None, help="checkpoint to write (default: weights/<model>_<workload>.itsu{mlp,gate})")
     p.add_argument("--report", default=None, help="JSON report (default: the checkpoint path with .json)")
-    p.add_argument("--train-events", type=int, default=2000)
+    p.add_argument("--train-events", type=int, default=None, help="default: 2000 (pair), 300 (gate)")
     p.add_argument("--eval-events", type=int, default=500)
     p.add_argument("--steps", type=int, default=20000)
     p.add_argument("--batch", type=int, default=8192)
     p.add_argument("--lr", type=float, default=2e-3)
-    p.add_argument("--target", type=float, default=0.997, help="road reproduction the threshold keeps on the training events")
+    p.add_argument("--target", type=float, default=None,
+                   help="road reproduction the threshold keeps on the training events (default: 0.997 pair, 0.999 gate)")
+    p.add_argument("--with-pair", default=None,
+                   help="gate: also evaluate the learned form with this pair-prefilter checkpoint enabled")
     p.add_argument("--seed", type=int, default=1)
-    p.add_argument("--chunk", type=int, default=100)
+    p.add_argument("--chunk", type=int, default=None)
     args = p.parse_args(argv)
-    args.out = args.out or CHECKPOINTS[args.workload]
+    gate_mode = args.model == "gate"
+    args.out = args.out or (GATE_CHECKPOINTS[args.workload] if gate_mode else CHECKPOINTS[args.workload])
+    args.train_events = args.train_events or (300 if gate_mode else 2000)
+    args.target = args.target or (0.999 if gate_mode else 0.997)
+    args.chunk = args.chunk or (50 if gate_mode else 100)
     import torch
 
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
     ctx = capi.Context(device=0)
     t0 = time.perf_counter()
-    data = collect(ctx, range(TRAIN_SEED0, TRAIN_SEED0 + args.train_events), device, chunk=args.chunk, workload=args.workload)
+    train_seeds = range(TRAIN_SEED0, TRAIN_SEED0 + args.train_events)
+    eval_seeds = range(EVAL_SEED0, EVAL_SEED0 + args.eval_events)
+    if gate_mode:
+        data = collect_gate(ctx, train_seeds, device, chunk=args.chunk, workload=args.workload)
+    else:
+        data = collect(ctx, train_seeds, device, chunk=args.chunk, workload=args.workload)
     collect_s = time.perf_counter() - t0
-    model, report = train(ctx, data, device, seed=args.seed, target=args.target, steps=args.steps, batch=args.batch, lr=args.lr)
+    trainer = train_gate if gate_mode else train
+    model, report = trainer(ctx, data, device, seed=args.seed, target=args.target, steps=args.steps, batch=args.batch, lr=args.lr)
     del data
-    ev = evaluate(ctx, model, range(EVAL_SEED0, EVAL_SEED0 + args.eval_events), device, chunk=args.chunk, workload=args.workload)
+    if gate_mode:
+        ev = evaluate(ctx, None, eval_seeds, device, chunk=args.chunk, workload=args.workload, gate=model)
+        if args.with_pair:
+            pair = capi.prefilter_load(args.with_pair)
+            ev_both = evaluate(ctx, pair, eval_seeds, device, chunk=args.chunk, workload=args.workload, gate=model)
+            ev = dict(gate_only=ev, gate_and_pair=ev_both, pair_checkpoint=os.path.basename(args.with_pair))
+        capi.gate_save(model, os.path.abspath(args.out))
+    else:
+        ev = evaluate(ctx, model, eval_seeds, device, chunk=args.chunk, workload=args.workload)
+        capi.prefilter_save(model, os.path.abspath(args.out))
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
-    capi.prefilter_save(model, args.out)
-    full = dict(workload=args.workload, train_events=args.train_events, train_seeds=[TRAIN_SEED0, TRAIN_SEED0 + args.train_events - 1],
-                eval_events=args.eval_events, eval_seeds=[EVAL_SEED0, EVAL_SEED0 + args.eval_events - 1],
-                collect_seconds=collect_s, train=report, evaluation=ev)
+    full = dict(model=args.model, workload=args.workload, train_events=args.train_events,
+                train_seeds=[TRAIN_SEED0, TRAIN_SEED0 + args.train_events - 1], eval_events=args.eval_events,
+                eval_seeds=[EVAL_SEED0, EVAL_SEED0 + args.eval_events - 1], collect_seconds=collect_s, train=report,
+                evaluation=ev)
     with open(args.report or os.path.splitext(args.out)[0] + ".json", "w") as fh:
         json.dump(full, fh, indent=1)
     print(json.dumps(full))
