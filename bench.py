@@ -59,17 +59,27 @@ def parse_args():
                     help="pbpb: central Pb-Pb-like events, 6000 tracks (the headline); uneven: log-uniform "
                          "20-8000 tracks; pileup: frames of 5 collisions of ~1500 tracks, 10%% noise")
     ap.add_argument("--frames", type=int, default=32, help="pile-up frames per step per GPU")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations' legs (the 256-event uneven batch and the 1024-frame pile-up stream)")
+    ap.add_argument("--uneven-events", type=int, default=256, help="events of the uneven-batch leg")
+    ap.add_argument("--stream-frames", type=int, default=1024, help="frames of the pile-up stream leg")
+    ap.add_argument("--stream-chunk", type=int, default=32, help="frames per call of the pile-up stream leg")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
-    ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter mode")
+    ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter modes")
     ap.add_argument("--prefilter", default=None,
-                    help="checkpoint of the learned prefilter (default: the one trained for the workload)")
+                    help="checkpoint of the learned pair prefilter (default: the one trained for the workload)")
+    ap.add_argument("--gate", default=None,
+                    help="checkpoint of the learned tracklet gate (default: the one trained for the workload)")
     args = ap.parse_args()
     if args.prefilter is None:
         own = os.path.join(PKG, "weights", "prefilter_%s.itsumlp" % args.workload)
         args.prefilter = own if os.path.exists(own) else os.path.join(PKG, "weights", "prefilter_pbpb.itsumlp")
+    if args.gate is None:
+        own = os.path.join(PKG, "weights", "gate_%s.itsugate" % args.workload)
+        args.gate = own if os.path.exists(own) else os.path.join(PKG, "weights", "gate_pbpb.itsugate")
     return args
 
 
@@ -116,8 +126,29 @@ def sum_over_ranks(dist, value, device=None):
 
 
 def shard_seed(seed, rank):
-    """Each rank's events come from its own seed (independent event shards, weak scaling)."""
+    """A per-rank seed for the legs whose streams are generated rank by rank (the pile-up stream)."""
     return seed + 7919 * rank
+
+
+def rank_events(workload, seed, per_rank, world, rank):
+    """This rank's share of ONE event list of per_rank * world events (weak scaling), split by
+    sorted-multiplicity round-robin (itsu.shard): central events all cost the same and are dealt
+    evenly; an uneven batch's events are balanced by N^2 cost. Returns (events, shard indices,
+    imbalance of the split)."""
+    from itsu import shard
+
+    n = per_rank * world
+    if workload == "uneven":
+        mults = gen.batch_multiplicities(seed, n_events=n)
+    else:
+        mults = np.full(n, TRACKS)
+    shards = shard.partition(shard.event_cost(mults), world)
+    mine = shards[rank]
+    if workload == "uneven":
+        events = gen.batch_events(seed, n_events=n, indices=mine)
+    else:
+        events = [gen.pbpb_event(seed * 100000 + i, TRACKS) for i in mine]
+    return events, mine, shard.imbalance(shard.event_cost(mults), shards)
 
 
 def whole_job_rate(dist, units_local, ms_local, device=None):
@@ -349,16 +380,17 @@ def run_ours(args):
 
     seed = shard_seed(args.seed, rank)
     frames = None
+    shard_info = None
     if args.workload == "pileup":
         frames = gen.pileup_stream(seed, args.frames, collisions=5, n_tracks=1500)
         events = [ev for ev in frames for _ in ev.vertices]
         f_clusters, f_offsets, f_vertices, f_vertex_frame = gen.pack_frames(frames)
         clusters, offsets, vertices = gen.pack_batch(events, [iv for ev in frames for iv in range(len(ev.vertices))])
-    elif args.workload == "uneven":
-        events = gen.batch_events(seed, n_events=args.events)
-        clusters, offsets, vertices = gen.pack_batch(events)
     else:
-        events = make_events(args.events, seed)
+        # one event list of events-per-GPU x world events, this rank's shard of it
+        events, mine, imb = rank_events(args.workload, args.seed, args.events, world, rank)
+        shard_info = {"events_total": args.events * world, "split": "sorted-multiplicity round-robin (N^2 cost, snake)",
+                      "cost_imbalance": imb}
         clusters, offsets, vertices = gen.pack_batch(events)
     n_events, n_clusters = len(events), len(clusters)
 
@@ -473,16 +505,31 @@ def run_ours(args):
     if ctx_e2e is not None:
         ctx_e2e.close()
 
-    # ---- learned-prefilter form: same inputs, same timing rules ----
-    learned = None
-    if not args.no_prefilter and os.path.exists(args.prefilter):
-        l_ms, l_cmp, l_prof, l_thr = learned_mode(ctx, launch, args, stream, dist, device)
-        learned = dict(ms=l_ms, cmp=l_cmp, prof=l_prof, threshold=l_thr)
+    # ---- learned forms: same inputs, same timing rules ----
+    # the tracklet gate alone, the pair prefilter alone, and both (where their checkpoints exist)
+    learned = {}
+    if not args.no_prefilter:
+        from itsu import capi as _capi
+
+        pair = _capi.prefilter_load(args.prefilter) if os.path.exists(args.prefilter) else None
+        gate = _capi.gate_load(args.gate) if os.path.exists(args.gate) else None
+        for name, p_model, g_model in (("tracklet_gate", None, gate), ("pair_prefilter", pair, None),
+                                       ("gate_and_pair", pair, gate)):
+            if (name != "pair_prefilter" and g_model is None) or (name != "tracklet_gate" and p_model is None):
+                continue
+            l_ms, l_cmp, l_prof = learned_mode(ctx, launch, args, stream, dist, device, p_model, g_model)
+            learned[name] = dict(ms=l_ms, cmp=l_cmp, prof=l_prof,
+                                 pair_threshold=None if p_model is None else float(p_model.logit_threshold),
+                                 gate_threshold=None if g_model is None else float(g_model.logit_threshold))
         launch()  # back to the plain graph (the profile below times the plain kernels)
         ctx.batch_status()
 
     # ---- road report (IOUtils::writeRoadsReport) on the device, over the roads left resident ----
     report = road_report_mode(ctx, events, frames, args, rank, world)
+    configs = None
+    if not args.no_configs and args.workload == "pbpb":
+        configs = {"uneven_batch": uneven_leg(args, stream, dist, device, local, peak_hbm()),
+                   "pileup_stream": pileup_stream_leg(args, stream, dist, device, local)}
     usage = ctx.memory_usage()
     arena = dict(usage, occupancy={k: (usage["used"][k] / usage["capacity"][k]) if usage["capacity"][k] else None
                                    for k in usage["capacity"]},
@@ -500,12 +547,7 @@ def run_ours(args):
         for k, v in kernel_bytes(c).items():
             own_bytes[k] = own_bytes.get(k, 0) + v
     top_name, top_ms = max(prof, key=lambda x: x[1])
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
-    except (OSError, KeyError, ValueError):
-        peak, peak_src = 6650.0, "fallback"
+    peak, peak_src = peak_hbm_with_source()
     achieved = (own_bytes[top_name] / (top_ms * 1e-3) / 1e9) if top_name in own_bytes else None
     per_kernel = {name: {"ms": round(t, 4), "own_bytes": own_bytes[name],
                          "gbs": own_bytes[name] / (t * 1e-3) / 1e9, "frac": own_bytes[name] / (t * 1e-3) / 1e9 / peak}
@@ -566,6 +608,7 @@ def run_ours(args):
                 "mode": "batched plain path, one CUDA graph per step" + ("; frames: raw clusters resident once per frame" if frames is not None else ""),
                 "launch_shape": tune if tune is not None else "default (256 threads, 8 blocks/SM, pruning on)",
                 "parallelism": "event shards, one rank per GPU" if world > 1 else "single GPU",
+                "sharding": shard_info,
                 "l2": "inputs larger than L2 (%.0f MB raw clusters, %.0f MB tracklets per step), no flush" % (
                     clusters.nbytes / 1e6, 16 * sum(sum(c["T"]) for c in counts) / 1e6),
             },
@@ -585,22 +628,9 @@ def run_ours(args):
                 "batched_plain_events_per_s": value,
                 "plain_single_event_events_per_s": single_eps,
                 "plain_single_event_note": "itsu_clusters_to_tracks, one vertex per synchronous call, host in/out, wall clock",
-                "learned_prefilter": None if learned is None else {
-                    "events_per_s": total_events / (learned["ms"] * 1e-3),
-                    "ms_per_step": learned["ms"] / args.steps,
-                    "vs_batched_plain": (total_events / (learned["ms"] * 1e-3)) / value,
-                    "road_reproduction": learned["cmp"]["road_reproduction"],
-                    "plain_roads": learned["cmp"]["plain_roads"],
-                    "learned_roads": learned["cmp"]["learned_roads"],
-                    "extra_roads": learned["cmp"]["extra"],
-                    "extra_fakes": learned["cmp"]["extra_fakes"],
-                    "cells_kept": learned["cmp"]["cells_kept"],
-                    "logit_threshold": learned["threshold"],
-                    "checkpoint": os.path.relpath(args.prefilter, ROOT),
-                    "kernel_ms": {name: round(t, 4) for name, t in learned["prof"]},
-                    "note": "same resident batch and timing as the plain value; fused BF16 MLP (mma.sync) in the cell stage",
-                },
+                "learned_prefilter": learned_summary(learned, total_events, value, args),
                 "road_report": report,
+                "configurations": configs,
             },
             "arena": arena,
             "kernel_ms": {name: round(t, 4) for name, t in prof},
@@ -615,6 +645,170 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+def peak_hbm_with_source():
+    """The HBM roofline denominator: MEASURED_PEAKS.json's copy bandwidth, else the fallback."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def peak_hbm():
+    return peak_hbm_with_source()[0]
+
+
+def timed_replays(launch, stream, steps, warmup, dist, device):
+    """CUDA-event time of `steps` launches after `warmup` untimed ones (max over ranks), in ms."""
+    import torch
+
+    for _ in range(warmup):
+        launch()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(steps):
+        launch()
+    end.record(stream)
+    torch.cuda.synchronize()
+    return max_over_ranks(dist, start.elapsed_time(end), device)
+
+
+def uneven_leg(args, stream, dist, device, local, peak):
+    """Configuration 3: one batch of `--uneven-events` events of log-uniform 20-8000 tracks (5%
+    noise, each its own vertex) per step, device-resident, one CUDA graph, the autotuner's shape
+    for the batch's band; its dominant kernel against its own compulsory bytes."""
+    import torch
+
+    from itsu import capi
+
+    world, rank, _ = dist_env()
+    evs = gen.batch_events(shard_seed(args.seed, rank) + 31, n_events=args.uneven_events)
+    clusters, offsets, vertices = gen.pack_batch(evs)
+    d = [torch.from_numpy(a.view(np.uint8) if a is clusters else a).to(device) for a in (clusters, offsets, vertices)]
+    ctx = capi.Context(device=local)
+    try:
+        ctx.set_stream(stream.cuda_stream)
+        batch = ctx.batch_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), len(evs), len(clusters))
+        ctx.batch_run(batch)
+        tune = None if args.no_autotune else ctx.autotune(repeats=2)
+        ms = timed_replays(lambda: ctx.batch_launch(batch), stream, args.steps, args.warmup, dist, device)
+        ctx.batch_status()
+        counts = []
+        for e in range(len(evs)):
+            c = ctx.counts(e)
+            counts.append(dict(N=list(c.clusters), T=list(c.tracklets), C=list(c.cells), E=list(c.neighbours), R=c.roads))
+        prof = ctx.profile(repeats=3)
+    finally:
+        ctx.close()
+    value, ms, total = whole_job_rate(dist, len(evs) * args.steps, ms, device)
+    own = {}
+    for c in counts:
+        for k, v in kernel_bytes(c).items():
+            own[k] = own.get(k, 0) + v
+    top, top_ms = max(prof, key=lambda x: x[1])
+    achieved = own[top] / (top_ms * 1e-3) / 1e9 if top in own else None
+    return {
+        "workload": "uneven_batch_loguniform_20_8000trk_5pct_noise", "events_per_step_per_gpu": len(evs),
+        "clusters_per_step_per_gpu": int(len(clusters)), "events_per_s": value, "clusters_per_s": value * len(clusters) / len(evs),
+        "ms_per_step": ms / args.steps, "launch_shape": tune, "roads_per_step_per_gpu": int(sum(c["R"] for c in counts)),
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "algorithmic_bytes_per_launch": own.get(top),
+                     "launch_ms": top_ms, "traffic": None},
+        "kernel_ms": {k: round(t, 4) for k, t in prof},
+        "note": "configuration 3 at its stated size; the per-event parity against single runs is tests/test_gpu_parity.py",
+    }
+
+
+def pileup_stream_leg(args, stream, dist, device, local):
+    """Configuration 5: a stream of `--stream-frames` frames of 5 overlapping collisions
+    (1050-1950 tracks each, vertices z ~ N(0, 5 cm), 10% noise), fed from pinned host memory
+    through itsu_frames_run_host in calls of `--stream-chunk` frames (each frame's clusters uploaded
+    once and tracked from each of its 5 vertices), roads back to the host: one step is the whole
+    stream. The plain form, and the learned form with the pile-up checkpoints where they exist."""
+    import ctypes
+    import multiprocessing as mp
+
+    import torch
+
+    from itsu import capi, prefilter
+    from itsu.capi import Frames
+
+    world, rank, _ = dist_env()
+    seed = shard_seed(args.seed, rank) + 57
+    rng = np.random.default_rng(seed)
+    mults = [int(rng.integers(1050, 1951)) for _ in range(args.stream_frames)]
+    jobs = [(seed * 1000003 + f, mults[f]) for f in range(args.stream_frames)]
+    with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
+        frames = pool.map(_pileup_frame_job, jobs, chunksize=8)
+    chunks = []
+    for k in range(0, len(frames), args.stream_chunk):
+        fr = frames[k:k + args.stream_chunk]
+        c, o, v, vf = gen.pack_frames(fr)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).pin_memory()  # noqa: E731
+        t = [pin(c), pin(o), pin(v), pin(vf)]
+        f = Frames()
+        f.clusters, f.frame_offsets, f.vertices, f.vertex_frame = (x.data_ptr() for x in t)
+        f.n_frames, f.n_vertices = len(fr), len(vf)
+        chunks.append(dict(t=t, f=f, runs=len(vf), clusters=len(c)))
+    runs = sum(ch["runs"] for ch in chunks)
+    frame_clusters = sum(ch["clusters"] for ch in chunks)
+    cap = 4 * max(ch["clusters"] for ch in chunks)  # roads per call: well below one per cluster
+    h_roads = torch.empty(cap * 32, dtype=torch.uint8, pin_memory=True)
+    h_off = torch.empty(max(ch["runs"] for ch in chunks) + 1, dtype=torch.int32, pin_memory=True)
+    ctx = capi.Context(device=local)
+    out = {"workload": "pileup_stream_5x1050_1950trk_10pct_noise", "frames_per_step_per_gpu": len(frames),
+           "frames_per_call": args.stream_chunk, "vertex_runs_per_step_per_gpu": runs,
+           "frame_clusters_per_step_per_gpu": int(frame_clusters),
+           "api": "itsu_frames_run_host per call (pinned host frames in, roads and road offsets out)", "forms": {}}
+    try:
+        ctx.set_stream(stream.cuda_stream)
+        n_roads = [0]
+
+        def one_step():
+            n_roads[0] = 0
+            for ch in chunks:
+                st = ctx.lib.itsu_frames_run_host(ctx.h, ctypes.byref(ch["f"]), ctypes.c_void_p(h_roads.data_ptr()), cap,
+                                                  ctypes.c_void_p(h_off.data_ptr()))
+                ctx._check(st)
+                n_roads[0] += int(h_off[ch["runs"]])
+
+        pair_path = os.path.join(PKG, "weights", "prefilter_pileup.itsumlp")
+        gate_path = os.path.join(PKG, "weights", "gate_pileup.itsugate")
+        pair = capi.prefilter_load(pair_path) if os.path.exists(pair_path) else None
+        gate = capi.gate_load(gate_path) if os.path.exists(gate_path) else None
+        forms = [("plain", None, None)]
+        if not args.no_prefilter and (pair is not None or gate is not None):
+            forms.append(("learned", pair, gate))
+        steps = max(1, min(args.steps, 3))
+        for name, p_model, g_model in forms:
+            if p_model is not None:
+                ctx.prefilter_set_model(p_model)
+            if g_model is not None:
+                ctx.gate_set_model(g_model)
+            prefilter.set_learned(ctx, p_model is not None, g_model is not None)
+            ms = timed_replays(one_step, stream, steps, 1, dist, device)
+            value, ms, _ = whole_job_rate(dist, runs * steps, ms, device)
+            out["forms"][name] = {"vertex_runs_per_s": value, "frames_per_s": value / 5.0, "ms_per_step": ms / steps,
+                                  "roads_per_step_per_gpu": n_roads[0], "steps": steps,
+                                  "networks": [k for k, m in (("pair_prefilter", p_model), ("tracklet_gate", g_model))
+                                               if m is not None]}
+        prefilter.set_learned(ctx, False, False)
+    finally:
+        ctx.close()
+    if "learned" in out["forms"]:
+        out["forms"]["learned"]["vs_plain"] = out["forms"]["learned"]["vertex_runs_per_s"] / out["forms"]["plain"]["vertex_runs_per_s"]
+        out["forms"]["learned"]["road_fraction_of_plain"] = (out["forms"]["learned"]["roads_per_step_per_gpu"] /
+                                                             max(out["forms"]["plain"]["roads_per_step_per_gpu"], 1))
+    return out
+
+
+def _pileup_frame_job(job):
+    seed, n_tracks = job
+    return gen.make_event(seed, n_tracks, pt_mean=0.6, noise=0.10, n_vertices=5)
 
 
 def road_report_mode(ctx, events, frames, args, rank, world):
@@ -668,22 +862,61 @@ def road_report_mode(ctx, events, frames, args, rank, world):
     return out
 
 
-def learned_mode(ctx, launch, args, stream, dist, device):
-    """The learned-prefilter form on the same resident inputs: K timed graph replays (max over
-    ranks), and its roads against the plain run's (exported just before)."""
+def learned_summary(learned, total_events, plain_value, args):
+    """The learned forms' bench entries: each form's rate against the batched plain path on the
+    same resident batch, its road reproduction and what it kept; the headline form is the fastest
+    one that reproduces at least 99.5% of the plain roads with no extra road."""
+    if not learned:
+        return None
+    out = {}
+    for name, r in learned.items():
+        eps = total_events / (r["ms"] * 1e-3)
+        out[name] = {
+            "events_per_s": eps, "ms_per_step": r["ms"] / args.steps, "vs_batched_plain": eps / plain_value,
+            "road_reproduction": r["cmp"]["road_reproduction"], "plain_roads": r["cmp"]["plain_roads"],
+            "learned_roads": r["cmp"]["learned_roads"], "extra_roads": r["cmp"]["extra"], "extra_fakes": r["cmp"]["extra_fakes"],
+            "tracklets_kept": r["cmp"]["tracklets_kept"], "cells_kept": r["cmp"]["cells_kept"],
+            "gate_logit_threshold": r["gate_threshold"], "pair_logit_threshold": r["pair_threshold"],
+            "kernel_ms": {k: round(t, 4) for k, t in r["prof"]},
+        }
+    ok = [k for k, v in out.items() if v["road_reproduction"] >= 0.995 and v["extra_roads"] == 0]
+    best = max(ok, key=lambda k: out[k]["events_per_s"]) if ok else None
+    return {
+        "headline_form": best,
+        "vs_batched_plain": out[best]["vs_batched_plain"] if best else None,
+        "road_reproduction": out[best]["road_reproduction"] if best else None,
+        "forms": out,
+        "checkpoints": {"pair_prefilter": os.path.relpath(args.prefilter, ROOT) if os.path.exists(args.prefilter) else None,
+                        "tracklet_gate": os.path.relpath(args.gate, ROOT) if os.path.exists(args.gate) else None},
+        "note": "same resident batch and timing as the plain value; tracklet gate: 8-16-16-1 ReLU MLP on every tracklet "
+                "before the tracklet scan; pair prefilter: 8-64-64-1 GELU MLP on the cell stage's pairs; BF16 MMAs, FP32 "
+                "accumulation",
+    }
+
+
+def learned_mode(ctx, launch, args, stream, dist, device, pair_model, gate_model):
+    """One learned form on the same resident inputs: K timed graph replays (max over ranks), and its
+    roads against the plain run's (exported just before)."""
     import torch
 
-    from itsu import capi, prefilter
+    from itsu import prefilter
 
+    prefilter.set_learned(ctx, False, False)
+    launch()
+    ctx.batch_status()
     plain_keys, plain_fake = prefilter.export_roads(ctx, device)
     plain_cells = ctx.prefilter_export()[0]
-    model = capi.prefilter_load(args.prefilter)
-    ctx.prefilter_set_model(model)
-    ctx.prefilter_enable(True)
+    plain_tracklets = ctx.gate_export()[0]
+    if pair_model is not None:
+        ctx.prefilter_set_model(pair_model)
+    if gate_model is not None:
+        ctx.gate_set_model(gate_model)
+    prefilter.set_learned(ctx, pair_model is not None, gate_model is not None)
     try:
         launch()  # captures the learned graph
         ctx.batch_status()
         learned_cells = ctx.prefilter_export()[0]
+        learned_tracklets = ctx.gate_export()[0]
         keys, fake = prefilter.export_roads(ctx, device)
         for _ in range(args.warmup):
             launch()
@@ -700,11 +933,12 @@ def learned_mode(ctx, launch, args, stream, dist, device):
         ms = max_over_ranks(dist, start.elapsed_time(end), device)
         prof = ctx.profile(repeats=3)
     finally:
-        ctx.prefilter_enable(False)
+        prefilter.set_learned(ctx, False, False)
     cmp = prefilter.compare_roads(plain_keys, plain_fake, keys, fake)
     cmp["road_reproduction"] = cmp["reproduced"] / max(cmp["plain_roads"], 1)
     cmp["cells_kept"] = learned_cells / max(plain_cells, 1)
-    return ms, cmp, prof, float(model.logit_threshold)
+    cmp["tracklets_kept"] = learned_tracklets / max(plain_tracklets, 1)
+    return ms, cmp, prof
 
 
 # ------------------------------------------------------------------------------------------

@@ -177,11 +177,23 @@ def pbpb_event(seed: int, n_tracks: int = 6000) -> Event:
     return make_event(seed, n_tracks, pt_mean=0.6, noise=0.05)
 
 
-def batch_events(seed: int, n_events: int = 256, lo: int = 20, hi: int = 8000) -> list:
-    """Uneven batch: multiplicity log-uniform over [lo, hi] tracks, own vertex per event."""
+def batch_multiplicities(seed: int, n_events: int = 256, lo: int = 20, hi: int = 8000) -> np.ndarray:
+    """The track counts of an uneven batch: log-uniform over [lo, hi]."""
     rng = np.random.default_rng(seed)
-    mults = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n_events))).astype(int)
-    return [make_event(seed * 100003 + i, int(m), pt_mean=0.6, noise=0.05) for i, m in enumerate(mults)]
+    return np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n_events))).astype(int)
+
+
+def batch_event(seed: int, index: int, n_tracks: int) -> Event:
+    """Event `index` of the uneven batch of `seed` (its own vertex, 5% noise)."""
+    return make_event(seed * 100003 + index, int(n_tracks), pt_mean=0.6, noise=0.05)
+
+
+def batch_events(seed: int, n_events: int = 256, lo: int = 20, hi: int = 8000, indices=None) -> list:
+    """Uneven batch: multiplicity log-uniform over [lo, hi] tracks, own vertex per event; only the
+    events at `indices` when given (a rank's shard of the batch)."""
+    mults = batch_multiplicities(seed, n_events, lo, hi)
+    idx = range(n_events) if indices is None else indices
+    return [batch_event(seed, i, mults[i]) for i in idx]
 
 
 def jet_event(seed: int, n_tracks: int = 100) -> Event:
