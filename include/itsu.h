@@ -46,6 +46,17 @@ typedef struct itsu_cluster {
   int32_t bin;     /* phi-z index table bin (filled by clustering) */
 } itsu_cluster;
 
+/* A cluster as the caller delivers it, before clustering: the arguments of the reference's raw
+ * constructor Cluster(clusterId, x, y, z, alpha, monteCarloId) (Cluster.cxx:27-33) without the
+ * fields clustering computes (phi, r, bin), in 24 bytes instead of 36: the host-facing calls that
+ * take it upload a third fewer bytes. */
+typedef struct itsu_cluster_in {
+  float x, y, z;
+  int32_t cluster_id;
+  float alpha;
+  int32_t mc_id;
+} itsu_cluster_in;
+
 typedef struct itsu_tracklet {
   int32_t first_cluster;  /* sorted index in layer L */
   int32_t second_cluster; /* sorted index in layer L+1 */
@@ -201,6 +212,11 @@ itsu_status itsu_batch_run(itsu_context *ctx, const itsu_batch *batch);
 itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
                                 const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
                                 int32_t *road_offsets);
+/* itsu_batch_run_host with 24-byte input records (itsu_cluster_in): the same runs and results,
+ * streamed the same way under ITSU_FLAG_STREAM_HOST. */
+itsu_status itsu_batch_run_host_compact(itsu_context *ctx, const itsu_cluster_in *clusters, const int32_t *layer_offsets,
+                                        const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
+                                        int32_t *road_offsets);
 /* Launches every stage of the batch on the context stream without waiting (CUDA-graph
  * replay after the first call with the same shape); itsu_batch_status waits and reports. */
 itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch);

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 from itsu import capi, gen
+from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -135,3 +136,32 @@ def test_streamed_batch_outgrowing_the_arena_falls_back_and_grows():
     finally:
         one.close()
         small.close()
+
+
+@pytest.mark.parametrize("streamed", [False, True])
+def test_compact_input_records_give_the_same_run(streamed):
+    """itsu_batch_run_host_compact (24-byte input records, the fields clustering computes left out)
+    gives the 36-byte call's roads and every per-event result bit for bit, one pass and streamed
+    (chunks on two arenas), with malformed input reported at the same cluster."""
+    events = [gen.pbpb_event(s, n_tracks=3000) for s in (81, 82)] + gen.batch_events(83, n_events=12) + [gen.jet_event(7)]
+    clusters, offsets, vertices = gen.pack_batch(events)
+    # streamed: small chunks, so that the batch splits
+    kw = dict(flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=60000) if streamed else {}
+    full = capi.Context(device=0, **kw)
+    comp = capi.Context(device=0, **kw)
+    try:
+        want_roads, want_off = full.batch_run_host(clusters, offsets, vertices)
+        got_roads, got_off = comp.batch_run_host_compact(capi.compact_clusters(clusters), offsets, vertices)
+        assert np.array_equal(want_off, got_off)
+        assert np.array_equal(want_roads.view(np.uint8), got_roads.view(np.uint8))
+        if not streamed:
+            for e in range(len(events)):
+                assert oracle.diff(comp.results(e), full.results(e)) == [], e
+        bad = capi.compact_clusters(clusters)
+        bad["x"][offsets[7 * 3 + 2] + 5] = np.nan
+        with pytest.raises(capi.ItsuError) as err:
+            comp.batch_run_host_compact(bad, offsets, vertices)
+        assert err.value.status == capi.ERR_INVALID and str(offsets[7 * 3 + 2] + 5) in str(err.value)
+    finally:
+        full.close()
+        comp.close()

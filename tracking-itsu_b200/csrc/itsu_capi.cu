@@ -112,6 +112,9 @@ struct itsu_context {
   int64_t n_clusters = 0;
   std::vector<int32_t> h_layer_off;
   const itsu_cluster *in_raw = nullptr;
+  const itsu_cluster_in *in_raw_in = nullptr;  // the 24-byte input records instead of in_raw (compact host calls)
+  itsu_cluster_in *raw_in = nullptr;           // their device copy
+  int64_t cap_raw_in = 0;
   const int32_t *in_raw_off = nullptr;
   const int32_t *in_layer_off = nullptr;
   int32_t *raw_off = nullptr;  // arena copy of a frames run's raw offsets (event class)
@@ -122,7 +125,7 @@ struct itsu_context {
   cudaGraphExec_t graph = nullptr;
   uint64_t graph_generation = 0;
   uint64_t generation = 1;  // bumped whenever a buffer is reallocated
-  const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  const void *graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int32_t graph_events = -1;
   int64_t graph_clusters = -1;
 
@@ -254,6 +257,7 @@ Arena arena_of(const itsu_context *ctx)
   a.n_events = ctx->n_events;
   a.n_clusters = ctx->n_clusters;
   a.raw = ctx->in_raw;
+  a.raw_in = ctx->in_raw_in;
   a.raw_off = ctx->in_raw_off;
   a.layer_off = ctx->in_layer_off;
   a.vtx = ctx->in_vtx;
@@ -558,7 +562,7 @@ itsu_status launch_all(itsu_context *ctx)
                     ctx->graph_tune[2] == tune.prune && ctx->graph_prefilter == ctx->prefilter &&
                     ctx->graph_gate == ctx->gate &&
                     ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
-                    ctx->graph_key[3] == ctx->in_raw_off &&
+                    ctx->graph_key[3] == ctx->in_raw_off && ctx->graph_key[4] == ctx->in_raw_in &&
                     ctx->graph_events == ctx->n_events && ctx->graph_clusters == ctx->n_clusters;
   if (!same) {
     drop_graph(ctx);
@@ -583,6 +587,7 @@ itsu_status launch_all(itsu_context *ctx)
     ctx->graph_key[1] = ctx->in_layer_off;
     ctx->graph_key[2] = ctx->in_vtx;
     ctx->graph_key[3] = ctx->in_raw_off;
+    ctx->graph_key[4] = ctx->in_raw_in;
     ctx->graph_tune[0] = tune.block;
     ctx->graph_tune[1] = tune.blocks_per_sm;
     ctx->graph_tune[2] = tune.prune;
@@ -708,6 +713,7 @@ itsu_status upload_vertex(itsu_context *ctx, const itsu_cluster *const layers[IT
   ctx->n_clusters = off[ITSU_LAYERS];
   ctx->h_layer_off = off;
   ctx->in_raw = ctx->raw;
+  ctx->in_raw_in = nullptr;
   ctx->in_raw_off = nullptr;
   ctx->in_layer_off = ctx->layer_off;
   ctx->in_vtx = ctx->vtx;
@@ -867,7 +873,7 @@ void itsu_context_destroy(itsu_context *ctx)
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->twin) itsu_context_destroy(ctx->twin);
   drop_graph(ctx);
-  release(ctx->raw); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
+  release(ctx->raw); release(ctx->raw_in); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
   release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->clu_aux); release(ctx->clu_crowded); release(ctx->trk_slots);
   release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
@@ -1109,6 +1115,7 @@ static itsu_status set_batch(itsu_context *ctx, const itsu_batch *batch)
   ctx->n_events = batch->n_events;
   ctx->n_clusters = batch->n_clusters;
   ctx->in_raw = batch->clusters;
+  ctx->in_raw_in = nullptr;
   ctx->in_raw_off = nullptr;
   ctx->in_layer_off = batch->layer_offsets;
   ctx->in_vtx = batch->vertices;
@@ -1142,7 +1149,7 @@ itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch)
   if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
   itsu_status st;
-  const bool same = batch && ctx->stage != kNone && !ctx->in_raw_off && batch->clusters == ctx->in_raw &&
+  const bool same = batch && ctx->stage != kNone && !ctx->in_raw_off && !ctx->in_raw_in && batch->clusters == ctx->in_raw &&
                     batch->layer_offsets == ctx->in_layer_off &&
                     batch->vertices == ctx->in_vtx && batch->n_events == ctx->n_events && batch->n_clusters == ctx->n_clusters;
   if (!same && (st = set_batch(ctx, batch)) != ITSU_OK) return st;
@@ -1380,7 +1387,33 @@ itsu_status ensure_twin(itsu_context *ctx)
 // chunk order. The first chunk is smaller, so that the device starts sooner. Sets *done to false,
 // with nothing reported, when the batch is too small to split or a chunk outgrew its arena: the
 // caller then runs the batch in one pass (which grows the arena).
-itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets, const float *vertices,
+// The host's raw clusters in either record format: 36-byte itsu_cluster or 24-byte itsu_cluster_in.
+struct HostClusters {
+  const itsu_cluster *full = nullptr;
+  const itsu_cluster_in *compact = nullptr;
+  bool any() const { return full || compact; }
+};
+
+// Uploads host clusters [a, b) to the context's raw buffer of their format (asynchronous on s).
+itsu_status upload_clusters(itsu_context *ctx, const HostClusters &h, int64_t a, int64_t b, cudaStream_t s)
+{
+  if (b <= a) return ITSU_OK;
+  if (h.compact) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw_in + a, h.compact + a, sizeof(itsu_cluster_in) * (b - a), cudaMemcpyHostToDevice, s));
+  } else {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw + a, h.full + a, sizeof(itsu_cluster) * (b - a), cudaMemcpyHostToDevice, s));
+  }
+  return ITSU_OK;
+}
+
+// A run's inputs start at cluster a of the context's raw buffer of the format.
+void point_inputs_at(itsu_context *x, const itsu_context *owner, const HostClusters &h, int64_t a)
+{
+  x->in_raw = h.compact ? nullptr : owner->raw + a;
+  x->in_raw_in = h.compact ? owner->raw_in + a : nullptr;
+}
+
+itsu_status run_host_streamed(itsu_context *ctx, const HostClusters &clusters, const int32_t *layer_offsets, const float *vertices,
                               int32_t n_events, int64_t n_clusters, itsu_road *roads, int64_t roads_capacity,
                               int32_t *road_offsets, bool *done)
 {
@@ -1465,10 +1498,7 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, vertices, sizeof(float) * 3 * (int64_t)n_events, cudaMemcpyHostToDevice, ctx->copy_stream));
   for (int c = 0; c < k_chunks; ++c) {
     const int64_t a = layer_offsets[(int64_t)ev[c] * ITSU_LAYERS], b = layer_offsets[(int64_t)ev[c + 1] * ITSU_LAYERS];
-    if (b > a) {
-      ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw + a, clusters + a, sizeof(itsu_cluster) * (b - a), cudaMemcpyHostToDevice,
-                                     ctx->copy_stream));
-    }
+    if ((st = upload_clusters(ctx, clusters, a, b, ctx->copy_stream)) != ITSU_OK) return st;
     ITSU_CUDA(ctx, cudaEventRecord(ctx->chunk_ready[c], ctx->copy_stream));
   }
 
@@ -1483,7 +1513,7 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
     ITSU_CUDA(ctx, cudaStreamWaitEvent(x->stream, ctx->chunk_ready[c], 0));
     x->n_events = ev[c + 1] - ev[c];
     x->n_clusters = b - a;
-    x->in_raw = ctx->raw + a;
+    point_inputs_at(x, ctx, clusters, a);
     x->in_raw_off = nullptr;
     x->in_layer_off = ctx->chunk_off + (int64_t)ev[c] * ITSU_LAYERS + c;
     x->in_vtx = ctx->vtx + 3 * (int64_t)ev[c];
@@ -1588,24 +1618,21 @@ itsu_status run_host_streamed(itsu_context *ctx, const itsu_cluster *clusters, c
   return ITSU_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
-                                const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
-                                int32_t *road_offsets)
+itsu_status batch_run_host(itsu_context *ctx, const HostClusters &clusters, const int32_t *layer_offsets, const float *vertices,
+                           int32_t n_events, itsu_road *roads, int64_t roads_capacity, int32_t *road_offsets)
 {
   if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
   if (n_events < 0 || (n_events > 0 && (!layer_offsets || !vertices))) return fail(ctx, ITSU_ERR_INVALID, "bad batch arguments");
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
   const int64_t n_clusters = n_events > 0 ? layer_offsets[(int64_t)n_events * ITSU_LAYERS] : 0;
-  if (n_clusters > 0 && !clusters) return fail(ctx, ITSU_ERR_INVALID, "null clusters");
+  if (n_clusters > 0 && !clusters.any()) return fail(ctx, ITSU_ERR_INVALID, "null clusters");
   if (layer_offsets && layer_offsets[0] != 0) return fail(ctx, ITSU_ERR_INVALID, "layer offsets must start at 0");
   for (int64_t k = 1; n_events > 0 && k <= (int64_t)n_events * ITSU_LAYERS; ++k) {
     if (layer_offsets[k] < layer_offsets[k - 1]) return fail(ctx, ITSU_ERR_INVALID, "layer offsets decrease at %lld", (long long)k);
   }
   itsu_status st;
+  if ((st = ensure_clusters(ctx, n_clusters, n_events)) != ITSU_OK) return st;
+  if (clusters.compact && (st = grow_buffer(ctx, ctx->raw_in, ctx->cap_raw_in, n_clusters)) != ITSU_OK) return st;
   if (ctx->flags & ITSU_FLAG_STREAM_HOST) {
     bool done = false;
     if ((st = run_host_streamed(ctx, clusters, layer_offsets, vertices, n_events, n_clusters, roads, roads_capacity, road_offsets,
@@ -1614,26 +1641,17 @@ itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters,
     }
     if (done) return ITSU_OK;
   }
-  if ((st = ensure_clusters(ctx, n_clusters, n_events)) != ITSU_OK) return st;
-  if (n_clusters > 0) {
-    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw, clusters, sizeof(itsu_cluster) * n_clusters, cudaMemcpyHostToDevice, ctx->stream));
-  }
+  if ((st = upload_clusters(ctx, clusters, 0, n_clusters, ctx->stream)) != ITSU_OK) return st;
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->layer_off, layer_offsets, sizeof(int32_t) * ((int64_t)n_events * ITSU_LAYERS + 1),
                                  cudaMemcpyHostToDevice, ctx->stream));
   ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->vtx, vertices, sizeof(float) * 3 * (int64_t)n_events, cudaMemcpyHostToDevice, ctx->stream));
-  itsu_batch b{};
-  b.clusters = ctx->raw;
-  b.layer_offsets = ctx->layer_off;
-  b.vertices = ctx->vtx;
-  b.n_events = n_events;
-  b.n_clusters = n_clusters;
   if ((st = ensure_outputs_for(ctx, n_clusters)) != ITSU_OK) return st;
   ctx->n_events = n_events;
   ctx->n_clusters = n_clusters;
-  ctx->in_raw = b.clusters;
+  point_inputs_at(ctx, ctx, clusters, 0);
   ctx->in_raw_off = nullptr;
-  ctx->in_layer_off = b.layer_offsets;
-  ctx->in_vtx = b.vertices;
+  ctx->in_layer_off = ctx->layer_off;
+  ctx->in_vtx = ctx->vtx;
   ctx->h_layer_off.assign(layer_offsets, layer_offsets + (int64_t)n_events * ITSU_LAYERS + 1);
   if ((st = run_all(ctx)) != ITSU_OK) return st;
   const int64_t total = ctx->h_status->total[itsu::kRoads];
@@ -1647,6 +1665,28 @@ itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters,
   }
   ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return ITSU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters, const int32_t *layer_offsets,
+                                const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
+                                int32_t *road_offsets)
+{
+  HostClusters h;
+  h.full = clusters;
+  return batch_run_host(ctx, h, layer_offsets, vertices, n_events, roads, roads_capacity, road_offsets);
+}
+
+itsu_status itsu_batch_run_host_compact(itsu_context *ctx, const itsu_cluster_in *clusters, const int32_t *layer_offsets,
+                                        const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
+                                        int32_t *road_offsets)
+{
+  HostClusters h;
+  h.compact = clusters;
+  return batch_run_host(ctx, h, layer_offsets, vertices, n_events, roads, roads_capacity, road_offsets);
 }
 
 itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, itsu_road *roads, int64_t roads_capacity,
@@ -1696,6 +1736,7 @@ itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, i
   ctx->n_events = nv;
   ctx->n_clusters = total;
   ctx->in_raw = ctx->raw;
+  ctx->in_raw_in = nullptr;
   ctx->in_raw_off = ctx->raw_off;
   ctx->in_layer_off = ctx->layer_off;
   ctx->in_vtx = ctx->vtx;

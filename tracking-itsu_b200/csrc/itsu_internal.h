@@ -81,8 +81,9 @@ struct Arena {
   int32_t n_events;
   int32_t pad_;
   int64_t n_clusters;
-  // inputs
+  // inputs (raw clusters in one of two record formats: raw_in set means the 24-byte one)
   const itsu_cluster *raw;
+  const itsu_cluster_in *raw_in;
   const int32_t *raw_off;  // per (run, layer): start of its raw clusters; null = same as layer_off
   const int32_t *layer_off;
   const float *vtx;

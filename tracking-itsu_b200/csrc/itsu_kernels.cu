@@ -320,6 +320,43 @@ __device__ __forceinline__ void stage_out(itsu_cluster *dst, const int32_t *stag
   }
 }
 
+// The 24-byte input record (itsu_cluster_in) in 4-byte words.
+constexpr int kClusterInWords = sizeof(itsu_cluster_in) / 4;
+static_assert(sizeof(itsu_cluster_in) == 24 && alignof(itsu_cluster_in) == 4, "input record layout");
+
+// A warp's 32 consecutive records of kWords words each, moved into its stage with coalesced loads.
+template <int kWords, typename Record>
+__device__ __forceinline__ void stage_in_words(int32_t *stage, const Record *src, int count)
+{
+  const int32_t *w = reinterpret_cast<const int32_t *>(src);
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < kWords; ++k) {
+    const int at = k * 32 + lane;
+    if (at < count * kWords) {
+      stage[at] = w[at];
+    }
+  }
+  __syncwarp();
+}
+
+// A lane's 24-byte input record from the stage, as a cluster whose phi, r and bin clustering fills.
+__device__ __forceinline__ itsu_cluster stage_get_in(const int32_t *stage, int lane)
+{
+  const int32_t *w = stage + lane * kClusterInWords;  // word stride 6: each access a 2-way bank conflict at most
+  itsu_cluster c;
+  c.x = __int_as_float(w[0]);
+  c.y = __int_as_float(w[1]);
+  c.z = __int_as_float(w[2]);
+  c.phi = 0.0f;
+  c.r = 0.0f;
+  c.cluster_id = w[3];
+  c.alpha = __int_as_float(w[4]);
+  c.mc_id = w[5];
+  c.bin = 0;
+  return c;
+}
+
 __device__ __forceinline__ itsu_cluster stage_get(const int32_t *stage, int lane)
 {
   itsu_cluster c;
@@ -375,9 +412,22 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   const int wb = min(n, warp * chunk), we = min(n, wb + chunk);
   for (int i0 = wb; i0 < we; i0 += 32) {
     const int count = min(32, we - i0);
-    stage_in(stage, a.raw + raw_begin + i0, count);
+    itsu_cluster c{};
+    if (a.raw_in) {
+      // 24-byte input records (x, y, z, id, alpha, MC id): read in 6-word strides, then the stage
+      // is reused for the 36-byte records once every lane has read its own
+      stage_in_words<kClusterInWords>(stage, a.raw_in + raw_begin + i0, count);
+      if (lane < count) {
+        c = stage_get_in(stage, lane);
+      }
+      __syncwarp();
+    } else {
+      stage_in(stage, a.raw + raw_begin + i0, count);
+      if (lane < count) {
+        c = stage_get(stage, lane);
+      }
+    }
     if (lane < count) {
-      itsu_cluster c = stage_get(stage, lane);
       const Transformed t = transform_cluster(layer, c.x, c.y, c.z, vx, vy);
       c.phi = t.phi;
       c.r = t.r;

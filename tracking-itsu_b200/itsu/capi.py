@@ -16,6 +16,18 @@ from .gen import CLUSTER_DTYPE
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG, "lib", "libitsu_b200.so")
 
+# itsu_cluster_in: the 24-byte input record of the compact host calls
+CLUSTER_IN_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("id", "<i4"), ("alpha", "<f4"), ("mc", "<i4")])
+
+
+def compact_clusters(clusters) -> np.ndarray:
+    """The 24-byte input records of 36-byte clusters (the fields clustering computes dropped)."""
+    out = np.zeros(len(clusters), CLUSTER_IN_DTYPE)
+    for k in CLUSTER_IN_DTYPE.names:
+        out[k] = clusters[k]
+    return out
+
+
 TRACKLET_DTYPE = np.dtype([("c1", "<i4"), ("c2", "<i4"), ("tan_lambda", "<f4"), ("phi", "<f4")])
 CELL_DTYPE = np.dtype(
     [("c1", "<i4"), ("c2", "<i4"), ("c3", "<i4"), ("t1", "<i4"), ("t2", "<i4"), ("nx", "<f4"), ("ny", "<f4"),
@@ -164,6 +176,9 @@ SIGNATURES = [
       ctypes.POINTER(ctypes.c_int32)]),
     ("itsu_batch_run", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Batch)]),
     ("itsu_batch_run_host", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+      ctypes.c_void_p]),
+    ("itsu_batch_run_host_compact", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_void_p]),
     ("itsu_batch_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Batch)]),
@@ -457,6 +472,24 @@ class Context:
         roads = np.zeros(roads_capacity, ROAD_DTYPE)
         self._check(self.lib.itsu_batch_run_host(self.h, _ptr(clusters), _ptr(layer_offsets), _ptr(vertices), n_events,
                                                  _ptr(roads), roads_capacity, _ptr(offs)))
+        roads = roads[: offs[-1]].copy()
+        roads["pad"] = 0
+        return roads, offs
+
+    def batch_run_host_compact(self, clusters_in, layer_offsets, vertices, roads_capacity=None):
+        """batch_run_host with 24-byte input records (CLUSTER_IN_DTYPE); returns (roads, road_offsets)."""
+        clusters_in = np.ascontiguousarray(clusters_in, CLUSTER_IN_DTYPE)
+        layer_offsets = np.ascontiguousarray(layer_offsets, np.int32)
+        vertices = np.ascontiguousarray(vertices, np.float32)
+        n_events = (len(layer_offsets) - 1) // 7
+        offs = np.zeros(n_events + 1, np.int32)
+        if roads_capacity is None:
+            self._check(self.lib.itsu_batch_run_host_compact(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices),
+                                                             n_events, None, 0, _ptr(offs)))
+            roads_capacity = int(offs[-1])
+        roads = np.zeros(roads_capacity, ROAD_DTYPE)
+        self._check(self.lib.itsu_batch_run_host_compact(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices), n_events,
+                                                         _ptr(roads), roads_capacity, _ptr(offs)))
         roads = roads[: offs[-1]].copy()
         roads["pad"] = 0
         return roads, offs
