@@ -468,7 +468,7 @@ def run_ours(args):
         ctx_e2e = capi.Context(device=local, flags=capi.FLAG_STREAM_HOST)
         ctx_e2e.set_stream(stream.cuda_stream)
         if tune is not None:
-            ctx_e2e.set_tune(tune["band"], tune["threads_per_block"], tune["blocks_per_sm"], tune["prune"])
+            ctx_e2e.set_tune(tune["band"], tune["threads_per_block"], tune["blocks_per_sm"], tune["prune"], tune["events_per_group"])
 
     def host_run():
         st = ctx_e2e.lib.itsu_batch_run_host_compact(ctx_e2e.h, ctypes.c_void_p(h_clusters.data_ptr()), ctypes.c_void_p(h_offsets.data_ptr()),

@@ -298,7 +298,9 @@ typedef struct itsu_tune {
   int32_t blocks_per_sm;
   int32_t prune;  /* tracklet candidate pruning index on (1) or off (0) */
   float ms;       /* best time of one run of the tuned inputs, 0 if untuned */
-  int32_t reserved_;
+  int32_t events_per_group; /* whole runs: the tracklet write and cell count passes run event group by
+                               event group, so that a group's tracklets are still in L2 when its
+                               cells gather them (0: all events at once) */
 } itsu_tune;
 int32_t itsu_multiplicity_band(int64_t n_clusters, int32_t n_events);
 itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best);

@@ -246,15 +246,16 @@ def test_launch_shapes_and_autotuner_keep_results(ctx):
     want = [ctx.results(e) for e in range(len(events))]
     band = ctx.lib.itsu_multiplicity_band(len(clusters), len(events))
     try:
-        for block, per_sm, prune in [(128, 4, 0), (512, 16, 1), (64, 2, 1)]:
-            ctx.set_tune(band, block, per_sm, prune)
-            assert ctx.get_tune(band)["threads_per_block"] == block
+        for block, per_sm, prune, group in [(128, 4, 0, 0), (512, 16, 1, 0), (64, 2, 1, 0), (256, 8, 1, 2), (64, 4, 1, 4)]:
+            ctx.set_tune(band, block, per_sm, prune, group)
+            assert ctx.get_tune(band)["threads_per_block"] == block and ctx.get_tune(band)["events_per_group"] == group
             roads, off = ctx.batch_run_host(clusters, offsets, vertices)
             assert np.array_equal(off, base_off) and np.array_equal(roads.view(np.uint8), base_roads.view(np.uint8))
             for e in range(len(events)):
-                _assert_same(ctx.results(e), want[e], "shape %d/%d/%d event %d" % (block, per_sm, prune, e))
+                _assert_same(ctx.results(e), want[e], "shape %d/%d/%d/%d event %d" % (block, per_sm, prune, group, e))
         best = ctx.autotune(repeats=1)
-        assert best["band"] == band and best["threads_per_block"] in (128, 256, 512) and best["ms"] > 0
+        assert best["band"] == band and best["threads_per_block"] in (64, 128, 256, 512) and best["ms"] > 0
+        assert best["events_per_group"] in (0, 8, 16, 32)
         roads, off = ctx.batch_run_host(clusters, offsets, vertices)
         assert np.array_equal(roads.view(np.uint8), base_roads.view(np.uint8))
     finally:
@@ -315,3 +316,34 @@ def test_clusters_beyond_z_range_match_oracle(ctx):
     roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
     _assert_same(ctx.results(1), want, "beyond-z batched")
     assert np.array_equal(roads[road_off[1]:road_off[2]].view(np.uint8), want["roads"].view(np.uint8))
+
+
+def test_event_groups_keep_results():
+    """The tracklet write and cell count passes run event group by event group (groups of 1, 3, 7
+    and 16 events, so group ends fall inside the 32-cluster and 32-tracklet blocks of the passes'
+    warps), whole runs and streamed chunks: the results equal the run without groups bit for bit."""
+    events = gen.batch_events(19, n_events=40) + [gen.jet_event(9), gen.pp_event(10)]
+    clusters, offsets, vertices = gen.pack_batch(events)
+    plain = capi.Context(device=0)
+    grouped = capi.Context(device=0)
+    streamed = capi.Context(device=0, flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=150000)
+    try:
+        want_roads, want_off = plain.batch_run_host(clusters, offsets, vertices)
+        want = [plain.results(e) for e in range(len(events))]
+        band = plain.lib.itsu_multiplicity_band(len(clusters), len(events))
+        for group in (1, 3, 7, 16):
+            grouped.set_tune(band, 256, 8, 1, group)
+            roads, off = grouped.batch_run_host(clusters, offsets, vertices)
+            assert np.array_equal(off, want_off) and np.array_equal(roads.view(np.uint8), want_roads.view(np.uint8)), group
+            for e in range(len(events)):
+                _assert_same(grouped.results(e), want[e], "groups of %d, event %d" % (group, e))
+            prof = grouped.profile(repeats=1)
+            assert any("event group" in name for name, _ in prof) and not any(name == "cells_count" for name, _ in prof)
+        for b in range(32):
+            streamed.set_tune(b, 256, 8, 1, 3)  # every chunk's band
+        roads, off = streamed.batch_run_host(clusters, offsets, vertices)
+        assert np.array_equal(off, want_off) and np.array_equal(roads.view(np.uint8), want_roads.view(np.uint8))
+    finally:
+        plain.close()
+        grouped.close()
+        streamed.close()

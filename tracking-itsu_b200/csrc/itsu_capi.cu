@@ -45,6 +45,7 @@ struct Tune {
   int prune = 1;
   float ms = 0.0f;
   bool set = false;
+  int group = 0;  // events per group of the interleaved tracklet write / cell count passes (0: no groups)
 };
 constexpr int kBands = 32;
 
@@ -90,6 +91,7 @@ struct itsu_context {
   float *vtx = nullptr;
   // tracklet class
   itsu_tracklet *tracklets = nullptr;
+  float2 *trk_slope = nullptr;  // (tanL, phi) of each tracklet, beside the records
   int32_t *trk_seg_id = nullptr, *cell_count = nullptr, *cell_off = nullptr, *cell_lookup = nullptr, *cell_crowded = nullptr;
   unsigned long long *cell_mask = nullptr;
   // cell class
@@ -111,6 +113,7 @@ struct itsu_context {
   int32_t n_events = 0;
   int64_t n_clusters = 0;
   std::vector<int32_t> h_layer_off;
+  std::vector<int64_t> group_bounds;  // event groups of the current whole run (whole_run_launch)
   const itsu_cluster *in_raw = nullptr;
   const itsu_cluster_in *in_raw_in = nullptr;  // the 24-byte input records instead of in_raw (compact host calls)
   itsu_cluster_in *raw_in = nullptr;           // their device copy
@@ -133,7 +136,7 @@ struct itsu_context {
   Tune tunes[kBands];
   Tune override_tune;
   bool tuning = false;
-  int graph_tune[3] = {0, 0, -1};
+  int graph_tune[4] = {0, 0, -1, -1};
   bool graph_prefilter = false;
   bool graph_gate = false;
 
@@ -248,7 +251,50 @@ Tune current_tune(const itsu_context *ctx)
 Launch launch_of(const itsu_context *ctx)
 {
   const Tune t = current_tune(ctx);
-  return Launch{ctx->stream, ctx->num_sms, t.block, t.blocks_per_sm};
+  Launch l{};
+  l.stream = ctx->stream;
+  l.num_sms = ctx->num_sms;
+  l.block = t.block;
+  l.blocks_per_sm = t.blocks_per_sm;
+  return l;
+}
+
+// Event groups of a run of n_events events with host layer offsets off[n_events * 7 + 1]: group g
+// holds events [g * group, (g + 1) * group) and, for the write pass, the inner clusters from the
+// first multiple of 32 at or after its first cluster (the previous group's write covers the few
+// before it, which only makes their tracklets exist sooner). No groups for one group or fewer.
+void group_bounds(const int32_t *off, int32_t n_events, int64_t n_clusters, int group, std::vector<int64_t> &out)
+{
+  out.clear();
+  if (group <= 0 || n_events <= group) return;
+  const int n_groups = (n_events + group - 1) / group;
+  out.push_back(0);
+  for (int g = 1; g < n_groups; ++g) {
+    const int64_t first = off[(int64_t)g * group * ITSU_LAYERS] - off[0];
+    out.push_back(std::min<int64_t>((first + 31) & ~int64_t(31), n_clusters));
+  }
+  out.push_back(n_clusters);
+}
+
+void attach_groups(Launch &l, const std::vector<int64_t> &bounds, int group)
+{
+  l.n_groups = bounds.empty() ? 0 : (int)bounds.size() - 1;
+  l.group_events = group;
+  l.groups = bounds.empty() ? nullptr : bounds.data();
+}
+
+// The launch shape of a whole run of the context's current inputs, with its event groups.
+Launch whole_run_launch(itsu_context *ctx)
+{
+  Launch l = launch_of(ctx);
+  const int group = current_tune(ctx).group;
+  if (group > 0 && (int64_t)ctx->h_layer_off.size() == (int64_t)ctx->n_events * ITSU_LAYERS + 1) {
+    group_bounds(ctx->h_layer_off.data(), ctx->n_events, ctx->n_clusters, group, ctx->group_bounds);
+  } else {
+    ctx->group_bounds.clear();
+  }
+  attach_groups(l, ctx->group_bounds, group);
+  return l;
 }
 
 Arena arena_of(const itsu_context *ctx)
@@ -280,6 +326,7 @@ Arena arena_of(const itsu_context *ctx)
   a.trk_lookup = ctx->trk_lookup;
   a.trk_seg = ctx->trk_seg;
   a.tracklets = ctx->tracklets;
+  a.trk_slope = ctx->trk_slope;
   a.trk_seg_id = ctx->trk_seg_id;
   a.cell_count = ctx->cell_count;
   a.cell_mask = ctx->cell_mask;
@@ -383,6 +430,7 @@ itsu_status ensure_tracklets(itsu_context *ctx, int64_t need)
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
     ITSU_CUDA(ctx, alloc(ctx, ctx->tracklets, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->trk_slope, cap));
     ITSU_CUDA(ctx, alloc(ctx, ctx->trk_seg_id, cap));
     ITSU_CUDA(ctx, alloc(ctx, ctx->cell_count, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx, ctx->cell_mask, cap));
@@ -542,7 +590,7 @@ void enqueue_run(const Arena &a, const Launch &l)
   itsu::launch_roads_write(a, l);
 }
 
-void enqueue_all(itsu_context *ctx) { enqueue_run(arena_of(ctx), launch_of(ctx)); }
+void enqueue_all(itsu_context *ctx) { enqueue_run(arena_of(ctx), whole_run_launch(ctx)); }
 
 void drop_graph(itsu_context *ctx)
 {
@@ -559,7 +607,7 @@ itsu_status launch_all(itsu_context *ctx)
   const Tune tune = current_tune(ctx);
   const bool same = ctx->graph && ctx->graph_generation == ctx->generation && ctx->graph_key[0] == ctx->in_raw &&
                     ctx->graph_tune[0] == tune.block && ctx->graph_tune[1] == tune.blocks_per_sm &&
-                    ctx->graph_tune[2] == tune.prune && ctx->graph_prefilter == ctx->prefilter &&
+                    ctx->graph_tune[2] == tune.prune && ctx->graph_tune[3] == tune.group && ctx->graph_prefilter == ctx->prefilter &&
                     ctx->graph_gate == ctx->gate &&
                     ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
                     ctx->graph_key[3] == ctx->in_raw_off && ctx->graph_key[4] == ctx->in_raw_in &&
@@ -591,6 +639,7 @@ itsu_status launch_all(itsu_context *ctx)
     ctx->graph_tune[0] = tune.block;
     ctx->graph_tune[1] = tune.blocks_per_sm;
     ctx->graph_tune[2] = tune.prune;
+    ctx->graph_tune[3] = tune.group;
     ctx->graph_prefilter = ctx->prefilter;
     ctx->graph_gate = ctx->gate;
     ctx->graph_events = ctx->n_events;
@@ -878,7 +927,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
-  release(ctx->tracklets); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->cell_off); release(ctx->cell_lookup); release(ctx->cell_crowded);
+  release(ctx->tracklets); release(ctx->trk_slope); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->cell_off); release(ctx->cell_lookup); release(ctx->cell_crowded);
   release(ctx->cells); release(ctx->cell_entries); release(ctx->cell_dca); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
@@ -1520,7 +1569,11 @@ itsu_status run_host_streamed(itsu_context *ctx, const HostClusters &clusters, c
     Arena arena = arena_of(x);
     arena.mlp = ctx->prefilter ? ctx->d_mlp : nullptr;  // the context's models serve both arenas
     arena.gate = ctx->gate ? ctx->d_gate : nullptr;
-    const Launch l = launch_of(x);
+    Launch l = launch_of(x);
+    std::vector<int64_t> bounds;  // the chunk's event groups (read while its launches are enqueued)
+    const int group = current_tune(x).group;
+    group_bounds(ctx->h_chunk_off + (int64_t)ev[c] * ITSU_LAYERS + c, x->n_events, x->n_clusters, group, bounds);
+    attach_groups(l, bounds, group);
     enqueue_run(arena, l);
     if (c > 0 && twin) ITSU_CUDA(ctx, cudaStreamWaitEvent(x->stream, ctx->chunk_done[c - 1], 0));
     itsu::launch_append_roads(arena, l, ctx->roads_all, ctx->road_off_all, ev[c], ctx->cap_roads_all, ctx->chunk_status + c);
@@ -1779,15 +1832,17 @@ itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best)
   ITSU_CUDA(ctx, cudaEventCreate(&e1));
   Tune winner;
   winner.ms = 1e30f;
-  const int blocks[] = {128, 256, 512}, per_sm[] = {4, 8, 16}, prunes[] = {1, 0};
+  const int blocks[] = {64, 128, 256, 512}, per_sm[] = {4, 8, 16}, prunes[] = {1, 0}, groups[] = {0, 8, 16, 32};
   ctx->tuning = true;
   cudaError_t err = cudaSuccess;
   for (int b : blocks) {
     for (int m : per_sm) {
       for (int p : prunes) {
-        ctx->override_tune = Tune{b, m, p, 0.0f, true};
+       for (int g : groups) {
+        if (g > 0 && (p == 0 || g >= ctx->n_events)) continue;  // groups only with pruning, and only below the batch
+        ctx->override_tune = Tune{b, m, p, 0.0f, true, g};
         const Arena a = arena_of(ctx);
-        const Launch l = launch_of(ctx);
+        const Launch l = whole_run_launch(ctx);
         float best_ms = 1e30f;
         for (int r = 0; r <= repeats && err == cudaSuccess; ++r) {  // the first pass warms up
           cudaEventRecord(e0, ctx->stream);
@@ -1804,6 +1859,7 @@ itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best)
           winner = ctx->override_tune;
           winner.ms = best_ms;
         }
+       }
       }
     }
   }
@@ -1824,6 +1880,7 @@ itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best)
     best->blocks_per_sm = winner.blocks_per_sm;
     best->prune = winner.prune;
     best->ms = winner.ms;
+    best->events_per_group = winner.group;
   }
   return ITSU_OK;
 }
@@ -1839,6 +1896,7 @@ itsu_status itsu_get_tune(itsu_context *ctx, int32_t band, itsu_tune *out)
   out->blocks_per_sm = t.set ? t.blocks_per_sm : d.blocks_per_sm;
   out->prune = t.set ? t.prune : d.prune;
   out->ms = t.set ? t.ms : 0.0f;
+  out->events_per_group = t.set ? t.group : d.group;
   return ITSU_OK;
 }
 
@@ -1851,7 +1909,8 @@ itsu_status itsu_set_tune(itsu_context *ctx, const itsu_tune *in)
     return fail(ctx, ITSU_ERR_INVALID, "launch shape %d threads x %d blocks/SM out of range", in->threads_per_block,
                 in->blocks_per_sm);
   }
-  ctx->tunes[in->band] = Tune{in->threads_per_block, in->blocks_per_sm, in->prune ? 1 : 0, in->ms, true};
+  if (in->events_per_group < 0) return fail(ctx, ITSU_ERR_INVALID, "events per group %d is negative", in->events_per_group);
+  ctx->tunes[in->band] = Tune{in->threads_per_block, in->blocks_per_sm, in->prune ? 1 : 0, in->ms, true, in->events_per_group};
   drop_graph(ctx);
   return ITSU_OK;
 }
@@ -1864,10 +1923,13 @@ itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_t
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
   int n_all = 0;
   const itsu::KernelStep *all = itsu::pipeline_steps(&n_all);
+  const Arena a = arena_of(ctx);
+  const Launch l = whole_run_launch(ctx);
   std::vector<itsu::KernelStep> steps;  // the steps that launch a kernel in this context's form
   for (int k = 0; k < n_all; ++k) {
     const int only = all[k].learned_only;
-    if (only == 0 || (only == itsu::kPairPrefilterStep && ctx->prefilter) || (only == itsu::kGateStep && ctx->gate)) {
+    if (only == 0 || (only == itsu::kPairPrefilterStep && ctx->prefilter) || (only == itsu::kGateStep && ctx->gate) ||
+        (only == itsu::kGroupedStep && l.n_groups > 0) || (only == itsu::kUngroupedStep && l.n_groups == 0)) {
       steps.push_back(all[k]);
     }
   }
@@ -1877,8 +1939,6 @@ itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_t
   for (auto &e : ev) {
     ITSU_CUDA(ctx, cudaEventCreate(&e));
   }
-  const Arena a = arena_of(ctx);
-  const Launch l = launch_of(ctx);
   cudaError_t err = cudaSuccess;
   for (int r = 0; r < repeats && err == cudaSuccess; ++r) {
     cudaEventRecord(ev[0], ctx->stream);

@@ -111,6 +111,7 @@ struct Arena {
   int32_t *trk_lookup;
   int32_t *trk_seg;
   itsu_tracklet *tracklets;
+  float2 *trk_slope;  // per tracklet its (tanL, phi) again, packed: the cell pass's precut reads only these
   int32_t *trk_seg_id;
   // cells
   int32_t *cell_count;
@@ -151,6 +152,12 @@ struct Launch {
   int num_sms;
   int block;          // threads per block of the per-item kernels (64..512, a multiple of 32)
   int blocks_per_sm;  // grid of the grid-stride kernels, in blocks per SM
+  // Event groups of a whole run (0 groups: none): the tracklet write and cell count passes run
+  // group after group, group g over events [g * group_events, ...) and inner clusters
+  // [groups[g], groups[g + 1]) (a host array of n_groups + 1 entries, read while launching).
+  int n_groups = 0;
+  int group_events = 0;
+  const int64_t *groups = nullptr;
 };
 
 // Stage launchers (asynchronous on l.stream).
@@ -195,11 +202,13 @@ void launch_report(const ReportArgs &r, cudaStream_t stream, int num_sms);
 
 // Every kernel of a run, in launch order, with its name (the instrumentation API times them
 // one by one). The stage launchers above enqueue consecutive ranges of this table.
-enum : int { kPairPrefilterStep = 1, kGateStep = 2 };
+// KernelStep::learned_only: the forms a step launches in (0: every run)
+enum : int { kPairPrefilterStep = 1, kGateStep = 2, kGroupedStep = 3, kUngroupedStep = 4 };
 struct KernelStep {
   const char *name;
   void (*launch)(const Arena &, const Launch &);
-  int learned_only;  // 0; or the learned network whose form alone launches it (kPairPrefilterStep, kGateStep)
+  int learned_only;  // 0, or the only form that launches it: a learned network's (kPairPrefilterStep, kGateStep),
+                     // runs with event groups (kGroupedStep) or without (kUngroupedStep)
 };
 const KernelStep *pipeline_steps(int *count);
 int kernels_per_run();  // kernels one plain run launches (the learned form adds the learned_only steps)

@@ -46,8 +46,6 @@ constexpr float kMaxAbsCoordinate = 1.0e6f;
 constexpr int kMaxPruneBin = 256;  // larger bins disable pruning for their layer
 constexpr int kPruneWords = kMaxPruneBin / 64;  // a pruned column's passes: a mask of this many 64-bit words
 static_assert(kMaxPruneBin % 64 == 0, "a pruned column's passes are whole 64-bit words");
-static_assert(sizeof(itsu_tracklet) == 16 && offsetof(itsu_tracklet, tan_lambda) == 8 && offsetof(itsu_tracklet, phi) == 12,
-              "the cell count pass reads (tanL, phi) as the second 8 bytes of a tracklet");
 
 __device__ __forceinline__ bool capacity_failed(const DevStatus *s) { return (*(volatile const int32_t *)&s->flags & kCapacityMask) != 0; }
 
@@ -695,10 +693,16 @@ __device__ __forceinline__ itsu_tracklet make_tracklet(float4 c, float4 d, int32
   return t;
 }
 
+__device__ __forceinline__ void store_tracklet(const Arena &a, int64_t out, const itsu_tracklet &t)
+{
+  a.tracklets[out] = t;
+  a.trk_slope[out] = make_float2(t.tan_lambda, t.phi);
+}
+
 __device__ __forceinline__ void write_tracklet(const Arena &a, int out, int64_t i_flat, int64_t j_flat, int seg)
 {
-  a.tracklets[out] = make_tracklet(a.xyzr[i_flat], a.xyzr[j_flat], (int32_t)(i_flat - a.layer_off[seg]),
-                                   (int32_t)(j_flat - a.layer_off[seg + 1]));
+  store_tracklet(a, out, make_tracklet(a.xyzr[i_flat], a.xyzr[j_flat], (int32_t)(i_flat - a.layer_off[seg]),
+                                       (int32_t)(j_flat - a.layer_off[seg + 1])));
 }
 
 constexpr int kTrackletSlots = kTrackletSlotsPerCluster;
@@ -1068,14 +1072,16 @@ __global__ void __launch_bounds__(kGateThreads) k_tracklets_gate(Arena a)
 // tracklets lookup entry is written here too. The tracklets of an inner cluster with more than
 // kTrackletSlots of them (not kept by the count pass) get their segment ids here and the rest
 // from k_tracklets_crowded.
-__global__ void __launch_bounds__(kMaxThreads, 2) k_tracklets_write(Arena a)  // 64 registers: 4 blocks of 256 per SM
+// Runs over the inner clusters [c0, c1) (c0 a multiple of 32, so that warps hold whole aligned
+// groups of 32 clusters): all of them, or one event group's share of them.
+__global__ void __launch_bounds__(kMaxThreads, 2) k_tracklets_write(Arena a, int64_t c0, int64_t c1)  // 64 registers: 4 blocks of 256 per SM
 {
   if (capacity_failed(a.status)) {
     return;
   }
-  const int64_t i = global_thread();
+  const int64_t i = c0 + global_thread();
   const int lane = threadIdx.x & 31;
-  const bool valid = i < a.n_clusters;
+  const bool valid = i < c1;
   int32_t first = 0, count = 0, local = 0, next_begin = 0;
   int seg = 0, sid = 0;
   float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -1112,7 +1118,7 @@ __global__ void __launch_bounds__(kMaxThreads, 2) k_tracklets_write(Arena a)  //
       if (owner_count <= kTrackletSlots) {
         const int32_t j = a.trk_slots[(int64_t)rank * a.slot_stride + i0 + owner];
         const float4 d = a.xyzr[owner_next + j];
-        a.tracklets[base + p] = make_tracklet(oc, d, owner_local, j);
+        store_tracklet(a, base + p, make_tracklet(oc, d, owner_local, j));
       }
     }
   }
@@ -1258,7 +1264,11 @@ __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const Ce
 // that the circle geometry runs with the lanes converged. Each pair that passes the geometry
 // becomes a cell entry (its tracklets, normal, curvature and DCA) in the warp's current chunk of
 // the entry scratch, so the write pass needs no geometry.
-__global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
+//
+// Runs over the first tracklets of events [e0, e1), or of all events when e1 is 0. Warps hold
+// aligned groups of 32 tracklets (their cells go to one scan tile); a group that straddles the
+// range's ends has its lanes outside the range idle.
+__global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a, int32_t e0, int32_t e1)
 {
   __shared__ unsigned long long masks[kMaxThreads / 32][32];
   if (capacity_failed(a.status)) {
@@ -1266,19 +1276,24 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t n = a.status->total[kTracklets];
+  const int64_t t0 = e1 > 0 ? a.trk_seg[(int64_t)e0 * ITSU_TRACKLET_LAYERS] : 0;
+  const int64_t t1 = e1 > 0 ? a.trk_seg[(int64_t)e1 * ITSU_TRACKLET_LAYERS] : n;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   int64_t chunk_pos = 0, chunk_end = 0;  // this warp's reserved cell entries (warp-uniform)
-  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
-    const CellLane s = cell_lane(a, base + lane, n);
+  for (int64_t base = (t0 & ~int64_t(31)) + ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < t1;
+       base += warps * 32) {
+    const int64_t k_lane = base + lane;
+    const bool active = k_lane >= t0 && k_lane < t1;
+    const CellLane s = cell_lane(a, active ? k_lane : n, n);
     const bool big = s.n_out > kMaxMaskedOut;
     unsigned long long window = 0;  // the outgoing tracklets that pass the cheap cuts
     if (!big && s.n_out > 0) {
       const float max_dz = kC.cell_max_dz[s.layer];  // n_out > 0: an active cell layer
-      // (tanL, phi), the second half of each 16-byte tracklet record
-      const float2 *tp = reinterpret_cast<const float2 *>(a.tracklets + s.j0) + 1;
+      // (tanL, phi) of the outgoing tracklets, packed 8 bytes each
+      const float2 *tp = a.trk_slope + s.j0;
 #pragma unroll 4
       for (int q = 0; q < s.n_out; ++q) {
-        const float2 t2 = tp[2 * q];
+        const float2 t2 = tp[q];
         window |= (unsigned long long)cell_precut_dz(s.t1_tan_lambda, s.t1_phi, t2.x, t2.y, s.c1, s.vz, max_dz) << q;
       }
     }
@@ -1364,7 +1379,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a)
     if (lane == 0 && batch_cells != 0) {
       atomicAdd(reinterpret_cast<unsigned long long *>(&a.scan_partials[base / kScanTile]), (unsigned long long)batch_cells);
     }
-    if (s.k < n) {
+    if (active) {
       a.cell_count[s.k] = count;
       a.cell_mask[s.k] = big ? 0ull : masks[warp][lane];
       a.cell_lookup[s.k] = ITSU_UNUSED_INDEX;  // the write pass fills it for tracklets with cells
@@ -1821,11 +1836,19 @@ void step_tracklets_gate(const Arena &a, const Launch &l)
   }
 }
 
+void launch_write_range(const Arena &a, const Launch &l, int64_t c0, int64_t c1)
+{
+  const int64_t blocks = (c1 - c0 + l.block - 1) / l.block;
+  if (blocks > 0) {
+    k_tracklets_write<<<(unsigned)blocks, l.block, 0, l.stream>>>(a, c0, c1);
+  }
+}
+
+// The write and cell count passes over all events at once (launches with no event groups).
 void step_tracklets_write(const Arena &a, const Launch &l)
 {
-  const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
-  if (blocks > 0) {
-    k_tracklets_write<<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
+  if (l.n_groups == 0) {
+    launch_write_range(a, l, 0, a.n_clusters);
   }
 }
 
@@ -1838,8 +1861,24 @@ void step_tracklet_segments(const Arena &a, const Launch &l)
 
 void step_cells_count(const Arena &a, const Launch &l)
 {
-  if (whole_warps(a, l)) {
-    k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a);
+  if (l.n_groups == 0 && whole_warps(a, l)) {
+    k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a, 0, 0);
+  }
+}
+
+// Event groups: the write pass of a group's inner clusters, then the cell count pass of its
+// tracklets, group after group, so that the tracklets a group's count pass gathers were written
+// moments before and are still in L2. Group g's clusters are [groups[g], groups[g + 1]) (multiples
+// of 32 up to the last), its events [g * group_events, (g + 1) * group_events).
+void step_write_count_groups(const Arena &a, const Launch &l)
+{
+  if (l.n_groups == 0 || !whole_warps(a, l)) {
+    return;
+  }
+  for (int g = 0; g < l.n_groups; ++g) {
+    launch_write_range(a, l, l.groups[g], l.groups[g + 1]);
+    const int32_t e0 = g * l.group_events, e1 = std::min(a.n_events, (g + 1) * l.group_events);
+    k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a, e0, e1);
   }
 }
 
@@ -1886,31 +1925,32 @@ const KernelStep kSteps[] = {
     {"scan_partials_tracklets", step_scan_partials<0>, 0},   // 4
     {"scan_apply_tracklets", step_scan_apply<0>, 0},         // 5
     {"tracklet_segments", step_tracklet_segments, 0},        // 6
-    {"tracklets_write", step_tracklets_write, 0},            // 7
-    {"tracklets_crowded", step_tracklets_crowded, 0},        // 8
-    {"cells_count", step_cells_count, 0},                    // 9  (c)
-    {"cells_prefilter", step_cells_prefilter, kPairPrefilterStep},  // 10 (learned form with the pair prefilter)
-    {"scan_partials_cells", step_scan_partials<1>, 0},       // 11
-    {"scan_apply_cells", step_scan_apply<1>, 0},             // 12
-    {"cell_segments", step_cell_segments, 0},                // 13
-    {"cells_scatter", step_cells_scatter, 0},                // 14
-    {"cells_crowded", step_cells_crowded, 0},                // 15
-    {"neighbour_reset", step_neighbour_reset, 0},            // 16 (d)
-    {"neighbours_count", step_neighbours<false>, 0},         // 17
-    {"scan_reduce_neighbours", step_scan_reduce<2>, 0},      // 18
-    {"scan_partials_neighbours", step_scan_partials<2>, 0},  // 19
-    {"scan_apply_neighbours", step_scan_apply<2>, 0},        // 20
-    {"neighbour_check", step_neighbour_check, 0},            // 21
-    {"neighbours_write", step_neighbours<true>, 0},          // 22
-    {"levels_1", step_levels<1>, 0},                         // 23
-    {"levels_2", step_levels<2>, 0},                         // 24
-    {"levels_3", step_levels<3>, 0},                         // 25
-    {"levels_4", step_levels<4>, 0},                         // 26
-    {"scan_reduce_roads", step_scan_reduce<3>, 0},           // 27 (e)
-    {"scan_partials_roads", step_scan_partials<3>, 0},       // 28
-    {"scan_apply_roads", step_scan_apply<3>, 0},             // 29
-    {"road_segments", step_road_segments, 0},                // 30
-    {"roads_write", step_roads, 0},                          // 31
+    {"tracklets_crowded", step_tracklets_crowded, 0},        // 7
+    {"tracklets_write", step_tracklets_write, kUngroupedStep},  // 8
+    {"cells_count", step_cells_count, kUngroupedStep},       // 9  (c)
+    {"tracklets_write+cells_count by event group", step_write_count_groups, kGroupedStep},  // 10
+    {"cells_prefilter", step_cells_prefilter, kPairPrefilterStep},  // 11 (learned form with the pair prefilter)
+    {"scan_partials_cells", step_scan_partials<1>, 0},       // 12
+    {"scan_apply_cells", step_scan_apply<1>, 0},             // 13
+    {"cell_segments", step_cell_segments, 0},                // 14
+    {"cells_scatter", step_cells_scatter, 0},                // 15
+    {"cells_crowded", step_cells_crowded, 0},                // 16
+    {"neighbour_reset", step_neighbour_reset, 0},            // 17 (d)
+    {"neighbours_count", step_neighbours<false>, 0},         // 18
+    {"scan_reduce_neighbours", step_scan_reduce<2>, 0},      // 19
+    {"scan_partials_neighbours", step_scan_partials<2>, 0},  // 20
+    {"scan_apply_neighbours", step_scan_apply<2>, 0},        // 21
+    {"neighbour_check", step_neighbour_check, 0},            // 22
+    {"neighbours_write", step_neighbours<true>, 0},          // 23
+    {"levels_1", step_levels<1>, 0},                         // 24
+    {"levels_2", step_levels<2>, 0},                         // 25
+    {"levels_3", step_levels<3>, 0},                         // 26
+    {"levels_4", step_levels<4>, 0},                         // 27
+    {"scan_reduce_roads", step_scan_reduce<3>, 0},           // 28 (e)
+    {"scan_partials_roads", step_scan_partials<3>, 0},       // 29
+    {"scan_apply_roads", step_scan_apply<3>, 0},             // 30
+    {"road_segments", step_road_segments, 0},                // 31
+    {"roads_write", step_roads, 0},                          // 32
 };
 constexpr int kNumSteps = sizeof(kSteps) / sizeof(kSteps[0]);
 
@@ -1971,18 +2011,18 @@ void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l)
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
 void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
-void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 13, a, l); }
-void launch_cells_write(const Arena &a, const Launch &l) { run_steps(14, 15, a, l); }
-void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(16, 21, a, l); }
-void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(22, 26, a, l); }
-void launch_roads_count(const Arena &a, const Launch &l) { run_steps(27, 30, a, l); }
-void launch_roads_write(const Arena &a, const Launch &l) { run_steps(31, 31, a, l); }
+void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 14, a, l); }
+void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 16, a, l); }
+void launch_neighbours_count(const Arena &a, const Launch &l) { run_steps(17, 22, a, l); }
+void launch_neighbours_write(const Arena &a, const Launch &l) { run_steps(23, 27, a, l); }
+void launch_roads_count(const Arena &a, const Launch &l) { run_steps(28, 31, a, l); }
+void launch_roads_write(const Arena &a, const Launch &l) { run_steps(32, 32, a, l); }
 
 int kernels_per_run()
 {
   int n = 0;
   for (const KernelStep &k : kSteps) {
-    n += k.learned_only ? 0 : 1;
+    n += (k.learned_only == 0 || k.learned_only == kUngroupedStep) ? 1 : 0;
   }
   return n;
 }

@@ -80,7 +80,7 @@ class Frames(ctypes.Structure):
 
 class Tune(ctypes.Structure):
     _fields_ = [("band", ctypes.c_int32), ("threads_per_block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("prune", ctypes.c_int32), ("ms", ctypes.c_float), ("reserved_", ctypes.c_int32)]
+                ("prune", ctypes.c_int32), ("ms", ctypes.c_float), ("events_per_group", ctypes.c_int32)]
 
 
 class MemoryUsage(ctypes.Structure):
@@ -544,16 +544,18 @@ class Context:
         """Tune the launch shape for the band of the last run; returns the chosen entry."""
         t = Tune()
         self._check(self.lib.itsu_autotune(self.h, repeats, ctypes.byref(t)))
-        return dict(band=t.band, threads_per_block=t.threads_per_block, blocks_per_sm=t.blocks_per_sm, prune=t.prune, ms=t.ms)
+        return dict(band=t.band, threads_per_block=t.threads_per_block, blocks_per_sm=t.blocks_per_sm, prune=t.prune, ms=t.ms,
+                    events_per_group=t.events_per_group)
 
-    def set_tune(self, band: int, threads_per_block: int, blocks_per_sm: int, prune: int = 1):
-        t = Tune(band, threads_per_block, blocks_per_sm, prune, 0.0, 0)
+    def set_tune(self, band: int, threads_per_block: int, blocks_per_sm: int, prune: int = 1, events_per_group: int = 0):
+        t = Tune(band, threads_per_block, blocks_per_sm, prune, 0.0, events_per_group)
         self._check(self.lib.itsu_set_tune(self.h, ctypes.byref(t)))
 
     def get_tune(self, band: int) -> dict:
         t = Tune()
         self._check(self.lib.itsu_get_tune(self.h, band, ctypes.byref(t)))
-        return dict(band=t.band, threads_per_block=t.threads_per_block, blocks_per_sm=t.blocks_per_sm, prune=t.prune, ms=t.ms)
+        return dict(band=t.band, threads_per_block=t.threads_per_block, blocks_per_sm=t.blocks_per_sm, prune=t.prune, ms=t.ms,
+                    events_per_group=t.events_per_group)
 
     # ---- learned prefilter ----
 
