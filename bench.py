@@ -9,16 +9,20 @@ pass of every kernel, replayed as one CUDA graph. The batch's inputs and interme
 flush between steps.
 
   value  events/s with the inputs already resident in HBM (device-side batch API)
-  e2e    events/s through the host-facing C ABI call (itsu_batch_run_host): pinned host clusters
-         in, roads out, every copy inside the timed region
-  roofline  the dominant kernel's algorithmic bytes / its CUDA-event duration, against the
-         measured HBM copy bandwidth
+  e2e    events/s through the host-facing C ABI call (itsu_batch_run_host_compact): pinned host
+         clusters (24-byte input records) in, roads out, every copy inside the timed region
+  roofline  the dominant kernel's own compulsory bytes / its CUDA-event duration, against the
+         measured HBM copy bandwidth (every main kernel's figure under roofline.kernels)
   cpu_baseline  the reference CPU Tracker (oracle/_ref, compiled from the reference's sources)
          on a bounded sample of the same events, one process per host core
+  modes  the learned forms (tracklet gate, pair prefilter, both) on the same batch, the road
+         report, and the other configurations: a 256-event uneven batch and a 1024-frame pile-up
+         stream
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-Multi-GPU (torchrun, one rank per GPU): every rank runs its own batch of events (weak
-scaling, no collective on the data path); the step time is the max over ranks.
+Multi-GPU (torchrun, one rank per GPU): one event list of events-per-GPU x N events, split by
+sorted-multiplicity round-robin (weak scaling, no collective on the data path); the step time is
+the max over ranks.
 """
 from __future__ import annotations
 

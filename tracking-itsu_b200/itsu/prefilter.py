@@ -1,9 +1,15 @@
-"""The learned tracklet-pair prefilter: training pipeline, threshold calibration, evaluation, and
-numpy restatements of its arithmetic (the tests' references).
+"""The learned form's two networks: training pipelines, threshold calibration, evaluation, and
+numpy restatements of their arithmetic (the tests' references).
 
-The model (include/itsu.h, itsu_prefilter_model) scores, inside the cell stage, each tracklet
-pair that passes the exact cell cuts; a pair whose logit is below the model's threshold does not
-become a cell. Everything below runs through the C ABI on one GPU:
+The tracklet gate (include/itsu.h, itsu_gate_model; 8 -> 16 -> 16 -> 1, ReLU) scores every
+tracklet before the tracklet scan; a tracklet whose logit is below the gate's threshold is not
+kept, so the cell stage enumerates only pairs of kept tracklets. It is trained on one sample per
+tracklet of plain runs (label 1: a found road uses it) and calibrated on road reproduction (a
+road survives iff its 6 tracklets are kept): ``python -m itsu.prefilter --model gate``.
+
+The pair prefilter (itsu_prefilter_model; 8 -> 64 -> 64 -> 1, GELU) scores, inside the cell stage,
+each tracklet pair that passes the exact cell cuts; a pair whose logit is below the model's
+threshold does not become a cell. Everything below runs through the C ABI on one GPU:
 
 1. ``collect``: plain batched runs over seeded central Pb-Pb-like events (6000 tracks, 5% noise);
    ``itsu_prefilter_export`` gives one sample per cell (its 8 pair features; label 1 when a
