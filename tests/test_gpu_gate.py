@@ -61,15 +61,21 @@ def _plain(ctx, torch_dev, events):
 
 
 def test_gate_export_matches_oracle_tracklets(ctx, torch_dev):
-    """Features bit-exact to the float32 restatement on the oracle's tracklets; labels and road
-    rows from the oracle's roads."""
+    """Features equal to the float32 restatement on the oracle's tracklets (bit for bit where the
+    device uses IEEE operations; the slope, dz and curvature use the hardware's fast division and
+    reciprocal square root, within 1e-5 relative + 1e-6 absolute); labels and road rows from the
+    oracle's roads."""
     ev = gen.pbpb_event(61, n_tracks=1500)
     want = oracle.run_vertex(ev.layers, ev.vertices[0])
     ctx.run_vertex(ev.layers, ev.vertices[0])
     f, l, r = prefilter.export_gate_samples(ctx, torch_dev)
     feats = prefilter.tracklet_features(want)
-    assert f.shape[0] == len(feats) > 0
-    assert np.array_equal(f.cpu().numpy().view(np.uint32), feats.view(np.uint32))
+    got = f.cpu().numpy()
+    assert got.shape[0] == len(feats) > 0
+    exact = [0, 4, 5, 7]
+    assert np.array_equal(got[:, exact].view(np.uint32), feats[:, exact].view(np.uint32))
+    approx = [1, 2, 3, 6]
+    assert np.all(np.abs(got[:, approx] - feats[:, approx]) <= 1e-6 + 1e-5 * np.abs(feats[:, approx]))
     rows = prefilter.road_tracklets(want)
     assert np.array_equal(r.cpu().numpy(), rows)
     labels = np.zeros(len(feats), np.uint8)

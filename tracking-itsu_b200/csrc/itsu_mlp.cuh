@@ -350,19 +350,25 @@ __device__ __forceinline__ float mlp_logits_warp(const MlpSmemT<H> &m, const __n
 // (c = (x, y, z, r), phi the clusters' azimuths about the vertex, as the clustering computed
 // them): |dphi| and dphi (wrapped to [-pi, pi]), the tracklet cut's dz (Tracker.cxx:93-95) and its
 // absolute value, the signed curvature of the circle through the vertex and both clusters, the
-// inner layer, the inner cluster's radius and its slope from the vertex.
+// inner layer, the inner cluster's radius and its slope from the vertex. The gate scores every
+// tracklet, so its features use the hardware's fast division and reciprocal square root
+// (__fdividef, rsqrtf: a few units in the last place); the export and the gate pass run this same
+// code, so training and inference see the same values.
 __device__ __forceinline__ void tracklet_features(int layer, float4 c1, float phi1, float4 c2, float phi2, float vx, float vy,
                                                   float vz, float f[kMlpIn])
 {
   constexpr float kPiF = 3.14159265358979323846f, kTwoPiF = 6.28318530717958647692f;
   float dphi = phi1 - phi2;
   dphi = dphi > kPiF ? dphi - kTwoPiF : (dphi < -kPiF ? dphi + kTwoPiF : dphi);
-  const float tan_lambda = (c1.z - vz) / c1.w;
+  const float tan_lambda = __fdividef(c1.z - vz, c1.w);
   const float dz = tan_lambda * (c2.w - c1.w) + c1.z - c2.z;
+  // curvature of the circle through the vertex and both clusters: 2 (u x v) / (|u| |v| |v - u|)
+  const float ux = c1.x - vx, uy = c1.y - vy, wx = c2.x - vx, wy = c2.y - vy, dx = wx - ux, dy = wy - uy;
+  const float prod = (ux * ux + uy * uy) * (wx * wx + wy * wy) * (dx * dx + dy * dy);
   f[0] = fabsf(dphi);
   f[1] = dz;
   f[2] = fabsf(dz);
-  f[3] = circle_curvature(vx, vy, c1.x, c1.y, c2.x, c2.y);
+  f[3] = prod > 0.0f ? 2.0f * (ux * wy - uy * wx) * rsqrtf(prod) : 0.0f;
   f[4] = (float)layer;
   f[5] = c1.w;
   f[6] = tan_lambda;
