@@ -296,7 +296,8 @@ typedef struct itsu_tune {
   int32_t band;
   int32_t threads_per_block;
   int32_t blocks_per_sm;
-  int32_t prune;  /* tracklet candidate pruning index on (1) or off (0) */
+  int32_t prune;  /* tracklet candidate pruning index off (0), on (1), or on and read from a
+                     shared-memory copy of each block's rows made by one bulk copy (2) */
   float ms;       /* best time of one run of the tuned inputs, 0 if untuned */
   int32_t events_per_group; /* whole runs: the tracklet write and cell count passes run event group by
                                event group, so that a group's tracklets are still in L2 when its

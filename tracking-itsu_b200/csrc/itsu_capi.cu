@@ -546,6 +546,9 @@ itsu_status sync_status(itsu_context *ctx)
   if (ctx->h_status->flags & itsu::kFlagLaunchShape) {
     return fail(ctx, ITSU_ERR_INVALID, "launch shape: the per-item passes need a block size that is a multiple of 32");
   }
+  if (ctx->h_status->flags & itsu::kFlagTimeout) {
+    return fail(ctx, ITSU_ERR_TIMEOUT, "a bounded device wait (a shared-memory bulk copy) gave up");
+  }
   return ITSU_OK;
 }
 
@@ -1832,14 +1835,14 @@ itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best)
   ITSU_CUDA(ctx, cudaEventCreate(&e1));
   Tune winner;
   winner.ms = 1e30f;
-  const int blocks[] = {64, 128, 256, 512}, per_sm[] = {4, 8, 16}, prunes[] = {1, 0}, groups[] = {0, 8, 16, 32};
+  const int blocks[] = {64, 128, 256, 512}, per_sm[] = {4, 8, 16}, prunes[] = {1, 2, 0}, groups[] = {0, 8, 16, 32};
   ctx->tuning = true;
   cudaError_t err = cudaSuccess;
   for (int b : blocks) {
     for (int m : per_sm) {
       for (int p : prunes) {
        for (int g : groups) {
-        if (g > 0 && (p == 0 || g >= ctx->n_events)) continue;  // groups only with pruning, and only below the batch
+        if (g > 0 && (p != 1 || g >= ctx->n_events)) continue;  // groups only with the plain pruning, below the batch
         ctx->override_tune = Tune{b, m, p, 0.0f, true, g};
         const Arena a = arena_of(ctx);
         const Launch l = whole_run_launch(ctx);
@@ -1910,7 +1913,8 @@ itsu_status itsu_set_tune(itsu_context *ctx, const itsu_tune *in)
                 in->blocks_per_sm);
   }
   if (in->events_per_group < 0) return fail(ctx, ITSU_ERR_INVALID, "events per group %d is negative", in->events_per_group);
-  ctx->tunes[in->band] = Tune{in->threads_per_block, in->blocks_per_sm, in->prune ? 1 : 0, in->ms, true, in->events_per_group};
+  if (in->prune < 0 || in->prune > 2) return fail(ctx, ITSU_ERR_INVALID, "prune %d: 0, 1 or 2", in->prune);
+  ctx->tunes[in->band] = Tune{in->threads_per_block, in->blocks_per_sm, in->prune, in->ms, true, in->events_per_group};
   drop_graph(ctx);
   return ITSU_OK;
 }

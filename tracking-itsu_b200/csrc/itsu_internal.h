@@ -34,11 +34,12 @@ enum : int32_t {
   kFlagCountOverflow = 32,
   kFlagCapScratch = 64,  // the cell entries of the count pass exceed their scratch
   kFlagLaunchShape = 128,  // a per-item pass was given a block size that is not whole warps (nothing ran)
+  kFlagTimeout = 256,      // a bounded device wait gave up (the run's results are not used)
 };
 constexpr int kTrackletSlotsPerCluster = 48;  // outer clusters the tracklet count pass keeps per inner cluster
 // Any of these stops every later kernel of the run (they check the mask first).
 constexpr int32_t kCapacityMask = kFlagCapTracklets | kFlagCapCells | kFlagCapNeighbours | kFlagCapRoads |
-                                  kFlagCountOverflow | kFlagCapScratch | kFlagLaunchShape;
+                                  kFlagCountOverflow | kFlagCapScratch | kFlagLaunchShape | kFlagTimeout;
 constexpr int kCellChunk = 64;  // cell entries a warp of the cell count pass reserves at a time
 
 // Totals and requirements of a run, written by the device.
@@ -102,7 +103,7 @@ struct Arena {
   float4 *zs;  // (z, r, phi, sorted index as int bits)
   float2 *seg_rrange;
   int32_t *seg_regular;  // per segment: 0 if not regular, else the pass-mask words its largest bin needs
-  int32_t prune_tracklets;  // use the index (tuning knob; results are identical either way)
+  int32_t prune_tracklets;  // use the index: 0 no, 1 yes, 2 yes, from a shared-memory copy (tuning knob; results are identical)
   // tracklets
   int32_t *trk_count;
   int32_t *trk_slots;  // slot n of inner cluster i at n * slot_stride + i: the outer clusters of its first tracklets

@@ -744,8 +744,11 @@ struct TrackletProbe {
 
 template <int kWords, typename OnPass>
 __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next, int4 rect, int layer, const TrackletProbe &probe,
-                                                bool prune, float zlo, float zhi, const float4 *zs, OnPass &&on_pass)
+                                                bool prune, float zlo, float zhi, const float4 *zs, int zs_off,
+                                                OnPass &&on_pass)
 {
+  // zs[k - zs_off] is the k-th entry of the next layer's z-sorted bin lists (zs_off > 0: a staged
+  // copy in shared memory that starts at entry zs_off)
   static_assert(kWords >= 1 && kWords <= kPruneWords, "mask words");
   int phi_bins = rect.w - rect.y + 1;
   if (phi_bins < 0) {
@@ -765,7 +768,7 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
         int lo = k0, hi = k1;  // first listed cluster with z >= zlo
         while (lo < hi) {
           const int mid = (lo + hi) >> 1;
-          if (zs[mid].x < zlo) {
+          if (zs[mid - zs_off].x < zlo) {
             lo = mid + 1;
           } else {
             hi = mid;
@@ -780,7 +783,7 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
           hit[w] = 0ull;
         }
         for (int k = lo; k < k1; ++k) {
-          const float4 q = zs[k];  // z, r, phi and the sorted index of the k-th cluster by z
+          const float4 q = zs[k - zs_off];  // z, r, phi and the sorted index of the k-th cluster by z
           if (!(q.x <= zhi)) {
             break;
           }
@@ -880,36 +883,154 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
   return s;
 }
 
+// staged: the block's copy in shared memory of the next layer's z-sorted entries from staged_off on
+// (null: read them from global memory)
 template <typename OnPass>
-__device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s, OnPass &&on_pass)
+__device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s, OnPass &&on_pass,
+                                           const float4 *staged = nullptr, int staged_off = 0)
 {
-  const float4 *zs = a.zs + s.next_begin;
+  const float4 *zs = staged ? staged : a.zs + s.next_begin;
+  const int off = staged ? staged_off : 0;
   if (s.words <= 1) {  // unpruned, or bins of at most 64 clusters
-    walk_candidates<1>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, on_pass);
+    walk_candidates<1>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, on_pass);
   } else if (s.words == 2) {
-    walk_candidates<2>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, on_pass);
+    walk_candidates<2>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, on_pass);
   } else {
-    walk_candidates<kPruneWords>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, on_pass);
+    walk_candidates<kPruneWords>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, on_pass);
   }
 }
 
+// ---- bulk copies into shared memory (cp.async.bulk, this GPU's memory, no multicast) ----
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to shared
+// memory, completing on `bar` (the calling thread also arrives on it, expecting those bytes).
+__device__ __forceinline__ void bulk_copy_to_shared(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(bytes), "r"(b)
+               : "memory");
+}
+
+// Waits for phase `parity` of `bar` to complete, at most `limit` tries; false if it did not.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int limit)
+{
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  for (int t = 0; t < limit; ++t) {
+    unsigned done;
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(done)
+                 : "r"(b), "r"(parity)
+                 : "memory");
+    if (done) {
+      return true;
+    }
+  }
+  return false;
+}
+
+constexpr int kStageEntries = 2048;  // the staged walk's shared copy: up to 2048 entries (32 KB) per block
+constexpr int kStageRows = 4;        // and up to 4 phi rows of the next layer
+constexpr int kWaitTries = 1 << 20;  // bounded waits: each try_wait suspends for a bounded time
+
+// The staged walk's set-up, block-wide: when every walking thread of the block walks pruned rows
+// of the same next layer, without a wrap around phi, and their rows (at most kStageRows) hold at
+// most kStageEntries entries, one bulk copy brings those entries into shared memory. Returns the
+// first staged entry's index in the layer (its *staged_count entries), or -1 with nothing staged.
+// A copy that does not complete within the bounded wait sets the timeout flag.
+__device__ int stage_rows(const Arena &a, const InnerCluster &s, float4 *stage, uint64_t *bar, int *staged_count)
+{
+  __shared__ int s_lo, s_hi, s_seg, s_ok, s_k0, s_m;
+  if (threadIdx.x == 0) {
+    s_lo = kPhiBins;
+    s_hi = -1;
+    s_seg = -1;
+    s_ok = 1;
+  }
+  __syncthreads();
+  if (s.walk) {
+    if (!s.prune || s.rect.y > s.rect.w) {
+      atomicAnd(&s_ok, 0);  // unpruned, or a window that wraps around phi
+    }
+    atomicMin(&s_lo, s.rect.y);
+    atomicMax(&s_hi, s.rect.w);
+    atomicMax(&s_seg, s.seg + 1);
+  }
+  __syncthreads();
+  if (s.walk && s.seg + 1 != s_seg) {
+    atomicAnd(&s_ok, 0);  // more than one next layer
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_m = 0;
+    s_k0 = -1;
+    if (s_ok && s_hi >= s_lo && s_hi - s_lo < kStageRows) {
+      const int e = s_seg / ITSU_LAYERS, next_layer = s_seg % ITSU_LAYERS;
+      const int32_t *table = a.index_tables + ((int64_t)e * ITSU_TRACKLET_LAYERS + next_layer - 1) * kTableSize;
+      const int k0 = table[s_lo * kPhiBins], k1 = table[min((s_hi + 1) * kPhiBins, kTableBins)];
+      if (k1 > k0 && k1 - k0 <= kStageEntries) {
+        s_k0 = k0;
+        s_m = k1 - k0;
+        mbar_init(bar, 1);
+        bulk_copy_to_shared(stage, a.zs + a.layer_off[s_seg] + k0, (unsigned)(s_m * sizeof(float4)), bar);
+      }
+    }
+  }
+  __syncthreads();
+  if (s_k0 < 0) {
+    return -1;
+  }
+  if (!mbar_wait(bar, 0, kWaitTries)) {
+    atomicOr(&a.status->flags, kFlagTimeout);
+    mbar_wait(bar, 0, kWaitTries);  // the copy may still land: wait once more before leaving
+    return -1;
+  }
+  *staged_count = s_m;
+  return s_k0;
+}
+
 // Count pass, one thread per inner cluster: the number of tracklets, and the outer clusters of
-// the first kTrackletSlots of them in emission order.
+// the first kTrackletSlots of them in emission order. kStaged: the block's walks read the next
+// layer's z-sorted entries from a shared-memory copy made by one bulk copy (stage_rows), where
+// they allow it.
+template <bool kStaged>
 __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
 {
+  extern __shared__ float4 stage[];  // kStaged: kStageEntries entries
+  __shared__ uint64_t bar;
   const int64_t i = global_thread();
   const bool valid = i < a.n_clusters;
   int count = 0;
+  InnerCluster s;
+  s.walk = false;
   if (valid) {
-    const InnerCluster s = inner_cluster(a, i);
-    if (s.walk) {
-      walk_inner(a, s, [&](int j) {
-        if (count < kTrackletSlots) {
-          a.trk_slots[count * a.slot_stride + i] = j;
-        }
-        ++count;
-      });
-    }
+    s = inner_cluster(a, i);
+  }
+  const float4 *staged = nullptr;
+  int staged_off = 0;
+  if constexpr (kStaged) {
+    int m = 0;
+    staged_off = stage_rows(a, s, stage, &bar, &m);
+    staged = staged_off >= 0 ? stage : nullptr;
+  }
+  if (s.walk && !(a.status->flags & kFlagTimeout)) {
+    walk_inner(
+        a, s,
+        [&](int j) {
+          if (count < kTrackletSlots) {
+            a.trk_slots[count * a.slot_stride + i] = j;
+          }
+          ++count;
+        },
+        staged, staged_off);
   }
   // the warp's 32 clusters lie in one scan tile: their tracklets go to its sum (the tracklet
   // scan has no reduce pass)
@@ -1823,8 +1944,10 @@ void step_tracklets_count(const Arena &a, const Launch &l)
     return;
   }
   const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
-  if (blocks > 0) {
-    k_tracklets_count<<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
+  if (blocks > 0 && a.prune_tracklets == 2) {  // the staged walk (tuning knob; results are identical)
+    k_tracklets_count<true><<<(unsigned)blocks, l.block, kStageEntries * sizeof(float4), l.stream>>>(a);
+  } else if (blocks > 0) {
+    k_tracklets_count<false><<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
   }
 }
 
