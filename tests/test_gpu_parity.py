@@ -246,7 +246,8 @@ def test_launch_shapes_and_autotuner_keep_results(ctx):
     want = [ctx.results(e) for e in range(len(events))]
     band = ctx.lib.itsu_multiplicity_band(len(clusters), len(events))
     try:
-        for block, per_sm, prune, group in [(128, 4, 0, 0), (512, 16, 1, 0), (64, 2, 1, 0), (256, 8, 1, 2), (64, 4, 1, 4)]:
+        for block, per_sm, prune, group in [(128, 4, 0, 0), (512, 16, 1, 0), (64, 2, 1, 0), (256, 8, 1, 2), (64, 4, 1, 4),
+                                            (256, 8, 2, 0), (512, 4, 2, 0)]:
             ctx.set_tune(band, block, per_sm, prune, group)
             assert ctx.get_tune(band)["threads_per_block"] == block and ctx.get_tune(band)["events_per_group"] == group
             roads, off = ctx.batch_run_host(clusters, offsets, vertices)
@@ -347,3 +348,19 @@ def test_event_groups_keep_results():
         plain.close()
         grouped.close()
         streamed.close()
+
+
+def test_staged_walk_matches_oracle(ctx):
+    """The staged tracklet walk (prune 2: each block's rows of the next layer copied into shared
+    memory by one bulk copy) on central events, a dense jet (bins above 128 clusters) and an
+    uneven batch: every output equals the oracle's."""
+    events = [gen.pbpb_event(3), gen.jet_event(3, 150)] + gen.batch_events(23, n_events=10)
+    clusters, offsets, vertices = gen.pack_batch(events)
+    band = ctx.lib.itsu_multiplicity_band(len(clusters), len(events))
+    try:
+        ctx.set_tune(band, 256, 8, 2)
+        ctx.batch_run_host(clusters, offsets, vertices)
+        for e, ev in enumerate(events):
+            _assert_same(ctx.results(e), oracle.run_vertex(ev.layers, ev.vertices[0]), "staged walk, event %d" % e)
+    finally:
+        ctx.set_tune(band, 256, 8, 1)
