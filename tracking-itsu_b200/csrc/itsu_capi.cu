@@ -97,7 +97,7 @@ struct itsu_context {
   // cell class
   itsu_cell *cells = nullptr;
   itsu::CellEntry *cell_entries = nullptr;
-  float4 *cell_feat = nullptr;  // learned form: two per cell entry, its pair prefilter features
+  float *cell_dca = nullptr;
   int64_t cap_cell_entries = 0;
   int32_t *cell_seg_id = nullptr, *nb_count = nullptr, *nb_off = nullptr, *nb_fill = nullptr, *road_count = nullptr,
           *road_off = nullptr;
@@ -337,7 +337,7 @@ Arena arena_of(const itsu_context *ctx)
   a.cells = ctx->cells;
   a.cell_seg_id = ctx->cell_seg_id;
   a.cell_entries = ctx->cell_entries;
-  a.cell_feat = ctx->cell_feat;
+  a.cell_dca = ctx->cell_dca;
   a.cap_cell_entries = ctx->cap_cell_entries;
   a.nb_count = ctx->nb_count;
   a.nb_off = ctx->nb_off;
@@ -460,7 +460,7 @@ itsu_status ensure_cell_entries(itsu_context *ctx, int64_t need)
     if (st != ITSU_OK) return st;
     const int64_t cap = grow_to(need);
     ITSU_CUDA(ctx, alloc(ctx, ctx->cell_entries, cap));
-    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_feat, 2 * cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_dca, cap));
     ctx->cap_cell_entries = cap;
     ctx->generation++;
   }
@@ -931,7 +931,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
   release(ctx->tracklets); release(ctx->trk_slope); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->cell_off); release(ctx->cell_lookup); release(ctx->cell_crowded);
-  release(ctx->cells); release(ctx->cell_entries); release(ctx->cell_feat); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
+  release(ctx->cells); release(ctx->cell_entries); release(ctx->cell_dca); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
   release(ctx->d_master); release(ctx->d_mlp);

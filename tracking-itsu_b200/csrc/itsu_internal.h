@@ -63,8 +63,8 @@ static_assert(offsetof(DevStatus, crowded) == offsetof(DevStatus, cell_entries) 
 // (local to layers L, L+1, L+2), its two tracklets (local to tracklet layers L and L+1), and what
 // its geometry gave. The write pass scatters each entry whose bit survived to cell_off[t1] + (the
 // rank of its bit among the tracklet's set bits) with no other gather; t1 < 0 marks an unused
-// slot. The learned prefilter scores entries in place (their features go to a separate array in
-// that form only).
+// slot. The learned prefilter scores entries in place (the DCA, one of its features, goes to a
+// separate array in that form only).
 struct __align__(16) CellEntry {
   int32_t t1;
   int32_t bit;
@@ -124,7 +124,7 @@ struct Arena {
   itsu_cell *cells;
   int32_t *cell_seg_id;
   CellEntry *cell_entries;  // scratch of the cell count pass
-  float4 *cell_feat;  // two per entry: its 8 pair prefilter features (written in the learned form only)
+  float *cell_dca;  // per entry, its DCA (written in the learned form only: a prefilter feature)
   int64_t cap_cell_entries;
   // neighbours, levels, roads
   int32_t *nb_count;

@@ -1389,9 +1389,6 @@ __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const Ce
 // Runs over the first tracklets of events [e0, e1), or of all events when e1 is 0. Warps hold
 // aligned groups of 32 tracklets (their cells go to one scan tile); a group that straddles the
 // range's ends has its lanes outside the range idle.
-// kPairFeatures: the learned form with the pair prefilter also writes each found pair's features
-// (a separate instantiation, so that the plain pass keeps its register budget).
-template <bool kPairFeatures>
 __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a, int32_t e0, int32_t e1)
 {
   __shared__ unsigned long long masks[kMaxThreads / 32][32];
@@ -1480,14 +1477,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a, int32_t e0
         dst[0] = make_int4((int)t1, b, e * ITSU_CELL_LAYERS + layer, t1_clusters.x);
         dst[1] = make_int4(t1_clusters.y, c3, (int)(t1 - ts[layer]), j0 + b - ts[layer + 1]);
         dst[2] = make_int4(__float_as_int(normal.x), __float_as_int(normal.y), __float_as_int(normal.z), __float_as_int(curvature));
-        if constexpr (kPairFeatures) {
-          // learned form with the pair prefilter: the pair's features beside its entry, from values
-          // this pass holds or just read (the scoring kernel then needs no gathers)
-          const float2 s1 = a.trk_slope[t1], s2 = a.trk_slope[j0 + b];
-          float f[kMlpIn];
-          pair_features(layer, s1.x, s1.y, s2.x, s2.y, c1, c2, a.xyzr[c3_base + c3], vx, vy, a.vtx[3 * e + 2], dca, f);
-          a.cell_feat[2 * slot] = make_float4(f[0], f[1], f[2], f[3]);
-          a.cell_feat[2 * slot + 1] = make_float4(f[4], f[5], f[6], f[7]);
+        if (a.mlp) {
+          a.cell_dca[slot] = dca;
         }
       }
     }
@@ -1528,8 +1519,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a, int32_t e0
   }
 }
 
-// Learned prefilter: scores the count pass's cell entries (their features, which the count pass
-// wrote beside them), 32 per warp on the tensor cores, and
+// Learned prefilter: scores the count pass's cell entries, 32 per warp on the tensor cores, and
 // drops those whose logit is below the model's threshold from their tracklet's mask and count
 // before the scan. The score and the exact cuts are combined with AND, so scoring only the pairs
 // that passed the cuts (whose geometry also gave the DCA feature) keeps the same cells as scoring
@@ -1558,8 +1548,16 @@ __global__ void __launch_bounds__(kPrefilterThreads) k_cells_prefilter(Arena a)
     }
     float f[kMlpIn];
     if (h.x >= 0) {
-      const float4 u = a.cell_feat[2 * i], v = a.cell_feat[2 * i + 1];  // written by the count pass
-      f[0] = u.x, f[1] = u.y, f[2] = u.z, f[3] = u.w, f[4] = v.x, f[5] = v.y, f[6] = v.z, f[7] = v.w;
+      const int4 g = reinterpret_cast<const int4 *>(a.cell_entries + i)[1];  // c2, c3, t1 local, t2 local
+      const int e = h.z / ITSU_CELL_LAYERS, layer = h.z % ITSU_CELL_LAYERS;
+      const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
+      const itsu_tracklet t1 = a.tracklets[h.x];
+      const itsu_tracklet t2 = a.tracklets[a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer + 1] + g.w];
+      const float4 c1 = a.xyzr[lo[layer] + h.w];
+      const float4 c2 = a.xyzr[lo[layer + 1] + g.x];
+      const float4 c3 = a.xyzr[lo[layer + 2] + g.y];
+      pair_features(layer, t1.tan_lambda, t1.phi, t2.tan_lambda, t2.phi, c1, c2, c3, a.vtx[3 * e], a.vtx[3 * e + 1],
+                    a.vtx[3 * e + 2], a.cell_dca[i], f);
     } else {
       for (int k = 0; k < kMlpIn; ++k) {
         f[k] = mlp.mean[k];
@@ -1984,19 +1982,10 @@ void step_tracklet_segments(const Arena &a, const Launch &l)
   k_tracklet_segments<<<(a.n_events * ITSU_TRACKLET_LAYERS + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
 }
 
-void launch_count_range(const Arena &a, const Launch &l, int32_t e0, int32_t e1)
-{
-  if (a.mlp) {
-    k_cells_count<true><<<fixed_grid(l), l.block, 0, l.stream>>>(a, e0, e1);
-  } else {
-    k_cells_count<false><<<fixed_grid(l), l.block, 0, l.stream>>>(a, e0, e1);
-  }
-}
-
 void step_cells_count(const Arena &a, const Launch &l)
 {
   if (l.n_groups == 0 && whole_warps(a, l)) {
-    launch_count_range(a, l, 0, 0);
+    k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a, 0, 0);
   }
 }
 
@@ -2012,7 +2001,7 @@ void step_write_count_groups(const Arena &a, const Launch &l)
   for (int g = 0; g < l.n_groups; ++g) {
     launch_write_range(a, l, l.groups[g], l.groups[g + 1]);
     const int32_t e0 = g * l.group_events, e1 = std::min(a.n_events, (g + 1) * l.group_events);
-    launch_count_range(a, l, e0, e1);
+    k_cells_count<<<fixed_grid(l), l.block, 0, l.stream>>>(a, e0, e1);
   }
 }
 
