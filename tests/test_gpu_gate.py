@@ -74,8 +74,13 @@ def test_gate_export_matches_oracle_tracklets(ctx, torch_dev):
     assert got.shape[0] == len(feats) > 0
     exact = [0, 4, 5, 7]
     assert np.array_equal(got[:, exact].view(np.uint32), feats[:, exact].view(np.uint32))
-    approx = [1, 2, 3, 6]
-    assert np.all(np.abs(got[:, approx] - feats[:, approx]) <= 1e-6 + 1e-5 * np.abs(feats[:, approx]))
+    # the slope and the curvature: a few units in the last place
+    for col in (3, 6):
+        assert np.all(np.abs(got[:, col] - feats[:, col]) <= 1e-7 + 1e-5 * np.abs(feats[:, col])), col
+    # dz = slope * (r2 - r1) + z1 - z2: the slope's error times the radius step, against terms of
+    # tens of cm (the cut it is compared with is 0.1-0.3 cm)
+    for col in (1, 2):
+        assert np.all(np.abs(got[:, col] - feats[:, col]) <= 2e-5), col
     rows = prefilter.road_tracklets(want)
     assert np.array_equal(r.cpu().numpy(), rows)
     labels = np.zeros(len(feats), np.uint8)
@@ -118,8 +123,9 @@ def test_gate_threshold_minus_infinity_gives_the_plain_run(ctx, torch_dev):
 
 
 def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev):
-    """Threshold at the median logit, on central events and a dense jet (inner clusters with more
-    than 48 tracklets): the gated run's tracklets are the plain tracklets scored at or above it
+    """Threshold at the 12% quantile of an untrained gate's logits, on central events and a dense
+    jet (inner clusters with more than 48 tracklets): the gated run's tracklets are the plain
+    tracklets scored at or above it
     (all of a crowded cluster's), in order; its roads are exactly the plain roads whose 6
     tracklets all survive, with the same labels."""
     events = [gen.pbpb_event(s, n_tracks=2500) for s in (66, 67)] + [gen.jet_event(5)]
@@ -129,7 +135,7 @@ def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev):
     m = _gate(f.cpu().numpy(), seed=11)
     ctx.gate_set_model(m)
     logits = _score(ctx, f, torch_dev)
-    thr = float(np.median(logits))
+    thr = float(np.quantile(logits, 0.12))  # keeps about 88%: some roads keep all 6 tracklets
     m.logit_threshold = thr
     ctx.gate_set_model(m)
     keep = ~(logits < thr)
@@ -145,7 +151,7 @@ def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev):
             crowded += int(big.sum())
             row += len(t)
     assert row == len(keep) and crowded > 0
-    assert 0.3 < keep.mean() < 0.8
+    assert 0.8 < keep.mean() < 0.95
     prefilter.set_learned(ctx, False, True)
     try:
         ctx.batch_run(b.batch)

@@ -2051,7 +2051,7 @@ const KernelStep kSteps[] = {
     {"tracklets_crowded", step_tracklets_crowded, 0},        // 7
     {"tracklets_write", step_tracklets_write, kUngroupedStep},  // 8
     {"cells_count", step_cells_count, kUngroupedStep},       // 9  (c)
-    {"tracklets_write+cells_count by event group", step_write_count_groups, kGroupedStep},  // 10
+    {"write_count_by_event_group", step_write_count_groups, kGroupedStep},  // 10 (tracklet write + cell count per group)
     {"cells_prefilter", step_cells_prefilter, kPairPrefilterStep},  // 11 (learned form with the pair prefilter)
     {"scan_partials_cells", step_scan_partials<1>, 0},       // 12
     {"scan_apply_cells", step_scan_apply<1>, 0},             // 13
