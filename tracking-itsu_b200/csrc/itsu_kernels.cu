@@ -1088,79 +1088,97 @@ __device__ __forceinline__ int owner_of(int excl, int t)
 
 // Learned form: the tracklet gate. After the count pass and before the tracklet scan, a warp per
 // 32 consecutive inner clusters scores their tracklets (the outer clusters the count pass kept in
-// their slots), 32 at a time on the tensor cores (8 -> 16 -> 16 -> 1, ReLU, BF16 / FP32), keeps
-// those whose logit is not below the gate's threshold (a NaN logit keeps its tracklet), moves the
-// kept slots to the front in their order and lowers the cluster's count and its scan tile's sum by
-// the dropped ones. The write pass then writes the kept tracklets in emission order, as in the plain
-// form. Inner clusters with more than kTrackletSlots tracklets keep all of them, unscored (the
-// crowded pass writes them).
+// their slots), 32 at a time on the tensor cores (8 -> 16 -> 16 -> 1, ReLU, BF16 / FP32, the
+// network in registers), keeps those whose logit is not below the gate's threshold (a NaN logit
+// keeps its tracklet), moves the kept slots to the front in their order and lowers the cluster's
+// count and its scan tile's sum by the dropped ones. The write pass then writes the kept tracklets
+// in emission order, as in the plain form. Inner clusters with more than kTrackletSlots tracklets
+// keep all of them, unscored (the crowded pass writes them).
+//
+// Per warp and group of 32 clusters, the flattened tracklets' owners and ranks are listed once in
+// shared memory (each cluster's lane writes its own entries), and each cluster's gate state (what
+// its features need of it) sits beside them, so that a tile reads its rows' owners, states and
+// slots without searches or shuffles; the lanes holding a row's logit keep or drop it.
 constexpr int kGateThreads = 256;
+constexpr int kGateWarps = kGateThreads / 32;
+
+struct __align__(16) GateLane {
+  GateInner g;
+  int32_t next;  // first cluster of the next layer
+  int32_t pad_;
+};
 
 __global__ void __launch_bounds__(kGateThreads) k_tracklets_gate(Arena a)
 {
   __shared__ GateSmem net;
-  __shared__ __align__(16) __nv_bfloat16 rows[kGateThreads / 32][32][kRowPitch];
-  __shared__ unsigned long long keep[kGateThreads / 32][32];
+  __shared__ __align__(16) __nv_bfloat16 rows[kGateWarps][32][kMlpIn];
+  __shared__ unsigned long long keep[kGateWarps][32];
+  __shared__ uint16_t owner_rank[kGateWarps][32 * kTrackletSlots];  // owner lane * 64 + rank
+  __shared__ GateLane lanes[kGateWarps][32];
   load_mlp(net, *a.gate);
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const GateRegs R = gate_regs(net);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
   const int64_t n = a.n_clusters;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
     const int64_t i = base + lane;
-    int count = 0, layer = 0;
-    int64_t next_begin = 0;
-    float4 c1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float phi1 = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    int count = 0;
     if (i < n) {
       count = a.trk_count[i];
       if (count > 0 && count <= kTrackletSlots) {
         const int seg = a.clu_seg[i], e = seg / ITSU_LAYERS;
-        layer = seg % ITSU_LAYERS;
-        c1 = a.xyzr[i];
-        phi1 = a.phi[i];
-        next_begin = a.layer_off[seg + 1];
-        vx = a.vtx[3 * e];
-        vy = a.vtx[3 * e + 1];
-        vz = a.vtx[3 * e + 2];
+        GateLane &s = lanes[warp][lane];
+        s.g = gate_inner(seg % ITSU_LAYERS, a.xyzr[i], a.phi[i], a.vtx[3 * e], a.vtx[3 * e + 1], a.vtx[3 * e + 2]);
+        s.next = a.layer_off[seg + 1];
       }
     }
     const bool scored = count <= kTrackletSlots;
+    const int mine = scored ? count : 0;
     keep[warp][lane] = 0ull;
     int total = 0;
-    const int excl = warp_exclusive_sum(scored ? count : 0, total);
+    const int excl = warp_exclusive_sum(mine, total);
+    for (int r = 0; r < mine; ++r) {
+      owner_rank[warp][excl + r] = (uint16_t)(lane * 64 + r);
+    }
     __syncwarp();
     for (int p0 = 0; p0 < total; p0 += 32) {
       const int p = p0 + lane;
-      const int owner = owner_of(excl, p);
-      const int rank = p - __shfl_sync(0xffffffffu, excl, owner);
-      const float4 oc = shfl4(c1, owner);
-      const float ophi = __shfl_sync(0xffffffffu, phi1, owner);
-      const int olayer = __shfl_sync(0xffffffffu, layer, owner);
-      const int64_t onext = __shfl_sync(0xffffffffu, next_begin, owner);
-      const float ovx = __shfl_sync(0xffffffffu, vx, owner), ovy = __shfl_sync(0xffffffffu, vy, owner);
-      const float ovz = __shfl_sync(0xffffffffu, vz, owner);
       float f[kMlpIn];
       if (p < total) {
-        const int64_t j = onext + a.trk_slots[(int64_t)rank * a.slot_stride + base + owner];
-        tracklet_features(olayer, oc, ophi, a.xyzr[j], a.phi[j], ovx, ovy, ovz, f);
+        const int orank = owner_rank[warp][p], owner = orank >> 6, rank = orank & 63;
+        const GateLane &o = lanes[warp][owner];
+        const int64_t j = o.next + a.trk_slots[(int64_t)rank * a.slot_stride + base + owner];
+        gate_features(o.g, a.xyzr[j], a.phi[j], f);
       } else {
 #pragma unroll
         for (int k = 0; k < kMlpIn; ++k) {
           f[k] = net.mean[k];
         }
       }
-      feature_row(net.mean, net.inv_std, f, rows[warp][lane]);
+      *reinterpret_cast<uint4 *>(&rows[warp][lane][0]) = gate_row(net.mean, net.inv_std, f);
       __syncwarp();
-      const float logit = mlp_logits_warp<false, kGateHidden, true>(net, rows[warp], nullptr);
-      if (p < total && !(logit < net.threshold)) {
-        atomicOr(&keep[warp][owner], 1ull << rank);
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        float lo, hi;
+        gate_forward_m16(R, rows[warp], mt, lo, hi);
+        if (t == 0) {  // this lane holds the logits of rows 16 mt + g and 16 mt + g + 8
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int q = p0 + mt * 16 + g + 8 * h;
+            const float logit = h ? hi : lo;
+            if (q < total && !(logit < net.threshold)) {
+              const int orank = owner_rank[warp][q];
+              atomicOr(&keep[warp][orank >> 6], 1ull << (orank & 63));
+            }
+          }
+        }
       }
-      __syncwarp();
+      __syncwarp();  // the rows are refilled for the next tile
     }
     // kept slots to the front, in order (coalesced across the warp's clusters, slot by slot)
     const unsigned long long m = keep[warp][lane];
-    const int scan_to = __reduce_max_sync(0xffffffffu, (unsigned)(scored ? count : 0));
+    const int scan_to = __reduce_max_sync(0xffffffffu, (unsigned)mine);
     int kept = 0;
     for (int q = 0; q < scan_to; ++q) {
       if (q < count && ((m >> q) & 1ull)) {

@@ -353,26 +353,131 @@ __device__ __forceinline__ float mlp_logits_warp(const MlpSmemT<H> &m, const __n
 // inner layer, the inner cluster's radius and its slope from the vertex. The gate scores every
 // tracklet, so its features use the hardware's fast division and reciprocal square root
 // (__fdividef, rsqrtf: a few units in the last place); the export and the gate pass run this same
-// code, so training and inference see the same values.
-__device__ __forceinline__ void tracklet_features(int layer, float4 c1, float phi1, float4 c2, float phi2, float vx, float vy,
-                                                  float vz, float f[kMlpIn])
+// code, so training and inference see the same values. What depends on the inner cluster alone
+// is computed once per inner cluster (GateInner).
+struct GateInner {
+  float ux, uy, uu;   // the inner cluster relative to the vertex, and its squared length
+  float z1, r1, phi1;
+  float tan_lambda;   // slope from the vertex
+  float vx, vy;
+  int layer;
+};
+
+__device__ __forceinline__ GateInner gate_inner(int layer, float4 c1, float phi1, float vx, float vy, float vz)
+{
+  GateInner g;
+  g.ux = c1.x - vx;
+  g.uy = c1.y - vy;
+  g.uu = g.ux * g.ux + g.uy * g.uy;
+  g.z1 = c1.z;
+  g.r1 = c1.w;
+  g.phi1 = phi1;
+  g.tan_lambda = __fdividef(c1.z - vz, c1.w);
+  g.vx = vx;
+  g.vy = vy;
+  g.layer = layer;
+  return g;
+}
+
+__device__ __forceinline__ void gate_features(const GateInner &g, float4 c2, float phi2, float f[kMlpIn])
 {
   constexpr float kPiF = 3.14159265358979323846f, kTwoPiF = 6.28318530717958647692f;
-  float dphi = phi1 - phi2;
+  float dphi = g.phi1 - phi2;
   dphi = dphi > kPiF ? dphi - kTwoPiF : (dphi < -kPiF ? dphi + kTwoPiF : dphi);
-  const float tan_lambda = __fdividef(c1.z - vz, c1.w);
-  const float dz = tan_lambda * (c2.w - c1.w) + c1.z - c2.z;
-  // curvature of the circle through the vertex and both clusters: 2 (u x v) / (|u| |v| |v - u|)
-  const float ux = c1.x - vx, uy = c1.y - vy, wx = c2.x - vx, wy = c2.y - vy, dx = wx - ux, dy = wy - uy;
-  const float prod = (ux * ux + uy * uy) * (wx * wx + wy * wy) * (dx * dx + dy * dy);
+  const float dz = g.tan_lambda * (c2.w - g.r1) + g.z1 - c2.z;
+  // curvature of the circle through the vertex and both clusters: 2 (u x w) / (|u| |w| |w - u|)
+  const float wx = c2.x - g.vx, wy = c2.y - g.vy, dx = wx - g.ux, dy = wy - g.uy;
+  const float prod = g.uu * (wx * wx + wy * wy) * (dx * dx + dy * dy);
   f[0] = fabsf(dphi);
   f[1] = dz;
   f[2] = fabsf(dz);
-  f[3] = prod > 0.0f ? 2.0f * (ux * wy - uy * wx) * rsqrtf(prod) : 0.0f;
-  f[4] = (float)layer;
-  f[5] = c1.w;
-  f[6] = tan_lambda;
+  f[3] = prod > 0.0f ? 2.0f * (g.ux * wy - g.uy * wx) * rsqrtf(prod) : 0.0f;
+  f[4] = (float)g.layer;
+  f[5] = g.r1;
+  f[6] = g.tan_lambda;
   f[7] = dphi;
+}
+
+__device__ __forceinline__ void tracklet_features(int layer, float4 c1, float phi1, float4 c2, float phi2, float vx, float vy,
+                                                  float vz, float f[kMlpIn])
+{
+  gate_features(gate_inner(layer, c1, phi1, vx, vy, vz), c2, phi2, f);
+}
+
+// The tracklet gate's network in registers: at 16 hidden units the whole network is 17 values
+// per lane, each lane holding its MMA fragments and the biases of its output columns, so the gate
+// pass reads no weights from memory per tile. The operands are those of mlp_forward_m16 (the k 8..15
+// halves of layer 1's operands are zero there), so the logits are the same, bit for bit.
+struct GateRegs {
+  uint32_t w1[2];     // layer 1 B fragment (k 2t, 2t+1; column g) per n-tile
+  uint32_t w2[2][2];  // layer 2 B fragments per n-tile
+  uint32_t w3[2];     // layer 3 B fragments (column 0 real)
+  float b1[2][2], b2[2][2];  // biases of the lane's output columns 2t, 2t+1 per n-tile
+  float b3;
+};
+
+__device__ __forceinline__ GateRegs gate_regs(const MlpSmemT<kGateHidden> &m)
+{
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  GateRegs r;
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt) {
+    r.w1[nt] = ld32(&m.w1[nt * 8 + g][2 * t]);
+    r.w2[nt][0] = ld32(&m.w2[nt * 8 + g][2 * t]);
+    r.w2[nt][1] = ld32(&m.w2[nt * 8 + g][2 * t + 8]);
+    r.b1[nt][0] = m.b1[nt * 8 + 2 * t];
+    r.b1[nt][1] = m.b1[nt * 8 + 2 * t + 1];
+    r.b2[nt][0] = m.b2[nt * 8 + 2 * t];
+    r.b2[nt][1] = m.b2[nt * 8 + 2 * t + 1];
+  }
+  r.w3[0] = ld32(&m.w3[g][2 * t]);
+  r.w3[1] = ld32(&m.w3[g][2 * t + 8]);
+  r.b3 = m.b3;
+  return r;
+}
+
+// Logits of rows 16 mt + g (lo) and 16 mt + g + 8 (hi) of a 32-row tile whose rows hold the 8
+// standardised BF16 features (valid in lanes with t == 0). All lanes of the warp take part.
+__device__ __forceinline__ void gate_forward_m16(const GateRegs &R, const __nv_bfloat16 (*rows)[kMlpIn], int mt, float &lo,
+                                                 float &hi)
+{
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const uint32_t a[4] = {ld32(&rows[mt * 16 + g][2 * t]), ld32(&rows[mt * 16 + g + 8][2 * t]), 0u, 0u};
+  uint32_t hk[4];
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt) {
+    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    mma_bf16(c, a, R.w1[nt], 0u);
+    hk[nt * 2 + 0] = pack_bf16(act<true>(c[0] + R.b1[nt][0]), act<true>(c[1] + R.b1[nt][1]));
+    hk[nt * 2 + 1] = pack_bf16(act<true>(c[2] + R.b1[nt][0]), act<true>(c[3] + R.b1[nt][1]));
+  }
+  float h2[2][4];
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt) {
+    h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.0f;
+    mma_bf16(h2[nt], hk, R.w2[nt][0], R.w2[nt][1]);
+  }
+  uint32_t ak[4];
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt) {
+    ak[nt * 2 + 0] = pack_bf16(act<true>(h2[nt][0] + R.b2[nt][0]), act<true>(h2[nt][1] + R.b2[nt][1]));
+    ak[nt * 2 + 1] = pack_bf16(act<true>(h2[nt][2] + R.b2[nt][0]), act<true>(h2[nt][3] + R.b2[nt][1]));
+  }
+  float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  mma_bf16(o, ak, R.w3[0], R.w3[1]);
+  lo = o[0] + R.b3;
+  hi = o[2] + R.b3;
+}
+
+// The 8 standardised BF16 features of one row (as feature_row rounds them), packed in 16 bytes.
+__device__ __forceinline__ uint4 gate_row(const float *mean, const float *inv_std, const float f[kMlpIn])
+{
+  uint32_t w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    w[k] = pack_bf16((f[2 * k] - mean[2 * k]) * inv_std[2 * k], (f[2 * k + 1] - mean[2 * k + 1]) * inv_std[2 * k + 1]);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 }  // namespace itsu
