@@ -416,9 +416,11 @@ itsu_status itsu_prefilter_gradient(itsu_context *ctx, const float *features, co
  * path spends most of its time. Its features, per tracklet: |dphi| and dphi of its clusters'
  * azimuths about the vertex, the tracklet cut's dz (Tracker.cxx:93-95) and |dz|, the signed
  * curvature of the circle through the vertex and its two clusters, the inner layer, the inner
- * cluster's radius and its slope from the vertex. Training labels come from plain runs (1 = the
- * tracklet is part of a found road). A learned run's tracklets, and so its cells and roads, are
- * subsets of the plain run's. Inner clusters with more than 48 tracklets keep all of theirs.
+ * cluster's radius and its slope from the vertex. The gate is a cascade: a learned per-layer
+ * window on |dphi| first (dphi_window below), the network on the tracklets inside it. Training
+ * labels come from plain runs (1 = the tracklet is part of a found road). A learned run's
+ * tracklets, and so its cells and roads, are subsets of the plain run's. Inner clusters with more
+ * than 48 tracklets inside the window keep all of them, unscored by the network.
  * The gate and the pair prefilter are enabled separately; the learned form is either or both. */
 #define ITSU_GATE_HIDDEN 16
 #define ITSU_GATE_PARAMS (ITSU_GATE_HIDDEN * ITSU_MLP_INPUTS + ITSU_GATE_HIDDEN + ITSU_GATE_HIDDEN * ITSU_GATE_HIDDEN + \
@@ -434,6 +436,13 @@ typedef struct itsu_gate_model {
   float mean[ITSU_MLP_INPUTS];
   float inv_std[ITSU_MLP_INPUTS];
   float logit_threshold;          /* a tracklet is kept unless its logit is below this */
+  /* The cascade's first stage, learned from the training tracklets on found roads: per inner
+   * layer, the largest |dphi| (the gate's feature 0) and |dz| (feature 2) a kept tracklet may
+   * have. The tracklet count pass applies both to every tracklet it finds and walks only the phi
+   * rows and z ranges they can reach; the network scores the tracklets inside them. pi and
+   * infinity: no first stage. */
+  float dphi_window[ITSU_TRACKLET_LAYERS];
+  float dz_window[ITSU_TRACKLET_LAYERS];
 } itsu_gate_model;
 
 /* Device buffers that itsu_gate_export fills; every array may be NULL (then not written). */

@@ -122,36 +122,71 @@ def test_gate_threshold_minus_infinity_gives_the_plain_run(ctx, torch_dev):
         prefilter.set_learned(ctx, False, False)
 
 
-def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev):
+def _windows_at(features, q):
+    """Per inner layer, the q-quantiles of the plain tracklets' |dphi| and |dz| (features 0 and 2),
+    as float32."""
+    wphi = np.full(6, np.pi, np.float32)
+    wz = np.full(6, np.inf, np.float32)
+    for layer in range(6):
+        on = features[:, 4] == layer
+        if on.any():
+            wphi[layer] = np.float32(np.quantile(features[on, 0], q))
+            wz[layer] = np.float32(np.quantile(features[on, 2], q))
+    return wphi, wz
+
+
+def _set_windows(m, wphi, wz):
+    for layer in range(6):
+        m.dphi_window[layer] = float(wphi[layer])
+        m.dz_window[layer] = float(wz[layer])
+
+
+@pytest.mark.parametrize("window_q", [None, 0.9])
+def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev, window_q):
     """Threshold at the 12% quantile of an untrained gate's logits, on central events and a dense
     jet (inner clusters with more than 48 tracklets): the gated run's tracklets are the plain
-    tracklets scored at or above it
-    (all of a crowded cluster's), in order; its roads are exactly the plain roads whose 6
-    tracklets all survive, with the same labels."""
+    tracklets scored at or above it (all of a crowded cluster's), in order; its roads are exactly
+    the plain roads whose 6 tracklets all survive, with the same labels. With the cascade's first
+    stage (window_q: per layer, |dphi| and |dz| windows at that quantile of the layer's plain
+    tracklets),
+    only the tracklets inside the window are scored or kept, and a cluster is crowded by the
+    tracklets inside it."""
     events = [gen.pbpb_event(s, n_tracks=2500) for s in (66, 67)] + [gen.jet_event(5)]
     b, f, l, r = _plain(ctx, torch_dev, events)
     pkeys, pfake = prefilter.export_roads(ctx, torch_dev)
     plain = [ctx.results(e) for e in range(len(events))]
-    m = _gate(f.cpu().numpy(), seed=11)
+    fn = f.cpu().numpy()
+    m = _gate(fn, seed=11)
+    inside = np.ones(len(fn), bool)
+    if window_q is not None:
+        wphi, wz = _windows_at(fn, window_q)
+        _set_windows(m, wphi, wz)
+        inside = prefilter.window_pass(fn, wphi, wz)
+        assert 0.7 < inside.mean() < 0.9
     ctx.gate_set_model(m)
     logits = _score(ctx, f, torch_dev)
-    thr = float(np.quantile(logits, 0.12))  # keeps about 88%: some roads keep all 6 tracklets
+    thr = float(np.quantile(logits[inside], 0.12))  # keeps about 88%: some roads keep all 6 tracklets
     m.logit_threshold = thr
     ctx.gate_set_model(m)
-    keep = ~(logits < thr)
-    # inner clusters with more than 48 tracklets keep all of them
+    keep = ~(logits < thr) & inside
+    # inner clusters with more than 48 tracklets (inside the window) keep all of them
     row = 0
     crowded = 0
     for e in range(len(events)):
         for layer in range(6):
             t = plain[e]["tracklets"][layer]
-            per = np.bincount(t["c1"], minlength=len(plain[e]["clusters"][layer]))
-            big = per[t["c1"]] > 48
+            ins = inside[row:row + len(t)]
+            per = np.bincount(t["c1"][ins], minlength=len(plain[e]["clusters"][layer]))
+            big = (per[t["c1"]] > 48) & ins
             keep[row:row + len(t)] |= big
             crowded += int(big.sum())
             row += len(t)
-    assert row == len(keep) and crowded > 0
-    assert 0.8 < keep.mean() < 0.95
+    assert row == len(keep)
+    if window_q is None:
+        assert crowded > 0
+        assert 0.8 < keep.mean() < 0.95
+    else:
+        assert 0.55 < keep.mean() < 0.85
     prefilter.set_learned(ctx, False, True)
     try:
         ctx.batch_run(b.batch)
@@ -167,7 +202,7 @@ def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev):
     finally:
         prefilter.set_learned(ctx, False, False)
     rows = r.cpu().numpy().astype(np.int64)
-    survives = keep[rows].all(axis=1)
+    survives = np.append(keep, True)[rows].all(axis=1)  # row -1: no tracklet in that layer
     cmp = prefilter.compare_roads(pkeys, pfake, lkeys, lfake)
     assert cmp["extra"] == 0 and cmp["extra_fakes"] == 0
     assert cmp["reproduced"] == int(survives.sum()) == cmp["learned_roads"]
@@ -175,6 +210,57 @@ def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev):
     # the surviving roads keep their Monte Carlo labels and fake flags (same 7 clusters)
     lab = {bytes(k): fk for k, fk in zip(np.ascontiguousarray(pkeys), pfake)}
     assert all(lab[bytes(k)] == fk for k, fk in zip(np.ascontiguousarray(lkeys), lfake))
+
+
+def test_gate_window_alone_keeps_the_tracklets_inside_it(ctx, torch_dev):
+    """The cascade's first stage alone (threshold -inf), the windows at each layer's median |dphi|
+    and |dz|: the gated run's tracklets are the plain tracklets inside their layer's windows, in
+    order, on central, pp and jet events and across the phi wrap; a zero window keeps none."""
+    events = [gen.pbpb_event(s, n_tracks=2000) for s in (68, 69)] + [gen.pp_event(70), gen.jet_event(5)]
+    b, f, _, _ = _plain(ctx, torch_dev, events)
+    plain = [ctx.results(e) for e in range(len(events))]
+    fn = f.cpu().numpy()
+    m = _gate(fn, threshold=float("-inf"))
+    wphi, wz = _windows_at(fn, 0.5)
+    _set_windows(m, wphi, wz)
+    inside = prefilter.window_pass(fn, wphi, wz)
+    assert 0.15 < inside.mean() < 0.5
+    # some kept tracklets cross phi = 0 (their clusters on both sides of the wrap)
+    wraps = 0
+    row = 0
+    for e in range(len(events)):
+        for layer in range(6):
+            t = plain[e]["tracklets"][layer]
+            p1 = plain[e]["clusters"][layer]["phi"][t["c1"]]
+            p2 = plain[e]["clusters"][layer + 1]["phi"][t["c2"]]
+            wraps += int((inside[row:row + len(t)] & (np.abs(p1 - p2) > np.pi)).sum())
+            row += len(t)
+    assert wraps > 0
+    ctx.gate_set_model(m)
+    prefilter.set_learned(ctx, False, True)
+    try:
+        ctx.batch_run(b.batch)
+        row = 0
+        layer3 = []
+        for e in range(len(events)):
+            got = ctx.results(e)
+            layer3.append(got["tracklets"][3].copy())
+            for layer in range(6):
+                pt = plain[e]["tracklets"][layer]
+                kept = pt[inside[row:row + len(pt)]]
+                row += len(pt)
+                assert np.array_equal(got["tracklets"][layer].view(np.uint8), kept.view(np.uint8)), (e, layer)
+        m.dphi_window[2] = 0.0
+        m.dz_window[4] = 0.0
+        ctx.gate_set_model(m)
+        ctx.batch_run(b.batch)
+        for e in range(len(events)):
+            got = ctx.results(e)["tracklets"]
+            assert len(got[2]) == 0 and len(got[4]) == 0, e
+            assert np.array_equal(got[3].view(np.uint8), layer3[e].view(np.uint8)), e  # the other layers' windows stay
+        assert sum(len(t) for t in layer3) > 0
+    finally:
+        prefilter.set_learned(ctx, False, False)
 
 
 def test_gate_and_pair_prefilter_together(ctx, torch_dev):

@@ -138,7 +138,7 @@ def test_compare_roads():
 
 
 def test_gate_model_layout_and_init():
-    assert ctypes.sizeof(capi.GateModel) == 4 * (capi.GATE_PARAMS + 2 * 8 + 1)
+    assert ctypes.sizeof(capi.GateModel) == 4 * (capi.GATE_PARAMS + 2 * 8 + 1 + 12)
     assert capi.GATE_PARAMS == 433
     assert ctypes.sizeof(capi.GateSamples) == 56
     a, b, c = capi.gate_init(1), capi.gate_init(1), capi.gate_init(2)
@@ -146,12 +146,46 @@ def test_gate_model_layout_and_init():
     p = a.params()
     assert np.all(np.abs(p[:128]) <= np.sqrt(6 / 24) + 1e-7)
     assert np.all(p[128:144] == 0) and a.logit_threshold == 0.0
+    assert list(a.dphi_window) == [np.float32(np.pi)] * 6  # no first stage until trained
+    assert list(a.dz_window) == [np.inf] * 6
+
+
+def test_gate_windows_fit_the_road_tracklets():
+    """The cascade's first stage: per layer, the margin times the largest |dphi| and |dz| of the
+    tracklets on roads (|dphi| at most the tracklet cut's 0.3); a layer without road tracklets
+    keeps no window; the test is inclusive."""
+    rng = np.random.default_rng(3)
+    f = np.zeros((600, 8), np.float32)
+    f[:, 4] = np.repeat(np.arange(6), 100)
+    f[:, 0] = rng.uniform(0, 0.3, 600)
+    f[:, 2] = rng.uniform(0, 0.2, 600)
+    on_road = np.flatnonzero((f[:, 4] != 5) & (rng.random(600) < 0.2))
+    f[on_road[0], 0] = 0.29  # its window would pass the cut
+    rows = np.full((len(on_road), 6), -1, np.int64)
+    rows[:, 0] = on_road
+    wphi, wz = prefilter.fit_windows(f, rows, margin=1.25)
+    for layer in range(5):
+        r = on_road[f[on_road, 4] == layer]
+        assert wphi[layer] == np.float32(min(0.3, 1.25 * f[r, 0].astype(np.float64).max()))
+        assert wz[layer] == np.float32(1.25 * f[r, 2].astype(np.float64).max())
+    assert wphi[5] == np.float32(0.3) and wz[5] == np.inf
+    assert wphi[int(f[on_road[0], 4])] == np.float32(0.3)
+    ok = prefilter.window_pass(f, wphi, wz)
+    assert ok[on_road].all()
+    edge = f.copy()
+    edge[:, 0] = wphi[edge[:, 4].astype(int)]
+    edge[:, 2] = wz[edge[:, 4].astype(int)]
+    assert prefilter.window_pass(edge, wphi, wz).all()
+    edge[:, 2] = np.nextafter(edge[:, 2], np.float32(np.inf))
+    assert not prefilter.window_pass(edge, wphi, wz)[:500].any()
 
 
 def test_gate_checkpoint_round_trip_and_kinds(tmp_path):
     """The gate's checkpoint has its own magic: neither kind loads as the other."""
     g = capi.gate_init(4)
     g.logit_threshold = -2.5
+    g.dphi_window[3] = 0.0625
+    g.dz_window[1] = 0.03125
     path = str(tmp_path / "g.itsugate")
     capi.gate_save(g, path)
     assert bytes(capi.gate_load(path)) == bytes(g)

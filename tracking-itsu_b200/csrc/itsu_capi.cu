@@ -17,6 +17,7 @@
 #include <cstring>
 #include <string>
 #include <unordered_map>
+#include <type_traits>
 #include <vector>
 
 #include "itsu.h"
@@ -2032,7 +2033,7 @@ struct NetOf<itsu_gate_model> {
   using Device = itsu::GateDevice;
   static constexpr int kHidden = ITSU_GATE_HIDDEN;
   static constexpr int kParams = ITSU_GATE_PARAMS;
-  static constexpr char kMagic[8] = {'I', 'T', 'S', 'U', 'G', 'A', 'T', '1'};
+  static constexpr char kMagic[8] = {'I', 'T', 'S', 'U', 'G', 'A', 'T', '3'};
   static constexpr const char *kName = "gate";
   static Model *&master(itsu_context *c) { return c->d_gate_master; }
   static Device *&device(itsu_context *c) { return c->d_gate; }
@@ -2108,6 +2109,12 @@ void net_init(Model *model, uint64_t seed)
   for (int i = 0; i < H; ++i) model->w3[i] = uniform(l3);
   for (int i = 0; i < ITSU_MLP_INPUTS; ++i) model->inv_std[i] = 1.0f;
   model->logit_threshold = 0.0f;
+  if constexpr (std::is_same<Model, itsu_gate_model>::value) {
+    for (int l = 0; l < ITSU_TRACKLET_LAYERS; ++l) {  // no first stage
+      model->dphi_window[l] = 3.14159265358979323846f;
+      model->dz_window[l] = HUGE_VALF;
+    }
+  }
 }
 
 template <class Model>
@@ -2172,6 +2179,15 @@ itsu_status net_set_model(itsu_context *ctx, const Model *model, const char *wha
   using N = NetOf<Model>;
   if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "%s: null context", what);
   if (!model) return fail(ctx, ITSU_ERR_INVALID, "%s: null model", what);
+  if constexpr (std::is_same<Model, itsu_gate_model>::value) {
+    for (int l = 0; l < ITSU_TRACKLET_LAYERS; ++l) {
+      // NaN or negative: the window would drop every tracklet
+      if (!(model->dphi_window[l] >= 0.0f) || !(model->dz_window[l] >= 0.0f)) {
+        return fail(ctx, ITSU_ERR_INVALID, "%s: window of layer %d (dphi %g, dz %g) is not a window", what, l,
+                    (double)model->dphi_window[l], (double)model->dz_window[l]);
+      }
+    }
+  }
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
   if (!N::master(ctx)) ITSU_CUDA(ctx, cudaMalloc((void **)&N::master(ctx), sizeof(Model)));
   if (!N::device(ctx)) ITSU_CUDA(ctx, cudaMalloc((void **)&N::device(ctx), N::device_bytes()));

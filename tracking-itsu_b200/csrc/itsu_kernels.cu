@@ -742,10 +742,12 @@ struct TrackletProbe {
   }
 };
 
+// win_row, win_rows: the phi rows whose candidates are walked (win_rows = kPhiBins: every row); of
+// the other rows only the bound candidate is tested.
 template <int kWords, typename OnPass>
 __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next, int4 rect, int layer, const TrackletProbe &probe,
                                                 bool prune, float zlo, float zhi, const float4 *zs, int zs_off,
-                                                OnPass &&on_pass)
+                                                int win_row, int win_rows, OnPass &&on_pass)
 {
   // zs[k - zs_off] is the k-th entry of the next layer's z-sorted bin lists (zs_off > 0: a staged
   // copy in shared memory that starts at entry zs_off)
@@ -761,8 +763,10 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
        phi_bin = (phi_bin + 1 == kPhiBins) ? 0 : phi_bin + 1, ++phi_count) {
     const int first_bin = bin_index(rect.x, phi_bin);
     const int max_bin = min(first_bin + rect.z - rect.x + 1, kTableBins);  // P5
+    const bool walk_row = win_rows >= kPhiBins ||
+                          (phi_bin < kPhiBins && (phi_bin - win_row + kPhiBins) % kPhiBins < win_rows);
     if (prune && phi_bin < kPhiBins) {
-      for (int col = zb_lo; col <= zb_hi; ++col) {
+      for (int col = zb_lo; walk_row && col <= zb_hi; ++col) {
         const int bin = phi_bin * kPhiBins + col;
         const int k0 = table[bin], k1 = table[bin + 1];
         int lo = k0, hi = k1;  // first listed cluster with z >= zlo
@@ -817,8 +821,8 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
     } else {
       const int first_row = table[first_bin];
       const int last_row = min(table[max_bin], n_next - 1);  // inclusive bound, P1
-      for (int j = first_row; j <= last_row; ++j) {
-        if (probe.pass(j)) {
+      for (int j = walk_row ? first_row : last_row; j <= last_row; ++j) {
+        if (probe.pass(j) && (walk_row || j == table[max_bin])) {
           on_pass(j);
         }
       }
@@ -830,6 +834,8 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
 // stage, and the probe, window and pruning bounds of its candidate walk.
 struct InnerCluster {
   bool walk;
+  GateWindow win;  // the learned form's first-stage windows for its tracklets
+  int win_row, win_rows;  // the phi rows its |dphi| window reaches (win_rows = kPhiBins: every row)
   int seg, e, layer;
   int4 rect;
   TrackletProbe probe;
@@ -841,6 +847,28 @@ struct InnerCluster {
   int64_t next_begin;
 };
 
+// The phi rows that hold the azimuths within half_width of phi (the window's rows, clamped into
+// 0..kPhiBins - 1): first row and count, in the walk's cyclic order.
+__device__ __forceinline__ void window_rows(float phi, float half_width, int *first, int *rows)
+{
+  float lo = phi - half_width, hi = phi + half_width;
+  lo = lo < 0.0f ? lo + kTwoPi : lo;
+  hi = hi >= kTwoPi ? hi - kTwoPi : hi;
+  const int r_lo = min(phi_bin_index(lo), kPhiBins - 1), r_hi = min(phi_bin_index(hi), kPhiBins - 1);
+  int n = r_hi - r_lo + 1;
+  *first = r_lo;
+  *rows = n <= 0 ? n + kPhiBins : n;
+}
+
+// With a tracklet gate (learned form), its first stage's windows for the layer narrow the walk: a
+// tracklet outside them is not kept. The walk keeps the plain rect and its row sequence (with the
+// reference's edge behaviour, e.g. a first row of 20 when the window's lower edge rounds to 2pi),
+// but of a row outside the |dphi| window (widened by 1e-3 rad against rounding) it only tests the
+// row's bound candidate (P1), which can lie in the next row; the pruned columns take the narrower
+// z range of the |dz| window (widened by 1e-3 cm). In a regular layer every cluster sits in its
+// own bin, so the walk still meets every plain candidate inside the windows, in the plain order;
+// other layers are walked whole. Every pass is then tested against the windows themselves
+// (gate_window_pass): the gated tracklets are exactly the plain tracklets inside the windows.
 __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
 {
   InnerCluster s;
@@ -859,7 +887,7 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
   const float dir_z = s.probe.tan_lambda * (kC.r[s.layer + 1] - s.probe.c.w) + s.probe.c.z;
   s.rect = bins_rect(s.probe.phi1, s.layer, dir_z);
   if (s.rect.x == 0 && s.rect.y == 0 && s.rect.z == 0 && s.rect.w == 0) {
-    return s;
+    return s;  // the reference's "no bins" rect (Tracker.cxx:66-70)
   }
   s.walk = true;
   s.next_begin = lo[s.layer + 1];
@@ -868,14 +896,23 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
   s.probe.max_dz = kC.trk_max_dz[s.layer];
   const int next_seg = s.seg + 1;
   s.words = a.seg_regular[next_seg];  // 0: not regular, else the mask words its largest bin needs
+  s.win_row = 0;
+  s.win_rows = kPhiBins;
+  if (a.gate) {
+    s.win = gate_window(*a.gate, s.layer, s.probe.c, s.probe.phi1, vz);
+    if (s.words != 0 && s.win.dphi + 1e-3f < kPhiCoordinateCut) {  // a wider window narrows nothing
+      window_rows(s.probe.phi1, s.win.dphi + 1e-3f, &s.win_row, &s.win_rows);
+    }
+  }
   s.prune = a.prune_tracklets && s.words != 0;
   s.zlo = s.zhi = 0;
   if (s.prune) {
     const float2 rr = a.seg_rrange[next_seg];
     const float p1 = s.probe.tan_lambda * (rr.x - s.probe.c.w) + s.probe.c.z;
     const float p2 = s.probe.tan_lambda * (rr.y - s.probe.c.w) + s.probe.c.z;
-    s.zlo = fminf(p1, p2) - s.probe.max_dz - 1e-3f;
-    s.zhi = fmaxf(p1, p2) + s.probe.max_dz + 1e-3f;
+    const float half = a.gate && s.words != 0 ? fminf(s.probe.max_dz, s.win.dz + 1e-3f) : s.probe.max_dz;
+    s.zlo = fminf(p1, p2) - half - 1e-3f;
+    s.zhi = fmaxf(p1, p2) + half + 1e-3f;
     s.prune = isfinite(s.zlo) && isfinite(s.zhi);
   }
   s.table = a.index_tables + ((int64_t)s.e * ITSU_TRACKLET_LAYERS + s.layer) * kTableSize;
@@ -892,11 +929,14 @@ __device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s
   const float4 *zs = staged ? staged : a.zs + s.next_begin;
   const int off = staged ? staged_off : 0;
   if (s.words <= 1) {  // unpruned, or bins of at most 64 clusters
-    walk_candidates<1>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, on_pass);
+    walk_candidates<1>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row, s.win_rows,
+                                     on_pass);
   } else if (s.words == 2) {
-    walk_candidates<2>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, on_pass);
+    walk_candidates<2>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row, s.win_rows,
+                                     on_pass);
   } else {
-    walk_candidates<kPruneWords>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, on_pass);
+    walk_candidates<kPruneWords>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row, s.win_rows,
+                                     on_pass);
   }
 }
 
@@ -1022,9 +1062,13 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
     staged = staged_off >= 0 ? stage : nullptr;
   }
   if (s.walk && !(a.status->flags & kFlagTimeout)) {
+    const bool windowed = a.gate != nullptr;
     walk_inner(
         a, s,
         [&](int j) {
+          if (windowed && !gate_window_pass(s.win, s.probe.xyzr[j], s.probe.phi[j])) {
+            return;  // learned form: outside the gate's first stage
+          }
           if (count < kTrackletSlots) {
             a.trk_slots[count * a.slot_stride + i] = j;
           }
@@ -1275,7 +1319,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_crowded(Arena a)
     const int64_t i = a.clu_crowded[q];
     const InnerCluster s = inner_cluster(a, i);
     int out = a.trk_off[i];
-    walk_inner(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, s.seg); });
+    const bool windowed = a.gate != nullptr;  // the count pass's first-stage test, the same way
+    walk_inner(a, s, [&](int j) {
+      if (!windowed || gate_window_pass(s.win, s.probe.xyzr[j], s.probe.phi[j])) {
+        write_tracklet(a, out++, i, s.next_begin + j, s.seg);
+      }
+    });
   }
 }
 
@@ -1755,57 +1804,63 @@ __global__ void k_neighbour_check(Arena a)
   }
 }
 
+// One cell of k_levels (below): its row sorted, its level and its number of chains.
+__device__ __forceinline__ void level_of(const Arena &a, int64_t c, int64_t prev_base, int layer)
+{
+  const int32_t b = a.nb_off[c], en = a.nb_off[c + 1];
+  int32_t *row = a.nb + b;
+  const int len = en - b;
+  for (int p = 1; p < len; ++p) {
+    const int32_t v = row[p];
+    int q = p - 1;
+    while (q >= 0 && row[q] > v) {
+      row[q + 1] = row[q];
+      --q;
+    }
+    row[q + 1] = v;
+  }
+  int level = 1;
+  for (int p = 0; p < len; ++p) {
+    level = max(level, a.cells[prev_base + row[p]].level + 1);
+  }
+  int64_t paths = 0;
+  bool overflow = false;
+  for (int p = 0; p < len; ++p) {
+    const int64_t nbi = prev_base + row[p];
+    if (a.cells[nbi].level == level - 1) {
+      paths += a.paths[nbi];
+      if (paths > INT_MAX) {
+        paths = INT_MAX;
+        overflow = true;
+      }
+    }
+  }
+  a.cells[c].level = level;
+  a.paths[c] = paths;
+  if (layer == ITSU_CELL_LAYERS - 1 && level == kCellsMinLevel) {
+    a.road_count[c] = (int32_t)paths;
+    if (overflow) {
+      atomicOr(&a.status->flags, kFlagCountOverflow);
+    }
+  }
+}
+
 // Rows of layer `layer` cells: sort ascending (the reference pushes in cell order), then the
 // level (Tracker.cxx:463-468: 1 + the highest neighbour level) and the number of
 // level-decreasing chains down to layer 0 (the roads a level-5 cell starts, Tracker.cxx:477-571).
+// The blocks of grid row y take the layer's cells of events y, y + gridDim.y, ... (each event's
+// cells of a layer are one range).
 __global__ void __launch_bounds__(kMaxThreads) k_levels(Arena a, int layer)
 {
   if (capacity_failed(a.status)) {
     return;
   }
-  const int64_t n = a.status->total[kCells];
-  for (int64_t c = global_thread(); c < n; c += grid_threads()) {
-    const int sid = a.cell_seg_id[c];
-    if (sid % ITSU_CELL_LAYERS != layer) {
-      continue;
-    }
-    const int e = sid / ITSU_CELL_LAYERS;
-    const int32_t b = a.nb_off[c], en = a.nb_off[c + 1];
-    int32_t *row = a.nb + b;
-    const int len = en - b;
-    for (int p = 1; p < len; ++p) {
-      const int32_t v = row[p];
-      int q = p - 1;
-      while (q >= 0 && row[q] > v) {
-        row[q + 1] = row[q];
-        --q;
-      }
-      row[q + 1] = v;
-    }
-    const int64_t prev_base = a.cell_seg[e * ITSU_CELL_LAYERS + layer - 1];
-    int level = 1;
-    for (int p = 0; p < len; ++p) {
-      level = max(level, a.cells[prev_base + row[p]].level + 1);
-    }
-    int64_t paths = 0;
-    bool overflow = false;
-    for (int p = 0; p < len; ++p) {
-      const int64_t nbi = prev_base + row[p];
-      if (a.cells[nbi].level == level - 1) {
-        paths += a.paths[nbi];
-        if (paths > INT_MAX) {
-          paths = INT_MAX;
-          overflow = true;
-        }
-      }
-    }
-    a.cells[c].level = level;
-    a.paths[c] = paths;
-    if (layer == ITSU_CELL_LAYERS - 1 && level == kCellsMinLevel) {
-      a.road_count[c] = (int32_t)paths;
-      if (overflow) {
-        atomicOr(&a.status->flags, kFlagCountOverflow);
-      }
+  for (int e = blockIdx.y; e < a.n_events; e += gridDim.y) {
+    const int32_t *cs = a.cell_seg + e * ITSU_CELL_LAYERS;
+    const int64_t prev_base = cs[layer - 1];
+    for (int64_t c = cs[layer] + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cs[layer + 1];
+         c += (int64_t)gridDim.x * blockDim.x) {
+      level_of(a, c, prev_base, layer);
     }
   }
 }
@@ -1837,90 +1892,113 @@ __device__ __forceinline__ int32_t cluster_mc(const Arena &a, const int32_t *lo,
   return a.sorted[lo[layer] + idx].mc_id;
 }
 
+// One road per lane: the roads of a warp's 32 consecutive cells form one contiguous range (the
+// scan of the roots' chain counts), which the lanes fill together, each lane taking the next road
+// of the range, finding its root cell (owner) and its rank k among the root's roads. The traversal
+// of Tracker.cxx:477-571 visits a cell's neighbours in row order and descends into those one level
+// down, so the root's k-th road is found by walking down the layers: at each, skip the neighbours
+// one level down whose whole subtrees (their chain counts, k_levels) lie before k, and descend into
+// the one holding it. A complete chain is labelled by Moore's vote over its 7 clusters
+// (Tracker.cxx:574-652) and stored with coalesced writes. The roots are the last layer's cells:
+// the blocks of grid row y take those of events y, y + gridDim.y, ...
 __global__ void __launch_bounds__(kMaxThreads) k_roads(Arena a)
 {
   if (capacity_failed(a.status)) {
     return;
   }
-  const int64_t n = a.status->total[kCells];
-  for (int64_t c = global_thread(); c < n; c += grid_threads()) {
-    int64_t out = a.road_off[c];
-    if (a.road_off[c + 1] == out) {
-      continue;
-    }
-    const int sid = a.cell_seg_id[c];
-    const int e = sid / ITSU_CELL_LAYERS;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (int e = blockIdx.y; e < a.n_events; e += gridDim.y) {
     const int32_t *cs = a.cell_seg + e * ITSU_CELL_LAYERS;
     const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
-    int32_t cur[ITSU_CELL_LAYERS];  // local cell index per layer along the current chain
-    int32_t it[ITSU_CELL_LAYERS];   // next neighbour slot per layer
-    int level[ITSU_CELL_LAYERS];
-    int l = ITSU_CELL_LAYERS - 1;
-    cur[l] = (int32_t)(c - cs[l]);
-    it[l] = a.nb_off[c];
-    level[l] = a.cells[c].level;
-    while (true) {
-      if (l == 0) {
-        // a complete chain: one road, labelled by Moore's vote over its 7 clusters (:574-652)
+    const int64_t n = cs[ITSU_CELL_LAYERS];  // the event's last cell + 1
+    for (int64_t base = cs[ITSU_CELL_LAYERS - 1] + warp * 32; base < n; base += warps * 32) {
+      const int64_t c = base + lane;
+      int32_t first = 0, count = 0;
+      if (c < n) {
+        first = a.road_off[c];
+        count = a.road_off[c + 1] - first;
+      }
+      int total = 0;
+      const int excl = warp_exclusive_sum(count, total);
+      if (total == 0) {
+        continue;
+      }
+      const int64_t out0 = __shfl_sync(0xffffffffu, first, 0);
+      for (int p0 = 0; p0 < total; p0 += 32) {
+        const int p = p0 + lane;
+        const int owner = owner_of(excl, p);
+        int64_t k = p - __shfl_sync(0xffffffffu, excl, owner);
+        if (p >= total) {
+          continue;
+        }
+        int64_t flat = base + owner;
+        int32_t cur[ITSU_CELL_LAYERS];  // local cell index per layer along the chain
+        cur[ITSU_CELL_LAYERS - 1] = (int32_t)(flat - cs[ITSU_CELL_LAYERS - 1]);
+        int level = kCellsMinLevel;
+        bool found = true;
+#pragma unroll
+        for (int l = ITSU_CELL_LAYERS - 1; l >= 1; --l) {
+          const int32_t j1 = a.nb_off[flat + 1];
+          bool down = false;
+          cur[l - 1] = 0;
+          for (int32_t j = a.nb_off[flat]; j < j1; ++j) {
+            const int32_t nb = a.nb[j];
+            const int64_t nflat = cs[l - 1] + nb;
+            if (a.cells[nflat].level == level - 1) {
+              const int64_t below = a.paths[nflat];
+              if (k < below) {
+                cur[l - 1] = nb;
+                flat = nflat;
+                down = true;
+                break;
+              }
+              k -= below;
+            }
+          }
+          found = found && down;
+          --level;
+        }
+        if (!found) {  // only when a chain count was capped (the count overflow flag is set)
+          atomicOr(&a.status->flags, kFlagCountOverflow);
+        }
         itsu_road road;
-        int max_value = ITSU_UNUSED_INDEX, count = 0;
+        int max_value = ITSU_UNUSED_INDEX, votes = 0;
         bool fake = false;
-        for (int k = 0; k < ITSU_CELL_LAYERS; ++k) {
-          road.cell_ids[k] = cur[k];
-          const itsu_cell &cell = a.cells[cs[k] + cur[k]];
-          if (k == 0) {
+#pragma unroll
+        for (int l = 0; l < ITSU_CELL_LAYERS; ++l) {
+          road.cell_ids[l] = cur[l];
+          const itsu_cell &cell = a.cells[cs[l] + cur[l]];
+          if (l == 0) {
             max_value = cluster_mc(a, lo, 0, cell.first_cluster);
-            count = 1;
+            votes = 1;
             const int second = cluster_mc(a, lo, 1, cell.second_cluster);
             if (second == max_value) {
-              ++count;
+              ++votes;
             } else {
               max_value = second;
-              count = 1;
+              votes = 1;
               fake = true;
             }
           }
-          const int current = cluster_mc(a, lo, k + 2, cell.third_cluster);
+          const int current = cluster_mc(a, lo, l + 2, cell.third_cluster);
           if (current == max_value) {
-            ++count;
+            ++votes;
           } else {
-            --count;
+            --votes;
             fake = true;
           }
-          if (count == 0) {
+          if (votes == 0) {
             max_value = current;
-            count = 1;
+            votes = 1;
           }
         }
         road.size = ITSU_CELL_LAYERS;
         road.label = max_value;
         road.is_fake = fake ? 1 : 0;
         road.pad_[0] = road.pad_[1] = road.pad_[2] = 0;
-        a.roads[out++] = road;
-        ++l;
-        continue;
-      }
-      const int64_t flat = cs[l] + cur[l];
-      const int32_t end = a.nb_off[flat + 1];
-      bool descended = false;
-      while (it[l] < end) {
-        const int32_t nb = a.nb[it[l]++];
-        const int64_t nflat = cs[l - 1] + nb;
-        const int nlevel = a.cells[nflat].level;
-        if (nlevel == level[l] - 1) {
-          cur[l - 1] = nb;
-          it[l - 1] = a.nb_off[nflat];
-          level[l - 1] = nlevel;
-          --l;
-          descended = true;
-          break;
-        }
-      }
-      if (!descended) {
-        if (l == ITSU_CELL_LAYERS - 1) {
-          break;
-        }
-        ++l;
+        a.roads[out0 + p] = road;
       }
     }
   }
@@ -1929,6 +2007,14 @@ __global__ void __launch_bounds__(kMaxThreads) k_roads(Arena a)
 // Grid of the grid-stride kernels: the tuned number of resident blocks per SM, scaled to the
 // block size so that the number of resident threads stays comparable.
 int fixed_grid(const Launch &l) { return l.num_sms * l.blocks_per_sm; }
+
+// Grid of the per-event kernels (a row of blocks per event, events beyond 65535 rows taken in
+// turn): about the same blocks in all as the grid-stride kernels.
+dim3 event_grid(const Arena &a, const Launch &l)
+{
+  const int rows = std::min(a.n_events, 65535);
+  return dim3((unsigned)std::max(1, (fixed_grid(l) + rows - 1) / rows), (unsigned)rows);
+}
 
 void step_status_init(const Arena &a, const Launch &l)
 {
@@ -2048,14 +2134,24 @@ void step_neighbours(const Arena &a, const Launch &l) { k_neighbours<kWrite><<<f
 void step_neighbour_check(const Arena &a, const Launch &l) { k_neighbour_check<<<1, 32, 0, l.stream>>>(a); }
 
 template <int kLayer>
-void step_levels(const Arena &a, const Launch &l) { k_levels<<<fixed_grid(l), l.block, 0, l.stream>>>(a, kLayer); }
+void step_levels(const Arena &a, const Launch &l)
+{
+  if (a.n_events > 0) {
+    k_levels<<<event_grid(a, l), l.block, 0, l.stream>>>(a, kLayer);
+  }
+}
 
 void step_road_segments(const Arena &a, const Launch &l)
 {
   k_road_segments<<<(a.n_events + kThreads) / kThreads, kThreads, 0, l.stream>>>(a);
 }
 
-void step_roads(const Arena &a, const Launch &l) { k_roads<<<fixed_grid(l), l.block, 0, l.stream>>>(a); }
+void step_roads(const Arena &a, const Launch &l)
+{
+  if (a.n_events > 0) {
+    k_roads<<<event_grid(a, l), l.block, 0, l.stream>>>(a);
+  }
+}
 
 // The whole run, kernel by kernel, in launch order.
 const KernelStep kSteps[] = {

@@ -71,6 +71,8 @@ struct MlpDeviceT {
   float threshold;
   float mean[kMlpIn];
   float inv_std[kMlpIn];
+  float window[6];     // the tracklet gate's per-layer |dphi| window (the pair prefilter: pi, unused)
+  float dz_window[6];  // and its |dz| window (the pair prefilter: infinity, unused)
 };
 
 // A network staged in shared memory in MMA-friendly, zero-padded form.
@@ -396,6 +398,35 @@ __device__ __forceinline__ void gate_features(const GateInner &g, float4 c2, flo
   f[5] = g.r1;
   f[6] = g.tan_lambda;
   f[7] = dphi;
+}
+
+// The cascade's first stage for one inner cluster: its per-layer windows on |dphi| and |dz| (the
+// gate's features 0 and 2, with the same arithmetic: the slope by the fast division of
+// gate_inner).
+struct GateWindow {
+  float dphi, dz;
+  float phi1, z1, r1, tan_lambda;
+};
+
+__device__ __forceinline__ GateWindow gate_window(const MlpDeviceT<kGateHidden> &m, int layer, float4 c1, float phi1, float vz)
+{
+  GateWindow w;
+  w.dphi = m.window[layer];
+  w.dz = m.dz_window[layer];
+  w.phi1 = phi1;
+  w.z1 = c1.z;
+  w.r1 = c1.w;
+  w.tan_lambda = __fdividef(c1.z - vz, c1.w);
+  return w;
+}
+
+__device__ __forceinline__ bool gate_window_pass(const GateWindow &w, float4 c2, float phi2)
+{
+  constexpr float kPiF = 3.14159265358979323846f, kTwoPiF = 6.28318530717958647692f;
+  float dphi = w.phi1 - phi2;
+  dphi = dphi > kPiF ? dphi - kTwoPiF : (dphi < -kPiF ? dphi + kTwoPiF : dphi);
+  const float dz = w.tan_lambda * (c2.w - w.r1) + w.z1 - c2.z;
+  return fabsf(dphi) <= w.dphi && fabsf(dz) <= w.dz;
 }
 
 __device__ __forceinline__ void tracklet_features(int layer, float4 c1, float phi1, float4 c2, float phi2, float vx, float vy,

@@ -58,8 +58,9 @@ __device__ __forceinline__ void publish_param(MlpDeviceT<H> *model, int i, float
   }
 }
 
+// window: the gate's per-layer |dphi| window in the master (null for the pair prefilter: pi).
 template <int H>
-__global__ void k_mlp_publish(const float *master, MlpDeviceT<H> *model)
+__global__ void k_mlp_publish(const float *master, const float *window, const float *dz_window, MlpDeviceT<H> *model)
 {
   constexpr int P = MlpShape<H>::kParams;
   for (int i = threadIdx.x; i < P; i += blockDim.x) {
@@ -68,6 +69,10 @@ __global__ void k_mlp_publish(const float *master, MlpDeviceT<H> *model)
   for (int i = threadIdx.x; i < kMlpIn; i += blockDim.x) {
     model->mean[i] = master[P + i];
     model->inv_std[i] = master[P + kMlpIn + i];
+  }
+  for (int i = threadIdx.x; i < 6; i += blockDim.x) {
+    model->window[i] = window ? window[i] : 3.14159265358979323846f;
+    model->dz_window[i] = dz_window ? dz_window[i] : HUGE_VALF;
   }
   if (threadIdx.x == 0) {
     model->threshold = master[P + 2 * kMlpIn];
@@ -528,7 +533,7 @@ void gradient_net(const MlpDeviceT<H> *model, const float *features, const uint8
 }  // namespace
 
 static_assert(sizeof(itsu_prefilter_model) == sizeof(float) * (kMlpParams + 2 * kMlpIn + 1), "pair model layout");
-static_assert(sizeof(itsu_gate_model) == sizeof(float) * (kGateParams + 2 * kMlpIn + 1), "gate model layout");
+static_assert(sizeof(itsu_gate_model) == sizeof(float) * (kGateParams + 2 * kMlpIn + 1 + 2 * ITSU_TRACKLET_LAYERS), "gate model layout");
 
 size_t mlp_device_bytes() { return sizeof(MlpDevice); }
 size_t gate_device_bytes() { return sizeof(GateDevice); }
@@ -537,12 +542,12 @@ int mlp_max_gradient_blocks() { return kMaxGradBlocks; }
 
 void launch_mlp_publish(const itsu_prefilter_model *master, MlpDevice *model, cudaStream_t stream)
 {
-  k_mlp_publish<kMlpHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], model);
+  k_mlp_publish<kMlpHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], nullptr, nullptr, model);
 }
 
 void launch_mlp_publish(const itsu_gate_model *master, GateDevice *model, cudaStream_t stream)
 {
-  k_mlp_publish<kGateHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], model);
+  k_mlp_publish<kGateHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], &master->dphi_window[0], &master->dz_window[0], model);
 }
 
 void launch_prefilter_export(const Arena &a, const itsu_prefilter_samples &out, int num_sms, cudaStream_t stream)

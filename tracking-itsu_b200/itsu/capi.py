@@ -97,6 +97,7 @@ MLP_INPUTS, MLP_HIDDEN = 8, 64
 MLP_PARAMS = MLP_HIDDEN * MLP_INPUTS + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
 
 
+TRACKLET_LAYERS = 6
 GATE_HIDDEN = 16
 GATE_PARAMS = GATE_HIDDEN * MLP_INPUTS + GATE_HIDDEN + GATE_HIDDEN * GATE_HIDDEN + GATE_HIDDEN + GATE_HIDDEN + 1
 
@@ -126,8 +127,10 @@ class PrefilterModel(ctypes.Structure):
 
 
 class GateModel(ctypes.Structure):
-    """itsu_gate_model: the tracklet gate (8 -> 16 -> 16 -> 1, ReLU); same field order."""
-    _fields_ = _model_fields(GATE_HIDDEN)
+    """itsu_gate_model: the tracklet gate (per-layer |dphi| and |dz| windows, then 8 -> 16 -> 16 -> 1,
+    ReLU); same field order."""
+    _fields_ = _model_fields(GATE_HIDDEN) + [("dphi_window", ctypes.c_float * TRACKLET_LAYERS),
+                                              ("dz_window", ctypes.c_float * TRACKLET_LAYERS)]
     N_PARAMS = GATE_PARAMS
     params = PrefilterModel.params
     arrays = PrefilterModel.arrays

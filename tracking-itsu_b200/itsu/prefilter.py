@@ -446,17 +446,60 @@ def ctx_has_gate(ctx) -> bool:
         return False
 
 
-def train_gate(ctx, data: dict, device, seed: int = 1, target: float = 0.999, log=print, **train_kw) -> tuple:
-    """Trains a tracklet gate on `data` (from collect_gate) and calibrates its threshold on road
-    reproduction (a road survives the gate iff all its 6 tracklets are kept); returns (model, report)."""
+PHI_CUT = 0.3  # the tracklet cut's phi window (the reference's kPhiCoordinateCut, Constants.h)
+
+
+def fit_windows(features: np.ndarray, road_rows: np.ndarray, margin: float = 1.25) -> tuple:
+    """The cascade's first stage: per inner layer, `margin` times the largest |dphi| (feature 0) and
+    |dz| (feature 2) of the tracklets on the training roads; the |dphi| window at most the tracklet
+    cut's own (a layer without a road tracklet keeps no window). Returns (dphi, dz) windows."""
+    rows = np.unique(road_rows[road_rows >= 0])
+    layer = features[rows, 4]
+    wphi = np.full(6, PHI_CUT, np.float32)
+    wz = np.full(6, np.inf, np.float32)
+    for l in range(6):
+        on = layer == l
+        dphi = features[rows[on], 0].astype(np.float64)
+        dz = features[rows[on], 2].astype(np.float64)
+        dphi, dz = dphi[np.isfinite(dphi)], dz[np.isfinite(dz)]
+        if len(dphi):
+            wphi[l] = np.float32(min(PHI_CUT, margin * float(dphi.max())))
+        if len(dz):
+            wz[l] = np.float32(margin * float(dz.max()))
+    return wphi, wz
+
+
+def window_pass(features: np.ndarray, dphi_window: np.ndarray, dz_window: np.ndarray | None = None) -> np.ndarray:
+    """The first stage's verdict per tracklet: |dphi| and |dz| within its layer's windows (the
+    device tests the same values, features 0 and 2, in float32)."""
+    layer = np.clip(features[:, 4], 0, 5).astype(np.int64)
+    ok = ~(features[:, 0] > dphi_window[layer])
+    if dz_window is not None:
+        ok &= ~(features[:, 2] > dz_window[layer])
+    return ok
+
+
+def train_gate(ctx, data: dict, device, seed: int = 1, target: float = 0.999, log=print, window_margin: float = 1.25,
+               **train_kw) -> tuple:
+    """Trains a tracklet gate on `data` (from collect_gate): the first stage's per-layer |dphi| and
+    |dz| windows from the road tracklets (fit_windows), then the network on the tracklets inside them,
+    its threshold calibrated on road reproduction (a road survives the gate iff all its 6 tracklets
+    pass both stages); returns (model, report)."""
     import torch
 
     model = capi.gate_init(seed)
-    mean, inv_std = standardisation(data["features"])
+    feats_np = data["features"].cpu().numpy()
+    rows = data["road_rows"].cpu().numpy()
+    wphi, wz = fit_windows(feats_np, rows, window_margin)
+    inside = window_pass(feats_np, wphi, wz)
+    for l in range(6):
+        model.dphi_window[l] = float(wphi[l])
+        model.dz_window[l] = float(wz[l])
+    mean, inv_std = standardisation(data["features"][torch.from_numpy(inside).to(data["features"].device)])
     for k in range(8):
         model.mean[k], model.inv_std[k] = float(mean[k]), float(inv_std[k])
     ctx.gate_set_model(model)
-    ok = torch.isfinite(data["features"]).all(dim=1)
+    ok = torch.isfinite(data["features"]).all(dim=1) & torch.from_numpy(inside).to(data["features"].device)
     f = data["features"][ok].contiguous()
     y = data["labels"][ok].contiguous()
     cfg = capi.train_config(**train_kw)
@@ -468,14 +511,15 @@ def train_gate(ctx, data: dict, device, seed: int = 1, target: float = 0.999, lo
     n = len(data["features"])
     logits_t = torch.empty(max(n, 1), dtype=torch.float32, device=device)
     ctx.gate_score(data["features"].data_ptr(), n, logits_t.data_ptr())
-    logits = logits_t[:n].cpu().numpy()
-    rows = data["road_rows"].cpu().numpy()
+    logits = np.where(inside, logits_t[:n].cpu().numpy(), -np.inf)  # outside the window: dropped by stage 1
     thr = calibrate(logits, rows, target)
     model.logit_threshold = thr
     ctx.gate_set_model(model)
     labels = data["labels"].cpu().numpy()
     kept = ~(logits < thr)
     report = dict(
+        dphi_window=[float(w) for w in wphi], dz_window=[float(w) for w in wz], window_margin=window_margin,
+        train_tracklets_inside_window=float(inside.mean()),
         samples=int(len(f)), positives=int(y.sum().item()), steps=int(cfg.steps), batch=int(cfg.batch), lr=float(cfg.lr),
         lr_final=float(cfg.lr_final), train_seconds=train_s, loss_first=float(np.mean(losses[:100])) if len(losses) else None,
         loss_last=float(np.mean(losses[-100:])) if len(losses) else None, threshold=thr, calibration_target=target,
