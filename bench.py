@@ -522,14 +522,22 @@ def run_ours(args):
 
         pair = _capi.prefilter_load(args.prefilter) if os.path.exists(args.prefilter) else None
         gate = _capi.gate_load(args.gate) if os.path.exists(args.gate) else None
-        for name, p_model, g_model in (("tracklet_gate", None, gate), ("pair_prefilter", pair, None),
-                                       ("gate_and_pair", pair, gate)):
-            if (name != "pair_prefilter" and g_model is None) or (name != "tracklet_gate" and p_model is None):
+        windows = None  # the gate's first stage alone: its windows, no layer scored by the network
+        if gate is not None:
+            windows = _capi.GateModel.from_buffer_copy(bytes(gate))
+            windows.mlp_layers = 0
+        forms = (("tracklet_gate", None, gate), ("gate_windows_only", None, windows), ("pair_prefilter", pair, None),
+                 ("gate_and_pair", pair, gate))
+        for name, p_model, g_model in forms:
+            if (name != "pair_prefilter" and g_model is None) or (name in ("pair_prefilter", "gate_and_pair") and p_model is None):
                 continue
+            if name == "gate_windows_only" and gate.mlp_layers == 0:
+                continue  # the committed gate is its windows already
             l_ms, l_cmp, l_prof = learned_mode(ctx, launch, args, stream, dist, device, p_model, g_model)
             learned[name] = dict(ms=l_ms, cmp=l_cmp, prof=l_prof,
                                  pair_threshold=None if p_model is None else float(p_model.logit_threshold),
-                                 gate_threshold=None if g_model is None else float(g_model.logit_threshold))
+                                 gate_threshold=None if g_model is None else float(g_model.logit_threshold),
+                                 gate_mlp_layers=None if g_model is None else int(g_model.mlp_layers))
         launch()  # back to the plain graph (the profile below times the plain kernels)
         ctx.batch_status()
 
@@ -790,8 +798,11 @@ def pileup_stream_leg(args, stream, dist, device, local):
         pair = capi.prefilter_load(pair_path) if os.path.exists(pair_path) else None
         gate = capi.gate_load(gate_path) if os.path.exists(gate_path) else None
         forms = [("plain", None, None)]
-        if not args.no_prefilter and (pair is not None or gate is not None):
-            forms.append(("learned", pair, gate))
+        if not args.no_prefilter and gate is not None:
+            # the tracklet gate alone: with the pair prefilter as well the frames keep under 99.5% of their roads
+            forms.append(("learned", None, gate))
+        elif not args.no_prefilter and pair is not None:
+            forms.append(("learned", pair, None))
         steps = max(1, min(args.steps, 3))
         for name, p_model, g_model in forms:
             if p_model is not None:
@@ -885,7 +896,8 @@ def learned_summary(learned, total_events, plain_value, args):
             "road_reproduction": r["cmp"]["road_reproduction"], "plain_roads": r["cmp"]["plain_roads"],
             "learned_roads": r["cmp"]["learned_roads"], "extra_roads": r["cmp"]["extra"], "extra_fakes": r["cmp"]["extra_fakes"],
             "tracklets_kept": r["cmp"]["tracklets_kept"], "cells_kept": r["cmp"]["cells_kept"],
-            "gate_logit_threshold": r["gate_threshold"], "pair_logit_threshold": r["pair_threshold"],
+            "gate_logit_threshold": r["gate_threshold"], "gate_mlp_layers": r["gate_mlp_layers"],
+            "pair_logit_threshold": r["pair_threshold"],
             "kernel_ms": {k: round(t, 4) for k, t in r["prof"]},
         }
     ok = [k for k, v in out.items() if v["road_reproduction"] >= 0.995 and v["extra_roads"] == 0]
@@ -897,9 +909,10 @@ def learned_summary(learned, total_events, plain_value, args):
         "forms": out,
         "checkpoints": {"pair_prefilter": os.path.relpath(args.prefilter, ROOT) if os.path.exists(args.prefilter) else None,
                         "tracklet_gate": os.path.relpath(args.gate, ROOT) if os.path.exists(args.gate) else None},
-        "note": "same resident batch and timing as the plain value; tracklet gate: 8-16-16-1 ReLU MLP on every tracklet "
-                "before the tracklet scan; pair prefilter: 8-64-64-1 GELU MLP on the cell stage's pairs; BF16 MMAs, FP32 "
-                "accumulation",
+        "note": "same resident batch and timing as the plain value; tracklet gate: learned per-layer |dphi| and |dz| "
+                "windows in the tracklet count pass, then an 8-16-16-1 ReLU MLP on the tracklets inside them (of the "
+                "layers in its mlp_layers) before the tracklet scan; gate_windows_only: the same gate's windows with no "
+                "layer scored; pair prefilter: 8-64-64-1 GELU MLP on the cell stage's pairs; BF16 MMAs, FP32 accumulation",
     }
 
 

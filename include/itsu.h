@@ -287,8 +287,9 @@ itsu_status itsu_roads_report(itsu_context *ctx, const itsu_road *roads, const i
 /* ---- launch-shape autotuner for batches (no counterpart in the reference) ----
  * Runs are grouped in multiplicity bands: band = floor(log2(mean clusters per event)). For the
  * band of the last run, itsu_autotune times every candidate launch shape (threads per block of
- * the per-item kernels 128/256/512, resident blocks per SM of the grid-stride kernels 4/8/16, the
- * tracklet candidate index on/off) on the inputs already resident, `repeats` times each, and
+ * the per-item kernels 64/128/256/512, resident blocks per SM of the grid-stride kernels 4/8/16,
+ * the tracklet candidate index off/on/staged, event groups of 0/8/16/32 events) on the inputs
+ * already resident, `repeats` times each, and
  * keeps the fastest for that band; later runs in the band use it. Results never depend on the
  * launch shape. itsu_get_tune / itsu_set_tune read and restore a band's entry (to persist a
  * tuned table). */
@@ -416,11 +417,12 @@ itsu_status itsu_prefilter_gradient(itsu_context *ctx, const float *features, co
  * path spends most of its time. Its features, per tracklet: |dphi| and dphi of its clusters'
  * azimuths about the vertex, the tracklet cut's dz (Tracker.cxx:93-95) and |dz|, the signed
  * curvature of the circle through the vertex and its two clusters, the inner layer, the inner
- * cluster's radius and its slope from the vertex. The gate is a cascade: a learned per-layer
- * window on |dphi| first (dphi_window below), the network on the tracklets inside it. Training
- * labels come from plain runs (1 = the tracklet is part of a found road). A learned run's
- * tracklets, and so its cells and roads, are subsets of the plain run's. Inner clusters with more
- * than 48 tracklets inside the window keep all of them, unscored by the network.
+ * cluster's radius and its slope from the vertex. The gate is a cascade: learned per-layer
+ * windows on |dphi| and |dz| first (dphi_window, dz_window below), the network on the tracklets
+ * inside them (of the layers in mlp_layers). Training labels come from plain runs (1 = the
+ * tracklet is part of a found road). A learned run's tracklets, and so its cells and roads, are
+ * subsets of the plain run's. Inner clusters with more than 48 tracklets inside the windows keep
+ * all of them, unscored by the network.
  * The gate and the pair prefilter are enabled separately; the learned form is either or both. */
 #define ITSU_GATE_HIDDEN 16
 #define ITSU_GATE_PARAMS (ITSU_GATE_HIDDEN * ITSU_MLP_INPUTS + ITSU_GATE_HIDDEN + ITSU_GATE_HIDDEN * ITSU_GATE_HIDDEN + \
@@ -443,6 +445,9 @@ typedef struct itsu_gate_model {
    * infinity: no first stage. */
   float dphi_window[ITSU_TRACKLET_LAYERS];
   float dz_window[ITSU_TRACKLET_LAYERS];
+  /* The layers the network scores: bit l set, inner layer l's tracklets inside the windows are
+   * scored; clear, the windows alone decide for that layer. 0x3f: every layer. */
+  int32_t mlp_layers;
 } itsu_gate_model;
 
 /* Device buffers that itsu_gate_export fills; every array may be NULL (then not written). */

@@ -141,8 +141,8 @@ def _set_windows(m, wphi, wz):
         m.dz_window[layer] = float(wz[layer])
 
 
-@pytest.mark.parametrize("window_q", [None, 0.9])
-def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev, window_q):
+@pytest.mark.parametrize("window_q,mlp_layers", [(None, 0x3f), (0.9, 0x3f), (0.9, 0x2b)])
+def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev, window_q, mlp_layers):
     """Threshold at the 12% quantile of an untrained gate's logits, on central events and a dense
     jet (inner clusters with more than 48 tracklets): the gated run's tracklets are the plain
     tracklets scored at or above it (all of a crowded cluster's), in order; its roads are exactly
@@ -150,7 +150,8 @@ def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev, window_q):
     stage (window_q: per layer, |dphi| and |dz| windows at that quantile of the layer's plain
     tracklets),
     only the tracklets inside the window are scored or kept, and a cluster is crowded by the
-    tracklets inside it."""
+    tracklets inside it. mlp_layers: the layers the network scores (the others keep every tracklet
+    inside the windows)."""
     events = [gen.pbpb_event(s, n_tracks=2500) for s in (66, 67)] + [gen.jet_event(5)]
     b, f, l, r = _plain(ctx, torch_dev, events)
     pkeys, pfake = prefilter.export_roads(ctx, torch_dev)
@@ -163,12 +164,14 @@ def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev, window_q):
         _set_windows(m, wphi, wz)
         inside = prefilter.window_pass(fn, wphi, wz)
         assert 0.7 < inside.mean() < 0.9
+    m.mlp_layers = mlp_layers
     ctx.gate_set_model(m)
     logits = _score(ctx, f, torch_dev)
-    thr = float(np.quantile(logits[inside], 0.12))  # keeps about 88%: some roads keep all 6 tracklets
+    scored = inside & (((mlp_layers >> fn[:, 4].astype(np.int64)) & 1) == 1)
+    thr = float(np.quantile(logits[scored], 0.12))  # keeps about 88%: some roads keep all 6 tracklets
     m.logit_threshold = thr
     ctx.gate_set_model(m)
-    keep = ~(logits < thr) & inside
+    keep = (~(logits < thr) | ~scored) & inside
     # inner clusters with more than 48 tracklets (inside the window) keep all of them
     row = 0
     crowded = 0
@@ -215,7 +218,8 @@ def test_gate_keeps_exactly_what_the_scorer_keeps(ctx, torch_dev, window_q):
 def test_gate_window_alone_keeps_the_tracklets_inside_it(ctx, torch_dev):
     """The cascade's first stage alone (threshold -inf), the windows at each layer's median |dphi|
     and |dz|: the gated run's tracklets are the plain tracklets inside their layer's windows, in
-    order, on central, pp and jet events and across the phi wrap; a zero window keeps none."""
+    order, on central, pp and jet events and across the phi wrap; a zero window keeps only exact
+    zeros, and the other layers' windows do not change."""
     events = [gen.pbpb_event(s, n_tracks=2000) for s in (68, 69)] + [gen.pp_event(70), gen.jet_event(5)]
     b, f, _, _ = _plain(ctx, torch_dev, events)
     plain = [ctx.results(e) for e in range(len(events))]
@@ -250,14 +254,21 @@ def test_gate_window_alone_keeps_the_tracklets_inside_it(ctx, torch_dev):
                 kept = pt[inside[row:row + len(pt)]]
                 row += len(pt)
                 assert np.array_equal(got["tracklets"][layer].view(np.uint8), kept.view(np.uint8)), (e, layer)
-        m.dphi_window[2] = 0.0
-        m.dz_window[4] = 0.0
+        # zero windows keep only the tracklets at exactly zero |dphi| (layer 2) or |dz| (layer 4)
+        wphi[2], wz[4] = 0.0, 0.0
+        _set_windows(m, wphi, wz)
+        inside = prefilter.window_pass(fn, wphi, wz)
         ctx.gate_set_model(m)
         ctx.batch_run(b.batch)
+        row = 0
         for e in range(len(events)):
             got = ctx.results(e)["tracklets"]
-            assert len(got[2]) == 0 and len(got[4]) == 0, e
-            assert np.array_equal(got[3].view(np.uint8), layer3[e].view(np.uint8)), e  # the other layers' windows stay
+            for layer in range(6):
+                pt = plain[e]["tracklets"][layer]
+                kept = pt[inside[row:row + len(pt)]]
+                row += len(pt)
+                assert np.array_equal(got[layer].view(np.uint8), kept.view(np.uint8)), (e, layer)
+            assert np.array_equal(got[3].view(np.uint8), layer3[e].view(np.uint8)), e
         assert sum(len(t) for t in layer3) > 0
     finally:
         prefilter.set_learned(ctx, False, False)

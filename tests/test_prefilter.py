@@ -138,7 +138,7 @@ def test_compare_roads():
 
 
 def test_gate_model_layout_and_init():
-    assert ctypes.sizeof(capi.GateModel) == 4 * (capi.GATE_PARAMS + 2 * 8 + 1 + 12)
+    assert ctypes.sizeof(capi.GateModel) == 4 * (capi.GATE_PARAMS + 2 * 8 + 1 + 12 + 1)
     assert capi.GATE_PARAMS == 433
     assert ctypes.sizeof(capi.GateSamples) == 56
     a, b, c = capi.gate_init(1), capi.gate_init(1), capi.gate_init(2)
@@ -148,6 +148,7 @@ def test_gate_model_layout_and_init():
     assert np.all(p[128:144] == 0) and a.logit_threshold == 0.0
     assert list(a.dphi_window) == [np.float32(np.pi)] * 6  # no first stage until trained
     assert list(a.dz_window) == [np.inf] * 6
+    assert a.mlp_layers == 0x3f
 
 
 def test_gate_windows_fit_the_road_tracklets():
@@ -186,6 +187,7 @@ def test_gate_checkpoint_round_trip_and_kinds(tmp_path):
     g.logit_threshold = -2.5
     g.dphi_window[3] = 0.0625
     g.dz_window[1] = 0.03125
+    g.mlp_layers = 0x2d
     path = str(tmp_path / "g.itsugate")
     capi.gate_save(g, path)
     assert bytes(capi.gate_load(path)) == bytes(g)

@@ -2033,7 +2033,7 @@ struct NetOf<itsu_gate_model> {
   using Device = itsu::GateDevice;
   static constexpr int kHidden = ITSU_GATE_HIDDEN;
   static constexpr int kParams = ITSU_GATE_PARAMS;
-  static constexpr char kMagic[8] = {'I', 'T', 'S', 'U', 'G', 'A', 'T', '3'};
+  static constexpr char kMagic[8] = {'I', 'T', 'S', 'U', 'G', 'A', 'T', '4'};
   static constexpr const char *kName = "gate";
   static Model *&master(itsu_context *c) { return c->d_gate_master; }
   static Device *&device(itsu_context *c) { return c->d_gate; }
@@ -2114,6 +2114,7 @@ void net_init(Model *model, uint64_t seed)
       model->dphi_window[l] = 3.14159265358979323846f;
       model->dz_window[l] = HUGE_VALF;
     }
+    model->mlp_layers = (1 << ITSU_TRACKLET_LAYERS) - 1;
   }
 }
 
@@ -2186,6 +2187,10 @@ itsu_status net_set_model(itsu_context *ctx, const Model *model, const char *wha
         return fail(ctx, ITSU_ERR_INVALID, "%s: window of layer %d (dphi %g, dz %g) is not a window", what, l,
                     (double)model->dphi_window[l], (double)model->dz_window[l]);
       }
+    }
+    if (model->mlp_layers < 0 || model->mlp_layers >= (1 << ITSU_TRACKLET_LAYERS)) {
+      return fail(ctx, ITSU_ERR_INVALID, "%s: mlp_layers 0x%x names layers beyond %d", what, (unsigned)model->mlp_layers,
+                  ITSU_TRACKLET_LAYERS - 1);
     }
   }
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -726,25 +726,33 @@ struct TrackletProbe {
   float phi1, tan_lambda, max_dz;
   const float4 *xyzr;  // next layer
   const float *phi;
+  GateWindow win;      // kGate: the learned form's first-stage windows
 
-  // Tracker.cxx:93-100 for a next-layer cluster at z2, r2, phi2
+  // Tracker.cxx:93-100 for a next-layer cluster at z2, r2, phi2; kGate: and inside the windows
+  template <bool kGate>
   __device__ __forceinline__ bool pass(float z2, float r2, float phi2) const
   {
     const float delta_z = fabsf(tan_lambda * (r2 - c.w) + c.z - z2);
     const float delta_phi = fabsf(phi1 - phi2);
-    return delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
+    const bool cut = delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
+    if constexpr (kGate) {
+      return cut && gate_window_pass(win, make_float4(0.0f, 0.0f, z2, r2), phi2);
+    }
+    return cut;
   }
 
+  template <bool kGate>
   __device__ __forceinline__ bool pass(int j) const
   {
     const float4 d = xyzr[j];
-    return pass(d.z, d.w, phi[j]);
+    return pass<kGate>(d.z, d.w, phi[j]);
   }
 };
 
 // win_row, win_rows: the phi rows whose candidates are walked (win_rows = kPhiBins: every row); of
-// the other rows only the bound candidate is tested.
-template <int kWords, typename OnPass>
+// the other rows only the bound candidate is tested (the first cluster of the first bin after the
+// row's last z column: past empty bins it can lie in any later row).
+template <int kWords, bool kGate, typename OnPass>
 __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next, int4 rect, int layer, const TrackletProbe &probe,
                                                 bool prune, float zlo, float zhi, const float4 *zs, int zs_off,
                                                 int win_row, int win_rows, OnPass &&on_pass)
@@ -791,7 +799,7 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
           if (!(q.x <= zhi)) {
             break;
           }
-          if (probe.pass(q.x, q.y, q.z)) {
+          if (probe.pass<kGate>(q.x, q.y, q.z)) {
             const int pos = __float_as_int(q.w) - k0;
             const unsigned long long bit = 1ull << (pos & 63);
 #pragma unroll
@@ -815,14 +823,14 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
       // bins), the candidate's z exceeds zhi and it fails the Δz cut: it is not read.
       const int x = table[max_bin];
       const bool beyond = rect.z + 1 < kZBins && rect.z + 1 > zb_top && table[max_bin + 1] > x;
-      if (!beyond && x < n_next && probe.pass(x)) {
+      if (!beyond && x < n_next && probe.pass<kGate>(x)) {
         on_pass(x);
       }
     } else {
       const int first_row = table[first_bin];
       const int last_row = min(table[max_bin], n_next - 1);  // inclusive bound, P1
       for (int j = walk_row ? first_row : last_row; j <= last_row; ++j) {
-        if (probe.pass(j) && (walk_row || j == table[max_bin])) {
+        if (probe.pass<kGate>(j) && (walk_row || j == table[max_bin])) {
           on_pass(j);
         }
       }
@@ -834,7 +842,6 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
 // stage, and the probe, window and pruning bounds of its candidate walk.
 struct InnerCluster {
   bool walk;
-  GateWindow win;  // the learned form's first-stage windows for its tracklets
   int win_row, win_rows;  // the phi rows its |dphi| window reaches (win_rows = kPhiBins: every row)
   int seg, e, layer;
   int4 rect;
@@ -867,8 +874,11 @@ __device__ __forceinline__ void window_rows(float phi, float half_width, int *fi
 // row's bound candidate (P1), which can lie in the next row; the pruned columns take the narrower
 // z range of the |dz| window (widened by 1e-3 cm). In a regular layer every cluster sits in its
 // own bin, so the walk still meets every plain candidate inside the windows, in the plain order;
-// other layers are walked whole. Every pass is then tested against the windows themselves
+// other layers are walked whole. Every candidate's cut includes the windows themselves
 // (gate_window_pass): the gated tracklets are exactly the plain tracklets inside the windows.
+// kGate: the learned form with a tracklet gate (a.gate set); the plain form's instantiation has
+// none of the windows' code.
+template <bool kGate>
 __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
 {
   InnerCluster s;
@@ -898,10 +908,10 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
   s.words = a.seg_regular[next_seg];  // 0: not regular, else the mask words its largest bin needs
   s.win_row = 0;
   s.win_rows = kPhiBins;
-  if (a.gate) {
-    s.win = gate_window(*a.gate, s.layer, s.probe.c, s.probe.phi1, vz);
-    if (s.words != 0 && s.win.dphi + 1e-3f < kPhiCoordinateCut) {  // a wider window narrows nothing
-      window_rows(s.probe.phi1, s.win.dphi + 1e-3f, &s.win_row, &s.win_rows);
+  if constexpr (kGate) {
+    s.probe.win = gate_window(*a.gate, s.layer, s.probe.c, s.probe.phi1, vz);
+    if (s.words != 0 && s.probe.win.dphi + 1e-3f < kPhiCoordinateCut) {  // a wider window narrows nothing
+      window_rows(s.probe.phi1, s.probe.win.dphi + 1e-3f, &s.win_row, &s.win_rows);
     }
   }
   s.prune = a.prune_tracklets && s.words != 0;
@@ -910,7 +920,7 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
     const float2 rr = a.seg_rrange[next_seg];
     const float p1 = s.probe.tan_lambda * (rr.x - s.probe.c.w) + s.probe.c.z;
     const float p2 = s.probe.tan_lambda * (rr.y - s.probe.c.w) + s.probe.c.z;
-    const float half = a.gate && s.words != 0 ? fminf(s.probe.max_dz, s.win.dz + 1e-3f) : s.probe.max_dz;
+    const float half = kGate ? fminf(s.probe.max_dz, s.probe.win.dz + 1e-3f) : s.probe.max_dz;
     s.zlo = fminf(p1, p2) - half - 1e-3f;
     s.zhi = fmaxf(p1, p2) + half + 1e-3f;
     s.prune = isfinite(s.zlo) && isfinite(s.zhi);
@@ -922,21 +932,21 @@ __device__ __forceinline__ InnerCluster inner_cluster(const Arena &a, int64_t i)
 
 // staged: the block's copy in shared memory of the next layer's z-sorted entries from staged_off on
 // (null: read them from global memory)
-template <typename OnPass>
+template <bool kGate, typename OnPass>
 __device__ __forceinline__ void walk_inner(const Arena &a, const InnerCluster &s, OnPass &&on_pass,
                                            const float4 *staged = nullptr, int staged_off = 0)
 {
   const float4 *zs = staged ? staged : a.zs + s.next_begin;
   const int off = staged ? staged_off : 0;
   if (s.words <= 1) {  // unpruned, or bins of at most 64 clusters
-    walk_candidates<1>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row, s.win_rows,
-                                     on_pass);
+    walk_candidates<1, kGate>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row,
+                              s.win_rows, on_pass);
   } else if (s.words == 2) {
-    walk_candidates<2>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row, s.win_rows,
-                                     on_pass);
+    walk_candidates<2, kGate>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row,
+                              s.win_rows, on_pass);
   } else {
-    walk_candidates<kPruneWords>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off, s.win_row, s.win_rows,
-                                     on_pass);
+    walk_candidates<kPruneWords, kGate>(s.table, s.n_next, s.rect, s.layer, s.probe, s.prune, s.zlo, s.zhi, zs, off,
+                                        s.win_row, s.win_rows, on_pass);
   }
 }
 
@@ -1037,12 +1047,17 @@ __device__ int stage_rows(const Arena &a, const InnerCluster &s, float4 *stage, 
   return s_k0;
 }
 
+constexpr int kGateCountThreads = 256;
+
 // Count pass, one thread per inner cluster: the number of tracklets, and the outer clusters of
 // the first kTrackletSlots of them in emission order. kStaged: the block's walks read the next
 // layer's z-sorted entries from a shared-memory copy made by one bulk copy (stage_rows), where
-// they allow it.
-template <bool kStaged>
-__global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
+// they allow it. kGate: the learned form's first stage (inner_cluster), at most 256 threads per
+// block and 48 registers (5 blocks per SM; measured 0.39 vs 0.43 ms per 128 events at 56). The
+// plain instantiation's explicit one-block minimum gives it 54 registers and no stack (40 and a
+// 24-byte stack without: 0.06 ms slower per 128 events).
+template <bool kStaged, bool kGate>
+__global__ void __launch_bounds__(kGate ? kGateCountThreads : kMaxThreads, kGate ? 5 : 1) k_tracklets_count(Arena a)
 {
   extern __shared__ float4 stage[];  // kStaged: kStageEntries entries
   __shared__ uint64_t bar;
@@ -1052,7 +1067,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
   InnerCluster s;
   s.walk = false;
   if (valid) {
-    s = inner_cluster(a, i);
+    s = inner_cluster<kGate>(a, i);
   }
   const float4 *staged = nullptr;
   int staged_off = 0;
@@ -1062,13 +1077,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_count(Arena a)
     staged = staged_off >= 0 ? stage : nullptr;
   }
   if (s.walk && !(a.status->flags & kFlagTimeout)) {
-    const bool windowed = a.gate != nullptr;
-    walk_inner(
+    walk_inner<kGate>(
         a, s,
         [&](int j) {
-          if (windowed && !gate_window_pass(s.win, s.probe.xyzr[j], s.probe.phi[j])) {
-            return;  // learned form: outside the gate's first stage
-          }
           if (count < kTrackletSlots) {
             a.trk_slots[count * a.slot_stride + i] = j;
           }
@@ -1137,7 +1148,8 @@ __device__ __forceinline__ int owner_of(int excl, int t)
 // keeps its tracklet), moves the kept slots to the front in their order and lowers the cluster's
 // count and its scan tile's sum by the dropped ones. The write pass then writes the kept tracklets
 // in emission order, as in the plain form. Inner clusters with more than kTrackletSlots tracklets
-// keep all of them, unscored (the crowded pass writes them).
+// keep all of them, unscored (the crowded pass writes them), and so do those of the layers the
+// network does not score (the model's mlp_layers).
 //
 // Per warp and group of 32 clusters, the flattened tracklets' owners and ranks are listed once in
 // shared memory (each cluster's lane writes its own entries), and each cluster's gate state (what
@@ -1152,98 +1164,131 @@ struct __align__(16) GateLane {
   int32_t pad_;
 };
 
-__global__ void __launch_bounds__(kGateThreads) k_tracklets_gate(Arena a)
+// The gate pass's per-warp shared memory.
+struct GateShared {
+  __align__(16) __nv_bfloat16 rows[kGateWarps][32][kMlpIn];
+  unsigned long long keep[kGateWarps][32];
+  uint16_t owner_rank[kGateWarps][32 * kTrackletSlots];  // owner lane * 64 + rank
+  GateLane lanes[kGateWarps][32];
+};
+
+// One warp group of k_tracklets_gate: the inner clusters base .. base + 31 of which those in
+// [start, end) take part (event e).
+__device__ __forceinline__ void gate_group(const Arena &a, const GateSmem &net, const GateRegs &R, GateShared &sh, int warp,
+                                           int64_t base, int64_t start, int64_t end, int e)
 {
-  __shared__ GateSmem net;
-  __shared__ __align__(16) __nv_bfloat16 rows[kGateWarps][32][kMlpIn];
-  __shared__ unsigned long long keep[kGateWarps][32];
-  __shared__ uint16_t owner_rank[kGateWarps][32 * kTrackletSlots];  // owner lane * 64 + rank
-  __shared__ GateLane lanes[kGateWarps][32];
-  load_mlp(net, *a.gate);
-  __syncthreads();
-  const GateRegs R = gate_regs(net);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-  const int64_t n = a.n_clusters;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 32; base < n; base += warps * 32) {
-    const int64_t i = base + lane;
-    int count = 0;
-    if (i < n) {
-      count = a.trk_count[i];
-      if (count > 0 && count <= kTrackletSlots) {
-        const int seg = a.clu_seg[i], e = seg / ITSU_LAYERS;
-        GateLane &s = lanes[warp][lane];
-        s.g = gate_inner(seg % ITSU_LAYERS, a.xyzr[i], a.phi[i], a.vtx[3 * e], a.vtx[3 * e + 1], a.vtx[3 * e + 2]);
-        s.next = a.layer_off[seg + 1];
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  __nv_bfloat16 (&rows)[32][kMlpIn] = sh.rows[warp];
+  unsigned long long (&keep)[32] = sh.keep[warp];
+  uint16_t (&owner_rank)[32 * kTrackletSlots] = sh.owner_rank[warp];
+  GateLane (&lanes)[32] = sh.lanes[warp];
+  const int64_t i = base + lane;
+  int count = 0;
+  bool scored = false;  // by the network: in the range, and not crowded
+  if (i >= start && i < end) {
+    count = a.trk_count[i];
+    if (count > 0 && count <= kTrackletSlots) {
+      const int seg = a.clu_seg[i];
+      scored = true;
+      GateLane &s = lanes[lane];
+      s.g = gate_inner(seg % ITSU_LAYERS, a.xyzr[i], a.phi[i], a.vtx[3 * e], a.vtx[3 * e + 1], a.vtx[3 * e + 2]);
+      s.next = a.layer_off[seg + 1];
+    }
+  }
+  const int mine = scored ? count : 0;
+  keep[lane] = 0ull;
+  int total = 0;
+  const int excl = warp_exclusive_sum(mine, total);
+  for (int r = 0; r < mine; ++r) {
+    owner_rank[excl + r] = (uint16_t)(lane * 64 + r);
+  }
+  __syncwarp();
+  for (int p0 = 0; p0 < total; p0 += 32) {
+    const int p = p0 + lane;
+    float f[kMlpIn];
+    if (p < total) {
+      const int orank = owner_rank[p], owner = orank >> 6, rank = orank & 63;
+      const GateLane &o = lanes[owner];
+      const int64_t j = o.next + a.trk_slots[(int64_t)rank * a.slot_stride + base + owner];
+      gate_features(o.g, a.xyzr[j], a.phi[j], f);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kMlpIn; ++k) {
+        f[k] = net.mean[k];
       }
     }
-    const bool scored = count <= kTrackletSlots;
-    const int mine = scored ? count : 0;
-    keep[warp][lane] = 0ull;
-    int total = 0;
-    const int excl = warp_exclusive_sum(mine, total);
-    for (int r = 0; r < mine; ++r) {
-      owner_rank[warp][excl + r] = (uint16_t)(lane * 64 + r);
-    }
+    *reinterpret_cast<uint4 *>(&rows[lane][0]) = gate_row(net.mean, net.inv_std, f);
     __syncwarp();
-    for (int p0 = 0; p0 < total; p0 += 32) {
-      const int p = p0 + lane;
-      float f[kMlpIn];
-      if (p < total) {
-        const int orank = owner_rank[warp][p], owner = orank >> 6, rank = orank & 63;
-        const GateLane &o = lanes[warp][owner];
-        const int64_t j = o.next + a.trk_slots[(int64_t)rank * a.slot_stride + base + owner];
-        gate_features(o.g, a.xyzr[j], a.phi[j], f);
-      } else {
 #pragma unroll
-        for (int k = 0; k < kMlpIn; ++k) {
-          f[k] = net.mean[k];
-        }
-      }
-      *reinterpret_cast<uint4 *>(&rows[warp][lane][0]) = gate_row(net.mean, net.inv_std, f);
-      __syncwarp();
+    for (int mt = 0; mt < 2; ++mt) {
+      float lo, hi;
+      gate_forward_m16(R, rows, mt, lo, hi);
+      if (t == 0) {  // this lane holds the logits of rows 16 mt + g and 16 mt + g + 8
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-        float lo, hi;
-        gate_forward_m16(R, rows[warp], mt, lo, hi);
-        if (t == 0) {  // this lane holds the logits of rows 16 mt + g and 16 mt + g + 8
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int q = p0 + mt * 16 + g + 8 * h;
-            const float logit = h ? hi : lo;
-            if (q < total && !(logit < net.threshold)) {
-              const int orank = owner_rank[warp][q];
-              atomicOr(&keep[warp][orank >> 6], 1ull << (orank & 63));
-            }
+        for (int h = 0; h < 2; ++h) {
+          const int q = p0 + mt * 16 + g + 8 * h;
+          const float logit = h ? hi : lo;
+          if (q < total && !(logit < net.threshold)) {
+            const int orank = owner_rank[q];
+            atomicOr(&keep[orank >> 6], 1ull << (orank & 63));
           }
         }
       }
-      __syncwarp();  // the rows are refilled for the next tile
     }
-    // kept slots to the front, in order (coalesced across the warp's clusters, slot by slot)
-    const unsigned long long m = keep[warp][lane];
-    const int scan_to = __reduce_max_sync(0xffffffffu, (unsigned)mine);
-    int kept = 0;
-    for (int q = 0; q < scan_to; ++q) {
-      if (q < count && ((m >> q) & 1ull)) {
-        if (kept != q) {
-          a.trk_slots[(int64_t)kept * a.slot_stride + i] = a.trk_slots[(int64_t)q * a.slot_stride + i];
-        }
-        ++kept;
+    __syncwarp();  // the rows are refilled for the next tile
+  }
+  // kept slots to the front, in order (coalesced across the warp's clusters, slot by slot)
+  const unsigned long long m = keep[lane];
+  const int scan_to = __reduce_max_sync(0xffffffffu, (unsigned)mine);
+  int kept = 0;
+  for (int q = 0; q < scan_to; ++q) {
+    if (q < count && ((m >> q) & 1ull)) {
+      if (kept != q) {
+        a.trk_slots[(int64_t)kept * a.slot_stride + i] = a.trk_slots[(int64_t)q * a.slot_stride + i];
+      }
+      ++kept;
+    }
+  }
+  int dropped = 0;
+  if (scored) {
+    a.trk_count[i] = kept;
+    dropped = count - kept;
+  }
+  // the warp's 32 clusters lie in one scan tile (the count pass added their tracklets to its sum)
+  const int warp_dropped = (int)__reduce_add_sync(0xffffffffu, (unsigned)dropped);
+  if (lane == 0 && warp_dropped != 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&a.scan_partials[base / kScanTile]),
+              (unsigned long long)(-(int64_t)warp_dropped));
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kGateThreads) k_tracklets_gate(Arena a)
+{
+  __shared__ GateSmem net;
+  __shared__ GateShared sh;
+  load_mlp(net, *a.gate);
+  __syncthreads();
+  const GateRegs R = gate_regs(net);
+  const int warp = threadIdx.x >> 5;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t first_warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  for (int e = blockIdx.y; e < a.n_events; e += gridDim.y) {
+    for (int l0 = 0; l0 < ITSU_TRACKLET_LAYERS; ++l0) {
+      if (!((net.layers >> l0) & 1u) || (l0 > 0 && ((net.layers >> (l0 - 1)) & 1u))) {
+        continue;  // not the first layer of a run of scored layers
+      }
+      int l1 = l0;
+      while (l1 + 1 < ITSU_TRACKLET_LAYERS && ((net.layers >> (l1 + 1)) & 1u)) {
+        ++l1;
+      }
+      // the inner clusters of layers l0..l1 of event e, in warp groups aligned to 32 (so that each
+      // group lies in one scan tile; a group's lanes outside the range take no part)
+      const int64_t start = a.layer_off[e * ITSU_LAYERS + l0], end = a.layer_off[e * ITSU_LAYERS + l1 + 1];
+      for (int64_t base = (start & ~(int64_t)31) + first_warp * 32; base < end; base += warps * 32) {
+        gate_group(a, net, R, sh, warp, base, start, end, e);
       }
     }
-    int dropped = 0;
-    if (i < n && scored && count > 0) {
-      a.trk_count[i] = kept;
-      dropped = count - kept;
-    }
-    // the warp's 32 clusters lie in one scan tile (the count pass added their tracklets to its sum)
-    const int warp_dropped = (int)__reduce_add_sync(0xffffffffu, (unsigned)dropped);
-    if (lane == 0 && warp_dropped != 0) {
-      atomicAdd(reinterpret_cast<unsigned long long *>(&a.scan_partials[base / kScanTile]),
-                (unsigned long long)(-(int64_t)warp_dropped));
-    }
-    __syncwarp();
   }
 }
 
@@ -1309,6 +1354,7 @@ __global__ void __launch_bounds__(kMaxThreads, 2) k_tracklets_write(Arena a, int
 
 // Write pass, part 2: the inner clusters with more than kTrackletSlots tracklets (listed by the
 // count pass, a handful per batch) walk their candidates again and write their tracklets in order.
+template <bool kGate>
 __global__ void __launch_bounds__(kMaxThreads) k_tracklets_crowded(Arena a)
 {
   if (capacity_failed(a.status)) {
@@ -1317,14 +1363,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_crowded(Arena a)
   const int64_t listed = min(a.status->trk_crowded, (int64_t)a.n_clusters);
   for (int64_t q = global_thread(); q < listed; q += grid_threads()) {
     const int64_t i = a.clu_crowded[q];
-    const InnerCluster s = inner_cluster(a, i);
+    const InnerCluster s = inner_cluster<kGate>(a, i);
     int out = a.trk_off[i];
-    const bool windowed = a.gate != nullptr;  // the count pass's first-stage test, the same way
-    walk_inner(a, s, [&](int j) {
-      if (!windowed || gate_window_pass(s.win, s.probe.xyzr[j], s.probe.phi[j])) {
-        write_tracklet(a, out++, i, s.next_begin + j, s.seg);
-      }
-    });
+    walk_inner<kGate>(a, s, [&](int j) { write_tracklet(a, out++, i, s.next_begin + j, s.seg); });
   }
 }
 
@@ -2046,20 +2087,34 @@ void step_tracklets_count(const Arena &a, const Launch &l)
     return;
   }
   const int64_t blocks = (a.n_clusters + l.block - 1) / l.block;
-  if (blocks > 0 && a.prune_tracklets == 2) {  // the staged walk (tuning knob; results are identical)
-    k_tracklets_count<true><<<(unsigned)blocks, l.block, kStageEntries * sizeof(float4), l.stream>>>(a);
-  } else if (blocks > 0) {
-    k_tracklets_count<false><<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
+  if (blocks <= 0) {
+    return;
+  }
+  const size_t stage_bytes = kStageEntries * sizeof(float4);
+  // the learned form's count pass takes at most kGateCountThreads threads per block (any whole
+  // warps give the same results)
+  const int gate_block = std::min(l.block, kGateCountThreads);
+  const unsigned gate_blocks = (unsigned)((a.n_clusters + gate_block - 1) / gate_block);
+  if (a.prune_tracklets == 2) {  // the staged walk (tuning knob; results are identical)
+    if (a.gate) {
+      k_tracklets_count<true, true><<<gate_blocks, gate_block, stage_bytes, l.stream>>>(a);
+    } else {
+      k_tracklets_count<true, false><<<(unsigned)blocks, l.block, stage_bytes, l.stream>>>(a);
+    }
+  } else if (a.gate) {
+    k_tracklets_count<false, true><<<gate_blocks, gate_block, 0, l.stream>>>(a);
+  } else {
+    k_tracklets_count<false, false><<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
   }
 }
 
 // Launches only in the learned form with the tracklet gate (a.gate set).
 void step_tracklets_gate(const Arena &a, const Launch &l)
 {
-  if (a.gate && a.n_clusters > 0) {
-    const int64_t tiles = (a.n_clusters + 31) / 32;
-    const int64_t blocks = std::min<int64_t>((tiles + kGateThreads / 32 - 1) / (kGateThreads / 32), (int64_t)l.num_sms * 8);
-    k_tracklets_gate<<<(unsigned)blocks, kGateThreads, 0, l.stream>>>(a);
+  if (a.gate && a.n_clusters > 0 && a.n_events > 0) {
+    const int rows = std::min(a.n_events, 65535);
+    const int per_event = std::max(1, (l.num_sms * 8 + rows - 1) / rows);
+    k_tracklets_gate<<<dim3((unsigned)per_event, (unsigned)rows), kGateThreads, 0, l.stream>>>(a);
   }
 }
 
@@ -2079,7 +2134,14 @@ void step_tracklets_write(const Arena &a, const Launch &l)
   }
 }
 
-void step_tracklets_crowded(const Arena &a, const Launch &l) { k_tracklets_crowded<<<l.num_sms, 128, 0, l.stream>>>(a); }
+void step_tracklets_crowded(const Arena &a, const Launch &l)
+{
+  if (a.gate) {
+    k_tracklets_crowded<true><<<l.num_sms, 128, 0, l.stream>>>(a);
+  } else {
+    k_tracklets_crowded<false><<<l.num_sms, 128, 0, l.stream>>>(a);
+  }
+}
 
 void step_tracklet_segments(const Arena &a, const Launch &l)
 {

@@ -73,6 +73,7 @@ struct MlpDeviceT {
   float inv_std[kMlpIn];
   float window[6];     // the tracklet gate's per-layer |dphi| window (the pair prefilter: pi, unused)
   float dz_window[6];  // and its |dz| window (the pair prefilter: infinity, unused)
+  uint32_t mlp_layers; // the gate: bit l, the network scores inner layer l (the pair prefilter: unused)
 };
 
 // A network staged in shared memory in MMA-friendly, zero-padded form.
@@ -88,6 +89,7 @@ struct __align__(16) MlpSmemT {
   float threshold;
   float mean[kMlpIn];
   float inv_std[kMlpIn];
+  uint32_t layers;  // the gate: the inner layers the network scores (bit l)
 };
 
 using MlpSmem = MlpSmemT<kMlpHidden>;
@@ -122,6 +124,7 @@ __device__ __forceinline__ void load_mlp(MlpSmemT<H> &s, const MlpDeviceT<H> &g)
   if (threadIdx.x == 0) {
     s.b3 = g.b3;
     s.threshold = g.threshold;
+    s.layers = g.mlp_layers;
   }
 }
 

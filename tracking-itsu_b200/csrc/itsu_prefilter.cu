@@ -60,7 +60,8 @@ __device__ __forceinline__ void publish_param(MlpDeviceT<H> *model, int i, float
 
 // window: the gate's per-layer |dphi| window in the master (null for the pair prefilter: pi).
 template <int H>
-__global__ void k_mlp_publish(const float *master, const float *window, const float *dz_window, MlpDeviceT<H> *model)
+__global__ void k_mlp_publish(const float *master, const float *window, const float *dz_window, const int32_t *mlp_layers,
+                              MlpDeviceT<H> *model)
 {
   constexpr int P = MlpShape<H>::kParams;
   for (int i = threadIdx.x; i < P; i += blockDim.x) {
@@ -76,6 +77,7 @@ __global__ void k_mlp_publish(const float *master, const float *window, const fl
   }
   if (threadIdx.x == 0) {
     model->threshold = master[P + 2 * kMlpIn];
+    model->mlp_layers = mlp_layers ? (uint32_t)*mlp_layers : 0x3fu;
   }
 }
 
@@ -533,7 +535,7 @@ void gradient_net(const MlpDeviceT<H> *model, const float *features, const uint8
 }  // namespace
 
 static_assert(sizeof(itsu_prefilter_model) == sizeof(float) * (kMlpParams + 2 * kMlpIn + 1), "pair model layout");
-static_assert(sizeof(itsu_gate_model) == sizeof(float) * (kGateParams + 2 * kMlpIn + 1 + 2 * ITSU_TRACKLET_LAYERS), "gate model layout");
+static_assert(sizeof(itsu_gate_model) == sizeof(float) * (kGateParams + 2 * kMlpIn + 1 + 2 * ITSU_TRACKLET_LAYERS + 1), "gate model layout");
 
 size_t mlp_device_bytes() { return sizeof(MlpDevice); }
 size_t gate_device_bytes() { return sizeof(GateDevice); }
@@ -542,12 +544,13 @@ int mlp_max_gradient_blocks() { return kMaxGradBlocks; }
 
 void launch_mlp_publish(const itsu_prefilter_model *master, MlpDevice *model, cudaStream_t stream)
 {
-  k_mlp_publish<kMlpHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], nullptr, nullptr, model);
+  k_mlp_publish<kMlpHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], nullptr, nullptr, nullptr, model);
 }
 
 void launch_mlp_publish(const itsu_gate_model *master, GateDevice *model, cudaStream_t stream)
 {
-  k_mlp_publish<kGateHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], &master->dphi_window[0], &master->dz_window[0], model);
+  k_mlp_publish<kGateHidden><<<1, 512, 0, stream>>>(&master->w1[0][0], &master->dphi_window[0], &master->dz_window[0],
+                                                     &master->mlp_layers, model);
 }
 
 void launch_prefilter_export(const Arena &a, const itsu_prefilter_samples &out, int num_sms, cudaStream_t stream)

@@ -130,7 +130,8 @@ class GateModel(ctypes.Structure):
     """itsu_gate_model: the tracklet gate (per-layer |dphi| and |dz| windows, then 8 -> 16 -> 16 -> 1,
     ReLU); same field order."""
     _fields_ = _model_fields(GATE_HIDDEN) + [("dphi_window", ctypes.c_float * TRACKLET_LAYERS),
-                                              ("dz_window", ctypes.c_float * TRACKLET_LAYERS)]
+                                              ("dz_window", ctypes.c_float * TRACKLET_LAYERS),
+                                              ("mlp_layers", ctypes.c_int32)]
     N_PARAMS = GATE_PARAMS
     params = PrefilterModel.params
     arrays = PrefilterModel.arrays

@@ -1,11 +1,13 @@
 """The learned form's two networks: training pipelines, threshold calibration, evaluation, and
 numpy restatements of their arithmetic (the tests' references).
 
-The tracklet gate (include/itsu.h, itsu_gate_model; 8 -> 16 -> 16 -> 1, ReLU) scores every
-tracklet before the tracklet scan; a tracklet whose logit is below the gate's threshold is not
-kept, so the cell stage enumerates only pairs of kept tracklets. It is trained on one sample per
-tracklet of plain runs (label 1: a found road uses it) and calibrated on road reproduction (a
-road survives iff its 6 tracklets are kept): ``python -m itsu.prefilter --model gate``.
+The tracklet gate (include/itsu.h, itsu_gate_model) is a cascade before the tracklet scan:
+learned per-layer windows on |dphi| and |dz| (fit_windows), tested in the tracklet count pass,
+then a network (8 -> 16 -> 16 -> 1, ReLU) on the tracklets inside them; a tracklet outside a
+window or whose logit is below the gate's threshold is not kept, so the cell stage enumerates only
+pairs of kept tracklets. It is trained on one sample per tracklet of plain runs (label 1: a found
+road uses it) and calibrated on road reproduction (a road survives iff its 6 tracklets are kept):
+``python -m itsu.prefilter --model gate``.
 
 The pair prefilter (itsu_prefilter_model; 8 -> 64 -> 64 -> 1, GELU) scores, inside the cell stage,
 each tracklet pair that passes the exact cell cuts; a pair whose logit is below the model's
@@ -449,10 +451,11 @@ def ctx_has_gate(ctx) -> bool:
 PHI_CUT = 0.3  # the tracklet cut's phi window (the reference's kPhiCoordinateCut, Constants.h)
 
 
-def fit_windows(features: np.ndarray, road_rows: np.ndarray, margin: float = 1.25) -> tuple:
-    """The cascade's first stage: per inner layer, `margin` times the largest |dphi| (feature 0) and
-    |dz| (feature 2) of the tracklets on the training roads; the |dphi| window at most the tracklet
-    cut's own (a layer without a road tracklet keeps no window). Returns (dphi, dz) windows."""
+def fit_windows(features: np.ndarray, road_rows: np.ndarray, margin: float = 1.25, quantile: float = 1.0) -> tuple:
+    """The cascade's first stage: per inner layer, `margin` times the `quantile` (1: the largest) of
+    |dphi| (feature 0) and of |dz| (feature 2) over the tracklets on the training roads; the |dphi|
+    window at most the tracklet cut's own (a layer without a road tracklet keeps no window).
+    Returns (dphi, dz) windows."""
     rows = np.unique(road_rows[road_rows >= 0])
     layer = features[rows, 4]
     wphi = np.full(6, PHI_CUT, np.float32)
@@ -463,9 +466,9 @@ def fit_windows(features: np.ndarray, road_rows: np.ndarray, margin: float = 1.2
         dz = features[rows[on], 2].astype(np.float64)
         dphi, dz = dphi[np.isfinite(dphi)], dz[np.isfinite(dz)]
         if len(dphi):
-            wphi[l] = np.float32(min(PHI_CUT, margin * float(dphi.max())))
+            wphi[l] = np.float32(min(PHI_CUT, margin * float(np.quantile(dphi, quantile))))
         if len(dz):
-            wz[l] = np.float32(margin * float(dz.max()))
+            wz[l] = np.float32(margin * float(np.quantile(dz, quantile)))
     return wphi, wz
 
 
@@ -479,52 +482,74 @@ def window_pass(features: np.ndarray, dphi_window: np.ndarray, dz_window: np.nda
     return ok
 
 
-def train_gate(ctx, data: dict, device, seed: int = 1, target: float = 0.999, log=print, window_margin: float = 1.25,
-               **train_kw) -> tuple:
+def per_layer_fractions(layer: np.ndarray, inside: np.ndarray, kept: np.ndarray) -> list:
+    """Per inner layer: its share of the tracklets, and the fractions inside the windows and kept
+    by both stages."""
+    out = []
+    for l in range(6):
+        on = layer == l
+        n = int(on.sum())
+        out.append(dict(layer=l, tracklets=n, share=n / max(len(layer), 1),
+                        inside_window=float(inside[on].mean()) if n else None,
+                        kept=float(kept[on].mean()) if n else None))
+    return out
+
+
+def train_gate(ctx, data: dict, device, seed: int = 1, target: float = 0.997, log=print, window_margin: float = 1.0,
+               window_quantile: float = 0.9999, mlp_layers: int = 0x04, **train_kw) -> tuple:
     """Trains a tracklet gate on `data` (from collect_gate): the first stage's per-layer |dphi| and
-    |dz| windows from the road tracklets (fit_windows), then the network on the tracklets inside them,
-    its threshold calibrated on road reproduction (a road survives the gate iff all its 6 tracklets
-    pass both stages); returns (model, report)."""
+    |dz| windows from the road tracklets (fit_windows), then the network on the tracklets inside them
+    of the inner layers in `mlp_layers` (bit l), its threshold calibrated on road reproduction (a
+    road survives the gate iff all its 6 tracklets pass both stages); returns (model, report)."""
     import torch
 
     model = capi.gate_init(seed)
     feats_np = data["features"].cpu().numpy()
     rows = data["road_rows"].cpu().numpy()
-    wphi, wz = fit_windows(feats_np, rows, window_margin)
+    wphi, wz = fit_windows(feats_np, rows, window_margin, window_quantile)
     inside = window_pass(feats_np, wphi, wz)
     for l in range(6):
         model.dphi_window[l] = float(wphi[l])
         model.dz_window[l] = float(wz[l])
-    mean, inv_std = standardisation(data["features"][torch.from_numpy(inside).to(data["features"].device)])
+    model.mlp_layers = mlp_layers
+    layer = np.clip(feats_np[:, 4], 0, 5).astype(np.int64)
+    scored = inside & (((mlp_layers >> layer) & 1) == 1)
+    mean, inv_std = standardisation(data["features"][torch.from_numpy(scored).to(data["features"].device)])
     for k in range(8):
         model.mean[k], model.inv_std[k] = float(mean[k]), float(inv_std[k])
     ctx.gate_set_model(model)
-    ok = torch.isfinite(data["features"]).all(dim=1) & torch.from_numpy(inside).to(data["features"].device)
+    ok = torch.isfinite(data["features"]).all(dim=1) & torch.from_numpy(scored).to(data["features"].device)
     f = data["features"][ok].contiguous()
     y = data["labels"][ok].contiguous()
     cfg = capi.train_config(**train_kw)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    losses = ctx.gate_train(f.data_ptr(), y.data_ptr(), len(f), cfg)
+    losses = ctx.gate_train(f.data_ptr(), y.data_ptr(), len(f), cfg) if len(f) else np.zeros(0)  # no layer scored: no network
     train_s = time.perf_counter() - t0
     model = ctx.gate_get_model()
     n = len(data["features"])
     logits_t = torch.empty(max(n, 1), dtype=torch.float32, device=device)
     ctx.gate_score(data["features"].data_ptr(), n, logits_t.data_ptr())
-    logits = np.where(inside, logits_t[:n].cpu().numpy(), -np.inf)  # outside the window: dropped by stage 1
+    logits = logits_t[:n].cpu().numpy()
+    logits = np.where(scored, logits, np.inf)  # layers the network does not score: kept
+    logits = np.where(inside, logits, -np.inf)  # outside the windows: dropped by stage 1
     thr = calibrate(logits, rows, target)
+    if not np.isfinite(thr):  # only the windows drop tracklets: the threshold is never used
+        thr = float("-inf")
     model.logit_threshold = thr
     ctx.gate_set_model(model)
     labels = data["labels"].cpu().numpy()
     kept = ~(logits < thr)
     report = dict(
         dphi_window=[float(w) for w in wphi], dz_window=[float(w) for w in wz], window_margin=window_margin,
+        window_quantile=window_quantile, mlp_layers=mlp_layers,
         train_tracklets_inside_window=float(inside.mean()),
         samples=int(len(f)), positives=int(y.sum().item()), steps=int(cfg.steps), batch=int(cfg.batch), lr=float(cfg.lr),
         lr_final=float(cfg.lr_final), train_seconds=train_s, loss_first=float(np.mean(losses[:100])) if len(losses) else None,
         loss_last=float(np.mean(losses[-100:])) if len(losses) else None, threshold=thr, calibration_target=target,
         train_tracklets_kept=float(kept.mean()), train_positive_tracklets_kept=float(kept[labels == 1].mean()),
         train_negative_tracklets_kept=float(kept[labels == 0].mean()),
+        per_layer=per_layer_fractions(feats_np[:, 4], inside, kept),
     )
     log("train gate: %s" % json.dumps(report))
     return model, report
@@ -602,16 +627,23 @@ def main(argv=None):
     p.add_argument("--batch", type=int, default=8192)
     p.add_argument("--lr", type=float, default=2e-3)
     p.add_argument("--target", type=float, default=None,
-                   help="road reproduction the threshold keeps on the training events (default: 0.997 pair, 0.999 gate)")
+                   help="road reproduction the threshold keeps on the training events (default: 0.997)")
     p.add_argument("--with-pair", default=None,
                    help="gate: also evaluate the learned form with this pair-prefilter checkpoint enabled")
     p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--window-margin", type=float, default=1.0,
+                   help="gate: its windows are this times the training roads' --window-quantile of |dphi| and |dz| per layer")
+    p.add_argument("--window-quantile", type=float, default=0.9999,
+                   help="gate: the quantile of the road tracklets' |dphi| and |dz| its windows start from (1: the largest)")
+    p.add_argument("--mlp-layers", type=lambda v: int(v, 0), default=0x04,
+                   help="gate: the inner layers its network scores, as a bit mask (0x3f: all six; default: layer 2, "
+                        "where the windows keep the most)")
     p.add_argument("--chunk", type=int, default=None)
     args = p.parse_args(argv)
     gate_mode = args.model == "gate"
     args.out = args.out or (GATE_CHECKPOINTS[args.workload] if gate_mode else CHECKPOINTS[args.workload])
     args.train_events = args.train_events or (300 if gate_mode else 2000)
-    args.target = args.target or (0.999 if gate_mode else 0.997)
+    args.target = args.target or 0.997
     args.chunk = args.chunk or (50 if gate_mode else 100)
     import torch
 
@@ -627,7 +659,10 @@ def main(argv=None):
         data = collect(ctx, train_seeds, device, chunk=args.chunk, workload=args.workload)
     collect_s = time.perf_counter() - t0
     trainer = train_gate if gate_mode else train
-    model, report = trainer(ctx, data, device, seed=args.seed, target=args.target, steps=args.steps, batch=args.batch, lr=args.lr)
+    extra = dict(window_margin=args.window_margin, window_quantile=args.window_quantile,
+                 mlp_layers=args.mlp_layers) if gate_mode else {}
+    model, report = trainer(ctx, data, device, seed=args.seed, target=args.target, steps=args.steps, batch=args.batch,
+                            lr=args.lr, **extra)
     del data
     if gate_mode:
         ev = evaluate(ctx, None, eval_seeds, device, chunk=args.chunk, workload=args.workload, gate=model)
