@@ -368,3 +368,41 @@ def test_committed_gate_reproduces_plain_roads(ctx, torch_dev):
     assert res["extra"] == 0
     assert res["road_reproduction"] >= 0.995, res
     assert res["tracklets_kept"] < 0.5, res
+
+
+def test_gate_windows_on_pileup_frames(ctx, torch_dev):
+    """Frames of 3 collisions (every vertex of a frame is one run over the frame's clusters): the
+    windows apply per run, about that run's vertex; each run's gated tracklets are its plain
+    tracklets inside the windows, in order, and the gated roads are plain roads."""
+    frames = gen.pileup_stream(19, n_frames=2, collisions=3, n_tracks=400)
+    clusters, offsets, vertices, vertex_frame = gen.pack_frames(frames)
+    prefilter.set_learned(ctx, False, False)
+    ctx.frames_run_host(clusters, offsets, vertices, vertex_frame)
+    n_runs = len(vertex_frame)
+    plain = [ctx.results(v) for v in range(n_runs)]
+    f, _, _ = prefilter.export_gate_samples(ctx, torch_dev)
+    pkeys, _ = prefilter.export_roads(ctx, torch_dev)
+    fn = f.cpu().numpy()
+    m = _gate(fn, threshold=float("-inf"))
+    wphi, wz = _windows_at(fn, 0.6)
+    _set_windows(m, wphi, wz)
+    inside = prefilter.window_pass(fn, wphi, wz)
+    ctx.gate_set_model(m)
+    prefilter.set_learned(ctx, False, True)
+    try:
+        ctx.frames_run_host(clusters, offsets, vertices, vertex_frame)
+        lkeys, _ = prefilter.export_roads(ctx, torch_dev)
+        row = 0
+        for v in range(n_runs):
+            got = ctx.results(v)
+            for layer in range(6):
+                pt = plain[v]["tracklets"][layer]
+                kept = pt[inside[row:row + len(pt)]]
+                row += len(pt)
+                assert np.array_equal(got["tracklets"][layer].view(np.uint8), kept.view(np.uint8)), (v, layer)
+        assert row == len(fn)
+    finally:
+        prefilter.set_learned(ctx, False, False)
+    p = {bytes(r) for r in np.ascontiguousarray(pkeys)}
+    assert all(bytes(r) in p for r in np.ascontiguousarray(lkeys))
+    assert 0 < len(lkeys) < len(pkeys)

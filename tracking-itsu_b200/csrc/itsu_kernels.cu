@@ -1047,17 +1047,16 @@ __device__ int stage_rows(const Arena &a, const InnerCluster &s, float4 *stage, 
   return s_k0;
 }
 
-constexpr int kGateCountThreads = 256;
+constexpr int kCountThreads = 256;
 
 // Count pass, one thread per inner cluster: the number of tracklets, and the outer clusters of
 // the first kTrackletSlots of them in emission order. kStaged: the block's walks read the next
 // layer's z-sorted entries from a shared-memory copy made by one bulk copy (stage_rows), where
-// they allow it. kGate: the learned form's first stage (inner_cluster), at most 256 threads per
-// block and 48 registers (5 blocks per SM; measured 0.39 vs 0.43 ms per 128 events at 56). The
-// plain instantiation's explicit one-block minimum gives it 54 registers and no stack (40 and a
-// 24-byte stack without: 0.06 ms slower per 128 events).
+// they allow it. kGate: the learned form's first stage (inner_cluster). At most kCountThreads
+// threads per block; measured per 128 events: the plain instantiation at 40 registers (6 blocks
+// per SM) 0.64 ms, at 48 0.66, at 54 0.72; the learned one at 48 (5 blocks) 0.39 ms, at 56 0.43.
 template <bool kStaged, bool kGate>
-__global__ void __launch_bounds__(kGate ? kGateCountThreads : kMaxThreads, kGate ? 5 : 1) k_tracklets_count(Arena a)
+__global__ void __launch_bounds__(kCountThreads, kGate ? 5 : 6) k_tracklets_count(Arena a)
 {
   extern __shared__ float4 stage[];  // kStaged: kStageEntries entries
   __shared__ uint64_t bar;
@@ -2091,20 +2090,20 @@ void step_tracklets_count(const Arena &a, const Launch &l)
     return;
   }
   const size_t stage_bytes = kStageEntries * sizeof(float4);
-  // the learned form's count pass takes at most kGateCountThreads threads per block (any whole
-  // warps give the same results)
-  const int gate_block = std::min(l.block, kGateCountThreads);
-  const unsigned gate_blocks = (unsigned)((a.n_clusters + gate_block - 1) / gate_block);
+  // the count pass takes at most kCountThreads threads per block (any whole warps give the same
+  // results)
+  const int block = std::min(l.block, kCountThreads);
+  const unsigned grid = (unsigned)((a.n_clusters + block - 1) / block);
   if (a.prune_tracklets == 2) {  // the staged walk (tuning knob; results are identical)
     if (a.gate) {
-      k_tracklets_count<true, true><<<gate_blocks, gate_block, stage_bytes, l.stream>>>(a);
+      k_tracklets_count<true, true><<<grid, block, stage_bytes, l.stream>>>(a);
     } else {
-      k_tracklets_count<true, false><<<(unsigned)blocks, l.block, stage_bytes, l.stream>>>(a);
+      k_tracklets_count<true, false><<<grid, block, stage_bytes, l.stream>>>(a);
     }
   } else if (a.gate) {
-    k_tracklets_count<false, true><<<gate_blocks, gate_block, 0, l.stream>>>(a);
+    k_tracklets_count<false, true><<<grid, block, 0, l.stream>>>(a);
   } else {
-    k_tracklets_count<false, false><<<(unsigned)blocks, l.block, 0, l.stream>>>(a);
+    k_tracklets_count<false, false><<<grid, block, 0, l.stream>>>(a);
   }
 }
 
