@@ -9,8 +9,9 @@ pass of every kernel, replayed as one CUDA graph. The batch's inputs and interme
 flush between steps.
 
   value  events/s with the inputs already resident in HBM (device-side batch API)
-  e2e    events/s through the host-facing C ABI call (itsu_batch_run_host_compact): pinned host
-         clusters (24-byte input records) in, roads out, every copy inside the timed region
+  e2e    events/s through the host-facing C ABI call (itsu_batch_run_host_tracks): pinned host
+         clusters (16-byte input records: coordinates and MC id) in, roads out, every copy inside
+         the timed region (modes.e2e_compact: the same with the 24-byte records)
   roofline  the dominant kernel's own compulsory bytes / its CUDA-event duration, against the
          measured HBM copy bandwidth (every main kernel's figure under roofline.kernels)
   cpu_baseline  the reference CPU Tracker (oracle/_ref, compiled from the reference's sources)
@@ -449,13 +450,20 @@ def run_ours(args):
     clock_summary = clocks.summary()
 
     # ---- e2e: host in / host out through the C ABI ----
-    # the host-facing call takes the 24-byte input records (itsu_cluster_in): what a caller holds
-    # before clustering, a third fewer bytes to upload than the 36-byte Cluster
+    # the host-facing call takes the 16-byte input records (itsu_cluster_track): what the roads
+    # and their labels need of each cluster, 4/9 of the 36-byte Cluster; the 24-byte records
+    # (itsu_cluster_in, all the raw constructor's arguments) are timed beside it
     from itsu import capi as _capi
 
-    clusters_in = _capi.compact_clusters(clusters)
-    h_clusters = torch.empty(clusters_in.nbytes, dtype=torch.uint8, pin_memory=True)
-    h_clusters.numpy()[:] = clusters_in.view(np.uint8)
+    def pinned(records):
+        t = torch.empty(records.nbytes, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[:] = records.view(np.uint8)
+        return t
+
+    clusters_in = _capi.track_clusters(clusters)
+    h_clusters = pinned(clusters_in)
+    h_compact = pinned(_capi.compact_clusters(clusters)) if frames is None else None
+    host_fn = "itsu_batch_run_host_tracks"
     h_offsets = torch.empty(len(offsets), dtype=torch.int32, pin_memory=True)
     h_offsets.numpy()[:] = offsets
     h_vertices = torch.empty(len(vertices), dtype=torch.float32, pin_memory=True)
@@ -475,9 +483,9 @@ def run_ours(args):
             ctx_e2e.set_tune(tune["band"], tune["threads_per_block"], tune["blocks_per_sm"], tune["prune"], tune["events_per_group"])
 
     def host_run():
-        st = ctx_e2e.lib.itsu_batch_run_host_compact(ctx_e2e.h, ctypes.c_void_p(h_clusters.data_ptr()), ctypes.c_void_p(h_offsets.data_ptr()),
-                                             ctypes.c_void_p(h_vertices.data_ptr()), n_events, ctypes.c_void_p(h_roads.data_ptr()),
-                                             roads_cap, ctypes.c_void_p(h_road_off.data_ptr()))
+        st = getattr(ctx_e2e.lib, host_fn)(ctx_e2e.h, ctypes.c_void_p(h_clusters.data_ptr()), ctypes.c_void_p(h_offsets.data_ptr()),
+                                           ctypes.c_void_p(h_vertices.data_ptr()), n_events, ctypes.c_void_p(h_roads.data_ptr()),
+                                           roads_cap, ctypes.c_void_p(h_road_off.data_ptr()))
         ctx_e2e._check(st)
 
     if frames is not None:
@@ -511,7 +519,22 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(dist, e_start.elapsed_time(e_end), device)
     assert int(h_road_off[-1]) == total_roads, "host path road count differs from the device path"
+    e2e_compact_ms = None
     if ctx_e2e is not None:
+        # the same call with the 24-byte records, timed the same way
+        host_fn, h_clusters = "itsu_batch_run_host_compact", h_compact
+        for _ in range(max(1, args.warmup)):
+            host_run()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e_start.record(stream)
+        for _ in range(args.steps):
+            host_run()
+        e_end.record(stream)
+        torch.cuda.synchronize()
+        e2e_compact_ms = max_over_ranks(dist, e_start.elapsed_time(e_end), device)
+        assert int(h_road_off[-1]) == total_roads, "compact host path road count differs from the device path"
         ctx_e2e.close()
 
     # ---- learned forms: same inputs, same timing rules ----
@@ -632,7 +655,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d_bytes),
                     "d2h_bytes_per_step": int(32 * total_roads + 4 * (n_events + 1)),
                     "api": "itsu_frames_run_host (pinned host buffers)" if frames is not None else
-                           "itsu_batch_run_host_compact (24-byte input records) with ITSU_FLAG_STREAM_HOST (chunks of events, uploads overlapping the work; pinned host buffers)"},
+                           "itsu_batch_run_host_tracks (16-byte input records: coordinates and MC id) with ITSU_FLAG_STREAM_HOST (chunks of events, uploads overlapping the work; pinned host buffers)"},
             "gpu_launches": kernels * args.steps,
             "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
@@ -643,6 +666,10 @@ def run_ours(args):
                          "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_src if peak_src == "measured" else "fallback 6.65 TB/s"},
             "modes": {
                 "batched_plain_events_per_s": value,
+                "e2e_compact": None if e2e_compact_ms is None else {
+                    "value": total_events / (e2e_compact_ms * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(24 * len(clusters) + offsets.nbytes + vertices.nbytes),
+                    "api": "itsu_batch_run_host_compact (24-byte input records), otherwise as e2e"},
                 "plain_single_event_events_per_s": single_eps,
                 "plain_single_event_note": "itsu_clusters_to_tracks, one vertex per synchronous call, host in/out, wall clock",
                 "learned_prefilter": learned_summary(learned, total_events, value, args),

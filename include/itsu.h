@@ -57,6 +57,15 @@ typedef struct itsu_cluster_in {
   int32_t mc_id;
 } itsu_cluster_in;
 
+/* A cluster as a caller that wants only roads and their Monte Carlo labels delivers it: what the
+ * tracking and the label vote read (coordinates and MC id), in 16 bytes. The sorted clusters of a
+ * run fed these records carry the cluster's index in its layer's input order as cluster_id and 0
+ * as alpha; every other output is the same as from the full records. */
+typedef struct itsu_cluster_track {
+  float x, y, z;
+  int32_t mc_id;
+} itsu_cluster_track;
+
 typedef struct itsu_tracklet {
   int32_t first_cluster;  /* sorted index in layer L */
   int32_t second_cluster; /* sorted index in layer L+1 */
@@ -217,6 +226,11 @@ itsu_status itsu_batch_run_host(itsu_context *ctx, const itsu_cluster *clusters,
 itsu_status itsu_batch_run_host_compact(itsu_context *ctx, const itsu_cluster_in *clusters, const int32_t *layer_offsets,
                                         const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
                                         int32_t *road_offsets);
+/* itsu_batch_run_host with 16-byte input records (itsu_cluster_track): the same roads, labels and
+ * fake flags, streamed the same way under ITSU_FLAG_STREAM_HOST (two thirds of the compact upload). */
+itsu_status itsu_batch_run_host_tracks(itsu_context *ctx, const itsu_cluster_track *clusters, const int32_t *layer_offsets,
+                                       const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
+                                       int32_t *road_offsets);
 /* Launches every stage of the batch on the context stream without waiting (CUDA-graph
  * replay after the first call with the same shape); itsu_batch_status waits and reports. */
 itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch);

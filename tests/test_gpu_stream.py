@@ -165,3 +165,38 @@ def test_compact_input_records_give_the_same_run(streamed):
     finally:
         full.close()
         comp.close()
+
+
+@pytest.mark.parametrize("streamed", [False, True])
+def test_track_input_records_give_the_same_roads(streamed):
+    """itsu_batch_run_host_tracks (16-byte records: coordinates and MC id) gives the 36-byte call's
+    roads, labels and fake flags bit for bit, one pass and streamed; its sorted clusters are the
+    full call's with each cluster's index in its layer's input order as the id and alpha 0, and
+    every other per-event result is the full call's."""
+    events = [gen.pbpb_event(s, n_tracks=3000) for s in (84, 85)] + gen.batch_events(86, n_events=12) + [gen.jet_event(8)]
+    clusters, offsets, vertices = gen.pack_batch(events)
+    kw = dict(flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=60000) if streamed else {}
+    full = capi.Context(device=0, **kw)
+    trk = capi.Context(device=0, **kw)
+    try:
+        want_roads, want_off = full.batch_run_host(clusters, offsets, vertices)
+        got_roads, got_off = trk.batch_run_host_tracks(capi.track_clusters(clusters), offsets, vertices)
+        assert np.array_equal(want_off, got_off)
+        assert np.array_equal(want_roads.view(np.uint8), got_roads.view(np.uint8))
+        if not streamed:
+            for e in range(len(events)):
+                want, got = full.results(e), trk.results(e)
+                for layer in range(7):
+                    w, g = want["clusters"][layer], got["clusters"][layer]
+                    base = offsets[7 * e + layer]
+                    # the full call's ids are its input indices here: the id is the input position
+                    order = w["id"] - clusters["id"][base] if len(w) else w["id"]
+                    assert np.array_equal(g["id"], np.asarray(order, np.int32)), (e, layer)
+                    assert np.all(g["alpha"] == 0)
+                    for k in ("x", "y", "z", "phi", "r", "mc", "bin"):
+                        assert np.array_equal(g[k].view(np.uint32), w[k].view(np.uint32)), (e, layer, k)
+                    want["clusters"][layer] = g
+                assert oracle.diff(got, want) == [], e
+    finally:
+        full.close()
+        trk.close()

@@ -119,6 +119,9 @@ struct itsu_context {
   const itsu_cluster_in *in_raw_in = nullptr;  // the 24-byte input records instead of in_raw (compact host calls)
   itsu_cluster_in *raw_in = nullptr;           // their device copy
   int64_t cap_raw_in = 0;
+  const itsu_cluster_track *in_raw_track = nullptr;  // the 16-byte input records instead (track host calls)
+  itsu_cluster_track *raw_track = nullptr;            // their device copy
+  int64_t cap_raw_track = 0;
   const int32_t *in_raw_off = nullptr;
   const int32_t *in_layer_off = nullptr;
   int32_t *raw_off = nullptr;  // arena copy of a frames run's raw offsets (event class)
@@ -129,7 +132,7 @@ struct itsu_context {
   cudaGraphExec_t graph = nullptr;
   uint64_t graph_generation = 0;
   uint64_t generation = 1;  // bumped whenever a buffer is reallocated
-  const void *graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  const void *graph_key[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int32_t graph_events = -1;
   int64_t graph_clusters = -1;
 
@@ -305,6 +308,7 @@ Arena arena_of(const itsu_context *ctx)
   a.n_clusters = ctx->n_clusters;
   a.raw = ctx->in_raw;
   a.raw_in = ctx->in_raw_in;
+  a.raw_track = ctx->in_raw_track;
   a.raw_off = ctx->in_raw_off;
   a.layer_off = ctx->in_layer_off;
   a.vtx = ctx->in_vtx;
@@ -615,6 +619,7 @@ itsu_status launch_all(itsu_context *ctx)
                     ctx->graph_gate == ctx->gate &&
                     ctx->graph_key[1] == ctx->in_layer_off && ctx->graph_key[2] == ctx->in_vtx &&
                     ctx->graph_key[3] == ctx->in_raw_off && ctx->graph_key[4] == ctx->in_raw_in &&
+                    ctx->graph_key[5] == ctx->in_raw_track &&
                     ctx->graph_events == ctx->n_events && ctx->graph_clusters == ctx->n_clusters;
   if (!same) {
     drop_graph(ctx);
@@ -640,6 +645,7 @@ itsu_status launch_all(itsu_context *ctx)
     ctx->graph_key[2] = ctx->in_vtx;
     ctx->graph_key[3] = ctx->in_raw_off;
     ctx->graph_key[4] = ctx->in_raw_in;
+    ctx->graph_key[5] = ctx->in_raw_track;
     ctx->graph_tune[0] = tune.block;
     ctx->graph_tune[1] = tune.blocks_per_sm;
     ctx->graph_tune[2] = tune.prune;
@@ -767,6 +773,7 @@ itsu_status upload_vertex(itsu_context *ctx, const itsu_cluster *const layers[IT
   ctx->h_layer_off = off;
   ctx->in_raw = ctx->raw;
   ctx->in_raw_in = nullptr;
+  ctx->in_raw_track = nullptr;
   ctx->in_raw_off = nullptr;
   ctx->in_layer_off = ctx->layer_off;
   ctx->in_vtx = ctx->vtx;
@@ -926,7 +933,7 @@ void itsu_context_destroy(itsu_context *ctx)
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->twin) itsu_context_destroy(ctx->twin);
   drop_graph(ctx);
-  release(ctx->raw); release(ctx->raw_in); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
+  release(ctx->raw); release(ctx->raw_in); release(ctx->raw_track); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
   release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->clu_aux); release(ctx->clu_crowded); release(ctx->trk_slots);
   release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
   release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
@@ -1169,6 +1176,7 @@ static itsu_status set_batch(itsu_context *ctx, const itsu_batch *batch)
   ctx->n_clusters = batch->n_clusters;
   ctx->in_raw = batch->clusters;
   ctx->in_raw_in = nullptr;
+  ctx->in_raw_track = nullptr;
   ctx->in_raw_off = nullptr;
   ctx->in_layer_off = batch->layer_offsets;
   ctx->in_vtx = batch->vertices;
@@ -1202,7 +1210,8 @@ itsu_status itsu_batch_launch(itsu_context *ctx, const itsu_batch *batch)
   if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "null context");
   ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
   itsu_status st;
-  const bool same = batch && ctx->stage != kNone && !ctx->in_raw_off && !ctx->in_raw_in && batch->clusters == ctx->in_raw &&
+  const bool same = batch && ctx->stage != kNone && !ctx->in_raw_off && !ctx->in_raw_in && !ctx->in_raw_track &&
+                    batch->clusters == ctx->in_raw &&
                     batch->layer_offsets == ctx->in_layer_off &&
                     batch->vertices == ctx->in_vtx && batch->n_events == ctx->n_events && batch->n_clusters == ctx->n_clusters;
   if (!same && (st = set_batch(ctx, batch)) != ITSU_OK) return st;
@@ -1440,18 +1449,22 @@ itsu_status ensure_twin(itsu_context *ctx)
 // chunk order. The first chunk is smaller, so that the device starts sooner. Sets *done to false,
 // with nothing reported, when the batch is too small to split or a chunk outgrew its arena: the
 // caller then runs the batch in one pass (which grows the arena).
-// The host's raw clusters in either record format: 36-byte itsu_cluster or 24-byte itsu_cluster_in.
+// The host's raw clusters in one of the record formats: 36-byte itsu_cluster, 24-byte
+// itsu_cluster_in or 16-byte itsu_cluster_track.
 struct HostClusters {
   const itsu_cluster *full = nullptr;
   const itsu_cluster_in *compact = nullptr;
-  bool any() const { return full || compact; }
+  const itsu_cluster_track *track = nullptr;
+  bool any() const { return full || compact || track; }
 };
 
 // Uploads host clusters [a, b) to the context's raw buffer of their format (asynchronous on s).
 itsu_status upload_clusters(itsu_context *ctx, const HostClusters &h, int64_t a, int64_t b, cudaStream_t s)
 {
   if (b <= a) return ITSU_OK;
-  if (h.compact) {
+  if (h.track) {
+    ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw_track + a, h.track + a, sizeof(itsu_cluster_track) * (b - a), cudaMemcpyHostToDevice, s));
+  } else if (h.compact) {
     ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw_in + a, h.compact + a, sizeof(itsu_cluster_in) * (b - a), cudaMemcpyHostToDevice, s));
   } else {
     ITSU_CUDA(ctx, cudaMemcpyAsync(ctx->raw + a, h.full + a, sizeof(itsu_cluster) * (b - a), cudaMemcpyHostToDevice, s));
@@ -1462,8 +1475,9 @@ itsu_status upload_clusters(itsu_context *ctx, const HostClusters &h, int64_t a,
 // A run's inputs start at cluster a of the context's raw buffer of the format.
 void point_inputs_at(itsu_context *x, const itsu_context *owner, const HostClusters &h, int64_t a)
 {
-  x->in_raw = h.compact ? nullptr : owner->raw + a;
+  x->in_raw = h.full ? owner->raw + a : nullptr;
   x->in_raw_in = h.compact ? owner->raw_in + a : nullptr;
+  x->in_raw_track = h.track ? owner->raw_track + a : nullptr;
 }
 
 itsu_status run_host_streamed(itsu_context *ctx, const HostClusters &clusters, const int32_t *layer_offsets, const float *vertices,
@@ -1690,6 +1704,7 @@ itsu_status batch_run_host(itsu_context *ctx, const HostClusters &clusters, cons
   itsu_status st;
   if ((st = ensure_clusters(ctx, n_clusters, n_events)) != ITSU_OK) return st;
   if (clusters.compact && (st = grow_buffer(ctx, ctx->raw_in, ctx->cap_raw_in, n_clusters)) != ITSU_OK) return st;
+  if (clusters.track && (st = grow_buffer(ctx, ctx->raw_track, ctx->cap_raw_track, n_clusters)) != ITSU_OK) return st;
   if (ctx->flags & ITSU_FLAG_STREAM_HOST) {
     bool done = false;
     if ((st = run_host_streamed(ctx, clusters, layer_offsets, vertices, n_events, n_clusters, roads, roads_capacity, road_offsets,
@@ -1746,6 +1761,15 @@ itsu_status itsu_batch_run_host_compact(itsu_context *ctx, const itsu_cluster_in
   return batch_run_host(ctx, h, layer_offsets, vertices, n_events, roads, roads_capacity, road_offsets);
 }
 
+itsu_status itsu_batch_run_host_tracks(itsu_context *ctx, const itsu_cluster_track *clusters, const int32_t *layer_offsets,
+                                       const float *vertices, int32_t n_events, itsu_road *roads, int64_t roads_capacity,
+                                       int32_t *road_offsets)
+{
+  HostClusters h;
+  h.track = clusters;
+  return batch_run_host(ctx, h, layer_offsets, vertices, n_events, roads, roads_capacity, road_offsets);
+}
+
 itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, itsu_road *roads, int64_t roads_capacity,
                                  int32_t *road_offsets)
 {
@@ -1794,6 +1818,7 @@ itsu_status itsu_frames_run_host(itsu_context *ctx, const itsu_frames *frames, i
   ctx->n_clusters = total;
   ctx->in_raw = ctx->raw;
   ctx->in_raw_in = nullptr;
+  ctx->in_raw_track = nullptr;
   ctx->in_raw_off = ctx->raw_off;
   ctx->in_layer_off = ctx->layer_off;
   ctx->in_vtx = ctx->vtx;

@@ -82,9 +82,11 @@ struct Arena {
   int32_t n_events;
   int32_t pad_;
   int64_t n_clusters;
-  // inputs (raw clusters in one of two record formats: raw_in set means the 24-byte one)
+  // inputs (raw clusters in one of three record formats: raw_track set means the 16-byte one,
+  // raw_in the 24-byte one, else raw)
   const itsu_cluster *raw;
   const itsu_cluster_in *raw_in;
+  const itsu_cluster_track *raw_track;
   const int32_t *raw_off;  // per (run, layer): start of its raw clusters; null = same as layer_off
   const int32_t *layer_off;
   const float *vtx;

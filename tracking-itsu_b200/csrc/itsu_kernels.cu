@@ -321,6 +321,7 @@ __device__ __forceinline__ void stage_out(itsu_cluster *dst, const int32_t *stag
 // The 24-byte input record (itsu_cluster_in) in 4-byte words.
 constexpr int kClusterInWords = sizeof(itsu_cluster_in) / 4;
 static_assert(sizeof(itsu_cluster_in) == 24 && alignof(itsu_cluster_in) == 4, "input record layout");
+static_assert(sizeof(itsu_cluster_track) == 16, "track record layout");
 
 // A warp's 32 consecutive records of kWords words each, moved into its stage with coalesced loads.
 template <int kWords, typename Record>
@@ -411,7 +412,19 @@ __global__ void __launch_bounds__(kSortThreads) k_cluster_sort(Arena a)
   for (int i0 = wb; i0 < we; i0 += 32) {
     const int count = min(32, we - i0);
     itsu_cluster c{};
-    if (a.raw_in) {
+    if (a.raw_track) {
+      // 16-byte input records (x, y, z, MC id): one aligned 16-byte load per lane; the cluster id
+      // is the record's index in its layer's input order, alpha 0
+      if (lane < count) {
+        const float4 q = reinterpret_cast<const float4 *>(a.raw_track + raw_begin + i0)[lane];
+        c.x = q.x;
+        c.y = q.y;
+        c.z = q.z;
+        c.cluster_id = i0 + lane;
+        c.alpha = 0.0f;
+        c.mc_id = __float_as_int(q.w);
+      }
+    } else if (a.raw_in) {
       // 24-byte input records (x, y, z, id, alpha, MC id): read in 6-word strides, then the stage
       // is reused for the 36-byte records once every lane has read its own
       stage_in_words<kClusterInWords>(stage, a.raw_in + raw_begin + i0, count);

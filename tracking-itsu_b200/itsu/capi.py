@@ -20,6 +20,18 @@ LIB_PATH = os.path.join(PKG, "lib", "libitsu_b200.so")
 CLUSTER_IN_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("id", "<i4"), ("alpha", "<f4"), ("mc", "<i4")])
 
 
+# itsu_cluster_track: the 16-byte input record of the track host calls (roads and labels only)
+CLUSTER_TRACK_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("mc", "<i4")])
+
+
+def track_clusters(clusters) -> np.ndarray:
+    """The 16-byte input records of clusters (coordinates and MC id)."""
+    out = np.zeros(len(clusters), CLUSTER_TRACK_DTYPE)
+    for k in CLUSTER_TRACK_DTYPE.names:
+        out[k] = clusters[k]
+    return out
+
+
 def compact_clusters(clusters) -> np.ndarray:
     """The 24-byte input records of 36-byte clusters (the fields clustering computes dropped)."""
     out = np.zeros(len(clusters), CLUSTER_IN_DTYPE)
@@ -183,6 +195,9 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_void_p]),
     ("itsu_batch_run_host_compact", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+      ctypes.c_void_p]),
+    ("itsu_batch_run_host_tracks", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_void_p]),
     ("itsu_batch_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Batch)]),
@@ -480,23 +495,29 @@ class Context:
         roads["pad"] = 0
         return roads, offs
 
-    def batch_run_host_compact(self, clusters_in, layer_offsets, vertices, roads_capacity=None):
+    def batch_run_host_compact(self, clusters_in, layer_offsets, vertices, roads_capacity=None, _fn="itsu_batch_run_host_compact",
+                               _dtype=CLUSTER_IN_DTYPE):
         """batch_run_host with 24-byte input records (CLUSTER_IN_DTYPE); returns (roads, road_offsets)."""
-        clusters_in = np.ascontiguousarray(clusters_in, CLUSTER_IN_DTYPE)
+        clusters_in = np.ascontiguousarray(clusters_in, _dtype)
+        fn = getattr(self.lib, _fn)
         layer_offsets = np.ascontiguousarray(layer_offsets, np.int32)
         vertices = np.ascontiguousarray(vertices, np.float32)
         n_events = (len(layer_offsets) - 1) // 7
         offs = np.zeros(n_events + 1, np.int32)
         if roads_capacity is None:
-            self._check(self.lib.itsu_batch_run_host_compact(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices),
-                                                             n_events, None, 0, _ptr(offs)))
+            self._check(fn(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices), n_events, None, 0, _ptr(offs)))
             roads_capacity = int(offs[-1])
         roads = np.zeros(roads_capacity, ROAD_DTYPE)
-        self._check(self.lib.itsu_batch_run_host_compact(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices), n_events,
-                                                         _ptr(roads), roads_capacity, _ptr(offs)))
+        self._check(fn(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices), n_events, _ptr(roads), roads_capacity,
+                       _ptr(offs)))
         roads = roads[: offs[-1]].copy()
         roads["pad"] = 0
         return roads, offs
+
+    def batch_run_host_tracks(self, clusters_track, layer_offsets, vertices, roads_capacity=None):
+        """batch_run_host with 16-byte input records (CLUSTER_TRACK_DTYPE); returns (roads, road_offsets)."""
+        return self.batch_run_host_compact(clusters_track, layer_offsets, vertices, roads_capacity,
+                                           _fn="itsu_batch_run_host_tracks", _dtype=CLUSTER_TRACK_DTYPE)
 
     def batch_device(self, clusters_ptr, layer_offsets_ptr, vertices_ptr, n_events, n_clusters) -> Batch:
         b = Batch()
