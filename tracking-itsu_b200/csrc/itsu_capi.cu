@@ -103,6 +103,7 @@ struct itsu_context {
   int32_t *cell_seg_id = nullptr, *nb_count = nullptr, *nb_off = nullptr, *nb_fill = nullptr, *road_count = nullptr,
           *road_off = nullptr;
   int64_t *paths = nullptr;
+  unsigned long long *nb_mask = nullptr;  // per cell, its passing candidates (neighbour count pass)
   // neighbour and road classes
   int32_t *nb = nullptr;
   itsu_road *roads = nullptr;
@@ -347,6 +348,7 @@ Arena arena_of(const itsu_context *ctx)
   a.nb_count = ctx->nb_count;
   a.nb_off = ctx->nb_off;
   a.nb_fill = ctx->nb_fill;
+  a.nb_mask = ctx->nb_mask;
   a.nb = ctx->nb;
   a.paths = ctx->paths;
   a.road_count = ctx->road_count;
@@ -483,6 +485,7 @@ itsu_status ensure_cells(itsu_context *ctx, int64_t need)
     ITSU_CUDA(ctx, alloc(ctx, ctx->nb_count, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx, ctx->nb_off, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx, ctx->nb_fill, cap));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->nb_mask, cap));
     ITSU_CUDA(ctx, alloc(ctx, ctx->paths, cap));
     ITSU_CUDA(ctx, alloc(ctx, ctx->road_count, cap + 1));
     ITSU_CUDA(ctx, alloc(ctx, ctx->road_off, cap + 1));
@@ -940,6 +943,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->road_seg); release(ctx->vtx);
   release(ctx->tracklets); release(ctx->trk_slope); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->cell_off); release(ctx->cell_lookup); release(ctx->cell_crowded);
   release(ctx->cells); release(ctx->cell_entries); release(ctx->cell_dca); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);
+  release(ctx->nb_mask);
   release(ctx->road_count); release(ctx->road_off); release(ctx->paths);
   release(ctx->nb); release(ctx->roads); release(ctx->scan_partials); release(ctx->d_status);
   release(ctx->d_master); release(ctx->d_mlp);

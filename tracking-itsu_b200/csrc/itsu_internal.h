@@ -132,6 +132,7 @@ struct Arena {
   int32_t *nb_count;
   int32_t *nb_off;
   int32_t *nb_fill;
+  unsigned long long *nb_mask;  // per cell of layers 0-3: its candidates that pass the cut (up to 64)
   int32_t *nb;
   int64_t *paths;
   int32_t *road_count;

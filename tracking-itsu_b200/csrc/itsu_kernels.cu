@@ -1818,6 +1818,11 @@ __global__ void __launch_bounds__(kMaxThreads) k_neighbour_reset(Arena a)
   }
 }
 
+// Tracker.cxx:416-474 (findCellsNeighbours): a cell of layer L and the cells of layer L + 1 built
+// on its second tracklet. The count pass evaluates the cut, counts each passing pair in its row
+// and keeps the passing candidates as a mask (rows of up to kMaxMaskedOut candidates); the write
+// pass, after the scan of the counts, fills the rows from the mask (re-evaluating the cut only for
+// cells with more candidates). Row order is restored by k_levels' sort.
 template <bool kWrite>
 __global__ void __launch_bounds__(kMaxThreads) k_neighbours(Arena a)
 {
@@ -1831,11 +1836,23 @@ __global__ void __launch_bounds__(kMaxThreads) k_neighbours(Arena a)
     if (layer >= ITSU_NEIGHBOUR_LAYERS) {
       continue;
     }
-    const itsu_cell cell = a.cells[c];
-    const int64_t ft = a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer + 1] + cell.second_tracklet;
+    const int32_t second = a.cells[c].second_tracklet;
+    const int64_t ft = a.trk_seg[e * ITSU_TRACKLET_LAYERS + layer + 1] + second;
     const int32_t j0 = a.cell_off[ft], j1 = a.cell_off[ft + 1];
+    const bool masked = j1 - j0 <= kMaxMaskedOut;
+    if (kWrite && masked) {
+      const int32_t c_local = (int32_t)(c - a.cell_seg[e * ITSU_CELL_LAYERS + layer]);
+      for (unsigned long long m = a.nb_mask[c]; m; m &= m - 1ull) {
+        const int32_t j = j0 + __ffsll((long long)m) - 1;
+        const int slot = atomicAdd(&a.nb_fill[j], 1);
+        a.nb[a.nb_off[j] + slot] = c_local;
+      }
+      continue;
+    }
+    const itsu_cell cell = a.cells[c];
     const float3 n1 = make_float3(cell.nx, cell.ny, cell.nz);
     const int32_t c_local = (int32_t)(c - a.cell_seg[e * ITSU_CELL_LAYERS + layer]);
+    unsigned long long mask = 0ull;
     for (int32_t j = j0; j < j1; ++j) {
       const itsu_cell next = a.cells[j];
       if (neighbour_cut(layer, n1, cell.curvature, make_float3(next.nx, next.ny, next.nz), next.curvature)) {
@@ -1844,8 +1861,14 @@ __global__ void __launch_bounds__(kMaxThreads) k_neighbours(Arena a)
           a.nb[a.nb_off[j] + slot] = c_local;
         } else {
           atomicAdd(&a.nb_count[j], 1);
+          if (masked) {
+            mask |= 1ull << (j - j0);
+          }
         }
       }
+    }
+    if (!kWrite && masked) {
+      a.nb_mask[c] = mask;
     }
   }
 }
