@@ -334,6 +334,10 @@ typedef struct itsu_kernel_time {
 /* Number of kernels one plain whole-path or batch run launches (the learned-prefilter form
  * launches one more, its scoring kernel). */
 int32_t itsu_kernels_per_run(void);
+/* The device's correctly rounded atan2 (include/itsu_atan2f.h, the azimuth of every cluster and
+ * tracklet) on n device-resident argument pairs, out[i] = atan2(y[i], x[i]), on the context's
+ * stream, synchronously: a self-check of the device build against the host's definition. */
+itsu_status itsu_atan2f_device(itsu_context *ctx, const float *y, const float *x, float *out, int64_t n);
 /* Re-runs the last batch `repeats` times with every kernel launched on its own and bracketed by
  * CUDA events on the context stream; fills up to `capacity` entries in launch order and sets
  * *count to the number of kernels of the context's form. Call after itsu_batch_run (or

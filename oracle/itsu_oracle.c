@@ -108,6 +108,10 @@ static float normalized_phi(float phi)
 }
 
 float oracle_atan2f(float y, float x) { return itsu_atan2f(y, x); }
+void oracle_atan2f_n(const float *y, const float *x, float *out, int64_t n)
+{
+  for (int64_t i = 0; i < n; ++i) out[i] = itsu_atan2f(y[i], x[i]);
+}
 
 /* Cluster.cxx:35-45 with MathUtils.h:37-45: vertex-relative phi and r, then the bin. */
 void oracle_transform_cluster(int layer, const float vertex[3], const itsu_cluster *raw, itsu_cluster *out)

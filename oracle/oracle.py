@@ -61,8 +61,7 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
+        build()  # rebuilt when the sources are newer
         L = ctypes.CDLL(LIB_PATH)
         L.oracle_run_vertex.restype = ctypes.c_void_p
         L.oracle_run_vertex.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
@@ -73,6 +72,8 @@ def lib():
         L.oracle_free.argtypes = [ctypes.c_void_p]
         L.oracle_atan2f.restype = ctypes.c_float
         L.oracle_atan2f.argtypes = [ctypes.c_float, ctypes.c_float]
+        L.oracle_atan2f_n.restype = None
+        L.oracle_atan2f_n.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
         L.oracle_run_batch.restype = ctypes.c_int64
         L.oracle_run_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]
         L.oracle_roads_report.restype = ctypes.c_int

@@ -197,6 +197,11 @@ def test_track_input_records_give_the_same_roads(streamed):
                         assert np.array_equal(g[k].view(np.uint32), w[k].view(np.uint32)), (e, layer, k)
                     want["clusters"][layer] = g
                 assert oracle.diff(got, want) == [], e
+        bad = capi.track_clusters(clusters)
+        bad["z"][offsets[7 * 4 + 3] + 2] = np.inf
+        with pytest.raises(capi.ItsuError) as err:
+            trk.batch_run_host_tracks(bad, offsets, vertices)
+        assert err.value.status == capi.ERR_INVALID and str(offsets[7 * 4 + 3] + 2) in str(err.value)
     finally:
         full.close()
         trk.close()

@@ -1850,6 +1850,17 @@ itsu_status itsu_relaunch(itsu_context *ctx)
 
 int32_t itsu_kernels_per_run(void) { return itsu::kernels_per_run(); }
 
+itsu_status itsu_atan2f_device(itsu_context *ctx, const float *y, const float *x, float *out, int64_t n)
+{
+  if (!ctx) return fail(nullptr, ITSU_ERR_INVALID, "itsu_atan2f_device: null context");
+  if (n < 0 || (n > 0 && (!y || !x || !out))) return fail(ctx, ITSU_ERR_INVALID, "itsu_atan2f_device: bad arguments");
+  ITSU_CUDA(ctx, cudaSetDevice(ctx->device));
+  itsu::launch_atan2f(y, x, out, n, ctx->num_sms, ctx->stream);
+  ITSU_CUDA(ctx, cudaGetLastError());
+  ITSU_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITSU_OK;
+}
+
 int32_t itsu_multiplicity_band(int64_t n_clusters, int32_t n_events) { return band_of(n_clusters, n_events); }
 
 itsu_status itsu_autotune(itsu_context *ctx, int32_t repeats, itsu_tune *best)

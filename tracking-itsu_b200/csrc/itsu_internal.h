@@ -166,6 +166,7 @@ struct Launch {
 
 // Stage launchers (asynchronous on l.stream).
 void launch_status_init(const Arena &a, const Launch &l);
+void launch_atan2f(const float *y, const float *x, float *out, int64_t n, int num_sms, cudaStream_t stream);
 void launch_cluster_sort(const Arena &a, const Launch &l);
 void launch_tracklets_count(const Arena &a, const Launch &l);
 void launch_tracklets_write(const Arena &a, const Launch &l);

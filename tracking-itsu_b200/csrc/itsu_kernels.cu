@@ -2080,6 +2080,13 @@ __global__ void __launch_bounds__(kMaxThreads) k_roads(Arena a)
   }
 }
 
+__global__ void k_atan2f(const float *y, const float *x, float *out, int64_t n)
+{
+  for (int64_t i = global_thread(); i < n; i += grid_threads()) {
+    out[i] = itsu_atan2f(y[i], x[i]);
+  }
+}
+
 // Grid of the grid-stride kernels: the tuned number of resident blocks per SM, scaled to the
 // block size so that the number of resident threads stays comparable.
 int fixed_grid(const Launch &l) { return l.num_sms * l.blocks_per_sm; }
@@ -2344,6 +2351,13 @@ const KernelStep *pipeline_steps(int *count)
 void launch_status_init(const Arena &a, const Launch &l) { run_steps(0, 0, a, l); }
 void launch_cluster_sort(const Arena &a, const Launch &l) { run_steps(1, 1, a, l); }
 void launch_tracklets_count(const Arena &a, const Launch &l) { run_steps(2, 6, a, l); }
+
+void launch_atan2f(const float *y, const float *x, float *out, int64_t n, int num_sms, cudaStream_t stream)
+{
+  if (n > 0) {
+    k_atan2f<<<num_sms * 4, 256, 0, stream>>>(y, x, out, n);
+  }
+}
 void launch_tracklets_write(const Arena &a, const Launch &l) { run_steps(7, 8, a, l); }
 void launch_cells_count(const Arena &a, const Launch &l) { run_steps(9, 14, a, l); }
 void launch_cells_write(const Arena &a, const Launch &l) { run_steps(15, 16, a, l); }

@@ -197,6 +197,7 @@ SIGNATURES = [
     ("itsu_batch_run_host_compact", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_void_p]),
+    ("itsu_atan2f_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),
     ("itsu_batch_run_host_tracks", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_void_p]),
@@ -513,6 +514,11 @@ class Context:
         roads = roads[: offs[-1]].copy()
         roads["pad"] = 0
         return roads, offs
+
+    def atan2f_device(self, y_ptr, x_ptr, out_ptr, n):
+        """The device's correctly rounded atan2 on n device-resident argument pairs."""
+        self._check(self.lib.itsu_atan2f_device(self.h, ctypes.c_void_p(y_ptr), ctypes.c_void_p(x_ptr),
+                                                ctypes.c_void_p(out_ptr), n))
 
     def batch_run_host_tracks(self, clusters_track, layer_offsets, vertices, roads_capacity=None):
         """batch_run_host with 16-byte input records (CLUSTER_TRACK_DTYPE); returns (roads, road_offsets)."""
