@@ -364,6 +364,7 @@ def cpu_baseline(events, budget_s):
     else:
         n, s = run_port_sample(events, workers, per_worker)
     return {"value": n / s, "unit": UNIT, "cores": workers, "kind": "reference" if ref else "port",
+            "value_1_core": 1.0 / per_event,  # the calibration event alone on one core
             "sample": "%d Pb-Pb-like events (%d per process, %d single-threaded processes, one per core) of the "
                       "benchmark workload; %s" % (n, per_worker, workers,
                                                   "reference CPU Tracker built from its sources (oracle/_ref/ref_cr)"
