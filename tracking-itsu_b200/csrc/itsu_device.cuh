@@ -83,14 +83,12 @@ __device__ __forceinline__ Transformed transform_cluster(int layer, float x, flo
 }
 
 // TrackingUtils.cxx:30-48 getBinsRect: {zMin, phiMin, zMax, phiMax}; all zero means empty.
-// half_width: the phi half-width of the window (the reference's kPhiCoordinateCut; the learned
-// form's narrower windows reach fewer phi rows).
-__device__ __forceinline__ int4 bins_rect(float phi, int layer, float dir_z, float half_width = kPhiCoordinateCut)
+__device__ __forceinline__ int4 bins_rect(float phi, int layer, float dir_z)
 {
   const float z_min = dir_z - 2 * kZCoordinateCut;
-  const float phi_min = phi - half_width;
+  const float phi_min = phi - kPhiCoordinateCut;
   const float z_max = dir_z + 2 * kZCoordinateCut;
-  const float phi_max = phi + half_width;
+  const float phi_max = phi + kPhiCoordinateCut;
   if (z_max < -kC.z_half[layer + 1] || z_min > kC.z_half[layer + 1] || z_min > z_max) {
     return make_int4(0, 0, 0, 0);
   }
