@@ -134,7 +134,7 @@ struct Arena {
   int32_t *nb_fill;
   unsigned long long *nb_mask;  // per cell of layers 0-3: its candidates that pass the cut (up to 64)
   int32_t *nb;
-  int64_t *paths;
+  int64_t *paths;  // per cell: its chain count and level (chain_word)
   int32_t *road_count;
   int32_t *road_off;
   int32_t *road_seg;

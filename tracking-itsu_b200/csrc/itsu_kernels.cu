@@ -1804,6 +1804,12 @@ __global__ void k_cell_segments(Arena a)
 // (d) neighbours and CA levels: Tracker<IsGPU>::findCellsNeighbours (Tracker.cxx:417-474)
 
 // Per-cell state of the neighbour and road stages, reset so that the stage can be re-run.
+// A cell's CA level and its number of level-decreasing chains down to layer 0, in one word
+// (chains << 3 | level; levels are 1..5 and chain counts are capped at INT_MAX).
+__device__ __forceinline__ int64_t chain_word(int64_t paths, int level) { return (paths << 3) | level; }
+__device__ __forceinline__ int chain_level(int64_t w) { return (int)(w & 7); }
+__device__ __forceinline__ int64_t chain_paths(int64_t w) { return w >> 3; }
+
 __global__ void __launch_bounds__(kMaxThreads) k_neighbour_reset(Arena a)
 {
   if (capacity_failed(a.status)) {
@@ -1814,7 +1820,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_neighbour_reset(Arena a)
     a.nb_count[c] = 0;
     a.nb_fill[c] = 0;
     a.road_count[c] = 0;
-    a.paths[c] = a.cell_seg_id[c] % ITSU_CELL_LAYERS == 0 ? 1 : 0;
+    a.paths[c] = a.cell_seg_id[c] % ITSU_CELL_LAYERS == 0 ? chain_word(1, 1) : 0;  // layer 0: one chain, level 1
   }
 }
 
@@ -1880,7 +1886,8 @@ __global__ void k_neighbour_check(Arena a)
   }
 }
 
-// One cell of k_levels (below): its row sorted, its level and its number of chains.
+// One cell of k_levels (below): its row sorted, its level and its number of chains (read from and
+// written to the neighbours' chain words, one 8-byte gather per neighbour).
 __device__ __forceinline__ void level_of(const Arena &a, int64_t c, int64_t prev_base, int layer)
 {
   const int32_t b = a.nb_off[c], en = a.nb_off[c + 1];
@@ -1897,14 +1904,14 @@ __device__ __forceinline__ void level_of(const Arena &a, int64_t c, int64_t prev
   }
   int level = 1;
   for (int p = 0; p < len; ++p) {
-    level = max(level, a.cells[prev_base + row[p]].level + 1);
+    level = max(level, chain_level(a.paths[prev_base + row[p]]) + 1);
   }
   int64_t paths = 0;
   bool overflow = false;
   for (int p = 0; p < len; ++p) {
-    const int64_t nbi = prev_base + row[p];
-    if (a.cells[nbi].level == level - 1) {
-      paths += a.paths[nbi];
+    const int64_t w = a.paths[prev_base + row[p]];
+    if (chain_level(w) == level - 1) {
+      paths += chain_paths(w);
       if (paths > INT_MAX) {
         paths = INT_MAX;
         overflow = true;
@@ -1912,7 +1919,7 @@ __device__ __forceinline__ void level_of(const Arena &a, int64_t c, int64_t prev
     }
   }
   a.cells[c].level = level;
-  a.paths[c] = paths;
+  a.paths[c] = chain_word(paths, level);
   if (layer == ITSU_CELL_LAYERS - 1 && level == kCellsMinLevel) {
     a.road_count[c] = (int32_t)paths;
     if (overflow) {
@@ -2022,8 +2029,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_roads(Arena a)
           for (int32_t j = a.nb_off[flat]; j < j1; ++j) {
             const int32_t nb = a.nb[j];
             const int64_t nflat = cs[l - 1] + nb;
-            if (a.cells[nflat].level == level - 1) {
-              const int64_t below = a.paths[nflat];
+            const int64_t w = a.paths[nflat];
+            if (chain_level(w) == level - 1) {
+              const int64_t below = chain_paths(w);
               if (k < below) {
                 cur[l - 1] = nb;
                 flat = nflat;
