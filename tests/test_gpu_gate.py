@@ -406,3 +406,29 @@ def test_gate_windows_on_pileup_frames(ctx, torch_dev):
     p = {bytes(r) for r in np.ascontiguousarray(pkeys)}
     assert all(bytes(r) in p for r in np.ascontiguousarray(lkeys))
     assert 0 < len(lkeys) < len(pkeys)
+
+
+def test_gate_through_the_streamed_host_call(ctx, torch_dev):
+    """The learned form through the streamed host call (chunks on two arenas, the context's gate
+    serving both): the same roads as the one-pass call with the same gate."""
+    events = [gen.pbpb_event(s, n_tracks=2500) for s in (74, 75)] + gen.batch_events(76, n_events=10)
+    clusters, offsets, vertices = gen.pack_batch(events)
+    _, f, _, _ = _plain(ctx, torch_dev, events)
+    m = _gate(f.cpu().numpy(), threshold=float("-inf"))
+    wphi, wz = _windows_at(f.cpu().numpy(), 0.7)
+    _set_windows(m, wphi, wz)
+    one = capi.Context(device=0)
+    streamed = capi.Context(device=0, flags=capi.FLAG_STREAM_HOST, stream_chunk_clusters=40000)
+    try:
+        plain_roads, _ = one.batch_run_host(clusters, offsets, vertices)
+        for c in (one, streamed):
+            c.gate_set_model(m)
+            c.gate_enable(True)
+        want_roads, want_off = one.batch_run_host(clusters, offsets, vertices)
+        got_roads, got_off = streamed.batch_run_host_tracks(capi.track_clusters(clusters), offsets, vertices)
+        assert np.array_equal(want_off, got_off)
+        assert np.array_equal(want_roads.view(np.uint8), got_roads.view(np.uint8))
+        assert 0 < len(want_roads) < len(plain_roads)
+    finally:
+        one.close()
+        streamed.close()
