@@ -496,34 +496,32 @@ class Context:
         roads["pad"] = 0
         return roads, offs
 
-    def batch_run_host_compact(self, clusters_in, layer_offsets, vertices, roads_capacity=None, _fn="itsu_batch_run_host_compact",
-                               _dtype=CLUSTER_IN_DTYPE):
-        """batch_run_host with 24-byte input records (CLUSTER_IN_DTYPE); returns (roads, road_offsets)."""
-        clusters_in = np.ascontiguousarray(clusters_in, _dtype)
-        fn = getattr(self.lib, _fn)
+    def _batch_run_host_records(self, fn_name, dtype, records, layer_offsets, vertices, roads_capacity):
+        records = np.ascontiguousarray(records, dtype)
+        fn = getattr(self.lib, fn_name)
         layer_offsets = np.ascontiguousarray(layer_offsets, np.int32)
         vertices = np.ascontiguousarray(vertices, np.float32)
         n_events = (len(layer_offsets) - 1) // 7
         offs = np.zeros(n_events + 1, np.int32)
         if roads_capacity is None:
-            self._check(fn(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices), n_events, None, 0, _ptr(offs)))
+            self._check(fn(self.h, _ptr(records), _ptr(layer_offsets), _ptr(vertices), n_events, None, 0, _ptr(offs)))
             roads_capacity = int(offs[-1])
         roads = np.zeros(roads_capacity, ROAD_DTYPE)
-        self._check(fn(self.h, _ptr(clusters_in), _ptr(layer_offsets), _ptr(vertices), n_events, _ptr(roads), roads_capacity,
+        self._check(fn(self.h, _ptr(records), _ptr(layer_offsets), _ptr(vertices), n_events, _ptr(roads), roads_capacity,
                        _ptr(offs)))
         roads = roads[: offs[-1]].copy()
         roads["pad"] = 0
         return roads, offs
 
-    def atan2f_device(self, y_ptr, x_ptr, out_ptr, n):
-        """The device's correctly rounded atan2 on n device-resident argument pairs."""
-        self._check(self.lib.itsu_atan2f_device(self.h, ctypes.c_void_p(y_ptr), ctypes.c_void_p(x_ptr),
-                                                ctypes.c_void_p(out_ptr), n))
+    def batch_run_host_compact(self, clusters_in, layer_offsets, vertices, roads_capacity=None):
+        """batch_run_host with 24-byte input records (CLUSTER_IN_DTYPE); returns (roads, road_offsets)."""
+        return self._batch_run_host_records("itsu_batch_run_host_compact", CLUSTER_IN_DTYPE, clusters_in, layer_offsets,
+                                            vertices, roads_capacity)
 
     def batch_run_host_tracks(self, clusters_track, layer_offsets, vertices, roads_capacity=None):
         """batch_run_host with 16-byte input records (CLUSTER_TRACK_DTYPE); returns (roads, road_offsets)."""
-        return self.batch_run_host_compact(clusters_track, layer_offsets, vertices, roads_capacity,
-                                           _fn="itsu_batch_run_host_tracks", _dtype=CLUSTER_TRACK_DTYPE)
+        return self._batch_run_host_records("itsu_batch_run_host_tracks", CLUSTER_TRACK_DTYPE, clusters_track, layer_offsets,
+                                            vertices, roads_capacity)
 
     def batch_device(self, clusters_ptr, layer_offsets_ptr, vertices_ptr, n_events, n_clusters) -> Batch:
         b = Batch()
