@@ -1970,9 +1970,11 @@ __global__ void k_road_segments(Arena a)
   }
 }
 
+// A sorted cluster's MC id, from its 16-byte auxiliary record (the batch's 36-byte sorted records
+// are twice the footprint, and the road vote's gathers hit L2 less often there).
 __device__ __forceinline__ int32_t cluster_mc(const Arena &a, const int32_t *lo, int layer, int32_t idx)
 {
-  return a.sorted[lo[layer] + idx].mc_id;
+  return a.clu_aux[lo[layer] + idx].z;
 }
 
 // One road per lane: the roads of a warp's 32 consecutive cells form one contiguous range (the
