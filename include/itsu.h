@@ -352,7 +352,7 @@ itsu_status itsu_batch_profile(itsu_context *ctx, int32_t repeats, itsu_kernel_t
  * logit is below the model's threshold does not become a cell. Its features, per pair: dphi, dz
  * and dtanL of the cell cuts (Tracker.cxx:161-171), the signed curvature of each tracklet's
  * circle through the primary vertex, the pair's DCA (Tracker.cxx:203-210), the inner layer
- * index and the first cluster's radius. The plain path is unchanged and stays the judge: a
+ * index and the first cluster's radius. The plain path is unchanged and stays the yardstick: a
  * learned run's cells are a subset of the plain run's, so its roads are plain roads. Training
  * labels come from plain runs (1 = the cell is on a found road). */
 #define ITSU_MLP_INPUTS 8

@@ -71,3 +71,22 @@ def test_reference_backend_is_built_against_the_library():
     ldd = subprocess.run(["ldd", oracle.ref_binary("b200")], capture_output=True, text=True, check=True).stdout
     line = [l for l in ldd.splitlines() if "libitsu_b200.so" in l]
     assert line and "not found" not in line[0] and "tracking-itsu_b200/lib" in line[0]
+
+
+def test_every_context_call_in_the_callers_exists():
+    """Every method the tests, the bench and the package call on a context (`ctx.<name>`) is a
+    method of capi.Context, so a wrapper cannot disappear from the binding while a GPU test, which
+    only runs on a B200, still calls it."""
+    import glob
+
+    files = glob.glob(os.path.join(ROOT, "tests", "*.py")) + [os.path.join(ROOT, "bench.py")]
+    files += glob.glob(os.path.join(ROOT, "tracking-itsu_b200", "itsu", "*.py"))
+    instance_fields = {"lib", "h"}
+    missing = set()
+    for path in files:
+        if os.path.basename(path) == "test_multirank_cpu.py":
+            continue  # its ctx is a multiprocessing context
+        for m in re.finditer(r"\bctx\w*\.([A-Za-z_]\w*)\b", open(path).read()):
+            if m.group(1) not in instance_fields and not hasattr(capi.Context, m.group(1)):
+                missing.add((os.path.basename(path), m.group(1)))
+    assert not missing, sorted(missing)

@@ -1,7 +1,7 @@
 """The learned tracklet gate on the GPU: sample export, the gate pass of the tracklet stage, the
 scorer, training gradients and the committed checkpoint.
 
-The plain path is the judge: a gated run must keep exactly the plain tracklets the gate scores at
+The plain path is the yardstick: a gated run must keep exactly the plain tracklets the gate scores at
 or above its threshold (inner clusters with more than 48 tracklets keep all of theirs), in the
 plain run's order; it must equal the plain run when the threshold keeps everything; and its roads
 must be exactly the plain roads whose 6 tracklets all survive.

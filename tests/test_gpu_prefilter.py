@@ -1,7 +1,7 @@
 """The learned prefilter on the GPU: sample export, the fused inference in the cell stage, the
 scorer, training gradients and the committed checkpoint.
 
-The plain path is the judge: a learned run must keep exactly the plain cells its model scores at
+The plain path is the yardstick: a learned run must keep exactly the plain cells its model scores at
 or above the threshold (the fused kernel and the scorer share their device code), it must equal
 the plain run when the threshold keeps everything, and its roads must be plain roads.
 """

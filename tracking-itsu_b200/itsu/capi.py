@@ -513,6 +513,11 @@ class Context:
         roads["pad"] = 0
         return roads, offs
 
+    def atan2f_device(self, y_ptr, x_ptr, out_ptr, n):
+        """The device's correctly rounded atan2 on n device-resident argument pairs."""
+        self._check(self.lib.itsu_atan2f_device(self.h, ctypes.c_void_p(y_ptr), ctypes.c_void_p(x_ptr),
+                                                ctypes.c_void_p(out_ptr), n))
+
     def batch_run_host_compact(self, clusters_in, layer_offsets, vertices, roads_capacity=None):
         """batch_run_host with 24-byte input records (CLUSTER_IN_DTYPE); returns (roads, road_offsets)."""
         return self._batch_run_host_records("itsu_batch_run_host_compact", CLUSTER_IN_DTYPE, clusters_in, layer_offsets,
