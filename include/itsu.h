@@ -524,8 +524,8 @@ itsu_status itsu_memory_usage_get(itsu_context *ctx, itsu_memory_usage *out);
  *   sorted         device out: n_clusters clusters, per layer sorted stably by bin
  *   index_tables   device out: 6 x 401 ints (tables of layers 1..6)
  * At most ITSU_NOALLOC_MAX_CLUSTERS clusters (ITSU_ERR_CAPACITY beyond). Runs on cuda_stream on
- * the current device and waits for it; the first call on a device looks up the scratch array's
- * address and should come before any stream capture. That address is cached for the life of the
+ * the current device and waits for it, so no call can be captured into a CUDA graph; the first
+ * call on a device looks up the scratch array's address, which is cached for the life of the
  * library: do not call this on a device after a cudaDeviceReset of it. All calls share the
  * scratch array: calls that overlap on the GPU race. Errors are reported through
  * itsu_last_error(NULL). */

@@ -10,12 +10,11 @@
 //
 // In host code, itsu_noalloc_scratch names a host-side stand-in, not the device array: its
 // device address is obtained once per device with cudaGetSymbolAddress, with that device current,
-// on the first call made on that device, and cached. That first call should therefore come
-// before any stream capture. The cached address belongs to the device's context at that time: a
+// on the first call made on that device, and cached. No call can be captured into a CUDA graph:
+// each one reads the layer offsets back and waits for its stream. The cached address belongs to the device's context at that time: a
 // cudaDeviceReset (or anything else that destroys the primary context) leaves it stale, so the
 // entry point must not be used on a device after it has been reset while the library stays
-// loaded. Every call also reads the layer offsets back and waits for its stream before it
-// returns. All calls share the one array and it keeps the last call's
+// loaded. All calls share the one array and it keeps the last call's
 // contents; the status word is cleared at the start of each call, everything else is written
 // before it is read. Calls whose work overlaps on the GPU (concurrent streams, or threads calling
 // at the same time) race on the array.
