@@ -89,6 +89,7 @@ struct itsu_context {
   float2 *seg_rrange = nullptr;
   int32_t *seg_regular = nullptr;
   int32_t *layer_off = nullptr, *index_tables = nullptr, *trk_seg = nullptr, *cell_seg = nullptr, *road_seg = nullptr;
+  int4 *cell_seginfo = nullptr;
   float *vtx = nullptr;
   // tracklet class
   itsu_tracklet *tracklets = nullptr;
@@ -331,6 +332,7 @@ Arena arena_of(const itsu_context *ctx)
   a.trk_off = ctx->trk_off;
   a.trk_lookup = ctx->trk_lookup;
   a.trk_seg = ctx->trk_seg;
+  a.cell_seginfo = ctx->cell_seginfo;
   a.tracklets = ctx->tracklets;
   a.trk_slope = ctx->trk_slope;
   a.trk_seg_id = ctx->trk_seg_id;
@@ -419,6 +421,7 @@ itsu_status ensure_clusters(itsu_context *ctx, int64_t n_clusters, int32_t n_eve
     ITSU_CUDA(ctx, alloc(ctx, ctx->vtx, (int64_t)cap * 3));
     ITSU_CUDA(ctx, alloc(ctx, ctx->index_tables, (int64_t)cap * ITSU_TRACKLET_LAYERS * ITSU_INDEX_TABLE_SIZE));
     ITSU_CUDA(ctx, alloc(ctx, ctx->trk_seg, (int64_t)cap * ITSU_TRACKLET_LAYERS + 1));
+    ITSU_CUDA(ctx, alloc(ctx, ctx->cell_seginfo, (int64_t)cap * ITSU_TRACKLET_LAYERS * 2));
     ITSU_CUDA(ctx, alloc(ctx, ctx->cell_seg, (int64_t)cap * ITSU_CELL_LAYERS + 1));
     ITSU_CUDA(ctx, alloc(ctx, ctx->road_seg, (int64_t)cap + 1));
     ITSU_CUDA(ctx, alloc(ctx, ctx->seg_rrange, (int64_t)cap * ITSU_LAYERS));
@@ -939,7 +942,7 @@ void itsu_context_destroy(itsu_context *ctx)
   release(ctx->raw); release(ctx->raw_in); release(ctx->raw_track); release(ctx->sorted); release(ctx->tmp); release(ctx->xyzr); release(ctx->phi);
   release(ctx->trk_count); release(ctx->trk_off); release(ctx->trk_lookup); release(ctx->zs); release(ctx->clu_seg); release(ctx->clu_aux); release(ctx->clu_crowded); release(ctx->trk_slots);
   release(ctx->seg_rrange); release(ctx->seg_regular); release(ctx->raw_off);
-  release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seg);
+  release(ctx->layer_off); release(ctx->index_tables); release(ctx->trk_seg); release(ctx->cell_seginfo); release(ctx->cell_seg);
   release(ctx->road_seg); release(ctx->vtx);
   release(ctx->tracklets); release(ctx->trk_slope); release(ctx->trk_seg_id); release(ctx->cell_count); release(ctx->cell_mask); release(ctx->cell_off); release(ctx->cell_lookup); release(ctx->cell_crowded);
   release(ctx->cells); release(ctx->cell_entries); release(ctx->cell_dca); release(ctx->cell_seg_id); release(ctx->nb_count); release(ctx->nb_off); release(ctx->nb_fill);

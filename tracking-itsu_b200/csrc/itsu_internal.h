@@ -116,6 +116,8 @@ struct Arena {
   itsu_tracklet *tracklets;
   float2 *trk_slope;  // per tracklet its (tanL, phi) again, packed: the cell pass's precut reads only these
   int32_t *trk_seg_id;
+  int4 *cell_seginfo;  // per tracklet segment, two records: {first cluster of L (-1: no cells), of L+1, of L+2,
+                       // first tracklet of L}, {first tracklet of L+1, vertex x, y, z (float bits)}
   // cells
   int32_t *cell_count;
   unsigned long long *cell_mask;  // per first tracklet: which outgoing tracklets make cells

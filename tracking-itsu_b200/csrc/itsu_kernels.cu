@@ -1381,7 +1381,23 @@ __global__ void __launch_bounds__(kMaxThreads) k_tracklets_crowded(Arena a)
   }
 }
 
-// trk_seg[6e+L] = first tracklet of (e, L); capacity check of the tracklet total.
+// Cell layer L of event e runs only if tracklet layers 0..L+1 are all non-empty
+// (Tracker.cxx:124-128); ts holds the event's first tracklet of each layer and the next event's.
+__device__ __forceinline__ bool cells_active(const int32_t *ts, int layer)
+{
+  for (int l = 0; l <= layer; ++l) {
+    if (ts[l + 1] - ts[l] <= 0 || ts[l + 2] - ts[l + 1] <= 0) {
+      return false;
+    }
+  }
+  return true;
+}
+
+// trk_seg[6e+L] = first tracklet of (e, L); capacity check of the tracklet total. For the cell
+// layers, the segment's cell-stage record too (cell_seginfo[2s], [2s+1]): the first cluster of
+// layers L, L+1, L+2 (the first -1 when cell layer L of the event does not run), the first
+// tracklet of layers L and L+1 and the vertex, so that each first tracklet's setup in the cell
+// count pass is two 16-byte loads of one record instead of a dozen loads of per-event offsets.
 __global__ void k_tracklet_segments(Arena a)
 {
   // the cells scan's tile sums start at zero: the cell count pass adds each warp's cells there
@@ -1402,23 +1418,23 @@ __global__ void k_tracklet_segments(Arena a)
     } else {
       const int e = s / ITSU_TRACKLET_LAYERS, layer = s % ITSU_TRACKLET_LAYERS;
       a.trk_seg[s] = a.trk_off[a.layer_off[e * ITSU_LAYERS + layer]];
+      if (layer < ITSU_CELL_LAYERS) {
+        const int32_t *lo = a.layer_off + e * ITSU_LAYERS;
+        int32_t ts[ITSU_LAYERS];
+        for (int l = 0; l < ITSU_LAYERS; ++l) {
+          ts[l] = a.trk_off[lo[l]];
+        }
+        const bool active = cells_active(ts, layer);
+        a.cell_seginfo[2 * s] = make_int4(active ? lo[layer] : -1, lo[layer + 1], lo[layer + 2], ts[layer]);
+        a.cell_seginfo[2 * s + 1] = make_int4(ts[layer + 1], __float_as_int(a.vtx[3 * e]), __float_as_int(a.vtx[3 * e + 1]),
+                                              __float_as_int(a.vtx[3 * e + 2]));
+      }
     }
   }
 }
 
 // ------------------------------------------------------------------------------------------
 // (c) cells: TrackerTraits<false>::computeLayerCells (Tracker.cxx:120-235)
-
-// Cell layer L of event e runs only if tracklet layers 0..L+1 are all non-empty (:124-128).
-__device__ __forceinline__ bool cells_active(const int32_t *ts, int layer)
-{
-  for (int l = 0; l <= layer; ++l) {
-    if (ts[l + 1] - ts[l] <= 0 || ts[l + 2] - ts[l + 1] <= 0) {
-      return false;
-    }
-  }
-  return true;
-}
 
 // Per-lane state of the warp-parallel cell stage: lane l owns first tracklet k = base + l.
 struct CellLane {
@@ -1447,27 +1463,30 @@ __device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t
   const itsu_tracklet t1 = a.tracklets[k];
   s.e = sid / ITSU_TRACKLET_LAYERS;
   s.layer = sid % ITSU_TRACKLET_LAYERS;
-  const int32_t *ts = a.trk_seg + s.e * ITSU_TRACKLET_LAYERS;
-  if (s.layer >= ITSU_CELL_LAYERS || !cells_active(ts, s.layer)) {
+  if (s.layer >= ITSU_CELL_LAYERS) {
     s.layer = ITSU_CELL_LAYERS;
     return s;
   }
-  const int32_t *lo = a.layer_off + s.e * ITSU_LAYERS;
+  const int4 A = a.cell_seginfo[2 * sid], B = a.cell_seginfo[2 * sid + 1];
+  if (A.x < 0) {
+    s.layer = ITSU_CELL_LAYERS;
+    return s;
+  }
   s.t1_tan_lambda = t1.tan_lambda;
   s.t1_phi = t1.phi;
   s.t1_first = t1.first_cluster;
   s.t1_second = t1.second_cluster;
-  s.c1 = a.xyzr[lo[s.layer] + t1.first_cluster];
-  const int64_t c2i = lo[s.layer + 1] + t1.second_cluster;
+  s.c1 = a.xyzr[A.x + t1.first_cluster];
+  const int64_t c2i = A.y + t1.second_cluster;
   s.c2 = a.xyzr[c2i];
   s.j0 = a.trk_off[c2i];
   s.n_out = a.trk_off[c2i + 1] - s.j0;
-  s.vx = a.vtx[3 * s.e];
-  s.vy = a.vtx[3 * s.e + 1];
-  s.vz = a.vtx[3 * s.e + 2];
-  s.c3_base = lo[s.layer + 2];
-  s.t1_local = (int32_t)(k - ts[s.layer]);
-  s.t2_base = ts[s.layer + 1];
+  s.vx = __int_as_float(B.y);
+  s.vy = __int_as_float(B.z);
+  s.vz = __int_as_float(B.w);
+  s.c3_base = A.z;
+  s.t1_local = (int32_t)(k - A.w);
+  s.t2_base = B.x;
   return s;
 }
 
@@ -1530,13 +1549,22 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a, int32_t e0
     unsigned long long window = 0;  // the outgoing tracklets that pass the cheap cuts
     if (!big && s.n_out > 0) {
       const float max_dz = kC.cell_max_dz[s.layer];  // n_out > 0: an active cell layer
-      // (tanL, phi) of the outgoing tracklets, packed 8 bytes each
+      // (tanL, phi) of the outgoing tracklets, packed 8 bytes each; the window's two 32-bit
+      // halves are filled by two loops (a 64-bit variable shift per candidate costs more)
       const float2 *tp = a.trk_slope + s.j0;
+      unsigned lo = 0u, hi = 0u;
+      const int n_lo = s.n_out < 32 ? s.n_out : 32;
 #pragma unroll 4
-      for (int q = 0; q < s.n_out; ++q) {
+      for (int q = 0; q < n_lo; ++q) {
         const float2 t2 = tp[q];
-        window |= (unsigned long long)cell_precut_dz(s.t1_tan_lambda, s.t1_phi, t2.x, t2.y, s.c1, s.vz, max_dz) << q;
+        lo |= (unsigned)cell_precut_dz(s.t1_tan_lambda, s.t1_phi, t2.x, t2.y, s.c1, s.vz, max_dz) << q;
       }
+#pragma unroll 4
+      for (int q = 32; q < s.n_out; ++q) {
+        const float2 t2 = tp[q];
+        hi |= (unsigned)cell_precut_dz(s.t1_tan_lambda, s.t1_phi, t2.x, t2.y, s.c1, s.vz, max_dz) << (q - 32);
+      }
+      window = ((unsigned long long)hi << 32) | lo;
     }
     masks[warp][lane] = 0ull;
     int total = 0;
