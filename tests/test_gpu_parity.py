@@ -365,3 +365,33 @@ def test_staged_walk_matches_oracle(ctx):
             _assert_same(ctx.results(e), oracle.run_vertex(ev.layers, ev.vertices[0]), "staged walk, event %d" % e)
     finally:
         ctx.set_tune(band, 256, 8, 1)
+
+
+def _without_layer3_tracklets(seed, n_tracks):
+    """An event whose layer-3 clusters are moved 100 cm along the beam, past the layer's end: no
+    tracklet reaches them from layer 2 or leaves them for layer 4 (the z cut), while the tracklet
+    layers 4 and 5 keep theirs. Cell layer 0 runs; cell layers 1-4 do not (Tracker.cxx:124-128),
+    although cell layer 4's first tracklets exist."""
+    ev = gen.pbpb_event(seed, n_tracks)
+    l3 = ev.layers[3].copy()
+    l3["z"] = l3["z"] + 100.0
+    ev.layers[3] = l3
+    return ev
+
+
+def test_inactive_cell_layers_match_oracle(ctx):
+    """Cell layers that do not run although their first tracklets exist: per vertex and inside a
+    batch beside ordinary events, against the oracle."""
+    odd = _without_layer3_tracklets(11, 1500)
+    want = oracle.run_vertex(odd.layers, odd.vertices[0])
+    sizes = [len(t) for t in want["tracklets"]]
+    assert sizes[2] == 0 and sizes[3] == 0 and sizes[4] > 0 and sizes[5] > 0, sizes
+    assert len(want["cells"][0]) > 0 and all(len(c) == 0 for c in want["cells"][1:])
+    _assert_same(ctx.run_vertex(odd.layers, odd.vertices[0]), want, "inactive cell layers")
+    events = [gen.pbpb_event(12, 1500), odd, gen.pbpb_event(13, 1500)]
+    clusters, offsets, vertices = gen.pack_batch(events)
+    roads, road_off = ctx.batch_run_host(clusters, offsets, vertices)
+    for e, ev in enumerate(events):
+        exp = oracle.run_vertex(ev.layers, ev.vertices[0])
+        _assert_same(ctx.results(e), exp, "batch event %d" % e)
+        assert np.array_equal(roads[road_off[e]:road_off[e + 1]].view(np.uint8), exp["roads"].view(np.uint8))
