@@ -815,9 +815,13 @@ __device__ __forceinline__ void walk_candidates(const int32_t *table, int n_next
           if (probe.pass<kGate>(q.x, q.y, q.z)) {
             const int pos = __float_as_int(q.w) - k0;
             const unsigned long long bit = 1ull << (pos & 63);
+            if constexpr (kWords == 1) {
+              hit[0] |= bit;  // a single-word layer's columns hold at most 64 clusters
+            } else {
 #pragma unroll
-            for (int w = 0; w < kWords; ++w) {
-              hit[w] |= (pos >> 6) == w ? bit : 0ull;
+              for (int w = 0; w < kWords; ++w) {
+                hit[w] |= (pos >> 6) == w ? bit : 0ull;
+              }
             }
           }
         }
@@ -1444,7 +1448,7 @@ struct CellLane {
   float4 c1, c2;
   float vx, vy, vz;
   int32_t j0, n_out;     // the outgoing tracklets of the tracklet's outer cluster: [j0, j0 + n_out)
-  int64_t c3_base;       // first cluster of layer L + 2
+  int32_t c3_base;       // first cluster of layer L + 2
   int32_t t1_local, t1_first, t1_second, t2_base;  // tracklet index in its layer, its clusters, first tracklet of layer L + 1
 };
 
@@ -1488,15 +1492,6 @@ __device__ __forceinline__ CellLane cell_lane(const Arena &a, int64_t k, int64_t
   s.t1_local = (int32_t)(k - A.w);
   s.t2_base = B.x;
   return s;
-}
-
-// Position of the r-th (from 0) set bit of m (m has more than r set bits).
-__device__ __forceinline__ int nth_set_bit(unsigned long long m, int r)
-{
-  for (int q = 0; q < r; ++q) {
-    m &= m - 1ull;
-  }
-  return __ffsll((long long)m) - 1;
 }
 
 __device__ __forceinline__ void write_cell(const Arena &a, int64_t out, const CellLane &s, const itsu_tracklet &t2, int32_t j,
@@ -1576,8 +1571,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a, int32_t e0
       const int r = p - __shfl_sync(0xffffffffu, excl, owner);
       const unsigned long long wmask = __shfl_sync(0xffffffffu, window, owner);
       const int32_t j0 = __shfl_sync(0xffffffffu, s.j0, owner);
-      const int64_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
-      const float4 c1 = shfl4(s.c1, owner), c2 = shfl4(s.c2, owner);
+      // the circle geometry reads x, y and r of the first two clusters, not z
+      const int32_t c3_base = __shfl_sync(0xffffffffu, s.c3_base, owner);
+      const float4 c1 = make_float4(__shfl_sync(0xffffffffu, s.c1.x, owner), __shfl_sync(0xffffffffu, s.c1.y, owner), 0.0f,
+                                    __shfl_sync(0xffffffffu, s.c1.w, owner));
+      const float4 c2 = make_float4(__shfl_sync(0xffffffffu, s.c2.x, owner), __shfl_sync(0xffffffffu, s.c2.y, owner), 0.0f,
+                                    __shfl_sync(0xffffffffu, s.c2.w, owner));
       const float vx = __shfl_sync(0xffffffffu, s.vx, owner), vy = __shfl_sync(0xffffffffu, s.vy, owner);
       const int layer = __shfl_sync(0xffffffffu, s.layer, owner);
       bool pass = false;
@@ -1586,7 +1585,18 @@ __global__ void __launch_bounds__(kMaxThreads) k_cells_count(Arena a, int32_t e0
       float3 normal = make_float3(0.0f, 0.0f, 0.0f);
       float curvature = 0.0f, dca = 0.0f;
       if (p < total) {
-        b = nth_set_bit(wmask, r);
+        {
+          // the owner's r-th passing outgoing tracklet: the r-th set bit of its window, found in
+          // the 32-bit half that holds it
+          const unsigned wlo = (unsigned)wmask;
+          const int plo = __popc(wlo);
+          const bool in_lo = r < plo;
+          unsigned m = in_lo ? wlo : (unsigned)(wmask >> 32);
+          for (int q = in_lo ? r : r - plo; q > 0; --q) {
+            m &= m - 1u;
+          }
+          b = __ffs(m) - 1 + (in_lo ? 0 : 32);
+        }
         c3 = a.tracklets[j0 + b].second_cluster;
         pass = cell_geometry(layer, c1, c2, a.xyzr[c3_base + c3], vx, vy, normal, curvature, dca);
         if (pass) {
