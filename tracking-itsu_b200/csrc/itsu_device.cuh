@@ -28,6 +28,15 @@ constexpr float kCellMaxDeltaPhi = 0.14f;
 constexpr float kZCoordinateCut = 0.5f;
 constexpr float kPhiCoordinateCut = 0.3f;
 constexpr int kCellsMinLevel = 5;
+// The wrap-around half of the reference's azimuth cuts, |delta_phi - 2pi| < cut in binary32, for a
+// binary32 delta_phi = |phi1 - phi2| in [0, kTwoPi] (both azimuths normalised to [0, kTwoPi], or
+// both atan2 results in [-pi, pi]): for delta_phi >= kPi the subtraction is exact (Sterbenz), so
+// the test is delta_phi > kTwoPi - cut in real arithmetic, i.e. delta_phi greater than the largest
+// binary32 value not above kTwoPi - cut; below kPi both forms are false. One compare instead of a
+// subtraction and a compare; tests/test_phi_wrap.py checks every binary32 delta_phi in
+// [kPi, kTwoPi] and a sample below.
+constexpr float kPhiWrapTracklet = 0x1.7eec82p+2f;  // largest binary32 <= kTwoPi - kPhiCoordinateCut
+constexpr float kPhiWrapCell = 0x1.8929f2p+2f;      // largest binary32 <= kTwoPi - kCellMaxDeltaPhi
 
 struct LayerConstants {
   float z_half[7];           // LayersZCoordinate
@@ -102,8 +111,7 @@ __device__ __forceinline__ bool tracklet_cut(int layer, float tan_lambda, float 
 {
   const float delta_z = fabsf(tan_lambda * (r2 - r1) + z1 - z2);
   const float delta_phi = fabsf(phi1 - phi2);
-  return delta_z < kC.trk_max_dz[layer] &&
-         (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
+  return delta_z < kC.trk_max_dz[layer] && (delta_phi < kPhiCoordinateCut || delta_phi > kPhiWrapTracklet);
 }
 
 // Tracker.cxx:161-173: the cheap cell cuts, which need only the two tracklets and the first
@@ -119,7 +127,7 @@ __device__ __forceinline__ bool cell_precut_dz(float t1_tan_lambda, float t1_phi
   const float dir_z = -average_tan_lambda * c1.w + c1.z;
   const float delta_z = fabsf(dir_z - vz);
   return (delta_tan_lambda < kCellMaxDeltaTanLambda) &
-         ((delta_phi < kCellMaxDeltaPhi) | (fabsf(delta_phi - kTwoPi) < kCellMaxDeltaPhi)) & (delta_z < max_dz);
+         ((delta_phi < kCellMaxDeltaPhi) | (delta_phi > kPhiWrapCell)) & (delta_z < max_dz);
 }
 
 __device__ __forceinline__ bool cell_precut(int layer, float t1_tan_lambda, float t1_phi, float t2_tan_lambda, float t2_phi,

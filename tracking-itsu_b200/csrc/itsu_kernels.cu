@@ -747,7 +747,7 @@ struct TrackletProbe {
   {
     const float delta_z = fabsf(tan_lambda * (r2 - c.w) + c.z - z2);
     const float delta_phi = fabsf(phi1 - phi2);
-    const bool cut = delta_z < max_dz && (delta_phi < kPhiCoordinateCut || fabsf(delta_phi - kTwoPi) < kPhiCoordinateCut);
+    const bool cut = delta_z < max_dz && (delta_phi < kPhiCoordinateCut || delta_phi > kPhiWrapTracklet);
     if constexpr (kGate) {
       return cut && gate_window_pass(win, make_float4(0.0f, 0.0f, z2, r2), phi2);
     }
